@@ -1,0 +1,299 @@
+/*
+ * pcg.h — C ABI of the B200 hot path of a PhysiCell-style simulator:
+ * LOD Thomas diffusion-decay with Dirichlet boundaries and per-cell
+ * secretion/uptake, spatial-hash cell-cell mechanics and the Adams-Bashforth
+ * position update.
+ *
+ * Every entry point returns a pcg_status (PCG_OK == 0) and never aborts;
+ * pcg_last_error_string() describes the last failure on a context.  Device
+ * memory is owned by the library; host pointers stay owned by the caller.
+ * Calls on one pcg_ctx are serialised on that context's CUDA stream and must
+ * come from one host thread at a time; separate contexts may be used from
+ * separate threads.  Floating-point layouts match the reference exactly:
+ *   density   float32 [s][k][j][i]        (src/microenvironment.mm:133-145)
+ *   cell SoA  float32 [field * max_cells + cell], 28 fields, fields 23..27
+ *             hold uint32 bits            (src/cell_data.cpp:101-180,
+ *                                          shaders/types.h:74-102)
+ *   rates     float64 [cell * S + s]      (src/cell_data.cpp:380-394)
+ */
+#ifndef PCG_H
+#define PCG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PCG_ABI_VERSION 1
+
+typedef int pcg_status;
+enum {
+    PCG_OK = 0,
+    PCG_ERR_INVALID = 1,     /* bad argument, size or state */
+    PCG_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    PCG_ERR_OOM = 3,         /* device allocation failed */
+    PCG_ERR_NO_DEVICE = 4,   /* no usable CUDA device */
+    PCG_ERR_BUDGET = 5,      /* request does not fit the serving memory budget */
+    PCG_ERR_NOT_FOUND = 6,   /* unknown request id */
+    PCG_ERR_NOT_READY = 7    /* request not finished yet */
+};
+
+/* Same layout as GridParams (shaders/types.h:23-37). */
+typedef struct {
+    uint32_t nx, ny, nz, n_substrates;
+    float dx, dy, dz, dt;
+    float x_min, y_min, z_min, _pad0;
+} pcg_grid_params;
+
+/* Same layout as SubstrateParams (shaders/types.h:40-48). */
+typedef struct {
+    float diffusion_coefficient, decay_rate, supply_rate, target_value;
+    uint32_t dirichlet_enabled;
+    float _pad[3];
+} pcg_substrate_params;
+
+/* Same layout as MechanicsParams (shaders/types.h:51-61). */
+typedef struct {
+    float dt, cell_cell_repulsion, cell_cell_adhesion, max_interaction_distance;
+    float mechanics_voxel_size;
+    uint32_t mech_grid_nx, mech_grid_ny, mech_grid_nz;
+} pcg_mechanics_params;
+
+/* Cell SoA field ids (shaders/types.h:74-102). */
+enum {
+    PCG_F_POS_X = 0, PCG_F_POS_Y, PCG_F_POS_Z,
+    PCG_F_VEL_X, PCG_F_VEL_Y, PCG_F_VEL_Z,
+    PCG_F_PREV_VX, PCG_F_PREV_VY, PCG_F_PREV_VZ,
+    PCG_F_RADIUS, PCG_F_NUCLEAR_RAD, PCG_F_TOTAL_VOL, PCG_F_NUCLEAR_VOL,
+    PCG_F_REPULSION, PCG_F_ADHESION, PCG_F_REL_MAX_ADH,
+    PCG_F_MOT_SPEED, PCG_F_MOT_BIAS, PCG_F_MOT_DIR_X, PCG_F_MOT_DIR_Y, PCG_F_MOT_DIR_Z,
+    PCG_F_ONCOPROTEIN, PCG_F_PRESSURE,
+    PCG_F_CELL_TYPE, PCG_F_CUR_PHASE, PCG_F_IS_ALIVE, PCG_F_VOXEL_IDX, PCG_F_MECH_VOXEL,
+    PCG_NUM_FIELDS
+};
+
+typedef struct pcg_ctx pcg_ctx;
+typedef struct pcg_me pcg_me;
+typedef struct pcg_cells pcg_cells;
+typedef struct pcg_mech pcg_mech;
+typedef struct pcg_batch pcg_batch;
+typedef struct pcg_server pcg_server;
+
+/* ------------------------------------------------------------------------
+ * Context — replaces MetalContext (src/metal_context.h:14-100): device,
+ * command queue (here a CUDA stream) and error reporting.
+ * ---------------------------------------------------------------------- */
+int pcg_abi_version(void);
+pcg_status pcg_create(int device, pcg_ctx** out);
+/* Use an existing CUDA stream (cudaStream_t passed as void*). */
+pcg_status pcg_create_on_stream(int device, void* stream, pcg_ctx** out);
+pcg_status pcg_destroy(pcg_ctx* ctx);
+/* MetalContext::waitForCompletion (metal_context.mm:448-461). */
+pcg_status pcg_sync(pcg_ctx* ctx);
+void* pcg_stream(pcg_ctx* ctx);
+const char* pcg_last_error_string(const pcg_ctx* ctx);
+/* Number of kernel launches this context has issued (graph launches count
+ * their kernel nodes). */
+uint64_t pcg_kernel_launches(const pcg_ctx* ctx);
+/* Page-locked host memory for the asynchronous whole-batch transfers. */
+pcg_status pcg_host_alloc(size_t bytes, void** out);
+pcg_status pcg_host_free(void* p);
+
+/* ------------------------------------------------------------------------
+ * Microenvironment — replaces Microenvironment (src/microenvironment.h:17-83).
+ * grid->n_substrates substrates; grid->nz == 1 is the 2-D case (x and y
+ * sweeps), nz > 1 adds a z sweep (decay split lambda*dt/3 per sweep) and the
+ * Dirichlet reset covers all six faces.
+ * ---------------------------------------------------------------------- */
+pcg_status pcg_me_create(pcg_ctx* ctx, const pcg_grid_params* grid,
+                         const pcg_substrate_params* substrates, pcg_me** out);
+pcg_status pcg_me_destroy(pcg_me* me);
+/* Microenvironment::initialize density fill (microenvironment.mm:139-145). */
+pcg_status pcg_me_fill(pcg_me* me, const float* value_per_substrate);
+/* Bulk setDensity / densityBuffer() read-back (microenvironment.mm:239-247);
+ * n_floats must equal nx*ny*nz*S. */
+pcg_status pcg_me_upload(pcg_me* me, const float* host, size_t n_floats);
+pcg_status pcg_me_download(pcg_me* me, float* host, size_t n_floats);
+/* Microenvironment::simulateDiffusionDecay (microenvironment.mm:191-200):
+ * the x, y (, z) sweeps only, n_steps times. */
+pcg_status pcg_me_diffuse(pcg_me* me, int n_steps);
+/* Microenvironment::applyDirichletBC (microenvironment.mm:212-237). */
+pcg_status pcg_me_apply_dirichlet(pcg_me* me);
+/* processSecretion (src/cell_phenotype.cpp:526-564) for every active cell
+ * of 'cells', applied per voxel in ascending cell index. */
+pcg_status pcg_me_secrete(pcg_me* me, pcg_cells* cells, double dt);
+/* One main-loop diffusion sub-step n_steps times (src/main.mm:341-366):
+ * sweeps -> Dirichlet reset (fused into the last sweep) -> secretion (when
+ * cells is not NULL), dt = grid->dt. */
+pcg_status pcg_me_step(pcg_me* me, pcg_cells* cells, int n_steps);
+/* Microenvironment::computeGradients + read-back (microenvironment.mm:282-342):
+ * three arrays of nx*ny*nz*S floats (any may be NULL). */
+pcg_status pcg_me_gradients(pcg_me* me, float* gx, float* gy, float* gz, size_t n_floats);
+/* Device pointer of the density block and the element pitch between
+ * substrates (>= nx*ny*nz). */
+pcg_status pcg_me_device_density(pcg_me* me, float** dptr, size_t* substrate_pitch);
+
+/* ------------------------------------------------------------------------
+ * Cells — the GPU-shared block of CellData (src/cell_data.h:19-244).
+ * ---------------------------------------------------------------------- */
+pcg_status pcg_cells_create(pcg_ctx* ctx, uint32_t max_cells, uint32_t n_substrates, pcg_cells** out);
+pcg_status pcg_cells_destroy(pcg_cells* cells);
+/* Upload n_cells cells from a host SoA whose field stride is soa_max_cells. */
+pcg_status pcg_cells_upload(pcg_cells* cells, const float* soa, uint32_t n_cells, uint32_t soa_max_cells);
+pcg_status pcg_cells_download(pcg_cells* cells, float* soa, uint32_t soa_max_cells);
+/* Partial transfers of fields [first, first + count). */
+pcg_status pcg_cells_upload_fields(pcg_cells* cells, uint32_t first, uint32_t count,
+                                   const float* soa, uint32_t soa_max_cells);
+pcg_status pcg_cells_download_fields(pcg_cells* cells, uint32_t first, uint32_t count,
+                                     float* soa, uint32_t soa_max_cells);
+/* Per-cell per-substrate rates [cell * S + s] (n_cells * S each; NULL =
+ * zeros) and the active mask (NULL = all cells; the reference skips cells
+ * whose current_death_model != 0, src/main.mm:360). */
+pcg_status pcg_cells_set_secretion(pcg_cells* cells, const double* secretion, const double* uptake,
+                                   const double* saturation, const double* net_export,
+                                   const uint8_t* active);
+pcg_status pcg_cells_count(pcg_cells* cells, uint32_t* n_cells);
+pcg_status pcg_cells_device_soa(pcg_cells* cells, float** dptr, uint32_t* max_cells);
+
+/* ------------------------------------------------------------------------
+ * Mechanics — replaces CellMechanics (src/cell_mechanics.h:15-87).
+ * Binning is a stable LSD radix sort of (mech voxel, cell index); the
+ * cell-start table replaces the 64-slot hash: voxelCellCount(v) =
+ * start[v+1] - start[v], voxelCells(v) = sorted + start[v].
+ * ---------------------------------------------------------------------- */
+/* CellMechanics::initialize (cell_mechanics.mm:112-171): the mechanics
+ * grid of params->mech_grid_* voxels of params->mechanics_voxel_size with
+ * origin (x_min, y_min, z_min). */
+pcg_status pcg_mech_create(pcg_ctx* ctx, const pcg_mechanics_params* params,
+                           float x_min, float y_min, float z_min, uint32_t max_cells, pcg_mech** out);
+pcg_status pcg_mech_destroy(pcg_mech* mech);
+/* CellMechanics::computeForces (cell_mechanics.mm:188-200): bin, sort,
+ * cell-start table, forces -> velocity and simple pressure. */
+pcg_status pcg_mech_forces(pcg_mech* mech, pcg_cells* cells);
+/* CellMechanics::integratePositions (cell_mechanics.mm:202-209). */
+pcg_status pcg_mech_integrate(pcg_mech* mech, pcg_cells* cells, float dt);
+/* CellMechanics::update (cell_mechanics.mm:173-186): forces + integrate. */
+pcg_status pcg_mech_update(pcg_mech* mech, pcg_cells* cells, float dt);
+/* CellMechanics::syncHashPointers (cell_mechanics.mm:211-222): copy the
+ * cell-start table (V + 1 entries) and the sorted cell indices (n_cells)
+ * to the host; either pointer may be NULL. */
+pcg_status pcg_mech_bins(pcg_mech* mech, uint32_t* start, uint32_t* sorted_cells);
+uint32_t pcg_mech_total_voxels(const pcg_mech* mech);
+/* Diagnostics: when on, the force pass also records per cell the number of
+ * neighbours within the cut-off and a hash of their indices (the sum of
+ * pcg_neighbor_hash(j) mod 2^32), read back with pcg_mech_neighbor_stats. */
+pcg_status pcg_mech_set_diagnostics(pcg_mech* mech, int on);
+pcg_status pcg_mech_neighbor_stats(pcg_mech* mech, uint32_t* count, uint32_t* hash);
+uint32_t pcg_neighbor_hash(uint32_t cell);
+
+/* ------------------------------------------------------------------------
+ * Batch — many independent simulations of uneven grid and cell counts
+ * advanced together: one CUDA graph per main-loop step, each phase one
+ * persistent kernel over a flattened work list of all instances.
+ * ---------------------------------------------------------------------- */
+enum { PCG_INST_REFRESH_VOXELS = 1 };   /* recompute voxel_index after integrate */
+
+typedef struct {
+    pcg_grid_params grid;                    /* diffusion grid; grid.dt = dt_diffusion */
+    const pcg_substrate_params* substrates;  /* grid.n_substrates entries */
+    const float* initial_density;            /* nx*ny*nz*S floats, or NULL */
+    const float* initial_values;             /* per-substrate fill when initial_density is NULL */
+    uint32_t n_cells;
+    const float* cells_soa;                  /* 28-field SoA with stride cells_soa_max */
+    uint32_t cells_soa_max;
+    const double* secretion;                 /* [cell * S + s], NULL = zeros */
+    const double* uptake;
+    const double* saturation;
+    const double* net_export;
+    const uint8_t* active;                   /* NULL = all active */
+    pcg_mechanics_params mech;               /* mechanics grid (cell_mechanics.mm:115-130) */
+    float dt_mechanics;
+    uint32_t flags;
+} pcg_instance_desc;
+
+typedef struct {
+    int use_graphs;        /* capture each step into a CUDA graph (default 1) */
+    int autotune;          /* pick tile shapes / block sizes by measurement (default 1) */
+    const char* tune_cache;/* JSON cache path for autotuned choices, or NULL */
+    int profile_phases;    /* record CUDA events around phases (default 0) */
+} pcg_batch_options;
+
+pcg_status pcg_batch_create(pcg_ctx* ctx, const pcg_instance_desc* instances, uint32_t n_instances,
+                            const pcg_batch_options* options, pcg_batch** out);
+pcg_status pcg_batch_destroy(pcg_batch* batch);
+/* Advance every instance by n_diffusion_steps main-loop sub-steps
+ * (src/main.mm:341-391 ordering; mechanics when each instance's accumulator
+ * reaches dt_mechanics). */
+pcg_status pcg_batch_step(pcg_batch* batch, int n_diffusion_steps);
+pcg_status pcg_batch_download_density(pcg_batch* batch, uint32_t instance, float* host, size_t n_floats);
+pcg_status pcg_batch_download_cells(pcg_batch* batch, uint32_t instance, float* soa, uint32_t soa_max_cells);
+pcg_status pcg_batch_upload_cells(pcg_batch* batch, uint32_t instance, const float* soa, uint32_t soa_max_cells);
+/* Whole-batch asynchronous transfers (the end-to-end path; host buffers
+ * should come from pcg_host_alloc).  Cells: one SoA of all instances' cells
+ * in instance order, field stride = total cells (28 * total floats).
+ * Density: the device arena as is (pcg_batch_density_layout gives each
+ * instance's offset and substrate pitch).  Neither waits for completion;
+ * pcg_sync does. */
+pcg_status pcg_batch_upload_all_cells(pcg_batch* batch, const float* soa, uint64_t n_floats);
+pcg_status pcg_batch_download_all_cells(pcg_batch* batch, float* soa, uint64_t n_floats);
+pcg_status pcg_batch_download_all_density(pcg_batch* batch, float* host, uint64_t n_floats);
+pcg_status pcg_batch_density_layout(pcg_batch* batch, uint32_t instance, uint64_t* offset, uint64_t* substrate_pitch,
+                                    uint64_t* arena_floats);
+/* Totals: voxels (sum nx*ny*nz), voxel-substrates, cells. */
+pcg_status pcg_batch_totals(pcg_batch* batch, uint64_t* voxels, uint64_t* voxel_substrates, uint64_t* cells);
+/* Kernel launches one main-loop sub-step issues: without / with a
+ * mechanics step. */
+pcg_status pcg_batch_step_launches(pcg_batch* batch, uint64_t* diffusion_step, uint64_t* mechanics_step);
+/* Per-phase device milliseconds accumulated since the last reset when
+ * profile_phases is on: [0] x sweep, [1] y sweep, [2] z sweep, [3] secretion,
+ * [4] mechanics bin+sort, [5] forces, [6] integrate.  Returns the counts of
+ * timed sweeps launches in *n_sweep_launches. */
+#define PCG_N_PHASES 7
+pcg_status pcg_batch_phase_times(pcg_batch* batch, float* ms, uint64_t* n_sweep_launches, int reset);
+/* Switch phase profiling on or off after creation. */
+pcg_status pcg_batch_set_profile(pcg_batch* batch, int on);
+/* Describe the chosen launch shapes as a short string. */
+const char* pcg_batch_describe(pcg_batch* batch);
+
+/* ------------------------------------------------------------------------
+ * Serving — continuous batching of parameter-sweep simulations.  Requests
+ * are admitted against a device-memory budget as slots and memory free up,
+ * their state stays resident on the device, and all admitted requests
+ * advance together in chunks of steps.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    uint64_t budget_bytes;     /* device bytes requests may hold (e.g. 150e9) */
+    uint32_t max_active;       /* slot limit, 0 = unlimited */
+    uint32_t steps_per_tick;   /* diffusion sub-steps per tick (default 100) */
+} pcg_serve_options;
+
+enum { PCG_REQ_QUEUED = 0, PCG_REQ_RUNNING = 1, PCG_REQ_DONE = 2 };
+
+pcg_status pcg_serve_create(pcg_ctx* ctx, const pcg_serve_options* options, pcg_server** out);
+pcg_status pcg_serve_destroy(pcg_server* srv);
+/* Queue a request (the host data is copied); *id receives its id. */
+pcg_status pcg_serve_submit(pcg_server* srv, const pcg_instance_desc* inst, uint32_t n_diffusion_steps,
+                            uint64_t* id);
+/* Admit what fits, advance every running request by one chunk, retire the
+ * finished ones.  *n_running / *n_queued / *n_finished_now may be NULL. */
+pcg_status pcg_serve_tick(pcg_server* srv, uint32_t* n_running, uint32_t* n_queued, uint32_t* n_finished_now);
+pcg_status pcg_serve_state(pcg_server* srv, uint64_t id, int* state);
+/* Results of a finished request; either pointer may be NULL. */
+pcg_status pcg_serve_fetch(pcg_server* srv, uint64_t id, float* density, size_t n_floats,
+                           float* soa, uint32_t soa_max_cells);
+/* Device seconds and wall seconds a request spent, from admission and from
+ * submission to completion. */
+pcg_status pcg_serve_request_times(pcg_server* srv, uint64_t id, double* submit_to_done_s,
+                                   double* admit_to_done_s);
+/* Totals since creation: voxel-steps, cell-steps (mechanics), bytes held now. */
+pcg_status pcg_serve_totals(pcg_server* srv, uint64_t* voxel_steps, uint64_t* cell_steps,
+                            uint64_t* bytes_in_use);
+/* Bytes the library would hold for one request (admission estimate). */
+uint64_t pcg_instance_bytes(const pcg_instance_desc* inst);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PCG_H */

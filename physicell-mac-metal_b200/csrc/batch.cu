@@ -1,0 +1,449 @@
+// batch.cu — many independent simulations advanced together.
+//
+// All instances share one density arena, one cell SoA and one mechanics
+// key space; every phase of a main-loop sub-step is one persistent kernel
+// over a flat work list of all instances (src/main.mm:341-391 ordering:
+// sweeps -> Dirichlet reset (fused) -> secretion -> [mechanics]).  The
+// sub-step with and without mechanics are each captured once into a CUDA
+// graph, so one step is one graph launch.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "batch.h"
+
+using namespace pcg;
+
+namespace pcg {
+
+uint64_t instance_bytes(const pcg_instance_desc& d)
+{
+    const uint64_t nv = static_cast<uint64_t>(d.grid.nx) * d.grid.ny * d.grid.nz;
+    const uint64_t S = d.grid.n_substrates;
+    const uint64_t pitch = (nv + 31) / 32 * 32;
+    const uint64_t n = d.n_cells;
+    const uint64_t V = static_cast<uint64_t>(d.mech.mech_grid_nx) * d.mech.mech_grid_ny * d.mech.mech_grid_nz;
+    uint64_t b = pitch * S * 4;                            // density
+    b += (nv / 32 + 3) * 32 * S;                           // tile lists (~32 B per 32 lines per axis)
+    b += n * (NUM_FIELDS * 4 + 4 + 1);                     // SoA, instance id, active
+    b += n * S * (4 * 8 + 3 * 8);                          // rates, secretion constants
+    b += n * 4 * 6 * 2;                                    // two sort workspaces
+    b += n * (16 + 16 + 8);                                // sorted SoA, diagnostics
+    b += (V + 1) * 4 * 2;                                  // counts, start
+    b += (n / 2048 + 1) * 256 * 4 * 2 + 4096;              // sort / scan scratch
+    return b;
+}
+
+int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const pcg_batch_options* opt,
+                  const std::vector<DevSource>* src, bool masked_steps)
+{
+    ctx = c;
+    masked = masked_steps;
+    auto from = [&](uint32_t i) -> const DevSource* {
+        return (src && i < src->size() && (*src)[i].batch) ? &(*src)[i] : nullptr;
+    };
+    if (n == 0) return fail(ctx, PCG_ERR_INVALID, "no instances");
+    use_graphs = opt ? opt->use_graphs != 0 : true;
+    profile = opt ? opt->profile_phases != 0 : false;
+    const bool tune = opt ? opt->autotune != 0 : true;
+    if (opt && opt->tune_cache) tune_cache = opt->tune_cache;
+    dt_diff = descs[0].grid.dt;
+    dt_mech = descs[0].dt_mechanics > 0.f ? descs[0].dt_mechanics : descs[0].mech.dt;
+    std::vector<DiffInstance> di(n);
+    uint64_t cells_total = 0, rates_total = 0, mvox_total = 0;
+    ncell.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const pcg_instance_desc& d = descs[i];
+        const float dm = d.dt_mechanics > 0.f ? d.dt_mechanics : d.mech.dt;
+        if (d.grid.dt != descs[0].grid.dt || dm != dt_mech)
+            return fail(ctx, PCG_ERR_INVALID, "instances of one batch must share dt_diffusion and dt_mechanics");
+        if (d.grid.n_substrates > 0 && !d.substrates) return fail(ctx, PCG_ERR_INVALID, "substrates is NULL");
+        if (d.n_cells > 0 && !from(i) && (!d.cells_soa || d.cells_soa_max < d.n_cells))
+            return fail(ctx, PCG_ERR_INVALID, "cells_soa missing or cells_soa_max < n_cells");
+        if (d.mech.mech_grid_nx == 0 || d.mech.mech_grid_ny == 0 || d.mech.mech_grid_nz == 0 ||
+            !(d.mech.mechanics_voxel_size > 0.f))
+            return fail(ctx, PCG_ERR_INVALID, "bad mechanics grid");
+        di[i].g = d.grid;
+        di[i].subs.assign(d.substrates, d.substrates + d.grid.n_substrates);
+        ncell[i] = d.n_cells;
+        cells_total += d.n_cells;
+        rates_total += static_cast<uint64_t>(d.n_cells) * d.grid.n_substrates;
+        mvox_total += static_cast<uint64_t>(d.mech.mech_grid_nx) * d.mech.mech_grid_ny * d.mech.mech_grid_nz;
+    }
+    if (cells_total > 0xFFFFFFF0ull || rates_total > 0xFFFFFFF0ull || mvox_total > 0xFFFFFFF0ull)
+        return fail(ctx, PCG_ERR_INVALID, "batch too large for 32-bit indices");
+    PCG_TRY(d.build(ctx, std::move(di)));
+    for (uint32_t i = 0; i < n; ++i) {
+        if (const DevSource* ds = from(i)) {
+            const DiffInstance& so = ds->batch->d.inst[ds->index];
+            const DiffInstance& de = d.inst[i];
+            if (so.nvox() != de.nvox() || so.g.n_substrates != de.g.n_substrates)
+                return fail(ctx, PCG_ERR_INVALID, "device source does not match the instance");
+            for (uint32_t s = 0; s < de.g.n_substrates; ++s)
+                PCG_CU(ctx, cudaMemcpyAsync(d.dens.as<float>() + de.dens_off + s * de.pitch,
+                                            ds->batch->d.dens.as<float>() + so.dens_off + s * so.pitch,
+                                            de.nvox() * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
+        } else if (descs[i].initial_density) {
+            PCG_TRY(d.upload(i, descs[i].initial_density));
+        } else if (descs[i].initial_values) {
+            PCG_TRY(d.fill(i, descs[i].initial_values));
+        }
+    }
+    // cells
+    PCG_TRY(c_.create(ctx, static_cast<uint32_t>(std::max<uint64_t>(cells_total, 1)),
+                      static_cast<uint32_t>(std::max<uint64_t>(rates_total, 1)), n));
+    c_.n = static_cast<uint32_t>(cells_total);
+    c_.n_rate = static_cast<uint32_t>(rates_total);
+    PCG_TRY(c_.set_cell_instances(ncell));
+    uint32_t coff = 0, roff = 0, moff = 0;
+    any_refresh = false;
+    for (uint32_t i = 0; i < n; ++i) {
+        const pcg_instance_desc& ds = descs[i];
+        CellInst& ci = c_.h_inst[i];
+        ci = CellInst{};
+        fill_diff_inst(ci, d.inst[i]);
+        fill_mech_inst(ci, ds.mech, ds.grid.x_min, ds.grid.y_min, ds.grid.z_min);
+        ci.dt_mech = dt_mech;
+        ci.cell_off = coff;
+        ci.n_cells = ds.n_cells;
+        ci.rate_off = roff;
+        ci.mvox_base = moff;
+        ci.flags = (ds.flags & PCG_INST_REFRESH_VOXELS) ? INST_REFRESH_VOXELS : 0u;
+        any_refresh = any_refresh || ci.flags;
+        if (ds.n_cells && from(i)) {
+            const Batch& sb = *from(i)->batch;
+            const CellInst& so = sb.c_.h_inst[from(i)->index];
+            if (so.n_cells != ds.n_cells || so.S != ds.grid.n_substrates)
+                return fail(ctx, PCG_ERR_INVALID, "device source cells do not match the instance");
+            PCG_CU(ctx, cudaMemcpy2DAsync(c_.soa.as<float>() + coff, static_cast<size_t>(c_.max_cells) * sizeof(float),
+                                          sb.c_.soa.as<float>() + so.cell_off,
+                                          static_cast<size_t>(sb.c_.max_cells) * sizeof(float),
+                                          static_cast<size_t>(ds.n_cells) * sizeof(float), NUM_FIELDS,
+                                          cudaMemcpyDeviceToDevice, ctx->stream));
+            const size_t cap_new = c_.rates.bytes / (4 * sizeof(double));
+            const size_t cap_old = sb.c_.rates.bytes / (4 * sizeof(double));
+            const size_t nr = static_cast<size_t>(ds.n_cells) * ds.grid.n_substrates;
+            for (int q = 0; q < 4; ++q)
+                PCG_CU(ctx, cudaMemcpyAsync(c_.rates.as<double>() + q * cap_new + roff,
+                                            sb.c_.rates.as<double>() + q * cap_old + so.rate_off, nr * sizeof(double),
+                                            cudaMemcpyDeviceToDevice, ctx->stream));
+            PCG_CU(ctx, cudaMemcpyAsync(c_.active.as<uint8_t>() + coff, sb.c_.active.as<uint8_t>() + so.cell_off,
+                                        ds.n_cells, cudaMemcpyDeviceToDevice, ctx->stream));
+            if (sb.c_.has_active) c_.has_active = true;
+            c_.coef_dirty = c_.order_dirty = true;
+        } else if (ds.n_cells) {
+            PCG_TRY(c_.upload_soa(coff, ds.n_cells, ds.cells_soa, ds.cells_soa_max, 0, NUM_FIELDS));
+            PCG_TRY(c_.set_rates(roff, ds.n_cells * ds.grid.n_substrates, ds.secretion, ds.uptake, ds.saturation,
+                                 ds.net_export));
+            PCG_TRY(c_.set_active(coff, ds.n_cells, ds.active));
+            if (ds.active) c_.has_active = true;
+        }
+        coff += ds.n_cells;
+        roff += ds.n_cells * ds.grid.n_substrates;
+        moff += ds.mech.mech_grid_nx * ds.mech.mech_grid_ny * ds.mech.mech_grid_nz;
+    }
+    c_.inst_dirty = true;
+    PCG_TRY(c_.sync_inst());
+    PCG_TRY(m_.create(ctx, moff, std::max<uint32_t>(coff, 1)));
+    PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    if (c_.n) PCG_TRY(c_.prepare_secretion(dt_diff, d.total_vox));
+    if (tune) {
+        if (!tune_cache.empty()) Tuner::get().load(tune_cache);
+        PCG_TRY(d.tune());
+        if (!tune_cache.empty()) Tuner::get().save(tune_cache);
+    }
+    for (int q = 0; q < 8; ++q) PCG_CU(ctx, cudaEventCreate(&ev[q]));
+    if (masked) {
+        PCG_CU(ctx, mask_d.alloc(n));
+        PCG_CU(ctx, cudaMemsetAsync(mask_d.p, STEP_DIFFUSE | STEP_MECH, n, ctx->stream));
+    }
+    PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    if (use_graphs) {
+        PCG_TRY(capture(false, &g_diff, &launches_diff));
+        PCG_TRY(capture(true, &g_mech, &launches_mech));
+    } else {
+        launches_diff = count_launches(false);
+        launches_mech = count_launches(true);
+    }
+    return PCG_OK;
+}
+
+Batch::~Batch()
+{
+    if (g_diff) cudaGraphExecDestroy(g_diff);
+    if (g_mech) cudaGraphExecDestroy(g_mech);
+    for (int q = 0; q < 8; ++q)
+        if (ev[q]) cudaEventDestroy(ev[q]);
+}
+
+uint64_t Batch::count_launches(bool mech) const
+{
+    uint64_t k = d.launches_per_step();
+    if (c_.n) k += 1;
+    if (mech && c_.n) {
+        k += m_.launches_forces(c_.n) - 1 + 1;   // bin..forces (memset excluded) + integrate
+        if (any_refresh) k += 1 + radix_sort_launches(c_.n, key_bits_for(d.total_vox + 1));
+    }
+    return k;
+}
+
+// One main-loop sub-step; 'timed' records phase events.
+int Batch::run_step(bool mech, bool timed, const uint8_t* mask)
+{
+    cudaStream_t st = ctx->stream;
+    if (timed) PCG_CU(ctx, cudaEventRecord(ev[0], st));
+    for (int a = 0; a < 3; ++a) {
+        PCG_TRY(d.sweep(a, true, mask));
+        if (timed) PCG_CU(ctx, cudaEventRecord(ev[1 + a], st));
+    }
+    if (c_.n) PCG_TRY(c_.secrete(d, mask));
+    if (timed) PCG_CU(ctx, cudaEventRecord(ev[4], st));
+    if (mech && c_.n) {
+        PCG_TRY(m_.binsort(c_));
+        if (timed) PCG_CU(ctx, cudaEventRecord(ev[5], st));
+        PCG_TRY(m_.force_pass(c_, mask));
+        if (timed) PCG_CU(ctx, cudaEventRecord(ev[6], st));
+        PCG_TRY(m_.integrate(c_, -1.0f, mask));
+        if (any_refresh) PCG_TRY(c_.build_order(d.total_vox));
+        if (timed) PCG_CU(ctx, cudaEventRecord(ev[7], st));
+    }
+    return PCG_OK;
+}
+
+int Batch::capture(bool mech, cudaGraphExec_t* out, uint64_t* launches)
+{
+    cudaStream_t st = ctx->stream;
+    const uint64_t before = ctx->launches;
+    PCG_CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = run_step(mech, false, masked ? mask_d.as<uint8_t>() : nullptr);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != PCG_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "end capture");
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "graph instantiate");
+    *launches = ctx->launches - before;
+    ctx->launches = before;   // captured, not executed
+    c_.order_dirty = false;   // ordering is rebuilt inside the mechanics graph when needed
+    return PCG_OK;
+}
+
+int Batch::step(int n_steps)
+{
+    if (n_steps < 0) return fail(ctx, PCG_ERR_INVALID, "n_steps < 0");
+    cudaStream_t st = ctx->stream;
+    for (int s = 0; s < n_steps; ++s) {
+        accum += dt_diff;
+        const bool mech = accum >= dt_mech - 0.5 * dt_diff;
+        if (mech) accum = 0.0;
+        if (profile) {
+            PCG_TRY(run_step(mech, true, nullptr));
+            PCG_CU(ctx, cudaEventSynchronize(mech ? ev[7] : ev[4]));
+            float ms = 0;
+            for (int a = 0; a < 3; ++a) {
+                PCG_CU(ctx, cudaEventElapsedTime(&ms, ev[a], ev[a + 1]));
+                phase_ms[a] += ms;
+            }
+            PCG_CU(ctx, cudaEventElapsedTime(&ms, ev[3], ev[4]));
+            phase_ms[3] += ms;
+            if (mech && c_.n) {
+                PCG_CU(ctx, cudaEventElapsedTime(&ms, ev[4], ev[5]));
+                phase_ms[4] += ms;
+                PCG_CU(ctx, cudaEventElapsedTime(&ms, ev[5], ev[6]));
+                phase_ms[5] += ms;
+                PCG_CU(ctx, cudaEventElapsedTime(&ms, ev[6], ev[7]));
+                phase_ms[6] += ms;
+            }
+            sweep_steps++;
+        } else if (use_graphs) {
+            PCG_CU(ctx, cudaGraphLaunch(mech ? g_mech : g_diff, st));
+            ctx->launches += mech ? launches_mech : launches_diff;
+        } else {
+            PCG_TRY(run_step(mech, false, nullptr));
+        }
+        if (mech) mech_steps++;
+        diff_steps++;
+    }
+    return PCG_OK;
+}
+
+int Batch::step_masked(const uint8_t* mask_host, bool any_mech)
+{
+    if (!masked) return fail(ctx, PCG_ERR_INVALID, "batch was not created for masked steps");
+    cudaStream_t st = ctx->stream;
+    PCG_CU(ctx, cudaMemcpyAsync(mask_d.p, mask_host, mask_d.bytes, cudaMemcpyHostToDevice, st));
+    if (use_graphs) {
+        PCG_CU(ctx, cudaGraphLaunch(any_mech ? g_mech : g_diff, st));
+        ctx->launches += any_mech ? launches_mech : launches_diff;
+    } else {
+        PCG_TRY(run_step(any_mech, false, mask_d.as<uint8_t>()));
+    }
+    diff_steps++;
+    if (any_mech) mech_steps++;
+    return PCG_OK;
+}
+
+std::string Batch::describe() const
+{
+    std::ostringstream o;
+    o << d.describe() << "forces(lanes=" << kForceLanes << ",block=" << m_.block << ") graphs=" << (use_graphs ? 1 : 0)
+      << " launches/step=" << launches_diff << "/" << launches_mech;
+    return o.str();
+}
+
+}  // namespace pcg
+
+struct pcg_batch {
+    Batch b;
+    std::string desc;
+};
+
+extern "C" {
+
+uint64_t pcg_instance_bytes(const pcg_instance_desc* inst) { return inst ? instance_bytes(*inst) : 0; }
+
+pcg_status pcg_batch_create(pcg_ctx* ctx, const pcg_instance_desc* inst, uint32_t n, const pcg_batch_options* opt,
+                            pcg_batch** out)
+{
+    if (!ctx || !out || (!inst && n)) return PCG_ERR_INVALID;
+    *out = nullptr;
+    pcg_batch* b = new (std::nothrow) pcg_batch();
+    if (!b) return PCG_ERR_OOM;
+    int rc = b->b.create(ctx, inst, n, opt);
+    if (rc != PCG_OK) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_destroy(pcg_batch* b)
+{
+    if (b) cudaStreamSynchronize(b->b.ctx->stream);
+    delete b;
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_step(pcg_batch* b, int n) { return b ? b->b.step(n) : PCG_ERR_INVALID; }
+
+pcg_status pcg_batch_download_density(pcg_batch* b, uint32_t i, float* host, size_t n)
+{
+    if (!b || !host || i >= b->b.d.inst.size()) return PCG_ERR_INVALID;
+    const DiffInstance& di = b->b.d.inst[i];
+    if (n != di.nvox() * di.g.n_substrates) return fail(b->b.ctx, PCG_ERR_INVALID, "density size mismatch");
+    return b->b.d.download(i, host);
+}
+
+pcg_status pcg_batch_download_cells(pcg_batch* b, uint32_t i, float* soa, uint32_t soa_max)
+{
+    if (!b || !soa || i >= b->b.ncell.size()) return PCG_ERR_INVALID;
+    const CellInst& ci = b->b.c_.h_inst[i];
+    if (soa_max < ci.n_cells) return fail(b->b.ctx, PCG_ERR_INVALID, "soa_max_cells < n_cells");
+    PCG_TRY(b->b.c_.download_soa(ci.cell_off, ci.n_cells, soa, soa_max, 0, NUM_FIELDS));
+    PCG_CU(b->b.ctx, cudaStreamSynchronize(b->b.ctx->stream));
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_upload_cells(pcg_batch* b, uint32_t i, const float* soa, uint32_t soa_max)
+{
+    if (!b || !soa || i >= b->b.ncell.size()) return PCG_ERR_INVALID;
+    const CellInst& ci = b->b.c_.h_inst[i];
+    if (soa_max < ci.n_cells) return fail(b->b.ctx, PCG_ERR_INVALID, "soa_max_cells < n_cells");
+    PCG_TRY(b->b.c_.upload_soa(ci.cell_off, ci.n_cells, soa, soa_max, 0, NUM_FIELDS));
+    PCG_CU(b->b.ctx, cudaStreamSynchronize(b->b.ctx->stream));
+    // volumes and voxel indices may have changed: rebuild the secretion constants and order now
+    PCG_TRY(b->b.c_.prepare_secretion(b->b.dt_diff, b->b.d.total_vox));
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_upload_all_cells(pcg_batch* b, const float* soa, uint64_t n_floats)
+{
+    if (!b || !soa) return PCG_ERR_INVALID;
+    Cells& c = b->b.c_;
+    if (n_floats != static_cast<uint64_t>(NUM_FIELDS) * c.n) return fail(b->b.ctx, PCG_ERR_INVALID, "size mismatch");
+    if (c.n == 0) return PCG_OK;
+    PCG_TRY(c.upload_soa(0, c.n, soa, c.n, 0, NUM_FIELDS));
+    PCG_TRY(c.prepare_secretion(b->b.dt_diff, b->b.d.total_vox));
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_download_all_cells(pcg_batch* b, float* soa, uint64_t n_floats)
+{
+    if (!b || !soa) return PCG_ERR_INVALID;
+    Cells& c = b->b.c_;
+    if (n_floats != static_cast<uint64_t>(NUM_FIELDS) * c.n) return fail(b->b.ctx, PCG_ERR_INVALID, "size mismatch");
+    return c.download_soa(0, c.n, soa, c.n, 0, NUM_FIELDS);
+}
+
+pcg_status pcg_batch_download_all_density(pcg_batch* b, float* host, uint64_t n_floats)
+{
+    if (!b || !host) return PCG_ERR_INVALID;
+    if (n_floats != b->b.d.dens_elems) return fail(b->b.ctx, PCG_ERR_INVALID, "size mismatch");
+    PCG_CU(b->b.ctx, cudaMemcpyAsync(host, b->b.d.dens.p, n_floats * sizeof(float), cudaMemcpyDeviceToHost,
+                                     b->b.ctx->stream));
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_density_layout(pcg_batch* b, uint32_t i, uint64_t* off, uint64_t* pitch, uint64_t* arena)
+{
+    if (!b || i >= b->b.d.inst.size()) return PCG_ERR_INVALID;
+    if (off) *off = b->b.d.inst[i].dens_off;
+    if (pitch) *pitch = b->b.d.inst[i].pitch;
+    if (arena) *arena = b->b.d.dens_elems;
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_totals(pcg_batch* b, uint64_t* voxels, uint64_t* vs, uint64_t* cells)
+{
+    if (!b) return PCG_ERR_INVALID;
+    if (voxels) *voxels = b->b.d.total_vox;
+    if (vs) *vs = b->b.d.total_vox_sub;
+    if (cells) *cells = b->b.c_.n;
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_step_launches(pcg_batch* b, uint64_t* ld, uint64_t* lm)
+{
+    if (!b) return PCG_ERR_INVALID;
+    if (ld) *ld = b->b.launches_diff;
+    if (lm) *lm = b->b.launches_mech;
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_phase_times(pcg_batch* b, float* ms, uint64_t* n_sweep_steps, int reset)
+{
+    if (!b) return PCG_ERR_INVALID;
+    if (ms)
+        for (int q = 0; q < PCG_N_PHASES; ++q) ms[q] = static_cast<float>(b->b.phase_ms[q]);
+    if (n_sweep_steps) *n_sweep_steps = b->b.sweep_steps;
+    if (reset) {
+        for (int q = 0; q < PCG_N_PHASES; ++q) b->b.phase_ms[q] = 0.0;
+        b->b.sweep_steps = 0;
+    }
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_set_profile(pcg_batch* b, int on)
+{
+    if (!b) return PCG_ERR_INVALID;
+    b->b.profile = on != 0;
+    return PCG_OK;
+}
+
+const char* pcg_batch_describe(pcg_batch* b)
+{
+    if (!b) return "";
+    b->desc = b->b.describe();
+    return b->desc.c_str();
+}
+
+}  // extern "C"

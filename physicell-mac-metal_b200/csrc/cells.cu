@@ -1,0 +1,372 @@
+// cells.cu — per-cell kernels (sm_100a): secretion/uptake, spatial binning,
+// sorted-SoA gather, neighbour forces and the Adams-Bashforth update.
+//
+// Reference semantics:
+//   secretion  src/cell_phenotype.cpp:526-564 (processSecretion), FP64 per
+//              cell, FP32 density store after every cell;
+//   binning    shaders/mechanics.metal:54-76 (FP32 divide + truncation);
+//   forces     shaders/mechanics.metal:91-216;
+//   integrate  shaders/integrate.metal:31-80, clamp box = mechanics grid
+//              (src/cell_mechanics.mm:147-159);
+//   voxel refresh  Microenvironment::voxelIndex (microenvironment.mm:261-269).
+// The reference's GPU hash and CPU secretion loop are racy; here every
+// result is deterministic: cells are sorted by (voxel, cell index) with a
+// stable radix sort and each voxel's cells are processed in that order.
+#include "pcg_kernels.cuh"
+
+namespace pcg {
+
+__device__ __forceinline__ uint32_t fbits(float f) { return __float_as_uint(f); }
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// (int)((p - lo) / h) with IEEE FP32 subtract and divide; cvt.rzi saturates
+// out-of-range values and maps NaN to 0.
+__device__ __forceinline__ int bin_of(float p, float lo, float h)
+{
+    return __float2int_rz(__fdiv_rn(__fsub_rn(p, lo), h));
+}
+
+// ------------------------------------------------------------------ secretion
+
+__global__ void k_sec_keys(const float* __restrict__ soa, uint32_t stride, uint32_t n,
+                           const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
+                           const uint8_t* __restrict__ active, uint32_t invalid_key, uint32_t* __restrict__ keys,
+                           uint32_t* __restrict__ vals)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const CellInst& in = insts[cell_inst[g]];
+    const uint32_t v = fbits(soa[static_cast<size_t>(F_VOXEL_IDX) * stride + g]);
+    const uint32_t nv = in.nx * in.ny * in.nz;
+    const bool ok = (active == nullptr || active[g] != 0) && v < nv && in.S > 0;
+    keys[g] = ok ? in.vox_base + v : invalid_key;
+    vals[g] = g;
+}
+
+// coef3[(rate index) * 3 + {0,1,2}] = {dt*ne/V_vox, ic*sec*sat, 1 + ic*(sec+upt)}
+// with ic = dt*V_cell/V_vox, exactly as processSecretion forms them.
+__global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, uint32_t n,
+                              const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
+                              const double* __restrict__ rates4, uint32_t n_rate, double dt,
+                              double* __restrict__ coef3)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const CellInst& in = insts[cell_inst[g]];
+    const double V_vox = __dmul_rn(__dmul_rn(static_cast<double>(in.dx), static_cast<double>(in.dy)),
+                                   static_cast<double>(in.dz));
+    const double V_cell = static_cast<double>(soa[static_cast<size_t>(F_TOTAL_VOL) * stride + g]);
+    const double ic = __ddiv_rn(__dmul_rn(dt, V_cell), V_vox);
+    const uint32_t base = in.rate_off + (g - in.cell_off) * in.S;
+    for (uint32_t s = 0; s < in.S; ++s) {
+        const uint32_t o = base + s;
+        const double sec = rates4[o], upt = rates4[n_rate + o], sat = rates4[2ull * n_rate + o],
+                     ne = rates4[3ull * n_rate + o];
+        coef3[3ull * o + 0] = __ddiv_rn(__dmul_rn(dt, ne), V_vox);
+        coef3[3ull * o + 1] = __dmul_rn(__dmul_rn(ic, sec), sat);
+        coef3[3ull * o + 2] = __dadd_rn(1.0, __dmul_rn(ic, __dadd_rn(sec, upt)));
+    }
+}
+
+// One thread per run of equal keys in the sorted order: applies the run's
+// cells to the voxel in ascending cell index, substrate by substrate.
+__global__ void k_secrete(float* __restrict__ dens, const uint32_t* __restrict__ skeys,
+                          const uint32_t* __restrict__ sorder, uint32_t n, const uint32_t* __restrict__ cell_inst,
+                          const CellInst* __restrict__ insts, const double* __restrict__ coef3, uint32_t invalid_key,
+                          const uint8_t* __restrict__ mask)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint32_t key = skeys[p];
+    if (key >= invalid_key) return;
+    if (p > 0 && skeys[p - 1] == key) return;
+    uint32_t q_end = p + 1;
+    while (q_end < n && skeys[q_end] == key) ++q_end;
+    const uint32_t ii = cell_inst[sorder[p]];
+    if (mask && !(mask[ii] & STEP_DIFFUSE)) return;
+    const CellInst& in = insts[ii];
+    const uint32_t v = key - in.vox_base;
+    for (uint32_t s = 0; s < in.S; ++s) {
+        float* d = dens + in.dens_off + s * in.sub_pitch + v;
+        float rho32 = *d;
+        for (uint32_t q = p; q < q_end; ++q) {
+            const uint32_t g = sorder[q];
+            const double* c = coef3 + 3ull * (in.rate_off + (g - in.cell_off) * in.S + s);
+            double rho = static_cast<double>(rho32);
+            rho = __dadd_rn(rho, c[0]);
+            rho = __ddiv_rn(__dadd_rn(rho, c[1]), c[2]);
+            if (rho < 0.0) rho = 0.0;
+            rho32 = __double2float_rn(rho);
+        }
+        *d = rho32;
+    }
+}
+
+// ------------------------------------------------------------------ mechanics
+
+__global__ void k_mech_bin(float* __restrict__ soa, uint32_t stride, uint32_t n, const uint32_t* __restrict__ cell_inst,
+                           const CellInst* __restrict__ insts, uint32_t* __restrict__ keys,
+                           uint32_t* __restrict__ vals, uint32_t* __restrict__ counts)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const CellInst& in = insts[cell_inst[g]];
+    const float px = soa[static_cast<size_t>(F_POS_X) * stride + g];
+    const float py = soa[static_cast<size_t>(F_POS_Y) * stride + g];
+    const float pz = soa[static_cast<size_t>(F_POS_Z) * stride + g];
+    const int vi = clampi(bin_of(px, in.mx_min, in.vs), 0, static_cast<int>(in.mnx) - 1);
+    const int vj = clampi(bin_of(py, in.my_min, in.vs), 0, static_cast<int>(in.mny) - 1);
+    const int vk = clampi(bin_of(pz, in.mz_min, in.vs), 0, static_cast<int>(in.mnz) - 1);
+    const uint32_t local = static_cast<uint32_t>(vk) * in.mny * in.mnx + static_cast<uint32_t>(vj) * in.mnx +
+                           static_cast<uint32_t>(vi);
+    soa[static_cast<size_t>(F_MECH_VOXEL) * stride + g] = __uint_as_float(local);
+    const uint32_t key = in.mvox_base + local;
+    keys[g] = key;
+    vals[g] = g;
+    atomicAdd(&counts[key], 1u);
+}
+
+__global__ void k_mech_gather(const float* __restrict__ soa, uint32_t stride, const uint32_t* __restrict__ sorder,
+                              uint32_t n, float4* __restrict__ spos, float4* __restrict__ sprm)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint32_t g = sorder[p];
+    spos[p] = make_float4(soa[static_cast<size_t>(F_POS_X) * stride + g], soa[static_cast<size_t>(F_POS_Y) * stride + g],
+                          soa[static_cast<size_t>(F_POS_Z) * stride + g], soa[static_cast<size_t>(F_RADIUS) * stride + g]);
+    sprm[p] = make_float4(soa[static_cast<size_t>(F_REPULSION) * stride + g],
+                          soa[static_cast<size_t>(F_ADHESION) * stride + g],
+                          soa[static_cast<size_t>(F_REL_MAX_ADH) * stride + g], 0.0f);
+}
+
+__device__ __forceinline__ uint32_t nbr_hash(uint32_t j)
+{
+    uint32_t x = j + 0x9E3779B9u;
+    x ^= x >> 16;
+    x *= 0x85EBCA6Bu;
+    x ^= x >> 13;
+    x *= 0xC2B2AE35u;
+    x ^= x >> 16;
+    return x;
+}
+
+// G lanes per cell (cells in sorted order); each neighbour row (dk, dj) is
+// one contiguous range of the sorted order covering di = -1..1, which the G
+// lanes stride through; partial sums are combined with a fixed xor-shuffle
+// tree, so the result does not depend on scheduling.
+template <int G>
+__global__ void __launch_bounds__(512) k_mech_forces(const float4* __restrict__ spos, const float4* __restrict__ sprm,
+                                                     const uint32_t* __restrict__ skeys,
+                                                     const uint32_t* __restrict__ sorder,
+                                                     const uint32_t* __restrict__ start, uint32_t n,
+                                                     const uint32_t* __restrict__ cell_inst,
+                                                     const CellInst* __restrict__ insts, float* __restrict__ soa,
+                                                     uint32_t stride, uint32_t* __restrict__ diag_cnt,
+                                                     uint32_t* __restrict__ diag_hash,
+                                                     const uint8_t* __restrict__ mask)
+{
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t p = gid / G;
+    const int sub = static_cast<int>(gid % G);
+    bool valid = p < n;
+    float fx = 0.f, fy = 0.f, fz = 0.f, P = 0.f;
+    uint32_t cnt = 0, hsh = 0, g = 0;
+    if (valid) {
+        g = sorder[p];
+        const uint32_t ii = cell_inst[g];
+        if (mask && !(mask[ii] & STEP_MECH)) valid = false;
+    }
+    if (valid) {
+        const CellInst& in = insts[cell_inst[g]];
+        const float4 me = spos[p];
+        const float4 mp = sprm[p];
+        const uint32_t local = skeys[p] - in.mvox_base;
+        const int mnx = static_cast<int>(in.mnx), mny = static_cast<int>(in.mny), mnz = static_cast<int>(in.mnz);
+        const int ci = static_cast<int>(local % in.mnx);
+        const int cj = static_cast<int>((local / in.mnx) % in.mny);
+        const int ck = static_cast<int>(local / (in.mnx * in.mny));
+        const float maxd2 = __fmul_rn(in.maxd, in.maxd);
+        const int ilo = ci > 0 ? ci - 1 : 0, ihi = ci + 1 < mnx ? ci + 1 : mnx - 1;
+        const int dk0 = mnz > 1 ? -1 : 0, dk1 = mnz > 1 ? 1 : 0;
+        for (int dk = dk0; dk <= dk1; ++dk) {
+            const int nk = ck + dk;
+            if (nk < 0 || nk >= mnz) continue;
+            for (int dj = -1; dj <= 1; ++dj) {
+                const int nj = cj + dj;
+                if (nj < 0 || nj >= mny) continue;
+                const uint32_t row = in.mvox_base + static_cast<uint32_t>(nk * mny + nj) * static_cast<uint32_t>(mnx);
+                const uint32_t q0 = start[row + ilo], q1 = start[row + ihi + 1];
+                for (uint32_t q = q0 + sub; q < q1; q += G) {
+                    if (q == p) continue;
+                    const float4 o = spos[q];
+                    // neighbour test exactly as mechanics.metal:159-165 (no contraction)
+                    const float ddx = __fsub_rn(me.x, o.x), ddy = __fsub_rn(me.y, o.y), ddz = __fsub_rn(me.z, o.z);
+                    const float dsq = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
+                    if (dsq >= maxd2 || dsq < 1e-12f) continue;
+                    if (diag_cnt) {
+                        ++cnt;
+                        hsh += nbr_hash(sorder[q] - in.cell_off);
+                    }
+                    const float dist = sqrtf(dsq);
+                    const float inv = 1.0f / dist;
+                    const float R = me.w + o.w;
+                    float F = 0.f;
+                    if (dist < R) {
+                        const float4 op = sprm[q];
+                        const float ov = 1.0f - dist / R;
+                        F += ov * ov * sqrtf(mp.x * op.x);
+                        P += ov * ov / 0.027288820670331f;
+                    }
+                    const float A = mp.z * R;
+                    if (dist < A) {
+                        const float op_adh = sprm[q].y;
+                        const float t = 1.0f - dist / A;
+                        F -= t * t * sqrtf(mp.y * op_adh);
+                    }
+                    fx += F * (ddx * inv);
+                    fy += F * (ddy * inv);
+                    fz += F * (ddz * inv);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+        P += __shfl_xor_sync(0xffffffffu, P, o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        hsh += __shfl_xor_sync(0xffffffffu, hsh, o);
+    }
+    if (valid && sub == 0) {
+        soa[static_cast<size_t>(F_VEL_X) * stride + g] = fx;
+        soa[static_cast<size_t>(F_VEL_Y) * stride + g] = fy;
+        soa[static_cast<size_t>(F_VEL_Z) * stride + g] = fz;
+        soa[static_cast<size_t>(F_PRESSURE) * stride + g] = P;
+        if (diag_cnt) {
+            diag_cnt[g] = cnt;
+            diag_hash[g] = hsh;
+        }
+    }
+}
+
+// AB2 in FP64 with explicit rounding, stored FP32: the FP64 value of
+// p + dt (1.5 v - 0.5 v_prev) rounded once (integrate.metal:273-285 keeps
+// FP32 storage; the oracle forms the same FP64 expression).
+__global__ void k_mech_integrate(float* __restrict__ soa, uint32_t stride, uint32_t n,
+                                 const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
+                                 float dt_override, const uint8_t* __restrict__ mask)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t ii = cell_inst[g];
+    if (mask && !(mask[ii] & STEP_MECH)) return;
+    const CellInst& in = insts[ii];
+    const double dt = static_cast<double>(dt_override >= 0.0f ? dt_override : in.dt_mech);
+    const float lo[3] = {in.mx_min, in.my_min, in.mz_min};
+    const float hi[3] = {in.box_hi_x, in.box_hi_y, in.box_hi_z};
+    float pos[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float* p = soa + static_cast<size_t>(F_POS_X + a) * stride + g;
+        const float v = soa[static_cast<size_t>(F_VEL_X + a) * stride + g];
+        float* pv = soa + static_cast<size_t>(F_PREV_VX + a) * stride + g;
+        const double inc = __dsub_rn(__dmul_rn(1.5, static_cast<double>(v)), __dmul_rn(0.5, static_cast<double>(*pv)));
+        double x = __dadd_rn(static_cast<double>(*p), __dmul_rn(dt, inc));
+        if (x < static_cast<double>(lo[a])) x = lo[a];
+        if (x > static_cast<double>(hi[a])) x = hi[a];
+        pos[a] = __double2float_rn(x);
+        *p = pos[a];
+        *pv = v;
+    }
+    if (in.flags & INST_REFRESH_VOXELS) {
+        const int i = clampi(bin_of(pos[0], in.x_min, in.dx), 0, static_cast<int>(in.nx) - 1);
+        const int j = clampi(bin_of(pos[1], in.y_min, in.dy), 0, static_cast<int>(in.ny) - 1);
+        const int k = clampi(bin_of(pos[2], in.z_min, in.dz), 0, static_cast<int>(in.nz) - 1);
+        const uint32_t v = static_cast<uint32_t>(k) * in.nx * in.ny + static_cast<uint32_t>(j) * in.nx +
+                           static_cast<uint32_t>(i);
+        soa[static_cast<size_t>(F_VOXEL_IDX) * stride + g] = __uint_as_float(v);
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+
+static inline unsigned blocks_for(uint64_t n, int b) { return static_cast<unsigned>((n + b - 1) / b); }
+
+cudaError_t launch_sec_keys(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n, const uint32_t* cell_inst,
+                            const CellInst* insts, const uint8_t* active, uint32_t invalid_key, uint32_t* keys,
+                            uint32_t* vals)
+{
+    if (n == 0) return cudaSuccess;
+    k_sec_keys<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, active, invalid_key, keys, vals);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
+                               const uint32_t* cell_inst, const CellInst* insts, const double* rates4, uint32_t n_rate,
+                               double dt, double* coef3)
+{
+    if (n == 0) return cudaSuccess;
+    k_sec_prepare<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, rates4, n_rate, dt, coef3);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
+                           const uint32_t* cell_inst, const CellInst* insts, const double* coef3, uint32_t invalid_key,
+                           const uint8_t* mask)
+{
+    if (n == 0) return cudaSuccess;
+    k_secrete<<<blocks_for(n, 256), 256, 0, st>>>(dens, skeys, sorder, n, cell_inst, insts, coef3, invalid_key, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n, const uint32_t* cell_inst,
+                            const CellInst* insts, uint32_t* keys, uint32_t* vals, uint32_t* counts)
+{
+    if (n == 0) return cudaSuccess;
+    k_mech_bin<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, keys, vals, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mech_gather(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* sorder, uint32_t n,
+                               float4* spos, float4* sprm)
+{
+    if (n == 0) return cudaSuccess;
+    k_mech_gather<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, sorder, n, spos, sprm);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* skeys,
+                               const uint32_t* sorder, const uint32_t* start, uint32_t n, const uint32_t* cell_inst,
+                               const CellInst* insts, float* soa, uint32_t stride, uint32_t* diag_cnt,
+                               uint32_t* diag_hash, const uint8_t* mask, int block)
+{
+    if (n == 0) return cudaSuccess;
+    const unsigned grid = blocks_for(static_cast<uint64_t>(n) * kForceLanes, block);
+    k_mech_forces<kForceLanes><<<grid, block, 0, st>>>(spos, sprm, skeys, sorder, start, n, cell_inst, insts, soa,
+                                                        stride, diag_cnt, diag_hash, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, uint32_t stride, uint32_t n, const uint32_t* cell_inst,
+                                  const CellInst* insts, float dt_override, const uint8_t* mask)
+{
+    if (n == 0) return cudaSuccess;
+    k_mech_integrate<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, dt_override, mask);
+    return cudaGetLastError();
+}
+
+uint32_t neighbor_hash_host(uint32_t j)
+{
+    uint32_t x = j + 0x9E3779B9u;
+    x ^= x >> 16;
+    x *= 0x85EBCA6Bu;
+    x ^= x >> 13;
+    x *= 0xC2B2AE35u;
+    x ^= x >> 16;
+    return x;
+}
+
+}  // namespace pcg

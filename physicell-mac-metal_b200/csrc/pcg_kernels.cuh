@@ -1,0 +1,163 @@
+// pcg_kernels.cuh — device data structures shared by the sm_100a kernels and
+// the host runtime, and the host-side launchers of every kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+namespace pcg {
+
+// Cell SoA field ids (shaders/types.h:74-102).
+enum Field : int {
+    F_POS_X = 0, F_POS_Y = 1, F_POS_Z = 2,
+    F_VEL_X = 3, F_VEL_Y = 4, F_VEL_Z = 5,
+    F_PREV_VX = 6, F_PREV_VY = 7, F_PREV_VZ = 8,
+    F_RADIUS = 9, F_TOTAL_VOL = 11,
+    F_REPULSION = 13, F_ADHESION = 14, F_REL_MAX_ADH = 15,
+    F_PRESSURE = 22, F_VOXEL_IDX = 26, F_MECH_VOXEL = 27,
+    NUM_FIELDS = 28
+};
+
+// ---------------------------------------------------------------- diffusion
+
+// Thomas constants of one (instance, substrate, axis) line family.  Every
+// line of the family has the same matrix, so c'_i and 1/den_i are one
+// table (float2 {c'_i, 1/den_i} at tab[0..n-1]) built on the host in FP64
+// from the reference's recurrence (shaders/diffusion_2d.metal:86-148):
+//   forward   d_1 = (rho_1 + fold) / b_bnd
+//             d_i = (rho_i [+ fold at i = n-2] + c d_{i-1}) / den_i
+//   backward  rho_i = d_i - c'_i rho_{i+1}
+// with den_i = b + c c'_{i-1}, c'_i = -c / den_i; written as
+// d_i = fma(-c'_i, d_{i-1}, (rho_i + fold_i) * inv_i) since c/den_i = -c'_i.
+struct LineRule {
+    uint32_t tab;   // first table entry
+    uint32_t n;     // line length
+    float c;        // D dt / h^2
+    float fold;     // Dirichlet RHS fold: c T (2 c T when n == 3), 0 without Dirichlet
+    float T;        // Dirichlet target
+    uint32_t dir;   // Dirichlet enabled
+    uint32_t inst;  // instance index (step mask lookup)
+    uint32_t _pad;
+};
+
+// A tile of lines for one sweep launch.  Row tiles (x sweep): 'count'
+// contiguous lines of length n starting at element 'base', line stride n.
+// Column tiles (y and z sweeps): 'count' (<= 32) adjacent columns starting
+// at 'base', element stride 'rs' along the line.
+struct SweepTile {
+    uint64_t base;
+    uint32_t rule;
+    uint32_t count;
+    uint32_t rs;    // element stride along a line
+    uint32_t i0;    // x index of the tile's first line (column tiles)
+    uint32_t nx;    // the instance's nx
+    uint32_t face;  // TILE_FACE: the Dirichlet reset is fused into this sweep;
+                    // TILE_FACE_ALL: every line of the tile lies on a face
+};
+enum : uint32_t { TILE_FACE = 1u, TILE_FACE_ALL = 2u };
+
+// ---------------------------------------------------------------- cells
+
+// Per-instance constants for secretion, binning, forces and integration.
+struct CellInst {
+    // diffusion grid (secretion, voxel refresh)
+    uint32_t nx, ny, nz, S;
+    float dx, dy, dz;
+    uint32_t flags;        // INST_REFRESH_VOXELS
+    float x_min, y_min, z_min, dt_mech;
+    uint64_t dens_off;     // element offset of substrate 0 in the density arena
+    uint64_t sub_pitch;    // elements between substrates
+    uint32_t vox_base;     // global diffusion-voxel key of voxel 0
+    uint32_t cell_off;     // global index of the instance's first cell
+    uint32_t n_cells;
+    uint32_t rate_off;     // index of (cell 0, substrate 0) in the rate arrays
+    // mechanics grid (cell_mechanics.mm:115-159): origin, voxel, clamp box
+    uint32_t mnx, mny, mnz, mvox_base;
+    float vs, maxd, mx_min, my_min;
+    float mz_min, box_hi_x, box_hi_y, box_hi_z;
+};
+
+enum : uint32_t { INST_REFRESH_VOXELS = 1u };
+
+// Per-instance step mask (nullptr = every instance runs): bit 0 = the
+// instance takes this diffusion step, bit 1 = it takes this mechanics step.
+enum : uint8_t { STEP_DIFFUSE = 1u, STEP_MECH = 2u };
+
+// ---------------------------------------------------------------- launchers
+// All launchers enqueue on 'st' and return the CUDA launch status.
+
+struct RowsCfg { int lines; int grid; };     // x sweep: lines per CTA tile, CTAs
+struct ColsCfg { int warps; int grid; };     // y/z sweeps: warps (tiles) per CTA, CTAs
+
+size_t sweep_rows_smem(int lines, int nmax);
+size_t sweep_cols_smem(int warps, int nmax);
+cudaError_t sweep_rows_prepare(int lines, int nmax);   // opt into large dynamic SMEM
+cudaError_t sweep_cols_prepare(int warps, int nmax);
+int sweep_rows_occupancy(int lines, int nmax);         // resident CTAs per SM
+int sweep_cols_occupancy(int warps, int nmax);
+
+cudaError_t launch_sweep_rows(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
+                              const LineRule* rules, const float2* tab, int nmax, const uint8_t* mask, RowsCfg cfg);
+cudaError_t launch_sweep_cols(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
+                              const LineRule* rules, const float2* tab, int nmax, int apply_faces,
+                              const uint8_t* mask, ColsCfg cfg);
+// Any line length: one thread per line, d' kept in place in global memory.
+cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
+                                const LineRule* rules, const float2* tab, int apply_faces, const uint8_t* mask,
+                                int grid);
+
+// applyDirichletBC over instances [0, n_inst): faces of Dirichlet substrates.
+struct FaceJob { uint64_t base; uint32_t nx, ny, nz; float T; };
+cudaError_t launch_dirichlet(cudaStream_t st, float* dens, const FaceJob* jobs, uint32_t njobs);
+
+// Central / one-sided gradients (microenvironment.mm:282-342).
+struct GradJob { uint64_t base; uint64_t out_base; uint32_t nx, ny, nz; float inv_dx, inv_dy, inv_dz; };
+cudaError_t launch_gradients(cudaStream_t st, const float* dens, float* gx, float* gy, float* gz,
+                             const GradJob* jobs, uint32_t njobs, uint64_t max_voxels);
+
+// Secretion: keys / coefficient preparation / ordered application.
+cudaError_t launch_sec_keys(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
+                            const uint32_t* cell_inst, const CellInst* insts, const uint8_t* active,
+                            uint32_t invalid_key, uint32_t* keys, uint32_t* vals);
+cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
+                               const uint32_t* cell_inst, const CellInst* insts, const double* rates4,
+                               uint32_t n_rate, double dt_override, double* coef3);
+cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, const uint32_t* sorder,
+                           uint32_t n, const uint32_t* cell_inst, const CellInst* insts,
+                           const double* coef3, uint32_t invalid_key, const uint8_t* mask);
+
+// Mechanics.
+cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
+                            const uint32_t* cell_inst, const CellInst* insts,
+                            uint32_t* keys, uint32_t* vals, uint32_t* counts);
+cudaError_t launch_mech_gather(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* sorder,
+                               uint32_t n, float4* spos, float4* sprm);
+cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* skeys,
+                               const uint32_t* sorder, const uint32_t* start, uint32_t n,
+                               const uint32_t* cell_inst, const CellInst* insts, float* soa, uint32_t stride,
+                               uint32_t* diag_cnt, uint32_t* diag_hash, const uint8_t* mask, int block);
+// dt_override >= 0 replaces every instance's dt_mech.
+cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
+                                  const uint32_t* cell_inst, const CellInst* insts, float dt_override,
+                                  const uint8_t* mask);
+// Lanes per cell in the force pass; fixed so that a cell's summation order
+// never depends on what else is in the batch.
+constexpr int kForceLanes = 8;
+
+// Radix sort of (key, value) pairs, stable, 'bits' significant key bits.
+// Scratch from radix_sort_scratch_bytes().  Result lands in (k_out, v_out).
+size_t radix_sort_scratch_bytes(uint32_t n, int bits);
+int radix_sort_launches(uint32_t n, int bits);
+cudaError_t radix_sort_pairs(cudaStream_t st, const uint32_t* k_in, const uint32_t* v_in,
+                             uint32_t* k_out, uint32_t* v_out, uint32_t* k_tmp, uint32_t* v_tmp,
+                             uint32_t n, int bits, void* scratch);
+
+// Exclusive prefix sum of n uint32 values (in may equal out).
+size_t scan_scratch_bytes(uint64_t n);
+int scan_launches(uint64_t n);
+cudaError_t scan_exclusive(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n, void* scratch);
+
+uint32_t neighbor_hash_host(uint32_t j);
+
+}  // namespace pcg

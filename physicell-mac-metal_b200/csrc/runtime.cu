@@ -1,0 +1,867 @@
+// runtime.cu — engines behind the C ABI (see runtime.h).
+#include "runtime.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+
+namespace pcg {
+
+int fail(pcg_ctx* ctx, int code, const std::string& msg)
+{
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(pcg_ctx* ctx, cudaError_t e, const char* what)
+{
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    if (ctx) ctx->err = m;
+    return e == cudaErrorMemoryAllocation ? PCG_ERR_OOM : PCG_ERR_CUDA;
+}
+
+cudaError_t DevBuf::alloc(size_t b)
+{
+    release();
+    if (b == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+    }
+    bytes = b;
+    return cudaSuccess;
+}
+
+void DevBuf::release()
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+cudaError_t HostBuf::alloc(size_t b)
+{
+    release();
+    if (b == 0) return cudaSuccess;
+    cudaError_t e = cudaMallocHost(&p, b);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+    }
+    bytes = b;
+    return cudaSuccess;
+}
+
+void HostBuf::release()
+{
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+int key_bits_for(uint64_t n_keys)
+{
+    int b = 0;
+    while ((1ull << b) < n_keys) ++b;
+    return b;
+}
+
+// ------------------------------------------------------------------ tuner
+
+static std::mutex g_tune_mu;
+
+Tuner& Tuner::get()
+{
+    static Tuner t;
+    return t;
+}
+
+bool Tuner::lookup(const std::string& key, int* value)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = table_.find(key);
+    if (it == table_.end()) return false;
+    *value = it->second;
+    return true;
+}
+
+void Tuner::store(const std::string& key, int value)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    table_[key] = value;
+}
+
+// Flat JSON object of "key": int pairs.
+void Tuner::load(const std::string& path)
+{
+    std::ifstream f(path);
+    if (!f) return;
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string s = ss.str();
+    size_t i = 0;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    while ((i = s.find('"', i)) != std::string::npos) {
+        const size_t j = s.find('"', i + 1);
+        if (j == std::string::npos) break;
+        const std::string key = s.substr(i + 1, j - i - 1);
+        const size_t c = s.find(':', j);
+        if (c == std::string::npos) break;
+        table_[key] = std::atoi(s.c_str() + c + 1);
+        i = s.find_first_of(",}", c);
+        if (i == std::string::npos) break;
+    }
+}
+
+void Tuner::save(const std::string& path)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    std::ofstream f(path);
+    if (!f) return;
+    f << "{\n";
+    size_t k = 0;
+    for (auto& kv : table_) f << "  \"" << kv.first << "\": " << kv.second << (++k < table_.size() ? ",\n" : "\n");
+    f << "}\n";
+}
+
+// ------------------------------------------------------------------ diffusion
+
+static constexpr int kRowsMaxN = 768;   // longest x line staged in shared memory
+static constexpr int kColsMaxN = 512;   // longest y/z line staged in shared memory
+static constexpr size_t kSmemTarget = 110 * 1024;   // default: two CTAs per SM
+
+static uint32_t axis_n(const pcg_grid_params& g, int a) { return a == 0 ? g.nx : (a == 1 ? g.ny : g.nz); }
+static float axis_h(const pcg_grid_params& g, int a) { return a == 0 ? g.dx : (a == 1 ? g.dy : g.dz); }
+
+uint32_t Diffusion::rule_of(size_t i, uint32_t s, int axis) const
+{
+    size_t k = 0;
+    for (size_t q = 0; q < i; ++q) k += inst[q].subs.size() * 3;
+    return rule_index_[k + s * 3 + axis];
+}
+
+int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
+{
+    ctx = c;
+    inst = std::move(instances);
+    dens_elems = 0;
+    total_vox = total_vox_sub = 0;
+    h_rules_.clear();
+    h_tab_.clear();
+    rule_index_.clear();
+    std::vector<FaceJob> fj;
+    for (size_t i = 0; i < inst.size(); ++i) {
+        DiffInstance& d = inst[i];
+        const pcg_grid_params& g = d.g;
+        if (g.nx == 0 || g.ny == 0 || g.nz == 0) return fail(ctx, PCG_ERR_INVALID, "grid with a zero dimension");
+        if (d.subs.size() != g.n_substrates) return fail(ctx, PCG_ERR_INVALID, "substrate count mismatch");
+        const uint64_t nv = d.nvox();
+        if (nv > 0xFFFFFFFFull) return fail(ctx, PCG_ERR_INVALID, "grid larger than 2^32 voxels");
+        d.pitch = (nv + 31) / 32 * 32;
+        d.dens_off = dens_elems;
+        d.vox_base = static_cast<uint32_t>(total_vox);
+        dens_elems += d.pitch * g.n_substrates;
+        total_vox += nv;
+        total_vox_sub += nv * g.n_substrates;
+        if (total_vox > 0xFFFFFFF0ull) return fail(ctx, PCG_ERR_INVALID, "more than 2^32 voxels in one batch");
+        const int nd = d.ndim();
+        for (uint32_t s = 0; s < g.n_substrates; ++s) {
+            const pcg_substrate_params& sp = d.subs[s];
+            for (int a = 0; a < 3; ++a) {
+                if (a == 2 && nd < 3) {
+                    rule_index_.push_back(0xFFFFFFFFu);
+                    continue;
+                }
+                const uint32_t n = axis_n(g, a);
+                const double h = axis_h(g, a);
+                // D dt / h^2 and the split decay, in FP64 from the FP32 parameters
+                // (microenvironment.mm:171-177; decay lambda dt / d per sweep)
+                const double cc = static_cast<double>(sp.diffusion_coefficient) * static_cast<double>(g.dt) / (h * h);
+                const double hd = static_cast<double>(sp.decay_rate) * static_cast<double>(g.dt) / nd;
+                const bool dir = sp.dirichlet_enabled != 0;
+                const double T = sp.target_value;
+                LineRule r{};
+                r.tab = static_cast<uint32_t>(h_tab_.size());
+                r.n = n;
+                r.c = static_cast<float>(cc);
+                r.T = sp.target_value;
+                r.dir = dir ? 1u : 0u;
+                r.inst = static_cast<uint32_t>(i);
+                h_tab_.resize(h_tab_.size() + std::max<uint32_t>(n, 2), make_float2(0.f, 0.f));
+                float2* tb = h_tab_.data() + r.tab;
+                const double b_int = 1.0 + 2.0 * cc + hd, b_bnd = 1.0 + cc + hd;
+                if (n == 3) {
+                    tb[1] = make_float2(0.f, static_cast<float>(1.0 / b_int));
+                    r.fold = dir ? static_cast<float>(2.0 * cc * T) : 0.f;
+                } else if (n >= 4) {
+                    double cp = -cc / b_bnd;
+                    tb[1] = make_float2(static_cast<float>(cp), static_cast<float>(1.0 / b_bnd));
+                    for (uint32_t m = 2; m + 2 < n; ++m) {
+                        const double den = b_int + cc * cp;
+                        cp = -cc / den;
+                        tb[m] = make_float2(static_cast<float>(cp), static_cast<float>(1.0 / den));
+                    }
+                    const double den = b_bnd + cc * cp;
+                    tb[n - 2] = make_float2(static_cast<float>(-cc / den), static_cast<float>(1.0 / den));
+                    r.fold = dir ? static_cast<float>(cc * T) : 0.f;
+                }
+                rule_index_.push_back(static_cast<uint32_t>(h_rules_.size()));
+                h_rules_.push_back(r);
+            }
+            if (sp.dirichlet_enabled) {
+                FaceJob f{};
+                f.base = d.dens_off + s * d.pitch;
+                f.nx = g.nx;
+                f.ny = g.ny;
+                f.nz = g.nz;
+                f.T = sp.target_value;
+                fj.push_back(f);
+            }
+        }
+    }
+    PCG_CU(ctx, dens.alloc(std::max<uint64_t>(dens_elems, 32) * sizeof(float)));
+    PCG_CU(ctx, cudaMemsetAsync(dens.p, 0, dens.bytes, ctx->stream));
+    PCG_CU(ctx, rules.alloc(std::max<size_t>(h_rules_.size(), 1) * sizeof(LineRule)));
+    PCG_CU(ctx, tab.alloc(std::max<size_t>(h_tab_.size(), 1) * sizeof(float2)));
+    if (!h_rules_.empty())
+        PCG_CU(ctx, cudaMemcpy(rules.p, h_rules_.data(), h_rules_.size() * sizeof(LineRule), cudaMemcpyHostToDevice));
+    if (!h_tab_.empty())
+        PCG_CU(ctx, cudaMemcpy(tab.p, h_tab_.data(), h_tab_.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    n_faces = static_cast<uint32_t>(fj.size());
+    PCG_CU(ctx, faces.alloc(std::max<size_t>(fj.size(), 1) * sizeof(FaceJob)));
+    if (!fj.empty()) PCG_CU(ctx, cudaMemcpy(faces.p, fj.data(), fj.size() * sizeof(FaceJob), cudaMemcpyHostToDevice));
+    for (int a = 0; a < 3; ++a) {
+        PCG_TRY(build_axis(a, 128));
+        PCG_TRY(default_configs(a));
+    }
+    return PCG_OK;
+}
+
+// Tile lists of one axis.  rows_lines = lines per row tile (x axis).
+int Diffusion::build_axis(int axis, int rows_lines)
+{
+    std::vector<SweepTile> smem_t, glob_t;
+    int smem_nmax = 0, glob_nmax = 0;
+    uint64_t smem_lines = 0, glob_lines = 0;
+    const int kind_smem = axis == 0 ? 0 : 1;
+    const int maxn = axis == 0 ? kRowsMaxN : kColsMaxN;
+    for (size_t i = 0; i < inst.size(); ++i) {
+        const DiffInstance& d = inst[i];
+        const pcg_grid_params& g = d.g;
+        const int nd = d.ndim();
+        if (axis == 2 && nd < 3) continue;
+        const uint32_t n = axis_n(g, axis);
+        const bool use_smem = static_cast<int>(n) <= maxn;
+        auto& out = use_smem ? smem_t : glob_t;
+        int& nmax = use_smem ? smem_nmax : glob_nmax;
+        uint64_t& nl = use_smem ? smem_lines : glob_lines;
+        nmax = std::max<int>(nmax, static_cast<int>(n));
+        const bool final_axis = axis == nd - 1;
+        for (uint32_t s = 0; s < g.n_substrates; ++s) {
+            const uint32_t rule = rule_of(i, s, axis);
+            const bool dir = d.subs[s].dirichlet_enabled != 0;
+            const uint64_t sbase = d.dens_off + s * d.pitch;
+            if (axis == 0) {
+                const uint64_t lines = static_cast<uint64_t>(g.ny) * g.nz;
+                const uint32_t L = use_smem ? static_cast<uint32_t>(rows_lines) : 32u;
+                for (uint64_t l0 = 0; l0 < lines; l0 += L) {
+                    SweepTile t{};
+                    t.base = sbase + l0 * g.nx;
+                    t.rule = rule;
+                    t.count = static_cast<uint32_t>(std::min<uint64_t>(L, lines - l0));
+                    t.rs = 1;
+                    t.nx = g.nx;
+                    out.push_back(t);
+                }
+                nl += lines;
+            } else {
+                // y: families over (i, k), stride nx; z: families over (i, j), stride nx*ny
+                const uint32_t outer = axis == 1 ? g.nz : g.ny;
+                const uint64_t ostride = axis == 1 ? static_cast<uint64_t>(g.nx) * g.ny : g.nx;
+                const uint32_t rs = axis == 1 ? g.nx : g.nx * g.ny;
+                for (uint32_t o = 0; o < outer; ++o) {
+                    for (uint32_t i0 = 0; i0 < g.nx; i0 += 32) {
+                        SweepTile t{};
+                        t.base = sbase + o * ostride + i0;
+                        t.rule = rule;
+                        t.count = std::min<uint32_t>(32, g.nx - i0);
+                        t.rs = rs;
+                        t.i0 = i0;
+                        t.nx = g.nx;
+                        if (final_axis && dir) {
+                            t.face = TILE_FACE;
+                            if (axis == 2 && (o == 0 || o + 1 == g.ny)) t.face |= TILE_FACE_ALL;
+                        }
+                        out.push_back(t);
+                    }
+                }
+                nl += static_cast<uint64_t>(g.nx) * outer;
+            }
+        }
+    }
+    // larger lines first so the persistent loop ends evenly
+    auto by_n = [&](const SweepTile& a, const SweepTile& b) { return h_rules_[a.rule].n > h_rules_[b.rule].n; };
+    std::stable_sort(smem_t.begin(), smem_t.end(), by_n);
+    std::stable_sort(glob_t.begin(), glob_t.end(), by_n);
+    std::vector<SweepList>& ls = lists[axis];
+    // keep existing launch configs when rebuilding
+    RowsCfg keep_rc{rows_lines, 1};
+    ColsCfg keep_cc{4, 1};
+    for (auto& l : ls) {
+        if (l.kind == 0) keep_rc = l.rc;
+        if (l.kind == 1) keep_cc = l.cc;
+    }
+    ls.clear();
+    ls.resize(2);
+    ls[0].kind = kind_smem;
+    ls[0].nmax = smem_nmax;
+    ls[0].n = static_cast<uint32_t>(smem_t.size());
+    ls[0].lines = smem_lines;
+    ls[0].rc = keep_rc;
+    ls[0].rc.lines = rows_lines;
+    ls[0].cc = keep_cc;
+    ls[1].kind = 2;
+    ls[1].nmax = glob_nmax;
+    ls[1].n = static_cast<uint32_t>(glob_t.size());
+    ls[1].lines = glob_lines;
+    for (int q = 0; q < 2; ++q) {
+        const auto& v = q == 0 ? smem_t : glob_t;
+        PCG_CU(ctx, ls[q].tiles.alloc(std::max<size_t>(v.size(), 1) * sizeof(SweepTile)));
+        if (!v.empty())
+            PCG_CU(ctx, cudaMemcpy(ls[q].tiles.p, v.data(), v.size() * sizeof(SweepTile), cudaMemcpyHostToDevice));
+    }
+    return PCG_OK;
+}
+
+int Diffusion::default_configs(int axis)
+{
+    for (auto& l : lists[axis]) {
+        if (l.n == 0) continue;
+        if (l.kind == 0) {
+            int occ = sweep_rows_occupancy(l.rc.lines, l.nmax);
+            if (occ <= 0) return fail(ctx, PCG_ERR_INVALID, "x sweep tile does not fit shared memory");
+            l.rc.grid = static_cast<int>(std::min<uint64_t>(l.n, static_cast<uint64_t>(occ) * ctx->sms));
+        } else if (l.kind == 1) {
+            int w = l.cc.warps;
+            while (w > 1 && sweep_cols_smem(w, l.nmax) > kSmemTarget) w >>= 1;
+            l.cc.warps = w;
+            int occ = sweep_cols_occupancy(w, l.nmax);
+            if (occ <= 0) return fail(ctx, PCG_ERR_INVALID, "column sweep tile does not fit shared memory");
+            const uint64_t ctas = (l.n + w - 1) / w;
+            l.cc.grid = static_cast<int>(std::min<uint64_t>(ctas, static_cast<uint64_t>(occ) * ctx->sms));
+        } else {
+            const uint64_t ctas = (static_cast<uint64_t>(l.n) * 32 + 127) / 128;
+            l.ggrid = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(ctas, 1), static_cast<uint64_t>(ctx->sms) * 16));
+        }
+    }
+    return PCG_OK;
+}
+
+int Diffusion::launch_list(const SweepList& l, bool fuse, const uint8_t* mask)
+{
+    if (l.n == 0) return PCG_OK;
+    float* d = dens.as<float>();
+    const SweepTile* t = l.tiles.as<SweepTile>();
+    const LineRule* r = rules.as<LineRule>();
+    const float2* tb = tab.as<float2>();
+    cudaError_t e;
+    if (l.kind == 0) e = launch_sweep_rows(ctx->stream, d, t, l.n, r, tb, l.nmax, mask, l.rc);
+    else if (l.kind == 1) e = launch_sweep_cols(ctx->stream, d, t, l.n, r, tb, l.nmax, fuse ? 1 : 0, mask, l.cc);
+    else e = launch_sweep_global(ctx->stream, d, t, l.n, r, tb, fuse ? 1 : 0, mask, l.ggrid);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep launch");
+    ctx->launches++;
+    return PCG_OK;
+}
+
+int Diffusion::sweep(int axis, bool fuse, const uint8_t* mask)
+{
+    for (const auto& l : lists[axis]) PCG_TRY(launch_list(l, fuse, mask));
+    return PCG_OK;
+}
+
+int Diffusion::sweeps(bool fuse, const uint8_t* mask)
+{
+    for (int a = 0; a < 3; ++a) PCG_TRY(sweep(a, fuse, mask));
+    return PCG_OK;
+}
+
+int Diffusion::launches_per_step(bool) const
+{
+    int k = 0;
+    for (int a = 0; a < 3; ++a)
+        for (const auto& l : lists[a]) k += l.n > 0 ? 1 : 0;
+    return k;
+}
+
+int Diffusion::dirichlet()
+{
+    if (n_faces == 0) return PCG_OK;
+    cudaError_t e = launch_dirichlet(ctx->stream, dens.as<float>(), faces.as<FaceJob>(), n_faces);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "dirichlet launch");
+    ctx->launches++;
+    return PCG_OK;
+}
+
+int Diffusion::gradients(float* gx, float* gy, float* gz)
+{
+    std::vector<GradJob> jobs;
+    uint64_t out = 0, maxv = 0;
+    for (const auto& d : inst) {
+        for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
+            GradJob j{};
+            j.base = d.dens_off + s * d.pitch;
+            j.out_base = out;
+            j.nx = d.g.nx;
+            j.ny = d.g.ny;
+            j.nz = d.g.nz;
+            j.inv_dx = 1.0f / d.g.dx;
+            j.inv_dy = 1.0f / d.g.dy;
+            j.inv_dz = 1.0f / d.g.dz;
+            jobs.push_back(j);
+            out += d.nvox();
+            maxv = std::max<uint64_t>(maxv, d.nvox());
+        }
+    }
+    if (jobs.empty()) return PCG_OK;
+    PCG_CU(ctx, grad_jobs.alloc(jobs.size() * sizeof(GradJob)));
+    PCG_CU(ctx, cudaMemcpyAsync(grad_jobs.p, jobs.data(), jobs.size() * sizeof(GradJob), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    cudaError_t e = launch_gradients(ctx->stream, dens.as<float>(), gx, gy, gz, grad_jobs.as<GradJob>(),
+                                     static_cast<uint32_t>(jobs.size()), maxv);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "gradients launch");
+    ctx->launches++;
+    // the job table must outlive the kernel
+    PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    return PCG_OK;
+}
+
+int Diffusion::upload(uint32_t i, const float* host, bool async_pinned)
+{
+    const DiffInstance& d = inst[i];
+    const size_t nv = d.nvox();
+    for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
+        float* dst = dens.as<float>() + d.dens_off + s * d.pitch;
+        PCG_CU(ctx, cudaMemcpyAsync(dst, host + s * nv, nv * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    if (!async_pinned) PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    return PCG_OK;
+}
+
+int Diffusion::download(uint32_t i, float* host, bool async_pinned)
+{
+    const DiffInstance& d = inst[i];
+    const size_t nv = d.nvox();
+    for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
+        const float* src = dens.as<float>() + d.dens_off + s * d.pitch;
+        PCG_CU(ctx, cudaMemcpyAsync(host + s * nv, src, nv * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (!async_pinned) PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    return PCG_OK;
+}
+
+int Diffusion::fill(uint32_t i, const float* values)
+{
+    const DiffInstance& d = inst[i];
+    std::vector<float> tmp(d.nvox());
+    for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
+        std::fill(tmp.begin(), tmp.end(), values[s]);
+        float* dst = dens.as<float>() + d.dens_off + s * d.pitch;
+        PCG_CU(ctx, cudaMemcpy(dst, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return PCG_OK;
+}
+
+uint64_t Diffusion::device_bytes() const
+{
+    uint64_t b = dens.bytes + rules.bytes + tab.bytes + faces.bytes;
+    for (int a = 0; a < 3; ++a)
+        for (const auto& l : lists[a]) b += l.tiles.bytes;
+    return b;
+}
+
+std::string Diffusion::describe() const
+{
+    std::ostringstream o;
+    const char* ax = "xyz";
+    for (int a = 0; a < 3; ++a)
+        for (const auto& l : lists[a]) {
+            if (l.n == 0) continue;
+            o << ax[a] << ":";
+            if (l.kind == 0) o << "rows(L=" << l.rc.lines << ",grid=" << l.rc.grid;
+            else if (l.kind == 1) o << "cols(warps=" << l.cc.warps << ",grid=" << l.cc.grid;
+            else o << "global(grid=" << l.ggrid;
+            o << ",tiles=" << l.n << ",nmax=" << l.nmax << ") ";
+        }
+    return o.str();
+}
+
+// Measure candidate launch shapes on the real data; the density is saved
+// before and restored after, so tuning leaves the state untouched.
+int Diffusion::tune()
+{
+    if (dens_elems == 0) return PCG_OK;
+    DevBuf backup;
+    if (backup.alloc(dens.bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return PCG_OK;   // not enough memory to tune safely: keep the defaults
+    }
+    PCG_CU(ctx, cudaMemcpyAsync(backup.p, dens.p, dens.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    cudaEvent_t e0, e1;
+    PCG_CU(ctx, cudaEventCreate(&e0));
+    PCG_CU(ctx, cudaEventCreate(&e1));
+    auto time_list = [&](SweepList& l, float* ms) -> int {
+        PCG_TRY(launch_list(l, false, nullptr));   // warm
+        PCG_CU(ctx, cudaEventRecord(e0, ctx->stream));
+        for (int r = 0; r < 3; ++r) PCG_TRY(launch_list(l, false, nullptr));
+        PCG_CU(ctx, cudaEventRecord(e1, ctx->stream));
+        PCG_CU(ctx, cudaEventSynchronize(e1));
+        PCG_CU(ctx, cudaEventElapsedTime(ms, e0, e1));
+        return PCG_OK;
+    };
+    auto bucket = [](uint64_t v) {
+        int b = 0;
+        while ((1ull << (b + 1)) <= v) ++b;
+        return b;
+    };
+    int rc = PCG_OK;
+    for (int a = 0; a < 3 && rc == PCG_OK; ++a) {
+        // x axis: lines per tile (changes the tile list)
+        if (lists[a].size() && lists[a][0].n > 0 && lists[a][0].kind == 0) {
+            const std::string key = "rows:n" + std::to_string(lists[a][0].nmax) + ":l" +
+                                    std::to_string(bucket(lists[a][0].lines));
+            int best = 0;
+            if (!Tuner::get().lookup(key, &best)) {
+                float best_ms = 1e30f;
+                for (int L : {32, 64, 128, 256}) {
+                    if (sweep_rows_smem(L, lists[a][0].nmax) > static_cast<size_t>(ctx->smem_optin)) continue;
+                    rc = build_axis(a, L);
+                    if (rc == PCG_OK) rc = default_configs(a);
+                    if (rc != PCG_OK) break;
+                    float ms = 0;
+                    rc = time_list(lists[a][0], &ms);
+                    if (rc != PCG_OK) break;
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = L;
+                    }
+                }
+                if (rc != PCG_OK) break;
+                Tuner::get().store(key, best);
+            }
+            rc = build_axis(a, best);
+            if (rc == PCG_OK) rc = default_configs(a);
+        }
+        // y/z axes: warps (column tiles) per CTA
+        if (rc == PCG_OK && lists[a].size() && lists[a][0].n > 0 && lists[a][0].kind == 1) {
+            SweepList& l = lists[a][0];
+            const std::string key = "cols:n" + std::to_string(l.nmax) + ":l" + std::to_string(bucket(l.lines));
+            int best = 0;
+            if (!Tuner::get().lookup(key, &best)) {
+                float best_ms = 1e30f;
+                for (int w : {1, 2, 4, 8}) {
+                    if (sweep_cols_smem(w, l.nmax) > static_cast<size_t>(ctx->smem_optin)) continue;
+                    const int occ = sweep_cols_occupancy(w, l.nmax);
+                    if (occ <= 0) continue;
+                    l.cc.warps = w;
+                    l.cc.grid = static_cast<int>(std::min<uint64_t>((l.n + w - 1) / w, static_cast<uint64_t>(occ) * ctx->sms));
+                    float ms = 0;
+                    rc = time_list(l, &ms);
+                    if (rc != PCG_OK) break;
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = w;
+                    }
+                }
+                if (rc != PCG_OK) break;
+                Tuner::get().store(key, best);
+            }
+            const int occ = sweep_cols_occupancy(best, l.nmax);
+            l.cc.warps = best;
+            l.cc.grid = static_cast<int>(std::min<uint64_t>((l.n + best - 1) / best, static_cast<uint64_t>(std::max(occ, 1)) * ctx->sms));
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaError_t ce = cudaMemcpyAsync(dens.p, backup.p, dens.bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+    if (rc != PCG_OK) return rc;
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "tune restore");
+    return PCG_OK;
+}
+
+// ------------------------------------------------------------------ cells
+
+void fill_diff_inst(CellInst& ci, const DiffInstance& d)
+{
+    ci.nx = d.g.nx;
+    ci.ny = d.g.ny;
+    ci.nz = d.g.nz;
+    ci.S = d.g.n_substrates;
+    ci.dx = d.g.dx;
+    ci.dy = d.g.dy;
+    ci.dz = d.g.dz;
+    ci.x_min = d.g.x_min;
+    ci.y_min = d.g.y_min;
+    ci.z_min = d.g.z_min;
+    ci.dens_off = d.dens_off;
+    ci.sub_pitch = d.pitch;
+    ci.vox_base = d.vox_base;
+}
+
+void fill_mech_inst(CellInst& ci, const pcg_mechanics_params& m, float x_min, float y_min, float z_min)
+{
+    ci.mnx = m.mech_grid_nx;
+    ci.mny = m.mech_grid_ny;
+    ci.mnz = m.mech_grid_nz;
+    ci.vs = m.mechanics_voxel_size;
+    ci.maxd = m.max_interaction_distance;
+    ci.mx_min = x_min;
+    ci.my_min = y_min;
+    ci.mz_min = z_min;
+    // integrate.metal:279-281 with the mechanics GridParams (cell_mechanics.mm:147-156), FP32
+    ci.box_hi_x = x_min + static_cast<float>(m.mech_grid_nx) * m.mechanics_voxel_size;
+    ci.box_hi_y = y_min + static_cast<float>(m.mech_grid_ny) * m.mechanics_voxel_size;
+    ci.box_hi_z = z_min + static_cast<float>(m.mech_grid_nz) * m.mechanics_voxel_size;
+    ci.dt_mech = m.dt;
+}
+
+int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_instances)
+{
+    ctx = c;
+    max_cells = std::max<uint32_t>(maxc, 1);
+    n = 0;
+    n_rate = 0;
+    h_inst.assign(std::max<uint32_t>(n_instances, 1), CellInst{});
+    PCG_CU(ctx, inst.alloc(h_inst.size() * sizeof(CellInst)));
+    PCG_CU(ctx, soa.alloc(static_cast<size_t>(NUM_FIELDS) * max_cells * sizeof(float)));
+    PCG_CU(ctx, cudaMemset(soa.p, 0, soa.bytes));
+    PCG_CU(ctx, cell_inst.alloc(static_cast<size_t>(max_cells) * sizeof(uint32_t)));
+    PCG_CU(ctx, cudaMemset(cell_inst.p, 0, cell_inst.bytes));
+    const size_t rc = std::max<uint32_t>(rate_capacity, 1);
+    PCG_CU(ctx, rates.alloc(4 * rc * sizeof(double)));
+    PCG_CU(ctx, cudaMemset(rates.p, 0, rates.bytes));
+    PCG_CU(ctx, coef.alloc(3 * rc * sizeof(double)));
+    PCG_CU(ctx, active.alloc(max_cells));
+    for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp})
+        PCG_CU(ctx, b->alloc(static_cast<size_t>(max_cells) * sizeof(uint32_t)));
+    PCG_CU(ctx, sort_scr.alloc(radix_sort_scratch_bytes(max_cells, 32)));
+    inst_dirty = coef_dirty = order_dirty = true;
+    return PCG_OK;
+}
+
+int Cells::sync_inst()
+{
+    if (!inst_dirty) return PCG_OK;
+    PCG_CU(ctx, cudaMemcpyAsync(inst.p, h_inst.data(), h_inst.size() * sizeof(CellInst), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    inst_dirty = false;
+    return PCG_OK;
+}
+
+int Cells::upload_soa(uint32_t off, uint32_t count, const float* host, uint32_t soa_max, uint32_t first,
+                      uint32_t nf)
+{
+    if (count == 0 || nf == 0) return PCG_OK;
+    float* dst = soa.as<float>() + static_cast<size_t>(first) * max_cells + off;
+    PCG_CU(ctx, cudaMemcpy2DAsync(dst, static_cast<size_t>(max_cells) * sizeof(float),
+                                  host + static_cast<size_t>(first) * soa_max, static_cast<size_t>(soa_max) * sizeof(float),
+                                  static_cast<size_t>(count) * sizeof(float), nf, cudaMemcpyHostToDevice, ctx->stream));
+    const uint32_t last = first + nf;
+    if (first <= F_TOTAL_VOL && F_TOTAL_VOL < last) coef_dirty = true;
+    if (first <= F_VOXEL_IDX && F_VOXEL_IDX < last) order_dirty = true;
+    return PCG_OK;
+}
+
+int Cells::download_soa(uint32_t off, uint32_t count, float* host, uint32_t soa_max, uint32_t first, uint32_t nf)
+{
+    if (count == 0 || nf == 0) return PCG_OK;
+    const float* src = soa.as<float>() + static_cast<size_t>(first) * max_cells + off;
+    PCG_CU(ctx, cudaMemcpy2DAsync(host + static_cast<size_t>(first) * soa_max, static_cast<size_t>(soa_max) * sizeof(float),
+                                  src, static_cast<size_t>(max_cells) * sizeof(float),
+                                  static_cast<size_t>(count) * sizeof(float), nf, cudaMemcpyDeviceToHost, ctx->stream));
+    return PCG_OK;
+}
+
+int Cells::set_rates(uint32_t off, uint32_t count, const double* sec, const double* upt, const double* sat,
+                     const double* ne)
+{
+    const size_t cap = rates.bytes / (4 * sizeof(double));
+    if (static_cast<size_t>(off) + count > cap) return fail(ctx, PCG_ERR_INVALID, "rate arrays exceed capacity");
+    const double* src[4] = {sec, upt, sat, ne};
+    for (int q = 0; q < 4; ++q) {
+        double* dst = rates.as<double>() + q * cap + off;
+        if (src[q])
+            PCG_CU(ctx, cudaMemcpyAsync(dst, src[q], static_cast<size_t>(count) * sizeof(double), cudaMemcpyHostToDevice,
+                                        ctx->stream));
+        else
+            PCG_CU(ctx, cudaMemsetAsync(dst, 0, static_cast<size_t>(count) * sizeof(double), ctx->stream));
+    }
+    PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    coef_dirty = true;
+    return PCG_OK;
+}
+
+int Cells::set_active(uint32_t off, uint32_t count, const uint8_t* act)
+{
+    if (act) {
+        PCG_CU(ctx, cudaMemcpy(active.as<uint8_t>() + off, act, count, cudaMemcpyHostToDevice));
+        has_active = true;
+    } else {
+        PCG_CU(ctx, cudaMemset(active.as<uint8_t>() + off, 1, count));
+    }
+    order_dirty = true;
+    return PCG_OK;
+}
+
+int Cells::set_cell_instances(const std::vector<uint32_t>& counts)
+{
+    std::vector<uint32_t> ci;
+    for (size_t i = 0; i < counts.size(); ++i) ci.insert(ci.end(), counts[i], static_cast<uint32_t>(i));
+    if (ci.size() > max_cells) return fail(ctx, PCG_ERR_INVALID, "more cells than capacity");
+    if (!ci.empty()) PCG_CU(ctx, cudaMemcpy(cell_inst.p, ci.data(), ci.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    return PCG_OK;
+}
+
+int Cells::build_order(uint64_t total_vox)
+{
+    PCG_TRY(sync_inst());
+    invalid_key = static_cast<uint32_t>(total_vox);
+    key_bits = key_bits_for(total_vox + 1);
+    cudaError_t e = launch_sec_keys(ctx->stream, soa.as<float>(), max_cells, n, cell_inst.as<uint32_t>(),
+                                    inst.as<CellInst>(), has_active ? active.as<uint8_t>() : nullptr, invalid_key,
+                                    keys.as<uint32_t>(), vals.as<uint32_t>());
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion keys");
+    e = radix_sort_pairs(ctx->stream, keys.as<uint32_t>(), vals.as<uint32_t>(), skeys.as<uint32_t>(),
+                         sorder.as<uint32_t>(), ktmp.as<uint32_t>(), vtmp.as<uint32_t>(), n, key_bits, sort_scr.p);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion sort");
+    ctx->launches += 1 + radix_sort_launches(n, key_bits);
+    order_dirty = false;
+    return PCG_OK;
+}
+
+int Cells::prepare_secretion(double dt, uint64_t total_vox)
+{
+    PCG_TRY(sync_inst());
+    if (coef_dirty || coef_dt != dt) {
+        const uint32_t cap = static_cast<uint32_t>(rates.bytes / (4 * sizeof(double)));
+        cudaError_t e = launch_sec_prepare(ctx->stream, soa.as<float>(), max_cells, n, cell_inst.as<uint32_t>(),
+                                           inst.as<CellInst>(), rates.as<double>(), cap, dt, coef.as<double>());
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion prepare");
+        ctx->launches++;
+        coef_dirty = false;
+        coef_dt = dt;
+    }
+    if (order_dirty || invalid_key != static_cast<uint32_t>(total_vox)) PCG_TRY(build_order(total_vox));
+    return PCG_OK;
+}
+
+int Cells::secrete(Diffusion& d, const uint8_t* mask)
+{
+    cudaError_t e = launch_secrete(ctx->stream, d.dens.as<float>(), skeys.as<uint32_t>(), sorder.as<uint32_t>(), n,
+                                   cell_inst.as<uint32_t>(), inst.as<CellInst>(), coef.as<double>(), invalid_key, mask);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion launch");
+    ctx->launches++;
+    return PCG_OK;
+}
+
+uint64_t Cells::device_bytes() const
+{
+    return inst.bytes + soa.bytes + cell_inst.bytes + rates.bytes + coef.bytes + active.bytes + keys.bytes + vals.bytes +
+           skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes;
+}
+
+// ------------------------------------------------------------------ mechanics
+
+int Mechanics::create(pcg_ctx* c, uint32_t tmv, uint32_t maxc)
+{
+    ctx = c;
+    total_mvox = tmv;
+    cap = std::max<uint32_t>(maxc, 1);
+    key_bits = key_bits_for(std::max<uint64_t>(tmv, 1));
+    for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp, &dcnt, &dhash})
+        PCG_CU(ctx, b->alloc(static_cast<size_t>(cap) * sizeof(uint32_t)));
+    PCG_CU(ctx, sort_scr.alloc(radix_sort_scratch_bytes(cap, key_bits)));
+    PCG_CU(ctx, counts.alloc((static_cast<size_t>(tmv) + 1) * sizeof(uint32_t)));
+    PCG_CU(ctx, start.alloc((static_cast<size_t>(tmv) + 1) * sizeof(uint32_t)));
+    PCG_CU(ctx, cudaMemset(start.p, 0, start.bytes));
+    PCG_CU(ctx, scan_scr.alloc(scan_scratch_bytes(static_cast<uint64_t>(tmv) + 1)));
+    PCG_CU(ctx, spos.alloc(static_cast<size_t>(cap) * sizeof(float4)));
+    PCG_CU(ctx, sprm.alloc(static_cast<size_t>(cap) * sizeof(float4)));
+    return PCG_OK;
+}
+
+int Mechanics::launches_forces(uint32_t n) const
+{
+    return 1 /*memset*/ + 1 /*bin*/ + radix_sort_launches(n, key_bits) + scan_launches(total_mvox + 1ull) + 1 /*gather*/ +
+           1 /*forces*/;
+}
+
+// computeForces: bin -> stable radix sort -> cell-start table -> sorted SoA -> forces
+int Mechanics::forces(Cells& c, const uint8_t* mask)
+{
+    PCG_TRY(binsort(c));
+    return force_pass(c, mask);
+}
+
+int Mechanics::binsort(Cells& c)
+{
+    if (c.n == 0) return PCG_OK;
+    if (c.n > cap) return fail(ctx, PCG_ERR_INVALID, "more cells than the mechanics capacity");
+    PCG_TRY(c.sync_inst());
+    cudaStream_t st = ctx->stream;
+    PCG_CU(ctx, cudaMemsetAsync(counts.p, 0, counts.bytes, st));
+    cudaError_t e = launch_mech_bin(st, c.soa.as<float>(), c.max_cells, c.n, c.cell_inst.as<uint32_t>(),
+                                    c.inst.as<CellInst>(), keys.as<uint32_t>(), vals.as<uint32_t>(), counts.as<uint32_t>());
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "bin launch");
+    e = radix_sort_pairs(st, keys.as<uint32_t>(), vals.as<uint32_t>(), skeys.as<uint32_t>(), sorder.as<uint32_t>(),
+                         ktmp.as<uint32_t>(), vtmp.as<uint32_t>(), c.n, key_bits, sort_scr.p);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "radix sort");
+    e = scan_exclusive(st, counts.as<uint32_t>(), start.as<uint32_t>(), static_cast<uint64_t>(total_mvox) + 1, scan_scr.p);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "start-table scan");
+    e = launch_mech_gather(st, c.soa.as<float>(), c.max_cells, sorder.as<uint32_t>(), c.n, spos.as<float4>(),
+                           sprm.as<float4>());
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "gather launch");
+    ctx->launches += launches_forces(c.n) - 2;   // the memset is not a kernel; forces counted below
+    return PCG_OK;
+}
+
+int Mechanics::force_pass(Cells& c, const uint8_t* mask)
+{
+    if (c.n == 0) return PCG_OK;
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = launch_mech_forces(st, spos.as<float4>(), sprm.as<float4>(), skeys.as<uint32_t>(), sorder.as<uint32_t>(),
+                           start.as<uint32_t>(), c.n, c.cell_inst.as<uint32_t>(), c.inst.as<CellInst>(), c.soa.as<float>(),
+                           c.max_cells, diag ? dcnt.as<uint32_t>() : nullptr, diag ? dhash.as<uint32_t>() : nullptr,
+                           mask, block);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "forces launch");
+    ctx->launches++;
+    return PCG_OK;
+}
+
+int Mechanics::integrate(Cells& c, float dt_override, const uint8_t* mask)
+{
+    if (c.n == 0) return PCG_OK;
+    PCG_TRY(c.sync_inst());
+    cudaError_t e = launch_mech_integrate(ctx->stream, c.soa.as<float>(), c.max_cells, c.n, c.cell_inst.as<uint32_t>(),
+                                          c.inst.as<CellInst>(), dt_override, mask);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "integrate launch");
+    ctx->launches++;
+    bool refresh = false;
+    for (const auto& ci : c.h_inst) refresh = refresh || (ci.flags & INST_REFRESH_VOXELS);
+    if (refresh) c.order_dirty = true;
+    return PCG_OK;
+}
+
+uint64_t Mechanics::device_bytes() const
+{
+    return keys.bytes + vals.bytes + skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + counts.bytes +
+           start.bytes + scan_scr.bytes + spos.bytes + sprm.bytes + dcnt.bytes + dhash.bytes;
+}
+
+}  // namespace pcg

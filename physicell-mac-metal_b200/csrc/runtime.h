@@ -1,0 +1,219 @@
+// runtime.h — host runtime behind the C ABI: device buffers, the diffusion /
+// cell / mechanics engines shared by the single-simulation API, the batch
+// and the server, launch-shape selection and the autotuner.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "pcg.h"
+#include "pcg_kernels.cuh"
+
+struct pcg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    int sms = 0;
+    int smem_optin = 0;
+    uint64_t launches = 0;
+};
+
+namespace pcg {
+
+int fail(pcg_ctx* ctx, int code, const std::string& msg);
+int cuda_fail(pcg_ctx* ctx, cudaError_t e, const char* what);
+
+#define PCG_CU(ctx, call)                                                   \
+    do {                                                                    \
+        cudaError_t e_ = (call);                                            \
+        if (e_ != cudaSuccess) return ::pcg::cuda_fail((ctx), e_, #call);   \
+    } while (0)
+#define PCG_TRY(x)                    \
+    do {                              \
+        int r_ = (x);                 \
+        if (r_ != PCG_OK) return r_;  \
+    } while (0)
+
+// Device allocation owned by the library.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept
+    {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            o.p = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    cudaError_t alloc(size_t b);
+    void release();
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// Page-locked host allocation (staging for end-to-end copies).
+struct HostBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    HostBuf() = default;
+    HostBuf(const HostBuf&) = delete;
+    HostBuf& operator=(const HostBuf&) = delete;
+    ~HostBuf() { release(); }
+    cudaError_t alloc(size_t b);
+    void release();
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// ------------------------------------------------------------------ tuning
+
+// Launch-shape choices, cached by shape bucket (process-wide, optionally
+// persisted as JSON).
+class Tuner {
+public:
+    static Tuner& get();
+    bool lookup(const std::string& key, int* value);
+    void store(const std::string& key, int value);
+    void load(const std::string& path);
+    void save(const std::string& path);
+private:
+    std::map<std::string, int> table_;
+};
+
+// ------------------------------------------------------------------ diffusion
+
+struct DiffInstance {
+    pcg_grid_params g{};
+    std::vector<pcg_substrate_params> subs;
+    uint64_t dens_off = 0;
+    uint64_t pitch = 0;       // elements between substrates (multiple of 32)
+    uint32_t vox_base = 0;
+    uint64_t nvox() const { return static_cast<uint64_t>(g.nx) * g.ny * g.nz; }
+    int ndim() const { return g.nz > 1 ? 3 : 2; }
+};
+
+struct SweepList {
+    int kind = 0;              // 0 row tiles (SMEM), 1 column tiles (SMEM), 2 any length (global)
+    int nmax = 0;
+    uint32_t n = 0;
+    DevBuf tiles;
+    RowsCfg rc{128, 1};
+    ColsCfg cc{4, 1};
+    int ggrid = 1;
+    uint64_t lines = 0;        // lines covered (for tuning keys)
+};
+
+class Diffusion {
+public:
+    pcg_ctx* ctx = nullptr;
+    std::vector<DiffInstance> inst;
+    uint64_t dens_elems = 0;
+    uint64_t total_vox = 0;        // sum nx*ny*nz
+    uint64_t total_vox_sub = 0;    // sum nx*ny*nz*S
+    DevBuf dens, rules, tab, faces, grad_jobs;
+    uint32_t n_faces = 0;
+    std::vector<SweepList> lists[3];
+    std::string shapes;
+
+    // Lays out the density arena, builds the Thomas tables and the tile
+    // lists; 'tune' measures launch shapes on the data (density must be
+    // initialised first when tuning, see tune()).
+    int build(pcg_ctx* c, std::vector<DiffInstance> instances);
+    int tune();                                    // restore-safe: density is saved and put back
+    int sweep(int axis, bool fuse_faces, const uint8_t* mask);
+    int sweeps(bool fuse_faces, const uint8_t* mask);
+    int dirichlet();
+    int gradients(float* gx, float* gy, float* gz);   // device arrays of total_vox_sub floats, dense per instance
+    int upload(uint32_t i, const float* host, bool async_pinned = false);
+    int download(uint32_t i, float* host, bool async_pinned = false);
+    int fill(uint32_t i, const float* values);
+    int launches_per_step(bool three_d_only = false) const;
+    uint64_t device_bytes() const;
+    std::string describe() const;
+
+private:
+    int build_axis(int axis, int rows_lines);
+    int default_configs(int axis);
+    int launch_list(const SweepList& l, bool fuse_faces, const uint8_t* mask);
+    std::vector<LineRule> h_rules_;
+    std::vector<float2> h_tab_;
+    std::vector<uint32_t> rule_index_;   // (inst, s, axis) -> rule
+    uint32_t rule_of(size_t i, uint32_t s, int axis) const;
+};
+
+// ------------------------------------------------------------------ cells
+
+class Cells {
+public:
+    pcg_ctx* ctx = nullptr;
+    uint32_t max_cells = 0;
+    uint32_t n = 0;
+    uint32_t n_rate = 0;          // sum over instances of n_cells * S
+    std::vector<CellInst> h_inst;
+    DevBuf inst, soa, cell_inst, rates, coef, active;
+    bool has_active = false;
+    bool inst_dirty = true, coef_dirty = true, order_dirty = true;
+    double coef_dt = -1.0;
+    // secretion ordering
+    DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr;
+    uint32_t invalid_key = 0;
+    int key_bits = 0;
+
+    int create(pcg_ctx* c, uint32_t max_cells, uint32_t rate_capacity, uint32_t n_instances);
+    int sync_inst();
+    int upload_soa(uint32_t cell_off, uint32_t count, const float* soa, uint32_t soa_max, uint32_t first_field,
+                   uint32_t n_fields);
+    int download_soa(uint32_t cell_off, uint32_t count, float* soa, uint32_t soa_max, uint32_t first_field,
+                     uint32_t n_fields);
+    int set_rates(uint32_t rate_off, uint32_t count, const double* sec, const double* upt, const double* sat,
+                  const double* ne);
+    int set_active(uint32_t cell_off, uint32_t count, const uint8_t* act);
+    int set_cell_instances(const std::vector<uint32_t>& per_instance_counts);
+    // Recompute secretion constants / ordering when stale.
+    int prepare_secretion(double dt, uint64_t total_vox);
+    int build_order(uint64_t total_vox);
+    int secrete(Diffusion& d, const uint8_t* mask);
+    uint64_t device_bytes() const;
+};
+
+// ------------------------------------------------------------------ mechanics
+
+class Mechanics {
+public:
+    pcg_ctx* ctx = nullptr;
+    uint32_t total_mvox = 0;
+    uint32_t cap = 0;
+    int key_bits = 0;
+    int block = 256;
+    bool diag = false;
+    DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr, counts, start, scan_scr, spos, sprm, dcnt, dhash;
+
+    int create(pcg_ctx* c, uint32_t total_mvox, uint32_t max_cells);
+    int forces(Cells& c, const uint8_t* mask);       // binsort + force_pass
+    int binsort(Cells& c);                           // bin, stable radix sort, cell-start table, sorted SoA
+    int force_pass(Cells& c, const uint8_t* mask);
+    int integrate(Cells& c, float dt_override, const uint8_t* mask);
+    int launches_forces(uint32_t n) const;
+    uint64_t device_bytes() const;
+};
+
+// Mechanics grid of the reference (cell_mechanics.mm:115-130).
+void fill_mech_inst(CellInst& ci, const pcg_mechanics_params& m, float x_min, float y_min, float z_min);
+void fill_diff_inst(CellInst& ci, const DiffInstance& d);
+
+int key_bits_for(uint64_t n_keys);
+
+}  // namespace pcg

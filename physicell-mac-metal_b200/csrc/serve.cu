@@ -1,0 +1,325 @@
+// serve.cu — continuous batching of simulation requests.
+//
+// Requests queue on submit (their host data is copied).  Each tick:
+//   1. admit queued requests, first come first served, while the running
+//      set stays within the slot limit and the device-memory budget;
+//   2. when the running set changed, build a new batch over it: requests
+//      that keep running move their fields and cells device-to-device from
+//      the old batch, new ones upload their inputs;
+//   3. advance every running request by min(steps_per_tick, fewest steps
+//      left) main-loop sub-steps — each sub-step is one graph launch over
+//      all of them, with a per-request mask so that every request keeps its
+//      own mechanics cadence (src/main.mm:375-391 accumulator);
+//   4. requests that reached their step count copy their results to the
+//      host and leave at the next tick.
+// A request's arithmetic never depends on what else runs (every kernel
+// treats instances independently and in a fixed order), so its result is
+// the same alone and in the mix.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "batch.h"
+
+using namespace pcg;
+
+namespace {
+
+double now_s()
+{
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Request {
+    uint64_t id = 0;
+    pcg_instance_desc desc{};
+    std::vector<pcg_substrate_params> subs;
+    std::vector<float> dens, init_vals, soa;
+    std::vector<double> rates[4];
+    std::vector<uint8_t> active;
+    uint32_t n_steps = 0, done = 0;
+    double accum = 0.0;
+    int state = PCG_REQ_QUEUED;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    uint64_t bytes = 0;
+    int slot = -1;   // index in the current batch
+    std::vector<float> out_dens, out_soa;
+};
+
+}  // namespace
+
+struct pcg_server {
+    pcg_ctx* ctx = nullptr;
+    pcg_serve_options opt{};
+    uint64_t next_id = 1;
+    std::map<uint64_t, std::unique_ptr<Request>> reqs;
+    std::deque<Request*> queue;
+    std::vector<Request*> running;
+    std::unique_ptr<Batch> batch;
+    uint64_t bytes_in_use = 0;
+    uint64_t voxel_steps = 0, cell_steps = 0;
+    HostBuf masks;
+};
+
+namespace {
+
+int rebuild(pcg_server* s)
+{
+    if (s->running.empty()) {
+        s->batch.reset();
+        return PCG_OK;
+    }
+    std::vector<pcg_instance_desc> descs;
+    std::vector<DevSource> src;
+    for (Request* r : s->running) {
+        descs.push_back(r->desc);
+        DevSource ds;
+        if (r->slot >= 0 && s->batch) {
+            ds.batch = s->batch.get();
+            ds.index = static_cast<uint32_t>(r->slot);
+        }
+        src.push_back(ds);
+    }
+    pcg_batch_options o{};
+    o.use_graphs = 1;
+    o.autotune = 0;   // cached or default shapes: rebuilds must stay cheap
+    std::unique_ptr<Batch> nb(new (std::nothrow) Batch());
+    if (!nb) return PCG_ERR_OOM;
+    PCG_TRY(nb->create(s->ctx, descs.data(), static_cast<uint32_t>(descs.size()), &o, &src, true));
+    PCG_CU(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    s->batch = std::move(nb);   // frees the old batch
+    for (size_t i = 0; i < s->running.size(); ++i) s->running[i]->slot = static_cast<int>(i);
+    return PCG_OK;
+}
+
+int finish(pcg_server* s, Request* r)
+{
+    Batch& b = *s->batch;
+    const uint32_t i = static_cast<uint32_t>(r->slot);
+    const DiffInstance& di = b.d.inst[i];
+    r->out_dens.resize(di.nvox() * di.g.n_substrates);
+    PCG_TRY(b.d.download(i, r->out_dens.data()));
+    const CellInst& ci = b.c_.h_inst[i];
+    r->out_soa.assign(static_cast<size_t>(NUM_FIELDS) * std::max<uint32_t>(ci.n_cells, 1), 0.f);
+    if (ci.n_cells) {
+        PCG_TRY(b.c_.download_soa(ci.cell_off, ci.n_cells, r->out_soa.data(), ci.n_cells, 0, NUM_FIELDS));
+        PCG_CU(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    }
+    r->state = PCG_REQ_DONE;
+    r->t_done = now_s();
+    s->bytes_in_use -= r->bytes;
+    return PCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pcg_status pcg_serve_create(pcg_ctx* ctx, const pcg_serve_options* opt, pcg_server** out)
+{
+    if (!ctx || !out) return PCG_ERR_INVALID;
+    *out = nullptr;
+    pcg_server* s = new (std::nothrow) pcg_server();
+    if (!s) return PCG_ERR_OOM;
+    s->ctx = ctx;
+    if (opt) s->opt = *opt;
+    if (s->opt.budget_bytes == 0) s->opt.budget_bytes = 150ull * 1000 * 1000 * 1000;
+    if (s->opt.steps_per_tick == 0) s->opt.steps_per_tick = 100;
+    *out = s;
+    return PCG_OK;
+}
+
+pcg_status pcg_serve_destroy(pcg_server* s)
+{
+    if (!s) return PCG_OK;
+    cudaStreamSynchronize(s->ctx->stream);
+    delete s;
+    return PCG_OK;
+}
+
+pcg_status pcg_serve_submit(pcg_server* s, const pcg_instance_desc* in, uint32_t n_steps, uint64_t* id)
+{
+    if (!s || !in || !id) return PCG_ERR_INVALID;
+    const pcg_instance_desc& d = *in;
+    if (d.grid.nx == 0 || d.grid.ny == 0 || d.grid.nz == 0) return fail(s->ctx, PCG_ERR_INVALID, "empty grid");
+    if (d.grid.n_substrates > 0 && !d.substrates) return fail(s->ctx, PCG_ERR_INVALID, "substrates is NULL");
+    if (d.n_cells > 0 && (!d.cells_soa || d.cells_soa_max < d.n_cells))
+        return fail(s->ctx, PCG_ERR_INVALID, "cells_soa missing or too small");
+    std::unique_ptr<Request> r(new (std::nothrow) Request());
+    if (!r) return PCG_ERR_OOM;
+    r->bytes = instance_bytes(d);
+    if (r->bytes > s->opt.budget_bytes) return fail(s->ctx, PCG_ERR_BUDGET, "request larger than the budget");
+    r->id = s->next_id++;
+    r->n_steps = n_steps;
+    r->t_submit = now_s();
+    r->desc = d;
+    const uint32_t S = d.grid.n_substrates;
+    const size_t nv = static_cast<size_t>(d.grid.nx) * d.grid.ny * d.grid.nz;
+    r->subs.assign(d.substrates, d.substrates + S);
+    r->desc.substrates = r->subs.data();
+    if (d.initial_density) {
+        r->dens.assign(d.initial_density, d.initial_density + nv * S);
+        r->desc.initial_density = r->dens.data();
+    }
+    if (d.initial_values) {
+        r->init_vals.assign(d.initial_values, d.initial_values + S);
+        r->desc.initial_values = r->init_vals.data();
+    }
+    if (d.n_cells) {
+        r->soa.resize(static_cast<size_t>(NUM_FIELDS) * d.n_cells);
+        for (int f = 0; f < NUM_FIELDS; ++f)
+            std::memcpy(r->soa.data() + static_cast<size_t>(f) * d.n_cells,
+                        d.cells_soa + static_cast<size_t>(f) * d.cells_soa_max, d.n_cells * sizeof(float));
+        r->desc.cells_soa = r->soa.data();
+        r->desc.cells_soa_max = d.n_cells;
+        const double* src[4] = {d.secretion, d.uptake, d.saturation, d.net_export};
+        const double** dst[4] = {&r->desc.secretion, &r->desc.uptake, &r->desc.saturation, &r->desc.net_export};
+        for (int q = 0; q < 4; ++q) {
+            if (src[q]) {
+                r->rates[q].assign(src[q], src[q] + static_cast<size_t>(d.n_cells) * S);
+                *dst[q] = r->rates[q].data();
+            } else {
+                *dst[q] = nullptr;
+            }
+        }
+        if (d.active) {
+            r->active.assign(d.active, d.active + d.n_cells);
+            r->desc.active = r->active.data();
+        }
+    }
+    *id = r->id;
+    s->queue.push_back(r.get());
+    s->reqs[r->id] = std::move(r);
+    return PCG_OK;
+}
+
+pcg_status pcg_serve_tick(pcg_server* s, uint32_t* n_running, uint32_t* n_queued, uint32_t* n_finished)
+{
+    if (!s) return PCG_ERR_INVALID;
+    uint32_t finished = 0;
+    bool changed = false;
+    // 1. retire requests finished in the previous tick
+    std::vector<Request*> keep;
+    for (Request* r : s->running) {
+        if (r->state == PCG_REQ_DONE) {
+            changed = true;
+            r->slot = -1;
+        } else {
+            keep.push_back(r);
+        }
+    }
+    s->running.swap(keep);
+    // 2. admit
+    const double dt_batch = s->running.empty() ? -1.0 : s->running[0]->desc.grid.dt;
+    while (!s->queue.empty()) {
+        Request* r = s->queue.front();
+        if (s->opt.max_active && s->running.size() >= s->opt.max_active) break;
+        if (s->bytes_in_use + r->bytes > s->opt.budget_bytes) break;
+        if (dt_batch >= 0.0 && r->desc.grid.dt != dt_batch) break;   // one time step per running set
+        s->queue.pop_front();
+        r->state = PCG_REQ_RUNNING;
+        r->t_admit = now_s();
+        r->slot = -1;
+        s->bytes_in_use += r->bytes;
+        s->running.push_back(r);
+        changed = true;
+    }
+    if (changed) PCG_TRY(rebuild(s));
+    // 3. advance
+    if (!s->running.empty()) {
+        Batch& b = *s->batch;
+        uint32_t k = s->opt.steps_per_tick;
+        for (Request* r : s->running) k = std::min(k, r->n_steps - r->done);
+        const size_t n = s->running.size();
+        if (s->masks.bytes < static_cast<size_t>(k) * n) PCG_CU(s->ctx, s->masks.alloc(static_cast<size_t>(k) * n));
+        uint8_t* m = s->masks.as<uint8_t>();
+        for (uint32_t st = 0; st < k; ++st) {
+            bool any = false;
+            for (size_t i = 0; i < n; ++i) {
+                Request* r = s->running[i];
+                const double dtd = r->desc.grid.dt;
+                const double dtm = r->desc.dt_mechanics > 0.f ? r->desc.dt_mechanics : r->desc.mech.dt;
+                r->accum += dtd;
+                const bool mech = r->accum >= dtm - 0.5 * dtd;
+                if (mech) {
+                    r->accum = 0.0;
+                    any = true;
+                    s->cell_steps += r->desc.n_cells;
+                }
+                m[st * n + i] = static_cast<uint8_t>(STEP_DIFFUSE | (mech ? STEP_MECH : 0));
+            }
+            PCG_TRY(b.step_masked(m + st * n, any));
+        }
+        PCG_CU(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+        for (Request* r : s->running) {
+            r->done += k;
+            s->voxel_steps += static_cast<uint64_t>(r->desc.grid.nx) * r->desc.grid.ny * r->desc.grid.nz * k;
+            if (r->done >= r->n_steps) {
+                PCG_TRY(finish(s, r));
+                ++finished;
+            }
+        }
+    }
+    if (n_running) *n_running = static_cast<uint32_t>(s->running.size() - finished);
+    if (n_queued) *n_queued = static_cast<uint32_t>(s->queue.size());
+    if (n_finished) *n_finished = finished;
+    return PCG_OK;
+}
+
+pcg_status pcg_serve_state(pcg_server* s, uint64_t id, int* state)
+{
+    if (!s || !state) return PCG_ERR_INVALID;
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return PCG_ERR_NOT_FOUND;
+    *state = it->second->state;
+    return PCG_OK;
+}
+
+pcg_status pcg_serve_fetch(pcg_server* s, uint64_t id, float* density, size_t n_floats, float* soa, uint32_t soa_max)
+{
+    if (!s) return PCG_ERR_INVALID;
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return PCG_ERR_NOT_FOUND;
+    Request* r = it->second.get();
+    if (r->state != PCG_REQ_DONE) return PCG_ERR_NOT_READY;
+    if (density) {
+        if (n_floats != r->out_dens.size()) return fail(s->ctx, PCG_ERR_INVALID, "density size mismatch");
+        std::memcpy(density, r->out_dens.data(), n_floats * sizeof(float));
+    }
+    if (soa && r->desc.n_cells) {
+        if (soa_max < r->desc.n_cells) return fail(s->ctx, PCG_ERR_INVALID, "soa_max_cells < n_cells");
+        for (int f = 0; f < NUM_FIELDS; ++f)
+            std::memcpy(soa + static_cast<size_t>(f) * soa_max,
+                        r->out_soa.data() + static_cast<size_t>(f) * r->desc.n_cells, r->desc.n_cells * sizeof(float));
+    }
+    return PCG_OK;
+}
+
+pcg_status pcg_serve_request_times(pcg_server* s, uint64_t id, double* submit_to_done, double* admit_to_done)
+{
+    if (!s) return PCG_ERR_INVALID;
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return PCG_ERR_NOT_FOUND;
+    Request* r = it->second.get();
+    if (r->state != PCG_REQ_DONE) return PCG_ERR_NOT_READY;
+    if (submit_to_done) *submit_to_done = r->t_done - r->t_submit;
+    if (admit_to_done) *admit_to_done = r->t_done - r->t_admit;
+    return PCG_OK;
+}
+
+pcg_status pcg_serve_totals(pcg_server* s, uint64_t* voxel_steps, uint64_t* cell_steps, uint64_t* bytes)
+{
+    if (!s) return PCG_ERR_INVALID;
+    if (voxel_steps) *voxel_steps = s->voxel_steps;
+    if (cell_steps) *cell_steps = s->cell_steps;
+    if (bytes) *bytes = s->bytes_in_use;
+    return PCG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,262 @@
+// sort.cu — stable LSD radix sort of (key, value) pairs and a warp-shuffle
+// exclusive scan (sm_100a).  Used to bin cells by mechanics voxel (the
+// cell-start table is the exclusive scan of per-voxel counts) and to order
+// cells by diffusion voxel for secretion.
+//
+// One radix pass over D-bit digits:
+//   k_radix_hist     per-tile digit histogram -> hist[digit * tiles + tile]
+//   scan_exclusive   over hist (digit-major, so equal digits keep tile order)
+//   k_radix_scatter  each warp ranks its contiguous 256 keys with
+//                    __match_any_sync (peers with the same digit) and a
+//                    per-warp running count, warps are combined in warp
+//                    order, and every key goes to
+//                    offset[digit][tile] + warp prefix + rank.
+// Ranks follow input order within a warp, warps follow tile order and
+// tiles follow the scanned histogram, so each pass is stable.
+#include "pcg_kernels.cuh"
+
+namespace pcg {
+
+namespace {
+constexpr int kThreads = 256;
+constexpr int kItems = 8;
+constexpr int kTile = kThreads * kItems;     // 2048 keys per tile
+constexpr int kWarps = kThreads / 32;
+constexpr int kDigitBits = 8;
+constexpr int kRadix = 1 << kDigitBits;
+constexpr uint32_t kMask = kRadix - 1;
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads) k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift,
+                                                         uint32_t* __restrict__ hist, uint32_t ntiles)
+{
+    __shared__ uint32_t h[kRadix];
+    for (int i = threadIdx.x; i < kRadix; i += kThreads) h[i] = 0;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * kTile;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const uint32_t i = base + k * kThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & kMask], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += kThreads) hist[d * ntiles + blockIdx.x] = h[d];
+}
+
+__global__ void __launch_bounds__(kThreads) k_radix_scatter(const uint32_t* __restrict__ kin,
+                                                            const uint32_t* __restrict__ vin,
+                                                            uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                            uint32_t n, int shift,
+                                                            const uint32_t* __restrict__ offsets, uint32_t ntiles)
+{
+    __shared__ uint32_t wcnt[kWarps][kRadix];
+    __shared__ uint32_t gbase[kRadix];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t base = blockIdx.x * kTile + warp * (32 * kItems);
+    uint32_t kk[kItems], vv[kItems], rk[kItems];
+    int dg[kItems];
+#pragma unroll
+    for (int r = 0; r < kItems; ++r) {
+        const uint32_t i = base + r * 32 + lane;
+        const bool ok = i < n;
+        kk[r] = ok ? kin[i] : 0u;
+        vv[r] = ok ? vin[i] : 0u;
+        dg[r] = ok ? static_cast<int>((kk[r] >> shift) & kMask) : kRadix;   // kRadix marks an empty lane
+        const uint32_t peers = __match_any_sync(0xffffffffu, dg[r]);
+        rk[r] = (ok ? wcnt[warp][dg[r]] : 0u) + __popc(peers & lt);
+        __syncwarp();
+        if (ok && lane == __ffs(peers) - 1) wcnt[warp][dg[r]] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += kThreads) {
+        uint32_t sum = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = wcnt[w][d];
+            wcnt[w][d] = sum;
+            sum += c;
+        }
+        gbase[d] = offsets[d * ntiles + blockIdx.x];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kItems; ++r) {
+        if (dg[r] < kRadix) {
+            const uint32_t dst = gbase[dg[r]] + wcnt[warp][dg[r]] + rk[r];
+            kout[dst] = kk[r];
+            vout[dst] = vv[r];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ scan
+
+// Exclusive scan of one 2048-value tile per block (8 consecutive values per
+// thread, warp shuffles across lanes, shared memory across warps); writes
+// the tile total to sums[blockIdx.x] when sums != nullptr.
+__global__ void __launch_bounds__(kThreads) k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                         uint64_t n, uint32_t* __restrict__ sums)
+{
+    __shared__ uint32_t wsum[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kTile + static_cast<uint64_t>(threadIdx.x) * kItems;
+    uint32_t v[kItems];
+    uint32_t tot = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const uint64_t i = base + k;
+        v[k] = i < n ? in[i] : 0u;
+        const uint32_t x = v[k];
+        v[k] = tot;
+        tot += x;
+    }
+    uint32_t incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kWarps ? wsum[lane] : 0u;
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < kWarps; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < kWarps) wsum[lane] = wi - w;
+        if (lane == kWarps - 1 && sums) sums[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    const uint32_t pre = wsum[warp] + (incl - tot);
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const uint64_t i = base + k;
+        if (i < n) out[i] = v[k] + pre;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_scan_add(uint32_t* __restrict__ out, uint64_t n,
+                                                       const uint32_t* __restrict__ offs)
+{
+    const uint32_t add = offs[blockIdx.x];
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kTile;
+    for (int k = threadIdx.x; k < kTile; k += kThreads) {
+        const uint64_t i = base + k;
+        if (i < n) out[i] += add;
+    }
+}
+
+static uint64_t tiles_of(uint64_t n) { return (n + kTile - 1) / kTile; }
+
+size_t scan_scratch_bytes(uint64_t n)
+{
+    size_t bytes = 0;
+    uint64_t m = tiles_of(n);
+    while (m > 1) {
+        bytes += ((m * sizeof(uint32_t) + 255) / 256) * 256;
+        m = tiles_of(m);
+    }
+    return bytes + 256;
+}
+
+int scan_launches(uint64_t n)
+{
+    int l = 1;
+    uint64_t m = tiles_of(n);
+    while (m > 1) {
+        l += 2;
+        m = tiles_of(m);
+    }
+    return l;
+}
+
+static cudaError_t scan_rec(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n, char* scratch)
+{
+    const uint64_t nt = tiles_of(n);
+    if (nt == 0) return cudaSuccess;
+    if (nt == 1) {
+        k_scan_tiles<<<1, kThreads, 0, st>>>(in, out, n, nullptr);
+        return cudaGetLastError();
+    }
+    uint32_t* sums = reinterpret_cast<uint32_t*>(scratch);
+    char* next = scratch + ((nt * sizeof(uint32_t) + 255) / 256) * 256;
+    k_scan_tiles<<<static_cast<unsigned>(nt), kThreads, 0, st>>>(in, out, n, sums);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = scan_rec(st, sums, sums, nt, next);
+    if (e != cudaSuccess) return e;
+    k_scan_add<<<static_cast<unsigned>(nt), kThreads, 0, st>>>(out, n, sums);
+    return cudaGetLastError();
+}
+
+cudaError_t scan_exclusive(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n, void* scratch)
+{
+    return scan_rec(st, in, out, n, static_cast<char*>(scratch));
+}
+
+// ------------------------------------------------------------------ sort
+
+static int passes_for(int bits) { return bits <= 0 ? 0 : (bits + kDigitBits - 1) / kDigitBits; }
+
+size_t radix_sort_scratch_bytes(uint32_t n, int bits)
+{
+    (void)bits;
+    const uint64_t nt = tiles_of(n ? n : 1);
+    const uint64_t hist = nt * kRadix;
+    return ((hist * sizeof(uint32_t) + 255) / 256) * 256 + scan_scratch_bytes(hist);
+}
+
+int radix_sort_launches(uint32_t n, int bits)
+{
+    const uint64_t nt = tiles_of(n ? n : 1);
+    const int p = passes_for(bits);
+    if (p == 0) return 2;
+    return p * (2 + scan_launches(nt * kRadix));
+}
+
+cudaError_t radix_sort_pairs(cudaStream_t st, const uint32_t* k_in, const uint32_t* v_in, uint32_t* k_out,
+                             uint32_t* v_out, uint32_t* k_tmp, uint32_t* v_tmp, uint32_t n, int bits, void* scratch)
+{
+    if (n == 0) return cudaSuccess;
+    const uint32_t nt = static_cast<uint32_t>(tiles_of(n));
+    uint32_t* hist = static_cast<uint32_t*>(scratch);
+    char* sscr = static_cast<char*>(scratch) + ((static_cast<uint64_t>(nt) * kRadix * sizeof(uint32_t) + 255) / 256) * 256;
+    const int passes = passes_for(bits);
+    if (passes == 0) {
+        cudaError_t e = cudaMemcpyAsync(k_out, k_in, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return e;
+        return cudaMemcpyAsync(v_out, v_in, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+    }
+    // ping-pong so that the last pass writes (k_out, v_out)
+    const uint32_t* ks = k_in;
+    const uint32_t* vs = v_in;
+    for (int p = 0; p < passes; ++p) {
+        const bool last = p == passes - 1;
+        // pass p writes out when (passes - 1 - p) is even, tmp otherwise
+        const bool to_out = ((passes - 1 - p) & 1) == 0;
+        uint32_t* kd = to_out ? k_out : k_tmp;
+        uint32_t* vd = to_out ? v_out : v_tmp;
+        const int shift = p * kDigitBits;
+        k_radix_hist<<<nt, kThreads, 0, st>>>(ks, n, shift, hist, nt);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        e = scan_exclusive(st, hist, hist, static_cast<uint64_t>(nt) * kRadix, sscr);
+        if (e != cudaSuccess) return e;
+        k_radix_scatter<<<nt, kThreads, 0, st>>>(ks, vs, kd, vd, n, shift, hist, nt);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        ks = kd;
+        vs = vd;
+        (void)last;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace pcg

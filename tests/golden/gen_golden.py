@@ -1,0 +1,114 @@
+"""Generate golden vectors by running the reference's own code on the CPU.
+
+Needs oracle/_ref/libpcg_ref.so, which oracle/Makefile builds from the
+reference tree (its Metal shader bodies compiled as C++ through
+oracle/ref/metal_shim.h, and its processSecretion from
+src/cell_phenotype.cpp).  Run from the repository root:
+
+    python tests/golden/gen_golden.py
+
+Writes tests/golden/*.npz: the seeded inputs and the reference's outputs.
+The oracle tests check the oracle against these files, so the pin travels
+without the reference tree.
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import pyoracle as po  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# (name, nx, ny, substrates [(D, decay, dirichlet, target)], steps, seed)
+DIFFUSION_CASES = [
+    ("diff_50x50_o2", 50, 50, [(1e5, 0.1, True, 38.0)], 3, 11),
+    ("diff_16x16_two", 16, 16, [(0.0, 0.1, False, 0.0), (1e3, 0.5, True, 5.0)], 4, 12),
+    ("diff_8x12_nodir", 8, 12, [(2.5e4, 0.2, False, 0.0)], 5, 13),
+    ("diff_3x7", 3, 7, [(1e5, 0.1, True, 38.0)], 2, 14),
+    ("diff_4x5", 4, 5, [(1e5, 0.1, True, 38.0), (3e3, 0.0, False, 1.0)], 2, 15),
+    ("diff_2x9", 2, 9, [(1e5, 0.1, True, 38.0)], 2, 16),
+    ("diff_33x17", 33, 17, [(7e4, 0.3, True, 10.0)], 3, 17),
+    ("diff_uniform_T", 12, 10, [(1e5, 0.1, True, 38.0)], 3, 18),
+]
+
+
+def gen_diffusion():
+    for name, nx, ny, subs_p, steps, seed in DIFFUSION_CASES:
+        rng = np.random.default_rng(seed)
+        S = len(subs_p)
+        g = po.make_grid(nx, ny, 1, S, dx=20.0, dt=0.01, x_min=-0.5 * nx * 20, y_min=-0.5 * ny * 20)
+        subs = po.make_subs(subs_p)
+        if name == "diff_uniform_T":
+            d0 = np.full(S * nx * ny, 38.0, np.float32)
+        else:
+            d0 = rng.uniform(0.0, 40.0, S * nx * ny).astype(np.float32)
+        d = d0.copy()
+        outs = []
+        for _ in range(steps):
+            po.ref_sweeps(d, g, subs)
+            po.ref_dirichlet(d, g, subs)
+            outs.append(d.copy())
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), nx=nx, ny=ny, subs=np.array(subs_p, np.float64),
+                            steps=steps, density0=d0, density_steps=np.stack(outs))
+
+
+def gen_secretion():
+    rng = np.random.default_rng(21)
+    nx, ny, S, n = 10, 10, 2, 300
+    g = po.make_grid(nx, ny, 1, S, dx=20.0, dt=0.01)
+    vox = rng.integers(0, nx * ny + 5, n).astype(np.uint32)      # a few out of range
+    vox[:40] = 7                                                  # a crowded voxel
+    vol = rng.uniform(1000, 4000, n).astype(np.float32)
+    sec = rng.uniform(0, 10, n * S)
+    upt = rng.uniform(0, 10, n * S)
+    sat = rng.uniform(0, 40, n * S)
+    ne = rng.uniform(-50, 50, n * S)
+    d0 = rng.uniform(0, 40, S * nx * ny).astype(np.float32)
+    d = d0.copy()
+    po.ref_secretion(d, g, vox, vol, sec, upt, sat, ne, 0.01)
+    np.savez_compressed(os.path.join(OUT, "secretion.npz"), nx=nx, ny=ny, S=S, voxel=vox, volume=vol, sec=sec,
+                        upt=upt, sat=sat, ne=ne, density0=d0, density1=d)
+
+
+def disc_cells(n, r, rng, max_cells, radius=8.41):
+    soa = np.zeros(28 * max_cells, np.float32)
+    rr = r * np.sqrt(rng.random(n))
+    th = rng.random(n) * 2 * np.pi
+    soa[0 * max_cells:0 * max_cells + n] = rr * np.cos(th)
+    soa[1 * max_cells:1 * max_cells + n] = rr * np.sin(th)
+    soa[9 * max_cells:9 * max_cells + n] = radius
+    soa[11 * max_cells:11 * max_cells + n] = 2494.0
+    soa[13 * max_cells:13 * max_cells + n] = 10.0
+    soa[14 * max_cells:14 * max_cells + n] = 0.4
+    soa[15 * max_cells:15 * max_cells + n] = 1.25
+    return soa
+
+
+def gen_mechanics():
+    rng = np.random.default_rng(31)
+    mc = 600
+    n = 500
+    m = po.mech_params(-500, 500, -500, 500, -10, 10, True, 0.1)
+    origin = (-500.0, -500.0, -10.0)
+    soa0 = disc_cells(n, 200.0, rng, mc)
+    soa0[3 * mc:3 * mc + n] = rng.normal(0, 1, n)       # previous-step velocities for AB2
+    soa0[6 * mc:6 * mc + n] = rng.normal(0, 1, n)
+    s = soa0.copy()
+    counts, cells = po.ref_forces(s, mc, n, m, origin)
+    forces = s.copy()
+    po.ref_integrate(s, mc, n, m, origin, 0.1)
+    np.savez_compressed(os.path.join(OUT, "mechanics_2d.npz"), max_cells=mc, n=n, soa0=soa0, hash_counts=counts,
+                        hash_cells=cells, soa_forces=forces, soa_integrated=s,
+                        mech=np.array([m.mech_grid_nx, m.mech_grid_ny, m.mech_grid_nz], np.uint32))
+
+
+if __name__ == "__main__":
+    if not po.ref_available():
+        sys.exit("oracle/_ref/libpcg_ref.so not built (make -C oracle with the reference tree present)")
+    gen_diffusion()
+    gen_secretion()
+    gen_mechanics()
+    print("golden vectors written to", OUT)

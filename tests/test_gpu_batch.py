@@ -1,0 +1,149 @@
+"""Batched and served simulations: every instance's result is bit-for-bit
+what it gets when it runs alone, and alone it matches the oracle."""
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def small_mix(pcg, seed=5):
+    """Uneven 2-D and 3-D instances with cells."""
+    from pcg import workloads
+    out = []
+    rng = np.random.default_rng(seed)
+    for i, (side, nz) in enumerate([(37, 1), (20, 20), (64, 1), (33, 29), (50, 1), (41, 41)]):
+        S = 1 + i % 3
+        two_d = nz == 1
+        g = pcg.make_grid(side, side, nz, S, dx=20.0, dt=0.01, z_min=-10.0 if two_d else 0.0)
+        subs = [(1e5, 0.1, True, 38.0)] + [(float(rng.uniform(1e3, 5e4)), float(rng.uniform(0, 0.5)),
+                                            bool(rng.integers(0, 2)), 2.0) for _ in range(S - 1)]
+        L = side * 20.0
+        n = int(rng.integers(50, 3000))
+        if two_d:
+            pos = np.stack([rng.uniform(0, L, n), rng.uniform(0, L, n), np.zeros(n)], 1).astype(np.float32)
+        else:
+            pos = rng.uniform(0.3 * L, 0.7 * L, (n, 3)).astype(np.float32)
+        out.append(workloads.instance(g, subs, pos, np.full(n, 8.41, np.float32), float(rng.uniform(5, 20)),
+                                      float(rng.uniform(0, 1)), 1.25, sec=rng.uniform(0, 5, n * S),
+                                      upt=rng.uniform(0, 10, n * S), sat=rng.uniform(0, 40, n * S),
+                                      ne=rng.uniform(-5, 5, n * S), two_d=two_d,
+                                      flags=pcg.INST_REFRESH_VOXELS if i % 2 else 0))
+    return out
+
+
+def run_batch(pcg, ctx, insts, steps, **kw):
+    b = pcg.Batch(ctx, insts, **kw)
+    b.step(steps)
+    ctx.sync()
+    res = [(b.density(i), b.cells(i)) for i in range(len(insts))]
+    b.close()
+    return res
+
+
+def test_batch_equals_alone_bitwise(ctx, pcg):
+    insts = small_mix(pcg)
+    steps = 23   # includes two mechanics steps
+    together = run_batch(pcg, ctx, insts, steps)
+    for i, inst in enumerate(insts):
+        alone = run_batch(pcg, ctx, [inst], steps)[0]
+        assert np.array_equal(together[i][0].view(np.uint32), alone[0].view(np.uint32)), f"density {i}"
+        assert np.array_equal(together[i][1].view(np.uint32), alone[1].view(np.uint32)), f"cells {i}"
+
+
+def test_graphs_equal_direct_launches(ctx, pcg):
+    insts = small_mix(pcg, seed=6)
+    a = run_batch(pcg, ctx, insts, 21, use_graphs=True)
+    b = run_batch(pcg, ctx, insts, 21, use_graphs=False, autotune=False)
+    for (da, ca), (db, cb) in zip(a, b):
+        assert np.array_equal(da.view(np.uint32), db.view(np.uint32))
+        assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32))
+
+
+def test_batch_instance_matches_oracle(ctx, pcg, po):
+    insts = small_mix(pcg, seed=7)
+    steps = 31
+    res = run_batch(pcg, ctx, insts, steps)
+    for i in (0, 1, 3):
+        inst = insts[i]
+        g = inst.grid
+        S, n = g.n_substrates, inst.n_cells
+        og = po.make_grid(g.nx, g.ny, g.nz, S, dx=g.dx, dt=g.dt, x_min=g.x_min, y_min=g.y_min, z_min=g.z_min)
+        osubs = po.make_subs([(s.diffusion_coefficient, s.decay_rate, bool(s.dirichlet_enabled), s.target_value)
+                              for s in inst.substrates[:S]])
+        m = inst.mech
+        om = po.Mech(m.dt, m.cell_cell_repulsion, m.cell_cell_adhesion, m.max_interaction_distance,
+                     m.mechanics_voxel_size, m.mech_grid_nx, m.mech_grid_ny, m.mech_grid_nz)
+        dens = np.repeat(inst.initial_values, g.nx * g.ny * g.nz).astype(np.float32)
+        soa = inst.soa.copy()
+        po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, steps, refresh=bool(inst.flags & 1))
+        b = np.asarray(dens, np.float64)
+        err = np.abs(res[i][0] - b) / np.maximum(np.abs(b), 1e-6 * np.abs(b).max())
+        assert err.max() <= 1e-5, (i, err.max())
+        assert np.abs(res[i][1][:3 * n].astype(np.float64) - soa[:3 * n]).max() <= 1e-4
+
+
+def test_upload_cells_between_steps(ctx, pcg):
+    insts = small_mix(pcg, seed=8)[:3]
+    b = pcg.Batch(ctx, insts)
+    b.step(12)
+    soa = b.cells(1)
+    n = insts[1].n_cells
+    soa[3 * n:4 * n] += 1.0          # a host-side velocity change (motility hook)
+    b.upload_cells(1, soa, n)
+    b.step(10)
+    ctx.sync()
+    assert np.isfinite(b.density(1)).all()
+    b.close()
+
+
+def test_served_results_equal_alone(ctx, pcg):
+    """Continuous batching: requests arrive over several ticks with different
+    step counts; each result is bit-for-bit its result alone."""
+    insts = small_mix(pcg, seed=9)
+    steps = [40, 25, 60, 33, 18, 47]
+    srv = pcg.Server(ctx, budget_bytes=int(4e9), steps_per_tick=10)
+    ids = []
+    for k, (inst, s) in enumerate(zip(insts, steps)):
+        ids.append(srv.submit(inst, s))
+        srv.tick()                      # arrivals interleave with progress
+    for _ in range(200):
+        r, q, _ = srv.tick()
+        if r == 0 and q == 0:
+            break
+    for rid, inst, s in zip(ids, insts, steps):
+        assert srv.state(rid) == pcg.REQ_DONE
+        d, c = srv.fetch(rid)
+        alone_d, alone_c = run_batch(pcg, ctx, [inst], s)[0]
+        assert np.array_equal(d.view(np.uint32), alone_d.view(np.uint32))
+        assert np.array_equal(c.view(np.uint32), alone_c.view(np.uint32))
+        t_total, t_run = srv.times(rid)
+        assert t_total >= t_run > 0
+    v, cs, held = srv.totals()
+    assert v > 0 and held == 0
+    srv.close()
+
+
+def test_server_respects_budget(ctx, pcg):
+    insts = small_mix(pcg, seed=10)
+    one = max(i.bytes() for i in insts)
+    srv = pcg.Server(ctx, budget_bytes=int(one * 2.2), steps_per_tick=5)
+    for inst in insts:
+        srv.submit(inst, 12)
+    peak = 0
+    for _ in range(100):
+        r, q, _ = srv.tick()
+        _, _, held = srv.totals()
+        assert held <= one * 2.2
+        peak = max(peak, r)
+        if r == 0 and q == 0:
+            break
+    assert peak <= 2
+    for rid in srv.requests:
+        assert srv.state(rid) == pcg.REQ_DONE
+    srv.close()
+    tiny = pcg.Server(ctx, budget_bytes=10)
+    with pytest.raises(pcg.PcgError):
+        tiny.submit(insts[0], 10)          # larger than the whole budget
+    tiny.close()
