@@ -203,7 +203,7 @@ int Batch::run_step(bool mech, bool timed, const uint8_t* mask)
     if (c_.n) PCG_TRY(c_.secrete(d, mask));
     if (timed) PCG_CU(ctx, cudaEventRecord(ev[4], st));
     if (mech && c_.n) {
-        PCG_TRY(m_.binsort(c_));
+        PCG_TRY(m_.binsort(c_, mask));
         if (timed) PCG_CU(ctx, cudaEventRecord(ev[5], st));
         PCG_TRY(m_.force_pass(c_, mask));
         if (timed) PCG_CU(ctx, cudaEventRecord(ev[6], st));

@@ -107,11 +107,13 @@ __global__ void k_secrete(float* __restrict__ dens, const uint32_t* __restrict__
 
 __global__ void k_mech_bin(float* __restrict__ soa, uint32_t stride, uint32_t n, const uint32_t* __restrict__ cell_inst,
                            const CellInst* __restrict__ insts, uint32_t* __restrict__ keys,
-                           uint32_t* __restrict__ vals, uint32_t* __restrict__ counts)
+                           uint32_t* __restrict__ vals, uint32_t* __restrict__ counts,
+                           const uint8_t* __restrict__ mask)
 {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
-    const CellInst& in = insts[cell_inst[g]];
+    const uint32_t ii = cell_inst[g];
+    const CellInst& in = insts[ii];
     const float px = soa[static_cast<size_t>(F_POS_X) * stride + g];
     const float py = soa[static_cast<size_t>(F_POS_Y) * stride + g];
     const float pz = soa[static_cast<size_t>(F_POS_Z) * stride + g];
@@ -120,7 +122,9 @@ __global__ void k_mech_bin(float* __restrict__ soa, uint32_t stride, uint32_t n,
     const int vk = clampi(bin_of(pz, in.mz_min, in.vs), 0, static_cast<int>(in.mnz) - 1);
     const uint32_t local = static_cast<uint32_t>(vk) * in.mny * in.mnx + static_cast<uint32_t>(vj) * in.mnx +
                            static_cast<uint32_t>(vi);
-    soa[static_cast<size_t>(F_MECH_VOXEL) * stride + g] = __uint_as_float(local);
+    // every cell is binned (the sort covers the whole batch) but only the
+    // instances taking this mechanics step store their bin
+    if (mask == nullptr || (mask[ii] & STEP_MECH)) soa[static_cast<size_t>(F_MECH_VOXEL) * stride + g] = __uint_as_float(local);
     const uint32_t key = in.mvox_base + local;
     keys[g] = key;
     vals[g] = g;
@@ -323,10 +327,11 @@ cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, 
 }
 
 cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n, const uint32_t* cell_inst,
-                            const CellInst* insts, uint32_t* keys, uint32_t* vals, uint32_t* counts)
+                            const CellInst* insts, uint32_t* keys, uint32_t* vals, uint32_t* counts,
+                            const uint8_t* mask)
 {
     if (n == 0) return cudaSuccess;
-    k_mech_bin<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, keys, vals, counts);
+    k_mech_bin<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, keys, vals, counts, mask);
     return cudaGetLastError();
 }
 

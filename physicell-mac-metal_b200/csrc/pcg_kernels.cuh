@@ -130,7 +130,7 @@ cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, 
 // Mechanics.
 cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
                             const uint32_t* cell_inst, const CellInst* insts,
-                            uint32_t* keys, uint32_t* vals, uint32_t* counts);
+                            uint32_t* keys, uint32_t* vals, uint32_t* counts, const uint8_t* mask);
 cudaError_t launch_mech_gather(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* sorder,
                                uint32_t n, float4* spos, float4* sprm);
 cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* skeys,

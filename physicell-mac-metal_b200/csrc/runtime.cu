@@ -805,11 +805,11 @@ int Mechanics::launches_forces(uint32_t n) const
 // computeForces: bin -> stable radix sort -> cell-start table -> sorted SoA -> forces
 int Mechanics::forces(Cells& c, const uint8_t* mask)
 {
-    PCG_TRY(binsort(c));
+    PCG_TRY(binsort(c, mask));
     return force_pass(c, mask);
 }
 
-int Mechanics::binsort(Cells& c)
+int Mechanics::binsort(Cells& c, const uint8_t* mask)
 {
     if (c.n == 0) return PCG_OK;
     if (c.n > cap) return fail(ctx, PCG_ERR_INVALID, "more cells than the mechanics capacity");
@@ -817,7 +817,7 @@ int Mechanics::binsort(Cells& c)
     cudaStream_t st = ctx->stream;
     PCG_CU(ctx, cudaMemsetAsync(counts.p, 0, counts.bytes, st));
     cudaError_t e = launch_mech_bin(st, c.soa.as<float>(), c.max_cells, c.n, c.cell_inst.as<uint32_t>(),
-                                    c.inst.as<CellInst>(), keys.as<uint32_t>(), vals.as<uint32_t>(), counts.as<uint32_t>());
+                                    c.inst.as<CellInst>(), keys.as<uint32_t>(), vals.as<uint32_t>(), counts.as<uint32_t>(), mask);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "bin launch");
     e = radix_sort_pairs(st, keys.as<uint32_t>(), vals.as<uint32_t>(), skeys.as<uint32_t>(), sorder.as<uint32_t>(),
                          ktmp.as<uint32_t>(), vtmp.as<uint32_t>(), c.n, key_bits, sort_scr.p);

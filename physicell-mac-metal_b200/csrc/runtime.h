@@ -203,7 +203,7 @@ public:
 
     int create(pcg_ctx* c, uint32_t total_mvox, uint32_t max_cells);
     int forces(Cells& c, const uint8_t* mask);       // binsort + force_pass
-    int binsort(Cells& c);                           // bin, stable radix sort, cell-start table, sorted SoA
+    int binsort(Cells& c, const uint8_t* mask);      // bin, stable radix sort, cell-start table, sorted SoA
     int force_pass(Cells& c, const uint8_t* mask);
     int integrate(Cells& c, float dt_override, const uint8_t* mask);
     int launches_forces(uint32_t n) const;

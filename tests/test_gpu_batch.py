@@ -126,8 +126,8 @@ def test_served_results_equal_alone(ctx, pcg):
 
 
 def test_server_respects_budget(ctx, pcg):
-    insts = small_mix(pcg, seed=10)
-    one = max(i.bytes() for i in insts)
+    insts = [small_mix(pcg, seed=10)[3]] * 6          # equal requests: two fit the budget at a time
+    one = insts[0].bytes()
     srv = pcg.Server(ctx, budget_bytes=int(one * 2.2), steps_per_tick=5)
     for inst in insts:
         srv.submit(inst, 12)
