@@ -6,59 +6,61 @@
 // (applyDirichletBC); :282-342 (computeGradients).  The z sweep applies the
 // same per-line rule along k.
 //
-// B200 layout.  density is [s][k][j][i] FP32 in HBM.  The per-line Thomas
-// constants are one table per (instance, substrate, axis) (LineRule), so the
-// forward pass is one FMUL + one FFMA per value and the backward pass one
-// FFMA.  Work is a flat list of tiles over all instances:
-//   x sweep   row tiles: L contiguous lines (one CTA, one line per thread),
-//             staged through padded shared memory (stride n|1, conflict-free)
-//             with cp.async, double-buffered across tiles;
-//   y/z sweep column tiles: 32 adjacent columns (one warp, one column per
-//             lane), each row a 128-byte coalesced segment, staged with
-//             cp.async, double-buffered per warp.
-// Each value is read from HBM once and written once per sweep.
+// The solve.  Every line of one (instance, substrate, axis) family has the
+// same matrix, so g_i = c / den_i and 1 / den_i are one table (LineRule,
+// built in FP64 on the host).  With h_i = (rho_i + fold_i) / den_i the
+// reference's forward and backward passes are two first-order linear
+// recurrences with the same coefficients:
+//     forward   d_i = g_i d_{i-1} + h_i        (d_0 = 0)
+//     backward  x_i = g_i x_{i+1} + d_i        (x_{n-1} = 0)
+// End nodes (and padding) have g = h = 0, so they are transparent; they
+// keep their value, or take the Dirichlet target.  A line is cut into
+// chunks held in registers: each thread runs both recurrences over its
+// chunk, and the chunks are joined by an exclusive scan of affine maps
+// (x -> A x + B), forward for d and in reverse for x.  Every value is read
+// from HBM once and written once per sweep; nothing is staged in shared
+// memory except the per-chunk maps of the y/z scan.
+//   x sweep   a segment of S = 8/16/32 lanes of one warp per line (the line
+//             is contiguous), chunks of m = ceil(n / S) values, scan with
+//             warp shuffles;
+//   y/z sweep lanes are 32 adjacent columns (each row a 128-byte segment),
+//             the 16 warps of a CTA are chunks along the line, scan through
+//             shared memory.
+// The chunking depends only on the line length, so a line's arithmetic is
+// the same whatever else shares the launch.
 #include "pcg_kernels.cuh"
 
 namespace pcg {
 
-__device__ __forceinline__ void cp_async4(float* smem, const float* gmem)
+__device__ __forceinline__ bool tile_on(const LineRule& r, const uint8_t* __restrict__ mask)
 {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+    return mask == nullptr || (mask[r.inst] & STEP_DIFFUSE);
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Solve one line in place; s[m * st] is position m.  Implements the rule of
-// diffusion_2d.metal:55-155 with the precomputed table (see LineRule).
+__device__ __forceinline__ bool on_face(const SweepTile& tile, int lane)
+{
+    if (tile.face & TILE_FACE_ALL) return true;
+    const uint32_t i = tile.i0 + static_cast<uint32_t>(lane);
+    return i == 0u || i + 1u == tile.nx;
+}
+
+// Reference rule for a whole line held at s[m * st] (used for lines too long
+// for the chunked kernels): the same recurrences, sequentially.
 __device__ __forceinline__ void solve_line(float* s, int st, const LineRule& r, const float2* __restrict__ tb)
 {
     const int n = static_cast<int>(r.n);
     if (n >= 3) {
-        const float f = r.fold;
-        if (n == 3) {
-            s[st] = (s[st] + f) * __ldg(&tb[1].y);
-        } else {
-            float d = (s[st] + f) * __ldg(&tb[1].y);
-            s[st] = d;
-            int i = 2;
-#pragma unroll 4
-            for (; i < n - 2; ++i) {
-                const float2 e = __ldg(&tb[i]);
-                d = fmaf(-e.x, d, s[i * st] * e.y);
-                s[i * st] = d;
-            }
-            {
-                const float2 e = __ldg(&tb[n - 2]);
-                d = fmaf(-e.x, d, (s[(n - 2) * st] + f) * e.y);
-                s[(n - 2) * st] = d;
-            }
-#pragma unroll 4
-            for (i = n - 3; i >= 1; --i) {
-                d = fmaf(-__ldg(&tb[i].x), d, s[i * st]);
-                s[i * st] = d;
-            }
+        float d = 0.f;
+        for (int i = 1; i <= n - 2; ++i) {
+            const float2 e = __ldg(&tb[i]);
+            const float f = (i == 1 || i == n - 2) ? r.fold : 0.f;
+            d = fmaf(-e.x, d, (s[i * st] + f) * e.y);
+            s[i * st] = d;
+        }
+        float x = 0.f;
+        for (int i = n - 2; i >= 1; --i) {
+            x = fmaf(-__ldg(&tb[i].x), x, s[i * st]);
+            s[i * st] = x;
         }
     }
     if (r.dir) {
@@ -69,120 +71,221 @@ __device__ __forceinline__ void solve_line(float* s, int st, const LineRule& r, 
 
 // ------------------------------------------------------------------ x sweep
 
-__device__ __forceinline__ void rows_issue(const SweepTile& tile, const LineRule* __restrict__ rules,
-                                           const float* __restrict__ dens, float* buf)
+template <int M>
+__global__ void __launch_bounds__(256) k_sweep_x(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
+                                                 uint32_t ntiles, const LineRule* __restrict__ rules,
+                                                 const float2* __restrict__ tab, const uint8_t* __restrict__ mask)
 {
-    const uint32_t n = rules[tile.rule].n;
-    const uint32_t P = n | 1u;
-    const uint32_t total = tile.count * n;
-    const float* g = dens + tile.base;
-    const uint32_t M = (n == 1u) ? 0u : (0xFFFFFFFFu / n + 1u);   // ceil(2^32 / n)
-    for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
-        const uint32_t line = (n == 1u) ? e : __umulhi(e, M);
-        const uint32_t pos = e - line * n;
-        cp_async4(buf + line * P + pos, g + e);
-    }
-}
-
-__device__ __forceinline__ bool tile_on(const LineRule& r, const uint8_t* __restrict__ mask)
-{
-    return mask == nullptr || (mask[r.inst] & STEP_DIFFUSE);
-}
-
-__global__ void __launch_bounds__(256) k_sweep_rows(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
-                                                    uint32_t ntiles, const LineRule* __restrict__ rules,
-                                                    const float2* __restrict__ tab, int pmax,
-                                                    const uint8_t* __restrict__ mask)
-{
-    extern __shared__ float sm[];
-    float* bufs[2] = {sm, sm + static_cast<size_t>(blockDim.x) * pmax};
-    uint32_t t = blockIdx.x;
-    if (t < ntiles) rows_issue(tiles[t], rules, dens, bufs[0]);
-    cp_async_commit();
-    int k = 0;
-    for (; t < ntiles; t += gridDim.x, k ^= 1) {
-        const uint32_t tn = t + gridDim.x;
-        if (tn < ntiles) rows_issue(tiles[tn], rules, dens, bufs[k ^ 1]);
-        cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t = gw; t < ntiles; t += nw) {
         const SweepTile tile = tiles[t];
         const LineRule r = rules[tile.rule];
-        const uint32_t n = r.n, P = n | 1u, total = tile.count * n;
-        float* buf = bufs[k];
-        if (!tile_on(r, mask)) {
-            __syncthreads();
-            continue;
+        if (!tile_on(r, mask)) continue;
+        const int n = static_cast<int>(r.n);
+        const int S = static_cast<int>(x_seg_lanes(r.n));
+        const int m = (n + S - 1) / S;
+        const int seg = lane / S, sl = lane % S;
+        const bool active = seg < static_cast<int>(tile.count);
+        float* g = dens + tile.base + static_cast<size_t>(seg) * n;
+        const float2* tb = tab + r.tab;
+        const int p0 = sl * m;
+        float v[M], gg[M];
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            const int p = p0 + k;
+            float x = 0.f, gk = 0.f, iv = 0.f;
+            if (k < m && active && p < n) {
+                x = g[p];
+                const float2 e = __ldg(&tb[p]);
+                gk = -e.x;
+                iv = e.y;
+            }
+            const float f = (p == 1 || p == n - 2) ? r.fold : 0.f;
+            v[k] = (x + f) * iv;
+            gg[k] = gk;
         }
-        if (threadIdx.x < tile.count) solve_line(buf + threadIdx.x * P, 1, r, tab + r.tab);
-        __syncthreads();
-        float* g = dens + tile.base;
-        const uint32_t M = (n == 1u) ? 0u : (0xFFFFFFFFu / n + 1u);
-        for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
-            const uint32_t line = (n == 1u) ? e : __umulhi(e, M);
-            g[e] = buf[line * P + (e - line * n)];
+        // forward: local recurrence, then the segment's exclusive scan
+        float d = 0.f, A = 1.f;
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            if (k < m) {
+                d = fmaf(gg[k], d, v[k]);
+                A *= gg[k];
+                v[k] = d;
+            }
         }
-        __syncthreads();
+        float B = d;
+        for (int o = 1; o < S; o <<= 1) {
+            const float Ap = __shfl_up_sync(0xffffffffu, A, o, S);
+            const float Bp = __shfl_up_sync(0xffffffffu, B, o, S);
+            if (sl >= o) {
+                B = fmaf(A, Bp, B);
+                A *= Ap;
+            }
+        }
+        float din = __shfl_up_sync(0xffffffffu, B, 1, S);
+        if (sl == 0) din = 0.f;
+        float run = 1.f;
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            if (k < m) {
+                run *= gg[k];
+                v[k] = fmaf(run, din, v[k]);
+            }
+        }
+        // backward: local recurrence from the chunk's end, reverse scan
+        float x = 0.f;
+        A = 1.f;
+#pragma unroll
+        for (int k = M - 1; k >= 0; --k) {
+            if (k < m) {
+                x = fmaf(gg[k], x, v[k]);
+                A *= gg[k];
+                v[k] = x;
+            }
+        }
+        B = x;
+        for (int o = 1; o < S; o <<= 1) {
+            const float Ap = __shfl_down_sync(0xffffffffu, A, o, S);
+            const float Bp = __shfl_down_sync(0xffffffffu, B, o, S);
+            if (sl + o < S) {
+                B = fmaf(A, Bp, B);
+                A *= Ap;
+            }
+        }
+        float xout = __shfl_down_sync(0xffffffffu, B, 1, S);
+        if (sl == S - 1) xout = 0.f;
+        run = 1.f;
+#pragma unroll
+        for (int k = M - 1; k >= 0; --k) {
+            if (k < m) {
+                run *= gg[k];
+                v[k] = fmaf(run, xout, v[k]);
+            }
+        }
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < M; ++k) {
+                const int p = p0 + k;
+                if (k < m && p < n) {
+                    if (p == 0 || p == n - 1) {
+                        if (r.dir) g[p] = r.T;
+                    } else {
+                        g[p] = v[k];
+                    }
+                }
+            }
+        }
     }
-    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------- y/z sweeps
 
-__device__ __forceinline__ void cols_issue(const SweepTile& tile, const LineRule* __restrict__ rules,
-                                           const float* __restrict__ dens, float* buf, int lane)
-{
-    if (static_cast<uint32_t>(lane) >= tile.count) return;
-    const uint32_t n = rules[tile.rule].n;
-    const float* g = dens + tile.base + lane;
-    const size_t rs = tile.rs;
-    for (uint32_t j = 0; j < n; ++j) cp_async4(buf + j * 32 + lane, g + j * rs);
-}
+constexpr int kColsWarps = 16;
 
-__device__ __forceinline__ bool on_face(const SweepTile& tile, int lane)
+template <int M>
+__global__ void __launch_bounds__(kColsWarps * 32) k_sweep_cols(float* __restrict__ dens,
+                                                                const SweepTile* __restrict__ tiles, uint32_t ntiles,
+                                                                const LineRule* __restrict__ rules,
+                                                                const float2* __restrict__ tab, int apply_faces,
+                                                                const uint8_t* __restrict__ mask)
 {
-    if (tile.face & TILE_FACE_ALL) return true;
-    const uint32_t i = tile.i0 + static_cast<uint32_t>(lane);
-    return i == 0u || i + 1u == tile.nx;
-}
-
-__global__ void __launch_bounds__(256) k_sweep_cols(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
-                                                    uint32_t ntiles, const LineRule* __restrict__ rules,
-                                                    const float2* __restrict__ tab, int nmax, int apply_faces,
-                                                    const uint8_t* __restrict__ mask)
-{
-    extern __shared__ float sm[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-    float* bufs[2];
-    bufs[0] = sm + static_cast<size_t>(warp) * 2 * nmax * 32;
-    bufs[1] = bufs[0] + static_cast<size_t>(nmax) * 32;
-    const uint32_t step = gridDim.x * wpb;
-    uint32_t t = blockIdx.x * wpb + warp;
-    if (t < ntiles) cols_issue(tiles[t], rules, dens, bufs[0], lane);
-    cp_async_commit();
-    int k = 0;
-    for (; t < ntiles; t += step, k ^= 1) {
-        const uint32_t tn = t + step;
-        if (tn < ntiles) cols_issue(tiles[tn], rules, dens, bufs[k ^ 1], lane);
-        cp_async_commit();
-        cp_async_wait<1>();
+    __shared__ float sA[kColsWarps][32], sB[kColsWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const SweepTile tile = tiles[t];
         const LineRule r = rules[tile.rule];
-        if (static_cast<uint32_t>(lane) < tile.count && tile_on(r, mask)) {
-            const int n = static_cast<int>(r.n);
-            float* col = bufs[k] + lane;
-            float* g = dens + tile.base + lane;
-            const size_t rs = tile.rs;
-            if (apply_faces && (tile.face & TILE_FACE) && on_face(tile, lane)) {
-                // applyDirichletBC fused: the whole line lies on a Dirichlet face
-                for (int j = 0; j < n; ++j) g[j * rs] = r.T;
-            } else {
-                solve_line(col, 32, r, tab + r.tab);
-                for (int j = 0; j < n; ++j) g[j * rs] = col[j * 32];
+        if (!tile_on(r, mask)) continue;   // uniform over the CTA
+        const int n = static_cast<int>(r.n);
+        const int m = static_cast<int>(cols_chunk(r.n));
+        const int W = (n + m - 1) / m;
+        const bool col_ok = lane < static_cast<int>(tile.count);
+        const bool face = apply_faces && (tile.face & TILE_FACE) && on_face(tile, lane);
+        const bool work = col_ok && !face && w < W;
+        float* col = dens + tile.base + lane;
+        const size_t rs = tile.rs;
+        const float2* tb = tab + r.tab;
+        const int p0 = w * m;
+        float v[M], gg[M];
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            const int p = p0 + k;
+            float x = 0.f, gk = 0.f, iv = 0.f;
+            if (k < m && work && p < n) {
+                x = col[p * rs];
+                const float2 e = __ldg(&tb[p]);
+                gk = -e.x;
+                iv = e.y;
+            }
+            const float f = (p == 1 || p == n - 2) ? r.fold : 0.f;
+            v[k] = (x + f) * iv;
+            gg[k] = gk;
+        }
+        float d = 0.f, A = 1.f;
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            if (k < m) {
+                d = fmaf(gg[k], d, v[k]);
+                A *= gg[k];
+                v[k] = d;
             }
         }
+        sA[w][lane] = A;
+        sB[w][lane] = d;
+        __syncthreads();
+        float din = 0.f;
+        for (int q = 0; q < w && q < W; ++q) din = fmaf(sA[q][lane], din, sB[q][lane]);
+        __syncthreads();
+        float run = 1.f;
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            if (k < m) {
+                run *= gg[k];
+                v[k] = fmaf(run, din, v[k]);
+            }
+        }
+        float x = 0.f;
+        A = 1.f;
+#pragma unroll
+        for (int k = M - 1; k >= 0; --k) {
+            if (k < m) {
+                x = fmaf(gg[k], x, v[k]);
+                A *= gg[k];
+                v[k] = x;
+            }
+        }
+        sA[w][lane] = A;
+        sB[w][lane] = x;
+        __syncthreads();
+        float xout = 0.f;
+        for (int q = W - 1; q > w; --q) xout = fmaf(sA[q][lane], xout, sB[q][lane]);
+        run = 1.f;
+#pragma unroll
+        for (int k = M - 1; k >= 0; --k) {
+            if (k < m) {
+                run *= gg[k];
+                v[k] = fmaf(run, xout, v[k]);
+            }
+        }
+        if (col_ok && w < W) {
+#pragma unroll
+            for (int k = 0; k < M; ++k) {
+                const int p = p0 + k;
+                if (k < m && p < n) {
+                    if (face) {
+                        col[p * rs] = r.T;   // applyDirichletBC fused: the line lies on a face
+                    } else if (p == 0 || p == n - 1) {
+                        if (r.dir) col[p * rs] = r.T;
+                    } else {
+                        col[p * rs] = v[k];
+                    }
+                }
+            }
+        }
+        __syncthreads();
     }
-    cp_async_wait<0>();
 }
 
 // ------------------------------------------------------- any line length
@@ -275,55 +378,52 @@ __global__ void k_gradients(const float* __restrict__ dens, float* __restrict__ 
 
 // ------------------------------------------------------------- launchers
 
-size_t sweep_rows_smem(int lines, int nmax) { return 2u * static_cast<size_t>(lines) * (nmax | 1) * sizeof(float); }
-size_t sweep_cols_smem(int warps, int nmax) { return 2u * static_cast<size_t>(warps) * nmax * 32 * sizeof(float); }
-
-// The attribute is per kernel, shared by every object in the process, so it
-// is always raised to the device's opt-in maximum (never lowered).
-static cudaError_t allow_max_smem(const void* fn)
-{
-    int dev = 0, optin = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    return e;
-}
-cudaError_t sweep_rows_prepare(int lines, int nmax)
-{
-    if (sweep_rows_smem(lines, nmax) > 232448) return cudaErrorInvalidValue;
-    return allow_max_smem(reinterpret_cast<const void*>(k_sweep_rows));
-}
-cudaError_t sweep_cols_prepare(int warps, int nmax)
-{
-    if (sweep_cols_smem(warps, nmax) > 232448) return cudaErrorInvalidValue;
-    return allow_max_smem(reinterpret_cast<const void*>(k_sweep_cols));
-}
-int sweep_rows_occupancy(int lines, int nmax)
+template <int M>
+static int occ_x(int block)
 {
     int b = 0;
-    if (sweep_rows_prepare(lines, nmax) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep_rows, lines, sweep_rows_smem(lines, nmax)) !=
-        cudaSuccess)
-        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep_x<M>, block, 0) != cudaSuccess) return 0;
     return b;
 }
-int sweep_cols_occupancy(int warps, int nmax)
+template <int M>
+static int occ_cols()
 {
     int b = 0;
-    if (sweep_cols_prepare(warps, nmax) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep_cols, warps * 32, sweep_cols_smem(warps, nmax)) !=
-        cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep_cols<M>, kColsWarps * 32, 0) != cudaSuccess)
         return 0;
     return b;
 }
 
-cudaError_t launch_sweep_rows(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                              const LineRule* rules, const float2* tab, int nmax, const uint8_t* mask, RowsCfg cfg)
+int sweep_x_occupancy(int nmax, int block)
+{
+    switch (x_chunk_template(static_cast<uint32_t>(nmax))) {
+        case 4: return occ_x<4>(block);
+        case 8: return occ_x<8>(block);
+        case 16: return occ_x<16>(block);
+        default: return 0;
+    }
+}
+
+int sweep_cols_occupancy(int nmax)
+{
+    switch (cols_chunk_template(static_cast<uint32_t>(nmax))) {
+        case 8: return occ_cols<8>();
+        case 16: return occ_cols<16>();
+        case 32: return occ_cols<32>();
+        default: return 0;
+    }
+}
+
+cudaError_t launch_sweep_x(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
+                           const LineRule* rules, const float2* tab, int nmax, const uint8_t* mask, RowsCfg cfg)
 {
     if (ntiles == 0) return cudaSuccess;
-    const int pmax = nmax | 1;
-    k_sweep_rows<<<cfg.grid, cfg.lines, sweep_rows_smem(cfg.lines, nmax), st>>>(dens, tiles, ntiles, rules, tab, pmax,
-                                                                                  mask);
+    switch (x_chunk_template(static_cast<uint32_t>(nmax))) {
+        case 4: k_sweep_x<4><<<cfg.grid, cfg.block, 0, st>>>(dens, tiles, ntiles, rules, tab, mask); break;
+        case 8: k_sweep_x<8><<<cfg.grid, cfg.block, 0, st>>>(dens, tiles, ntiles, rules, tab, mask); break;
+        case 16: k_sweep_x<16><<<cfg.grid, cfg.block, 0, st>>>(dens, tiles, ntiles, rules, tab, mask); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
@@ -332,8 +432,13 @@ cudaError_t launch_sweep_cols(cudaStream_t st, float* dens, const SweepTile* til
                               const uint8_t* mask, ColsCfg cfg)
 {
     if (ntiles == 0) return cudaSuccess;
-    k_sweep_cols<<<cfg.grid, cfg.warps * 32, sweep_cols_smem(cfg.warps, nmax), st>>>(dens, tiles, ntiles, rules, tab,
-                                                                                       nmax, apply_faces, mask);
+    const int b = kColsWarps * 32;
+    switch (cols_chunk_template(static_cast<uint32_t>(nmax))) {
+        case 8: k_sweep_cols<8><<<cfg.grid, b, 0, st>>>(dens, tiles, ntiles, rules, tab, apply_faces, mask); break;
+        case 16: k_sweep_cols<16><<<cfg.grid, b, 0, st>>>(dens, tiles, ntiles, rules, tab, apply_faces, mask); break;
+        case 32: k_sweep_cols<32><<<cfg.grid, b, 0, st>>>(dens, tiles, ntiles, rules, tab, apply_faces, mask); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -87,22 +87,43 @@ enum : uint8_t { STEP_DIFFUSE = 1u, STEP_MECH = 2u };
 // ---------------------------------------------------------------- launchers
 // All launchers enqueue on 'st' and return the CUDA launch status.
 
-struct RowsCfg { int lines; int grid; };     // x sweep: lines per CTA tile, CTAs
-struct ColsCfg { int warps; int grid; };     // y/z sweeps: warps (tiles) per CTA, CTAs
+struct RowsCfg { int block; int grid; };    // x sweep: threads per CTA (one tile per warp), CTAs
+struct ColsCfg { int grid; };               // y/z sweeps: CTAs of 16 warps (one tile per CTA)
 
-size_t sweep_rows_smem(int lines, int nmax);
-size_t sweep_cols_smem(int warps, int nmax);
-cudaError_t sweep_rows_prepare(int lines, int nmax);   // opt into large dynamic SMEM
-cudaError_t sweep_cols_prepare(int warps, int nmax);
-int sweep_rows_occupancy(int lines, int nmax);         // resident CTAs per SM
-int sweep_cols_occupancy(int warps, int nmax);
+// Chunking of a line, a function of its length only (so results do not
+// depend on what shares a launch).
+//   x:   S lanes of one warp per line (8, 16 or 32), chunks of ceil(n / S)
+//   y/z: chunks of max(4, ceil(n / 16)) rows, one per warp of the CTA
+__host__ __device__ inline uint32_t x_seg_lanes(uint32_t n) { return n <= 32 ? 8u : (n <= 64 ? 16u : 32u); }
+__host__ __device__ inline uint32_t x_lines_per_tile(uint32_t n) { return 32u / x_seg_lanes(n); }
+__host__ __device__ inline uint32_t cols_chunk(uint32_t n)
+{
+    const uint32_t c = (n + 15) / 16;
+    return c < 4 ? 4u : c;
+}
+// register chunk capacity (template) for the longest line of a launch; 0 =
+// too long for the chunked kernels (handled one thread per line)
+inline int x_chunk_template(uint32_t nmax)
+{
+    const uint32_t m = (nmax + x_seg_lanes(nmax) - 1) / x_seg_lanes(nmax);
+    return m <= 4 ? 4 : (m <= 8 ? 8 : (m <= 16 ? 16 : 0));
+}
+inline int cols_chunk_template(uint32_t nmax)
+{
+    const uint32_t m = cols_chunk(nmax);
+    return m <= 8 ? 8 : (m <= 16 ? 16 : (m <= 32 ? 32 : 0));
+}
+constexpr uint32_t kChunkedMaxN = 512;
 
-cudaError_t launch_sweep_rows(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                              const LineRule* rules, const float2* tab, int nmax, const uint8_t* mask, RowsCfg cfg);
+int sweep_x_occupancy(int nmax, int block);   // resident CTAs per SM
+int sweep_cols_occupancy(int nmax);
+
+cudaError_t launch_sweep_x(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
+                           const LineRule* rules, const float2* tab, int nmax, const uint8_t* mask, RowsCfg cfg);
 cudaError_t launch_sweep_cols(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
                               const LineRule* rules, const float2* tab, int nmax, int apply_faces,
                               const uint8_t* mask, ColsCfg cfg);
-// Any line length: one thread per line, d' kept in place in global memory.
+// Any line length: one thread per line, d kept in place in global memory.
 cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
                                 const LineRule* rules, const float2* tab, int apply_faces, const uint8_t* mask,
                                 int grid);

@@ -131,9 +131,6 @@ void Tuner::save(const std::string& path)
 
 // ------------------------------------------------------------------ diffusion
 
-static constexpr int kRowsMaxN = 768;   // longest x line staged in shared memory
-static constexpr int kColsMaxN = 512;   // longest y/z line staged in shared memory
-static constexpr size_t kSmemTarget = 110 * 1024;   // default: two CTAs per SM
 
 static uint32_t axis_n(const pcg_grid_params& g, int a) { return a == 0 ? g.nx : (a == 1 ? g.ny : g.nz); }
 static float axis_h(const pcg_grid_params& g, int a) { return a == 0 ? g.dx : (a == 1 ? g.dy : g.dz); }
@@ -236,30 +233,31 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
     PCG_CU(ctx, faces.alloc(std::max<size_t>(fj.size(), 1) * sizeof(FaceJob)));
     if (!fj.empty()) PCG_CU(ctx, cudaMemcpy(faces.p, fj.data(), fj.size() * sizeof(FaceJob), cudaMemcpyHostToDevice));
     for (int a = 0; a < 3; ++a) {
-        PCG_TRY(build_axis(a, 128));
+        PCG_TRY(build_axis(a));
         PCG_TRY(default_configs(a));
     }
     return PCG_OK;
 }
 
-// Tile lists of one axis.  rows_lines = lines per row tile (x axis).
-int Diffusion::build_axis(int axis, int rows_lines)
+// Tile lists of one axis: lines up to kChunkedMaxN go to the chunked
+// kernels (x: x_lines_per_tile(n) lines per warp tile; y/z: 32 columns per
+// CTA tile), longer lines to the one-thread-per-line kernel.
+int Diffusion::build_axis(int axis)
 {
-    std::vector<SweepTile> smem_t, glob_t;
-    int smem_nmax = 0, glob_nmax = 0;
-    uint64_t smem_lines = 0, glob_lines = 0;
-    const int kind_smem = axis == 0 ? 0 : 1;
-    const int maxn = axis == 0 ? kRowsMaxN : kColsMaxN;
+    std::vector<SweepTile> fast_t, glob_t;
+    int fast_nmax = 0, glob_nmax = 0;
+    uint64_t fast_lines = 0, glob_lines = 0;
+    const int kind_fast = axis == 0 ? 0 : 1;
     for (size_t i = 0; i < inst.size(); ++i) {
         const DiffInstance& d = inst[i];
         const pcg_grid_params& g = d.g;
         const int nd = d.ndim();
         if (axis == 2 && nd < 3) continue;
         const uint32_t n = axis_n(g, axis);
-        const bool use_smem = static_cast<int>(n) <= maxn;
-        auto& out = use_smem ? smem_t : glob_t;
-        int& nmax = use_smem ? smem_nmax : glob_nmax;
-        uint64_t& nl = use_smem ? smem_lines : glob_lines;
+        const bool fast = n <= kChunkedMaxN;
+        auto& out = fast ? fast_t : glob_t;
+        int& nmax = fast ? fast_nmax : glob_nmax;
+        uint64_t& nl = fast ? fast_lines : glob_lines;
         nmax = std::max<int>(nmax, static_cast<int>(n));
         const bool final_axis = axis == nd - 1;
         for (uint32_t s = 0; s < g.n_substrates; ++s) {
@@ -268,7 +266,7 @@ int Diffusion::build_axis(int axis, int rows_lines)
             const uint64_t sbase = d.dens_off + s * d.pitch;
             if (axis == 0) {
                 const uint64_t lines = static_cast<uint64_t>(g.ny) * g.nz;
-                const uint32_t L = use_smem ? static_cast<uint32_t>(rows_lines) : 32u;
+                const uint32_t L = fast ? x_lines_per_tile(n) : 32u;
                 for (uint64_t l0 = 0; l0 < lines; l0 += L) {
                     SweepTile t{};
                     t.base = sbase + l0 * g.nx;
@@ -306,31 +304,21 @@ int Diffusion::build_axis(int axis, int rows_lines)
     }
     // larger lines first so the persistent loop ends evenly
     auto by_n = [&](const SweepTile& a, const SweepTile& b) { return h_rules_[a.rule].n > h_rules_[b.rule].n; };
-    std::stable_sort(smem_t.begin(), smem_t.end(), by_n);
+    std::stable_sort(fast_t.begin(), fast_t.end(), by_n);
     std::stable_sort(glob_t.begin(), glob_t.end(), by_n);
     std::vector<SweepList>& ls = lists[axis];
-    // keep existing launch configs when rebuilding
-    RowsCfg keep_rc{rows_lines, 1};
-    ColsCfg keep_cc{4, 1};
-    for (auto& l : ls) {
-        if (l.kind == 0) keep_rc = l.rc;
-        if (l.kind == 1) keep_cc = l.cc;
-    }
     ls.clear();
     ls.resize(2);
-    ls[0].kind = kind_smem;
-    ls[0].nmax = smem_nmax;
-    ls[0].n = static_cast<uint32_t>(smem_t.size());
-    ls[0].lines = smem_lines;
-    ls[0].rc = keep_rc;
-    ls[0].rc.lines = rows_lines;
-    ls[0].cc = keep_cc;
+    ls[0].kind = kind_fast;
+    ls[0].nmax = fast_nmax;
+    ls[0].n = static_cast<uint32_t>(fast_t.size());
+    ls[0].lines = fast_lines;
     ls[1].kind = 2;
     ls[1].nmax = glob_nmax;
     ls[1].n = static_cast<uint32_t>(glob_t.size());
     ls[1].lines = glob_lines;
     for (int q = 0; q < 2; ++q) {
-        const auto& v = q == 0 ? smem_t : glob_t;
+        const auto& v = q == 0 ? fast_t : glob_t;
         PCG_CU(ctx, ls[q].tiles.alloc(std::max<size_t>(v.size(), 1) * sizeof(SweepTile)));
         if (!v.empty())
             PCG_CU(ctx, cudaMemcpy(ls[q].tiles.p, v.data(), v.size() * sizeof(SweepTile), cudaMemcpyHostToDevice));
@@ -338,27 +326,34 @@ int Diffusion::build_axis(int axis, int rows_lines)
     return PCG_OK;
 }
 
+// Launch shape of one list: 'param' is the x kernel's CTA size or the
+// y/z kernel's CTAs per SM (0 = as many as fit).
+int Diffusion::config_list(SweepList& l, int param)
+{
+    if (l.n == 0) return PCG_OK;
+    if (l.kind == 0) {
+        const int block = param > 0 ? param : 256;
+        const int occ = sweep_x_occupancy(l.nmax, block);
+        if (occ <= 0) return fail(ctx, PCG_ERR_INVALID, "x sweep launch does not fit");
+        const uint64_t warps = static_cast<uint64_t>(block / 32);
+        const uint64_t ctas = (l.n + warps - 1) / warps;
+        l.rc.block = block;
+        l.rc.grid = static_cast<int>(std::min<uint64_t>(ctas, static_cast<uint64_t>(occ) * ctx->sms));
+    } else if (l.kind == 1) {
+        const int occ = sweep_cols_occupancy(l.nmax);
+        if (occ <= 0) return fail(ctx, PCG_ERR_INVALID, "column sweep launch does not fit");
+        const int per_sm = param > 0 ? std::min(param, occ) : occ;
+        l.cc.grid = static_cast<int>(std::min<uint64_t>(l.n, static_cast<uint64_t>(per_sm) * ctx->sms));
+    } else {
+        const uint64_t ctas = (static_cast<uint64_t>(l.n) * 32 + 127) / 128;
+        l.ggrid = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(ctas, 1), static_cast<uint64_t>(ctx->sms) * 16));
+    }
+    return PCG_OK;
+}
+
 int Diffusion::default_configs(int axis)
 {
-    for (auto& l : lists[axis]) {
-        if (l.n == 0) continue;
-        if (l.kind == 0) {
-            int occ = sweep_rows_occupancy(l.rc.lines, l.nmax);
-            if (occ <= 0) return fail(ctx, PCG_ERR_INVALID, "x sweep tile does not fit shared memory");
-            l.rc.grid = static_cast<int>(std::min<uint64_t>(l.n, static_cast<uint64_t>(occ) * ctx->sms));
-        } else if (l.kind == 1) {
-            int w = l.cc.warps;
-            while (w > 1 && sweep_cols_smem(w, l.nmax) > kSmemTarget) w >>= 1;
-            l.cc.warps = w;
-            int occ = sweep_cols_occupancy(w, l.nmax);
-            if (occ <= 0) return fail(ctx, PCG_ERR_INVALID, "column sweep tile does not fit shared memory");
-            const uint64_t ctas = (l.n + w - 1) / w;
-            l.cc.grid = static_cast<int>(std::min<uint64_t>(ctas, static_cast<uint64_t>(occ) * ctx->sms));
-        } else {
-            const uint64_t ctas = (static_cast<uint64_t>(l.n) * 32 + 127) / 128;
-            l.ggrid = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(ctas, 1), static_cast<uint64_t>(ctx->sms) * 16));
-        }
-    }
+    for (auto& l : lists[axis]) PCG_TRY(config_list(l, 0));
     return PCG_OK;
 }
 
@@ -370,7 +365,7 @@ int Diffusion::launch_list(const SweepList& l, bool fuse, const uint8_t* mask)
     const LineRule* r = rules.as<LineRule>();
     const float2* tb = tab.as<float2>();
     cudaError_t e;
-    if (l.kind == 0) e = launch_sweep_rows(ctx->stream, d, t, l.n, r, tb, l.nmax, mask, l.rc);
+    if (l.kind == 0) e = launch_sweep_x(ctx->stream, d, t, l.n, r, tb, l.nmax, mask, l.rc);
     else if (l.kind == 1) e = launch_sweep_cols(ctx->stream, d, t, l.n, r, tb, l.nmax, fuse ? 1 : 0, mask, l.cc);
     else e = launch_sweep_global(ctx->stream, d, t, l.n, r, tb, fuse ? 1 : 0, mask, l.ggrid);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep launch");
@@ -492,8 +487,8 @@ std::string Diffusion::describe() const
         for (const auto& l : lists[a]) {
             if (l.n == 0) continue;
             o << ax[a] << ":";
-            if (l.kind == 0) o << "rows(L=" << l.rc.lines << ",grid=" << l.rc.grid;
-            else if (l.kind == 1) o << "cols(warps=" << l.cc.warps << ",grid=" << l.cc.grid;
+            if (l.kind == 0) o << "x-chunked(block=" << l.rc.block << ",grid=" << l.rc.grid;
+            else if (l.kind == 1) o << "cols-chunked(grid=" << l.cc.grid;
             else o << "global(grid=" << l.ggrid;
             o << ",tiles=" << l.n << ",nmax=" << l.nmax << ") ";
         }
@@ -530,60 +525,29 @@ int Diffusion::tune()
     };
     int rc = PCG_OK;
     for (int a = 0; a < 3 && rc == PCG_OK; ++a) {
-        // x axis: lines per tile (changes the tile list)
-        if (lists[a].size() && lists[a][0].n > 0 && lists[a][0].kind == 0) {
-            const std::string key = "rows:n" + std::to_string(lists[a][0].nmax) + ":l" +
-                                    std::to_string(bucket(lists[a][0].lines));
-            int best = 0;
-            if (!Tuner::get().lookup(key, &best)) {
-                float best_ms = 1e30f;
-                for (int L : {32, 64, 128, 256}) {
-                    if (sweep_rows_smem(L, lists[a][0].nmax) > static_cast<size_t>(ctx->smem_optin)) continue;
-                    rc = build_axis(a, L);
-                    if (rc == PCG_OK) rc = default_configs(a);
-                    if (rc != PCG_OK) break;
-                    float ms = 0;
-                    rc = time_list(lists[a][0], &ms);
-                    if (rc != PCG_OK) break;
-                    if (ms < best_ms) {
-                        best_ms = ms;
-                        best = L;
-                    }
-                }
+        SweepList& l = lists[a][0];
+        if (l.n == 0) continue;
+        const std::string key = std::string(l.kind == 0 ? "x" : "cols") + ":n" + std::to_string(l.nmax) + ":l" +
+                                std::to_string(bucket(l.lines));
+        int best = 0;
+        if (!Tuner::get().lookup(key, &best)) {
+            float best_ms = 1e30f;
+            const std::vector<int> cands = l.kind == 0 ? std::vector<int>{64, 128, 256} : std::vector<int>{1, 2, 3, 4, 0};
+            for (int c : cands) {
+                rc = config_list(l, c);
                 if (rc != PCG_OK) break;
-                Tuner::get().store(key, best);
-            }
-            rc = build_axis(a, best);
-            if (rc == PCG_OK) rc = default_configs(a);
-        }
-        // y/z axes: warps (column tiles) per CTA
-        if (rc == PCG_OK && lists[a].size() && lists[a][0].n > 0 && lists[a][0].kind == 1) {
-            SweepList& l = lists[a][0];
-            const std::string key = "cols:n" + std::to_string(l.nmax) + ":l" + std::to_string(bucket(l.lines));
-            int best = 0;
-            if (!Tuner::get().lookup(key, &best)) {
-                float best_ms = 1e30f;
-                for (int w : {1, 2, 4, 8}) {
-                    if (sweep_cols_smem(w, l.nmax) > static_cast<size_t>(ctx->smem_optin)) continue;
-                    const int occ = sweep_cols_occupancy(w, l.nmax);
-                    if (occ <= 0) continue;
-                    l.cc.warps = w;
-                    l.cc.grid = static_cast<int>(std::min<uint64_t>((l.n + w - 1) / w, static_cast<uint64_t>(occ) * ctx->sms));
-                    float ms = 0;
-                    rc = time_list(l, &ms);
-                    if (rc != PCG_OK) break;
-                    if (ms < best_ms) {
-                        best_ms = ms;
-                        best = w;
-                    }
-                }
+                float ms = 0;
+                rc = time_list(l, &ms);
                 if (rc != PCG_OK) break;
-                Tuner::get().store(key, best);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = c;
+                }
             }
-            const int occ = sweep_cols_occupancy(best, l.nmax);
-            l.cc.warps = best;
-            l.cc.grid = static_cast<int>(std::min<uint64_t>((l.n + best - 1) / best, static_cast<uint64_t>(std::max(occ, 1)) * ctx->sms));
+            if (rc != PCG_OK) break;
+            Tuner::get().store(key, best);
         }
+        rc = config_list(l, best);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

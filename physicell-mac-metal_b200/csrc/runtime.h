@@ -110,8 +110,8 @@ struct SweepList {
     int nmax = 0;
     uint32_t n = 0;
     DevBuf tiles;
-    RowsCfg rc{128, 1};
-    ColsCfg cc{4, 1};
+    RowsCfg rc{256, 1};
+    ColsCfg cc{1};
     int ggrid = 1;
     uint64_t lines = 0;        // lines covered (for tuning keys)
 };
@@ -145,8 +145,9 @@ public:
     std::string describe() const;
 
 private:
-    int build_axis(int axis, int rows_lines);
+    int build_axis(int axis);
     int default_configs(int axis);
+    int config_list(SweepList& l, int param);
     int launch_list(const SweepList& l, bool fuse_faces, const uint8_t* mask);
     std::vector<LineRule> h_rules_;
     std::vector<float2> h_tab_;

@@ -1,0 +1,178 @@
+// pcg_host.h — C++ drop-ins for the reference's Microenvironment and
+// CellMechanics classes (src/microenvironment.h:17-83,
+// src/cell_mechanics.h:15-87), implemented over the C ABI of include/pcg.h.
+//
+// The public methods keep the reference's names, arguments and meaning.
+// The configuration and cell store are template parameters so that the
+// reference's own SimConfig (src/config_parser.h:136-177) and CellData
+// (src/cell_data.h:19-244) plug in unchanged; pcg::SimConfig and
+// pcg::CellStore below carry just the members these classes read.
+//
+// Memory model.  The reference shares one buffer between CPU and GPU
+// (Apple UMA).  Here the state lives on the device and a host mirror is kept
+// for the calls that hand out host pointers (densityBuffer(), the CellData
+// block): a host pointer handed out marks the mirror as possibly written,
+// and the next device operation uploads it first.  Callers that stay on the
+// device path (step(), secreteAll()) never copy.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "pcg.h"
+
+namespace pcg {
+
+struct SubstrateConfig {
+    std::string name;
+    float diffusion_coeff = 0.0f;
+    float decay_rate = 0.0f;
+    float initial_value = 0.0f;
+    bool dirichlet_enabled = false;
+    float dirichlet_value = 0.0f;
+};
+
+struct SimConfig {
+    pcg_grid_params grid{};          // grid.dx / dy / dz are read
+    float x_min = 0, x_max = 0, y_min = 0, y_max = 0, z_min = 0, z_max = 0;
+    bool use_2D = true;
+    float dt_diffusion = 0.01f;
+    float dt_mechanics = 0.1f;
+    std::vector<SubstrateConfig> substrates;
+};
+
+// The GPU-shared part of CellData: 28 float/uint fields of max_cells each
+// (src/cell_data.cpp:101-180) plus the per-cell per-substrate rates.
+struct CellStore {
+    explicit CellStore(uint32_t max_cells, uint32_t n_substrates = 0);
+    uint32_t num_cells = 0;
+    uint32_t max_cells = 0;
+    uint32_t n_substrates = 0;
+    std::vector<float> block;        // [field * max_cells + cell]
+    float* position_x = nullptr;     // == block.data(), as in CellData
+    std::vector<double> secretion_rate, uptake_rate, saturation_density, net_export_rate;
+    std::vector<uint32_t> current_death_model;
+    float* field(int f) { return block.data() + static_cast<size_t>(f) * max_cells; }
+    uint32_t addCell();
+};
+
+class Error : public std::runtime_error {
+public:
+    Error(int status, const std::string& what) : std::runtime_error(what), status(status) {}
+    int status;
+};
+
+// Replaces MetalContext (src/metal_context.h:14-100).
+class Context {
+public:
+    explicit Context(int device = 0);
+    ~Context();
+    Context(const Context&) = delete;
+    Context& operator=(const Context&) = delete;
+    pcg_ctx* get() const { return ctx_; }
+    void waitForCompletion();
+    void check(int status) const;
+private:
+    pcg_ctx* ctx_ = nullptr;
+};
+
+class Microenvironment {
+public:
+    Microenvironment() = default;
+    ~Microenvironment();
+
+    template <class Config>
+    void initialize(const Config& config, Context* ctx);
+
+    // x, y (, z) sweeps on the device (microenvironment.mm:191-200)
+    void simulateDiffusionDecay();
+    // microenvironment.mm:212-237
+    void applyDirichletBC();
+    // One main-loop diffusion sub-step on the device: sweeps, Dirichlet reset
+    // and secretion of every active cell (main.mm:341-363).
+    template <class Cells>
+    void step(Cells& cells);
+    // processSecretion for all cells at once, ascending cell index per voxel
+    template <class Cells>
+    void secreteAll(Cells& cells, double dt);
+
+    float getDensity(uint32_t voxel_index, uint32_t substrate_index) const;
+    void setDensity(uint32_t voxel_index, uint32_t substrate_index, float value);
+    // microenvironment.mm:249-259 (single voxel, CPU formula, on the mirror)
+    void applySecretion(uint32_t voxel_index, uint32_t substrate_index, float secretion_rate, float uptake_rate,
+                        float saturation_density, float dt);
+
+    uint32_t numVoxels() const { return grid_.nx * grid_.ny * grid_.nz; }
+    uint32_t voxelIndex(float x, float y, float z) const;   // microenvironment.mm:261-269
+    pcg_grid_params getGridParams() const { return grid_; }
+
+    void computeGradients();
+    void getGradient(uint32_t voxel_index, uint32_t substrate_index, float& gx, float& gy, float& gz) const;
+    float* gradientX() { return gx_.data(); }
+    float* gradientY() { return gy_.data(); }
+    float* gradientZ() { return gz_.data(); }
+
+    // Host view of the density (read back from the device); writes through
+    // it reach the device before the next device operation.
+    float* densityBuffer();
+    const pcg_substrate_params* substrateParams() const { return subs_.data(); }
+    pcg_me* handle() const { return me_; }
+
+    // keeps the host mirror and the device consistent before a device call
+    void push_host_writes();
+private:
+    void pull();
+    Context* ctx_ = nullptr;
+    pcg_me* me_ = nullptr;
+    pcg_grid_params grid_{};
+    std::vector<pcg_substrate_params> subs_;
+    std::vector<float> mirror_, gx_, gy_, gz_;
+    bool mirror_valid_ = false, mirror_dirty_ = false;
+    friend class CellMechanics;
+};
+
+class CellMechanics {
+public:
+    CellMechanics() = default;
+    ~CellMechanics();
+
+    template <class Config>
+    void initialize(const Config& config, Context* ctx, uint32_t max_cells = 200000);
+
+    // clear/build/forces + integrate (cell_mechanics.mm:173-186)
+    template <class Cells>
+    void update(Cells& cells, float dt);
+    // bin + sort + cell-start table + forces (cell_mechanics.mm:188-200)
+    template <class Cells>
+    void computeForces(Cells& cells, float dt);
+    // AB2 + clamp (cell_mechanics.mm:202-209)
+    template <class Cells>
+    void integratePositions(Cells& cells, float dt);
+
+    uint32_t totalMechVoxels() const { return total_; }
+    const pcg_mechanics_params& params() const { return params_; }
+    uint32_t voxelIndexFromPosition(float px, float py, float pz) const;   // cell_mechanics.h:40-50
+    uint32_t voxelCellCount(uint32_t v) const;                             // cell_mechanics.h:53-56
+    const uint32_t* voxelCells(uint32_t v) const;                          // cell_mechanics.h:59-62
+    void syncHashPointers();                                               // cell_mechanics.mm:211-222
+
+    pcg_cells* device_cells() const { return cells_; }
+private:
+    template <class Cells>
+    void push(Cells& cells);
+    template <class Cells>
+    void pull(Cells& cells);
+    Context* ctx_ = nullptr;
+    pcg_mech* mech_ = nullptr;
+    pcg_cells* cells_ = nullptr;
+    pcg_mechanics_params params_{};
+    float ox_ = 0, oy_ = 0, oz_ = 0;
+    uint32_t total_ = 0, max_cells_ = 0, n_substrates_ = 0;
+    std::vector<uint32_t> start_, sorted_;
+};
+
+}  // namespace pcg
+
+#include "pcg_host_impl.h"

@@ -1,0 +1,138 @@
+// pcg_host_impl.h — template members of the host drop-ins (included by pcg_host.h).
+#pragma once
+
+#include <algorithm>
+#include <cstring>
+
+namespace pcg {
+
+// Device cell store shared by Microenvironment and CellMechanics for one
+// host cell block (the reference shares the CellData GPU block the same way).
+pcg_cells* device_store(Context* ctx, const void* host_block, uint32_t max_cells, uint32_t n_substrates);
+
+template <class Cells>
+inline const float* block_of(const Cells& c) { return c.position_x; }
+
+template <class Config>
+void Microenvironment::initialize(const Config& config, Context* ctx)
+{
+    ctx_ = ctx;
+    // microenvironment.mm:117-130: truncating voxel counts, nz = 1 in 2-D
+    grid_ = pcg_grid_params{};
+    grid_.nx = static_cast<uint32_t>((config.x_max - config.x_min) / config.grid.dx);
+    grid_.ny = static_cast<uint32_t>((config.y_max - config.y_min) / config.grid.dy);
+    grid_.nz = config.use_2D ? 1u : static_cast<uint32_t>((config.z_max - config.z_min) / config.grid.dz);
+    grid_.dx = config.grid.dx;
+    grid_.dy = config.grid.dy;
+    grid_.dz = config.grid.dz;
+    grid_.x_min = config.x_min;
+    grid_.y_min = config.y_min;
+    grid_.z_min = config.z_min;
+    grid_.dt = config.dt_diffusion;
+    grid_.n_substrates = static_cast<uint32_t>(config.substrates.size());
+    subs_.assign(grid_.n_substrates, pcg_substrate_params{});
+    std::vector<float> init(grid_.n_substrates);
+    for (uint32_t s = 0; s < grid_.n_substrates; ++s) {
+        subs_[s].diffusion_coefficient = config.substrates[s].diffusion_coeff;
+        subs_[s].decay_rate = config.substrates[s].decay_rate;
+        subs_[s].supply_rate = 0.0f;
+        subs_[s].target_value = config.substrates[s].dirichlet_value;
+        subs_[s].dirichlet_enabled = config.substrates[s].dirichlet_enabled ? 1u : 0u;
+        init[s] = config.substrates[s].initial_value;
+    }
+    ctx_->check(pcg_me_create(ctx_->get(), &grid_, subs_.data(), &me_));
+    if (grid_.n_substrates) ctx_->check(pcg_me_fill(me_, init.data()));
+    mirror_.assign(static_cast<size_t>(numVoxels()) * grid_.n_substrates, 0.0f);
+    mirror_valid_ = mirror_dirty_ = false;
+}
+
+template <class Cells>
+void Microenvironment::secreteAll(Cells& cells, double dt)
+{
+    push_host_writes();
+    pcg_cells* dc = device_store(ctx_, block_of(cells), cells.max_cells, grid_.n_substrates);
+    // the CPU owns the cell block: refresh the device copy and the rates
+    ctx_->check(pcg_cells_upload(dc, block_of(cells), cells.num_cells, cells.max_cells));
+    std::vector<uint8_t> active(cells.num_cells, 1);
+    for (uint32_t i = 0; i < cells.num_cells && i < cells.current_death_model.size(); ++i)
+        active[i] = cells.current_death_model[i] == 0 ? 1 : 0;   // main.mm:360
+    ctx_->check(pcg_cells_set_secretion(dc, cells.secretion_rate.data(), cells.uptake_rate.data(),
+                                        cells.saturation_density.data(), cells.net_export_rate.data(),
+                                        active.data()));
+    ctx_->check(pcg_me_secrete(me_, dc, dt));
+    mirror_valid_ = false;
+}
+
+template <class Cells>
+void Microenvironment::step(Cells& cells)
+{
+    simulateDiffusionDecay();
+    applyDirichletBC();
+    secreteAll(cells, static_cast<double>(grid_.dt));
+}
+
+template <class Config>
+void CellMechanics::initialize(const Config& config, Context* ctx, uint32_t max_cells)
+{
+    ctx_ = ctx;
+    // cell_mechanics.mm:115-130
+    const float vs = 30.0f;
+    params_ = pcg_mechanics_params{};
+    params_.dt = config.dt_mechanics;
+    params_.cell_cell_repulsion = 10.0f;
+    params_.cell_cell_adhesion = 0.4f;
+    params_.max_interaction_distance = vs;
+    params_.mechanics_voxel_size = vs;
+    params_.mech_grid_nx = std::max(1u, static_cast<uint32_t>((config.x_max - config.x_min) / vs));
+    params_.mech_grid_ny = std::max(1u, static_cast<uint32_t>((config.y_max - config.y_min) / vs));
+    params_.mech_grid_nz = config.use_2D ? 1u : std::max(1u, static_cast<uint32_t>((config.z_max - config.z_min) / vs));
+    total_ = params_.mech_grid_nx * params_.mech_grid_ny * params_.mech_grid_nz;
+    ox_ = config.x_min;
+    oy_ = config.y_min;
+    oz_ = config.z_min;
+    max_cells_ = max_cells;
+    n_substrates_ = static_cast<uint32_t>(config.substrates.size());
+    ctx_->check(pcg_mech_create(ctx_->get(), &params_, ox_, oy_, oz_, max_cells_, &mech_));
+}
+
+template <class Cells>
+void CellMechanics::push(Cells& cells)
+{
+    cells_ = device_store(ctx_, block_of(cells), cells.max_cells, n_substrates_);
+    ctx_->check(pcg_cells_upload(cells_, block_of(cells), cells.num_cells, cells.max_cells));
+}
+
+template <class Cells>
+void CellMechanics::pull(Cells& cells)
+{
+    ctx_->check(pcg_cells_download(cells_, const_cast<float*>(block_of(cells)), cells.max_cells));
+}
+
+template <class Cells>
+void CellMechanics::computeForces(Cells& cells, float)
+{
+    if (cells.num_cells == 0) return;
+    push(cells);
+    ctx_->check(pcg_mech_forces(mech_, cells_));
+    pull(cells);
+}
+
+template <class Cells>
+void CellMechanics::integratePositions(Cells& cells, float dt)
+{
+    if (cells.num_cells == 0) return;
+    push(cells);
+    ctx_->check(pcg_mech_integrate(mech_, cells_, dt));
+    pull(cells);
+}
+
+template <class Cells>
+void CellMechanics::update(Cells& cells, float dt)
+{
+    if (cells.num_cells == 0) return;
+    push(cells);
+    ctx_->check(pcg_mech_update(mech_, cells_, dt));
+    pull(cells);
+}
+
+}  // namespace pcg
