@@ -324,7 +324,7 @@ def main():
 
     # end to end through the C ABI with pinned host buffers
     n_soa = 28 * cells
-    _, _, arena = batch.layout(0)
+    arena = batch.layout(0)[3]
     soa_h = pcg.PinnedArray((n_soa,))
     soa_out = pcg.PinnedArray((n_soa,))
     dens_out = pcg.PinnedArray((arena,))

@@ -37,7 +37,8 @@ enum {
     PCG_ERR_NO_DEVICE = 4,   /* no usable CUDA device */
     PCG_ERR_BUDGET = 5,      /* request does not fit the serving memory budget */
     PCG_ERR_NOT_FOUND = 6,   /* unknown request id */
-    PCG_ERR_NOT_READY = 7    /* request not finished yet */
+    PCG_ERR_NOT_READY = 7,   /* request not finished yet */
+    PCG_ERR_DEVICE = 8       /* a kernel stopped early (bounded wait ran out, unaligned copy refused) */
 };
 
 /* Same layout as GridParams (shaders/types.h:23-37). */
@@ -90,7 +91,8 @@ pcg_status pcg_create(int device, pcg_ctx** out);
 /* Use an existing CUDA stream (cudaStream_t passed as void*). */
 pcg_status pcg_create_on_stream(int device, void* stream, pcg_ctx** out);
 pcg_status pcg_destroy(pcg_ctx* ctx);
-/* MetalContext::waitForCompletion (metal_context.mm:448-461). */
+/* MetalContext::waitForCompletion (metal_context.mm:448-461); also reports
+ * PCG_ERR_DEVICE when a kernel stopped early since the last sync. */
 pcg_status pcg_sync(pcg_ctx* ctx);
 void* pcg_stream(pcg_ctx* ctx);
 const char* pcg_last_error_string(const pcg_ctx* ctx);
@@ -131,9 +133,10 @@ pcg_status pcg_me_step(pcg_me* me, pcg_cells* cells, int n_steps);
 /* Microenvironment::computeGradients + read-back (microenvironment.mm:282-342):
  * three arrays of nx*ny*nz*S floats (any may be NULL). */
 pcg_status pcg_me_gradients(pcg_me* me, float* gx, float* gy, float* gz, size_t n_floats);
-/* Device pointer of the density block and the element pitch between
- * substrates (>= nx*ny*nz). */
-pcg_status pcg_me_device_density(pcg_me* me, float** dptr, size_t* substrate_pitch);
+/* Device pointer of the density block.  On the device, rows of x are
+ * row_pitch floats apart (nx rounded up to 4, so rows start on 16 bytes)
+ * and substrates substrate_pitch floats apart. */
+pcg_status pcg_me_device_density(pcg_me* me, float** dptr, size_t* row_pitch, size_t* substrate_pitch);
 
 /* ------------------------------------------------------------------------
  * Cells — the GPU-shared block of CellData (src/cell_data.h:19-244).
@@ -239,8 +242,8 @@ pcg_status pcg_batch_upload_cells(pcg_batch* batch, uint32_t instance, const flo
 pcg_status pcg_batch_upload_all_cells(pcg_batch* batch, const float* soa, uint64_t n_floats);
 pcg_status pcg_batch_download_all_cells(pcg_batch* batch, float* soa, uint64_t n_floats);
 pcg_status pcg_batch_download_all_density(pcg_batch* batch, float* host, uint64_t n_floats);
-pcg_status pcg_batch_density_layout(pcg_batch* batch, uint32_t instance, uint64_t* offset, uint64_t* substrate_pitch,
-                                    uint64_t* arena_floats);
+pcg_status pcg_batch_density_layout(pcg_batch* batch, uint32_t instance, uint64_t* offset, uint64_t* row_pitch,
+                                    uint64_t* substrate_pitch, uint64_t* arena_floats);
 /* Totals: voxels (sum nx*ny*nz), voxel-substrates, cells. */
 pcg_status pcg_batch_totals(pcg_batch* batch, uint64_t* voxels, uint64_t* voxel_substrates, uint64_t* cells);
 /* Kernel launches one main-loop sub-step issues: without / with a

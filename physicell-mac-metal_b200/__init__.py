@@ -117,7 +117,7 @@ _SIGS = [
     ("pcg_me_secrete", C.c_int, [_P, _P, C.c_double]),
     ("pcg_me_step", C.c_int, [_P, _P, C.c_int]),
     ("pcg_me_gradients", C.c_int, [_P, _F32P, _F32P, _F32P, C.c_size_t]),
-    ("pcg_me_device_density", C.c_int, [_P, C.POINTER(_F32P), C.POINTER(C.c_size_t)]),
+    ("pcg_me_device_density", C.c_int, [_P, C.POINTER(_F32P), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("pcg_cells_create", C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
     ("pcg_cells_destroy", C.c_int, [_P]),
     ("pcg_cells_upload", C.c_int, [_P, _F32P, C.c_uint32, C.c_uint32]),
@@ -149,7 +149,7 @@ _SIGS = [
     ("pcg_batch_download_all_cells", C.c_int, [_P, _F32P, C.c_uint64]),
     ("pcg_batch_download_all_density", C.c_int, [_P, _F32P, C.c_uint64]),
     ("pcg_batch_density_layout", C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
-                                           C.POINTER(C.c_uint64)]),
+                                           C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_batch_totals", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_batch_step_launches", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_batch_phase_times", C.c_int, [_P, _F32P, C.POINTER(C.c_uint64), C.c_int]),
@@ -535,9 +535,11 @@ class Batch:
         return v.value, vs.value, c.value
 
     def layout(self, i):
-        off, pitch, arena = C.c_uint64(), C.c_uint64(), C.c_uint64()
-        self.ctx.check(lib().pcg_batch_density_layout(self.h, i, C.byref(off), C.byref(pitch), C.byref(arena)))
-        return off.value, pitch.value, arena.value
+        """(offset, row_pitch, substrate_pitch, arena_floats) of instance i's density on the device."""
+        off, rp, pitch, arena = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self.ctx.check(lib().pcg_batch_density_layout(self.h, i, C.byref(off), C.byref(rp), C.byref(pitch),
+                                                      C.byref(arena)))
+        return off.value, rp.value, pitch.value, arena.value
 
     def upload_all_cells(self, soa):
         self.ctx.check(lib().pcg_batch_upload_all_cells(self.h, _f32(soa), soa.size))

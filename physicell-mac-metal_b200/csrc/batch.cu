@@ -86,7 +86,7 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
             for (uint32_t s = 0; s < de.g.n_substrates; ++s)
                 PCG_CU(ctx, cudaMemcpyAsync(d.dens.as<float>() + de.dens_off + s * de.pitch,
                                             ds->batch->d.dens.as<float>() + so.dens_off + s * so.pitch,
-                                            de.nvox() * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
+                                            de.rows() * de.px * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
         } else if (descs[i].initial_density) {
             PCG_TRY(d.upload(i, descs[i].initial_density));
         } else if (descs[i].initial_values) {
@@ -393,10 +393,12 @@ pcg_status pcg_batch_download_all_density(pcg_batch* b, float* host, uint64_t n_
     return PCG_OK;
 }
 
-pcg_status pcg_batch_density_layout(pcg_batch* b, uint32_t i, uint64_t* off, uint64_t* pitch, uint64_t* arena)
+pcg_status pcg_batch_density_layout(pcg_batch* b, uint32_t i, uint64_t* off, uint64_t* row_pitch, uint64_t* pitch,
+                                    uint64_t* arena)
 {
     if (!b || i >= b->b.d.inst.size()) return PCG_ERR_INVALID;
     if (off) *off = b->b.d.inst[i].dens_off;
+    if (row_pitch) *row_pitch = b->b.d.inst[i].px;
     if (pitch) *pitch = b->b.d.inst[i].pitch;
     if (arena) *arena = b->b.d.dens_elems;
     return PCG_OK;

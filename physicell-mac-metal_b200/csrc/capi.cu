@@ -133,6 +133,12 @@ static pcg_status create_ctx(int device, void* stream, pcg_ctx** out)
         }
         c->own_stream = true;
     }
+    if (cudaMalloc(&c->status, sizeof(unsigned)) != cudaSuccess || cudaMemset(c->status, 0, sizeof(unsigned)) != cudaSuccess) {
+        g_create_err = "status word allocation failed";
+        if (c->own_stream) cudaStreamDestroy(c->stream);
+        delete c;
+        return PCG_ERR_OOM;
+    }
     *out = c;
     return PCG_OK;
 }
@@ -147,6 +153,7 @@ pcg_status pcg_destroy(pcg_ctx* ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->status) cudaFree(ctx->status);
     delete ctx;
     return PCG_OK;
 }
@@ -155,6 +162,13 @@ pcg_status pcg_sync(pcg_ctx* ctx)
 {
     if (!ctx) return PCG_ERR_INVALID;
     PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    unsigned st = 0;
+    PCG_CU(ctx, cudaMemcpy(&st, ctx->status, sizeof st, cudaMemcpyDeviceToHost));
+    if (st) {
+        PCG_CU(ctx, cudaMemset(ctx->status, 0, sizeof st));
+        return fail(ctx, PCG_ERR_DEVICE, std::string("a kernel stopped early:") + ((st & PCG_DEV_TIMEOUT) ? " wait limit reached" : "") +
+                                              ((st & PCG_DEV_ALIGN) ? " unaligned bulk copy refused" : ""));
+    }
     return PCG_OK;
 }
 
@@ -286,11 +300,12 @@ pcg_status pcg_me_gradients(pcg_me* me, float* gx, float* gy, float* gz, size_t 
     return PCG_OK;
 }
 
-pcg_status pcg_me_device_density(pcg_me* me, float** dptr, size_t* pitch)
+pcg_status pcg_me_device_density(pcg_me* me, float** dptr, size_t* row_pitch, size_t* substrate_pitch)
 {
     if (!me) return PCG_ERR_INVALID;
     if (dptr) *dptr = me->d.dens.as<float>();
-    if (pitch) *pitch = me->d.inst[0].pitch;
+    if (row_pitch) *row_pitch = me->d.inst[0].px;
+    if (substrate_pitch) *substrate_pitch = me->d.inst[0].pitch;
     return PCG_OK;
 }
 

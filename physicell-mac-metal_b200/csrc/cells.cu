@@ -87,8 +87,10 @@ __global__ void k_secrete(float* __restrict__ dens, const uint32_t* __restrict__
     if (mask && !(mask[ii] & STEP_DIFFUSE)) return;
     const CellInst& in = insts[ii];
     const uint32_t v = key - in.vox_base;
+    // dense voxel index -> padded-row device offset
+    const uint64_t off = static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
     for (uint32_t s = 0; s < in.S; ++s) {
-        float* d = dens + in.dens_off + s * in.sub_pitch + v;
+        float* d = dens + in.dens_off + s * in.sub_pitch + off;
         float rho32 = *d;
         for (uint32_t q = p; q < q_end; ++q) {
             const uint32_t g = sorder[q];

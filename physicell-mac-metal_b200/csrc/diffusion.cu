@@ -9,25 +9,28 @@
 // The solve.  Every line of one (instance, substrate, axis) family has the
 // same matrix, so g_i = c / den_i and 1 / den_i are one table (LineRule,
 // built in FP64 on the host).  With h_i = (rho_i + fold_i) / den_i the
-// reference's forward and backward passes are two first-order linear
-// recurrences with the same coefficients:
+// reference's two passes are
 //     forward   d_i = g_i d_{i-1} + h_i        (d_0 = 0)
 //     backward  x_i = g_i x_{i+1} + d_i        (x_{n-1} = 0)
-// End nodes (and padding) have g = h = 0, so they are transparent; they
-// keep their value, or take the Dirichlet target.  A line is cut into
-// chunks held in registers: each thread runs both recurrences over its
-// chunk, and the chunks are joined by an exclusive scan of affine maps
-// (x -> A x + B), forward for d and in reverse for x.  Every value is read
-// from HBM once and written once per sweep; nothing is staged in shared
-// memory except the per-chunk maps of the y/z scan.
-//   x sweep   a segment of S = 8/16/32 lanes of one warp per line (the line
-//             is contiguous), chunks of m = ceil(n / S) values, scan with
-//             warp shuffles;
-//   y/z sweep lanes are 32 adjacent columns (each row a 128-byte segment),
-//             the 16 warps of a CTA are chunks along the line, scan through
-//             shared memory.
-// The chunking depends only on the line length, so a line's arithmetic is
-// the same whatever else shares the launch.
+// one FMUL + one FFMA, then one FFMA per value.  End nodes keep their value
+// or take the Dirichlet target.
+//
+// Data movement.  density is [s][k][j][i] FP32 with rows padded to a pitch
+// px = nx rounded up to 4 floats, so every row starts on 16 bytes.  Each
+// warp of a persistent CTA runs its own pipeline of shared-memory stages:
+// its lane 0 (x) or all lanes (y/z, one row each) issue 1-D TMA bulk copies
+// (cp.async.bulk) of the warp's next tiles into free stages, completion is
+// counted on one mbarrier per stage, the warp solves the current stage in
+// place and writes it back with bulk stores.  Two tiles per warp are in
+// flight while one is solved, so HBM sees a deep queue with few threads.
+//   x tile:   32 lines (one per lane) stored [line][px]; lanes walk their
+//             lines skewed by the lane index (lane t reaches position i at
+//             step i + t) so that the 32 lanes always hit 32 banks;
+//   y/z tile: 32 adjacent columns x n rows stored [row][32]; lane = column,
+//             each row one 128-byte bulk copy.
+// Every value is read from HBM once and written once per sweep.  Waits are
+// bounded: a wait that runs out records PCG_DEV_TIMEOUT in the status word,
+// drains what it issued, and returns.
 #include "pcg_kernels.cuh"
 
 namespace pcg {
@@ -44,9 +47,274 @@ __device__ __forceinline__ bool on_face(const SweepTile& tile, int lane)
     return i == 0u || i + 1u == tile.nx;
 }
 
-// Reference rule for a whole line held at s[m * st] (used for lines too long
-// for the chunked kernels): the same recurrences, sequentially.
-__device__ __forceinline__ void solve_line(float* s, int st, const LineRule& r, const float2* __restrict__ tb)
+// ------------------------------------------------------------------ TMA / mbarrier helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait: about one second of SM clock, then PCG_DEV_TIMEOUT.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned* status)
+{
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > (2ll << 30)) {
+            atomicOr(status, PCG_DEV_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
+
+// global -> shared, completion counted on 'bar' (16-byte aligned, size % 16 == 0)
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(smem_dst)),
+                 "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// shared -> global in this thread's bulk group
+__device__ __forceinline__ void bulk_store(void* gdst, const void* smem_src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(smem_src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ bool aligned16(const void* p, uint32_t bytes)
+{
+    return ((reinterpret_cast<uintptr_t>(p) | bytes) & 15u) == 0 && bytes > 0;
+}
+
+// ------------------------------------------------------------------ tile geometry
+
+// Bytes of one row copy of a column tile (count columns rounded up to 4).
+__device__ __forceinline__ uint32_t col_row_bytes(uint32_t count) { return ((count + 3u) & ~3u) * 4u; }
+
+// Issue the loads of 'tile' into stage 'st' (all lanes take part).
+template <bool kRows>
+__device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const LineRule* __restrict__ rules,
+                                                const float* __restrict__ dens, float* st, uint64_t* bar, int lane,
+                                                unsigned* status)
+{
+    const uint32_t n = rules[tile.rule].n;
+    const float* src = dens + tile.base;
+    if (kRows) {
+        const uint32_t bytes = tile.count * tile.rs * 4u;     // count lines of pitch rs
+        if (lane == 0) {
+            if (!aligned16(src, bytes)) {
+                atomicOr(status, PCG_DEV_ALIGN);
+                mbar_arrive_expect_tx(bar, 0);
+                return false;
+            }
+            mbar_arrive_expect_tx(bar, bytes);
+            bulk_load(st, src, bytes, bar);
+        }
+    } else {
+        const uint32_t rb = col_row_bytes(tile.count);
+        if (!aligned16(src, rb) || (tile.rs & 3u)) {
+            if (lane == 0) {
+                atomicOr(status, PCG_DEV_ALIGN);
+                mbar_arrive_expect_tx(bar, 0);
+            }
+            return false;
+        }
+        if (lane == 0) mbar_arrive_expect_tx(bar, rb * n);
+        __syncwarp();
+        for (uint32_t j = lane; j < n; j += 32) bulk_load(st + j * 32, src + static_cast<size_t>(j) * tile.rs, rb, bar);
+    }
+    return true;
+}
+
+template <bool kRows>
+__device__ __forceinline__ void issue_tile_store(const SweepTile& tile, const LineRule* __restrict__ rules,
+                                                 float* __restrict__ dens, const float* st, int lane)
+{
+    float* dst = dens + tile.base;
+    if (kRows) {
+        if (lane == 0) {
+            bulk_store(dst, st, tile.count * tile.rs * 4u);
+            bulk_commit();
+        }
+    } else {
+        const uint32_t n = rules[tile.rule].n;
+        const uint32_t rb = col_row_bytes(tile.count);
+        for (uint32_t j = lane; j < n; j += 32) bulk_store(dst + static_cast<size_t>(j) * tile.rs, st + j * 32, rb);
+        bulk_commit();
+    }
+}
+
+// ------------------------------------------------------------------ solves in shared memory
+
+// x tile: lane t solves line t (if t < count) stored at st + t * px.  Steps
+// are skewed by the lane index so the lanes touch distinct banks
+// (px is a multiple of 4, so px - 1 and px + 1 are odd).
+__device__ __forceinline__ void solve_rows(float* st, const SweepTile& tile, const LineRule& r,
+                                           const float2* __restrict__ tb, int lane)
+{
+    const int n = static_cast<int>(r.n);
+    const int px = static_cast<int>(tile.rs);
+    const bool act = lane < static_cast<int>(tile.count);
+    float* row = st + lane * px;
+    const float f = r.fold;
+    if (n >= 3) {
+        float d = 0.f;
+        for (int k = 0; k < n - 2 + 31; ++k) {
+            const int i = 1 + k - lane;   // this lane's interior position at step k
+            if (act && i >= 1 && i <= n - 2) {
+                const float2 e = __ldg(&tb[i]);
+                const float fi = (i == 1 || i == n - 2) ? f : 0.f;
+                d = fmaf(-e.x, d, (row[i] + fi) * e.y);
+                row[i] = d;
+            }
+        }
+        float x = 0.f;
+        for (int k = 0; k < n - 2 + 31; ++k) {
+            const int i = n - 2 - (k - lane);
+            if (act && i >= 1 && i <= n - 2) {
+                x = fmaf(-__ldg(&tb[i].x), x, row[i]);
+                row[i] = x;
+            }
+        }
+    }
+    if (act && r.dir) {
+        row[0] = r.T;
+        row[n - 1] = r.T;
+    }
+}
+
+// y/z tile: lane = column, rows at st + j * 32.
+__device__ __forceinline__ void solve_cols(float* st, const SweepTile& tile, const LineRule& r,
+                                           const float2* __restrict__ tb, int lane, bool apply_faces)
+{
+    if (lane >= static_cast<int>(tile.count)) return;
+    const int n = static_cast<int>(r.n);
+    float* col = st + lane;
+    if (apply_faces && (tile.face & TILE_FACE) && on_face(tile, lane)) {
+        for (int j = 0; j < n; ++j) col[j * 32] = r.T;   // applyDirichletBC fused: the line lies on a face
+        return;
+    }
+    if (n >= 3) {
+        const float f = r.fold;
+        float d = 0.f;
+#pragma unroll 4
+        for (int j = 1; j <= n - 2; ++j) {
+            const float2 e = __ldg(&tb[j]);
+            const float fj = (j == 1 || j == n - 2) ? f : 0.f;
+            d = fmaf(-e.x, d, (col[j * 32] + fj) * e.y);
+            col[j * 32] = d;
+        }
+        float x = 0.f;
+#pragma unroll 4
+        for (int j = n - 2; j >= 1; --j) {
+            x = fmaf(-__ldg(&tb[j].x), x, col[j * 32]);
+            col[j * 32] = x;
+        }
+    }
+    if (r.dir) {
+        col[0] = r.T;
+        col[(n - 1) * 32] = r.T;
+    }
+}
+
+// ------------------------------------------------------------------ pipelined kernel
+
+// Shared memory: kBarBytes of mbarriers ([warp][stage]), then the stages
+// ([warp][stage][stage_floats], 128-byte aligned).
+constexpr int kBarBytes = 512;   // up to 16 warps x 4 stages
+
+template <bool kRows>
+__global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
+                                                   uint32_t ntiles, const LineRule* __restrict__ rules,
+                                                   const float2* __restrict__ tab, int stage_floats, int nstages,
+                                                   int apply_faces, const uint8_t* __restrict__ mask,
+                                                   unsigned* __restrict__ status)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem) + warp * nstages;
+    float* stages = reinterpret_cast<float*>(smem + kBarBytes) + static_cast<size_t>(warp) * nstages * stage_floats;
+    if (lane == 0)
+        for (int s = 0; s < nstages; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncwarp();
+
+    const uint32_t gw = blockIdx.x * nwarps + warp, tw = gridDim.x * nwarps;
+    const uint32_t ntw = gw < ntiles ? (ntiles - gw + tw - 1) / tw : 0u;
+    const int ahead = nstages - 2;   // loads in flight while one stage is solved and one drains
+    uint32_t issued = 0;
+    bool ok = true;
+    for (; issued < ntw && static_cast<int>(issued) < ahead; ++issued) {
+        const int s = static_cast<int>(issued % nstages);
+        issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, stages + s * stage_floats, &bars[s], lane, status);
+    }
+    for (uint32_t k = 0; k < ntw; ++k) {
+        // refill: tile k + ahead goes to the stage last stored two tiles ago
+        if (issued < ntw) {
+            bulk_wait_read<1>();
+            __syncwarp();
+            const int s = static_cast<int>(issued % nstages);
+            issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, stages + s * stage_floats, &bars[s], lane,
+                                   status);
+            ++issued;
+        }
+        const int s = static_cast<int>(k % nstages);
+        if (!mbar_wait(&bars[s], (k / nstages) & 1u, status)) {
+            ok = false;
+            break;
+        }
+        const SweepTile tile = tiles[gw + k * tw];
+        const LineRule r = rules[tile.rule];
+        float* st = stages + s * stage_floats;
+        if (tile_on(r, mask)) {
+            if (kRows) solve_rows(st, tile, r, tab + r.tab, lane);
+            else solve_cols(st, tile, r, tab + r.tab, lane, apply_faces != 0);
+        }
+        fence_async_smem();
+        __syncwarp();
+        issue_tile_store<kRows>(tile, rules, dens, st, lane);
+    }
+    if (!ok) {
+        // let every load this warp issued land before the CTA exits (bounded)
+        for (uint32_t k = 0; k < issued; ++k) {
+            const int s = static_cast<int>(k % nstages);
+            if (!mbar_wait(&bars[s], (k / nstages) & 1u, status)) break;
+        }
+    }
+    bulk_wait_all();
+}
+
+// ------------------------------------------------------- any line length
+
+// Reference rule for a whole line held at s[m * st], sequentially (lines
+// longer than the shared-memory tiles).
+__device__ __forceinline__ void solve_line(float* s, size_t st, const LineRule& r, const float2* __restrict__ tb)
 {
     const int n = static_cast<int>(r.n);
     if (n >= 3) {
@@ -69,227 +337,6 @@ __device__ __forceinline__ void solve_line(float* s, int st, const LineRule& r, 
     }
 }
 
-// ------------------------------------------------------------------ x sweep
-
-template <int M>
-__global__ void __launch_bounds__(256) k_sweep_x(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
-                                                 uint32_t ntiles, const LineRule* __restrict__ rules,
-                                                 const float2* __restrict__ tab, const uint8_t* __restrict__ mask)
-{
-    const int lane = threadIdx.x & 31;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t t = gw; t < ntiles; t += nw) {
-        const SweepTile tile = tiles[t];
-        const LineRule r = rules[tile.rule];
-        if (!tile_on(r, mask)) continue;
-        const int n = static_cast<int>(r.n);
-        const int S = static_cast<int>(x_seg_lanes(r.n));
-        const int m = (n + S - 1) / S;
-        const int seg = lane / S, sl = lane % S;
-        const bool active = seg < static_cast<int>(tile.count);
-        float* g = dens + tile.base + static_cast<size_t>(seg) * n;
-        const float2* tb = tab + r.tab;
-        const int p0 = sl * m;
-        float v[M], gg[M];
-#pragma unroll
-        for (int k = 0; k < M; ++k) {
-            const int p = p0 + k;
-            float x = 0.f, gk = 0.f, iv = 0.f;
-            if (k < m && active && p < n) {
-                x = g[p];
-                const float2 e = __ldg(&tb[p]);
-                gk = -e.x;
-                iv = e.y;
-            }
-            const float f = (p == 1 || p == n - 2) ? r.fold : 0.f;
-            v[k] = (x + f) * iv;
-            gg[k] = gk;
-        }
-        // forward: local recurrence, then the segment's exclusive scan
-        float d = 0.f, A = 1.f;
-#pragma unroll
-        for (int k = 0; k < M; ++k) {
-            if (k < m) {
-                d = fmaf(gg[k], d, v[k]);
-                A *= gg[k];
-                v[k] = d;
-            }
-        }
-        float B = d;
-        for (int o = 1; o < S; o <<= 1) {
-            const float Ap = __shfl_up_sync(0xffffffffu, A, o, S);
-            const float Bp = __shfl_up_sync(0xffffffffu, B, o, S);
-            if (sl >= o) {
-                B = fmaf(A, Bp, B);
-                A *= Ap;
-            }
-        }
-        float din = __shfl_up_sync(0xffffffffu, B, 1, S);
-        if (sl == 0) din = 0.f;
-        float run = 1.f;
-#pragma unroll
-        for (int k = 0; k < M; ++k) {
-            if (k < m) {
-                run *= gg[k];
-                v[k] = fmaf(run, din, v[k]);
-            }
-        }
-        // backward: local recurrence from the chunk's end, reverse scan
-        float x = 0.f;
-        A = 1.f;
-#pragma unroll
-        for (int k = M - 1; k >= 0; --k) {
-            if (k < m) {
-                x = fmaf(gg[k], x, v[k]);
-                A *= gg[k];
-                v[k] = x;
-            }
-        }
-        B = x;
-        for (int o = 1; o < S; o <<= 1) {
-            const float Ap = __shfl_down_sync(0xffffffffu, A, o, S);
-            const float Bp = __shfl_down_sync(0xffffffffu, B, o, S);
-            if (sl + o < S) {
-                B = fmaf(A, Bp, B);
-                A *= Ap;
-            }
-        }
-        float xout = __shfl_down_sync(0xffffffffu, B, 1, S);
-        if (sl == S - 1) xout = 0.f;
-        run = 1.f;
-#pragma unroll
-        for (int k = M - 1; k >= 0; --k) {
-            if (k < m) {
-                run *= gg[k];
-                v[k] = fmaf(run, xout, v[k]);
-            }
-        }
-        if (active) {
-#pragma unroll
-            for (int k = 0; k < M; ++k) {
-                const int p = p0 + k;
-                if (k < m && p < n) {
-                    if (p == 0 || p == n - 1) {
-                        if (r.dir) g[p] = r.T;
-                    } else {
-                        g[p] = v[k];
-                    }
-                }
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------- y/z sweeps
-
-constexpr int kColsWarps = 16;
-
-template <int M>
-__global__ void __launch_bounds__(kColsWarps * 32) k_sweep_cols(float* __restrict__ dens,
-                                                                const SweepTile* __restrict__ tiles, uint32_t ntiles,
-                                                                const LineRule* __restrict__ rules,
-                                                                const float2* __restrict__ tab, int apply_faces,
-                                                                const uint8_t* __restrict__ mask)
-{
-    __shared__ float sA[kColsWarps][32], sB[kColsWarps][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const SweepTile tile = tiles[t];
-        const LineRule r = rules[tile.rule];
-        if (!tile_on(r, mask)) continue;   // uniform over the CTA
-        const int n = static_cast<int>(r.n);
-        const int m = static_cast<int>(cols_chunk(r.n));
-        const int W = (n + m - 1) / m;
-        const bool col_ok = lane < static_cast<int>(tile.count);
-        const bool face = apply_faces && (tile.face & TILE_FACE) && on_face(tile, lane);
-        const bool work = col_ok && !face && w < W;
-        float* col = dens + tile.base + lane;
-        const size_t rs = tile.rs;
-        const float2* tb = tab + r.tab;
-        const int p0 = w * m;
-        float v[M], gg[M];
-#pragma unroll
-        for (int k = 0; k < M; ++k) {
-            const int p = p0 + k;
-            float x = 0.f, gk = 0.f, iv = 0.f;
-            if (k < m && work && p < n) {
-                x = col[p * rs];
-                const float2 e = __ldg(&tb[p]);
-                gk = -e.x;
-                iv = e.y;
-            }
-            const float f = (p == 1 || p == n - 2) ? r.fold : 0.f;
-            v[k] = (x + f) * iv;
-            gg[k] = gk;
-        }
-        float d = 0.f, A = 1.f;
-#pragma unroll
-        for (int k = 0; k < M; ++k) {
-            if (k < m) {
-                d = fmaf(gg[k], d, v[k]);
-                A *= gg[k];
-                v[k] = d;
-            }
-        }
-        sA[w][lane] = A;
-        sB[w][lane] = d;
-        __syncthreads();
-        float din = 0.f;
-        for (int q = 0; q < w && q < W; ++q) din = fmaf(sA[q][lane], din, sB[q][lane]);
-        __syncthreads();
-        float run = 1.f;
-#pragma unroll
-        for (int k = 0; k < M; ++k) {
-            if (k < m) {
-                run *= gg[k];
-                v[k] = fmaf(run, din, v[k]);
-            }
-        }
-        float x = 0.f;
-        A = 1.f;
-#pragma unroll
-        for (int k = M - 1; k >= 0; --k) {
-            if (k < m) {
-                x = fmaf(gg[k], x, v[k]);
-                A *= gg[k];
-                v[k] = x;
-            }
-        }
-        sA[w][lane] = A;
-        sB[w][lane] = x;
-        __syncthreads();
-        float xout = 0.f;
-        for (int q = W - 1; q > w; --q) xout = fmaf(sA[q][lane], xout, sB[q][lane]);
-        run = 1.f;
-#pragma unroll
-        for (int k = M - 1; k >= 0; --k) {
-            if (k < m) {
-                run *= gg[k];
-                v[k] = fmaf(run, xout, v[k]);
-            }
-        }
-        if (col_ok && w < W) {
-#pragma unroll
-            for (int k = 0; k < M; ++k) {
-                const int p = p0 + k;
-                if (k < m && p < n) {
-                    if (face) {
-                        col[p * rs] = r.T;   // applyDirichletBC fused: the line lies on a face
-                    } else if (p == 0 || p == n - 1) {
-                        if (r.dir) col[p * rs] = r.T;
-                    } else {
-                        col[p * rs] = v[k];
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// ------------------------------------------------------- any line length
-
 __global__ void __launch_bounds__(128) k_sweep_global(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
                                                       uint32_t ntiles, const LineRule* __restrict__ rules,
                                                       const float2* __restrict__ tab, int apply_faces,
@@ -303,12 +350,14 @@ __global__ void __launch_bounds__(128) k_sweep_global(float* __restrict__ dens, 
         if (static_cast<uint32_t>(lane) >= tile.count) continue;
         const LineRule r = rules[tile.rule];
         if (!tile_on(r, mask)) continue;
-        const uint32_t ls = tile.rs == 1u ? r.n : 1u;
-        float* g = dens + tile.base + static_cast<size_t>(lane) * ls;
-        if (apply_faces && (tile.face & TILE_FACE) && on_face(tile, lane)) {
-            for (uint32_t j = 0; j < r.n; ++j) g[static_cast<size_t>(j) * tile.rs] = r.T;
+        const bool rows = (tile.face & TILE_ROWS) != 0;
+        // row tiles: lines tile.rs apart, unit stride; column tiles: adjacent lines, stride tile.rs
+        float* g = dens + tile.base + (rows ? static_cast<size_t>(lane) * tile.rs : static_cast<size_t>(lane));
+        const size_t st = rows ? 1 : tile.rs;
+        if (!rows && apply_faces && (tile.face & TILE_FACE) && on_face(tile, lane)) {
+            for (uint32_t j = 0; j < r.n; ++j) g[j * st] = r.T;
         } else {
-            solve_line(g, static_cast<int>(tile.rs), r, tab + r.tab);
+            solve_line(g, st, r, tab + r.tab);
         }
     }
 }
@@ -320,7 +369,7 @@ __global__ void k_dirichlet(float* __restrict__ dens, const FaceJob* __restrict_
     const FaceJob jb = jobs[blockIdx.x];
     float* base = dens + jb.base;
     const uint32_t nx = jb.nx, ny = jb.ny, nz = jb.nz;
-    const size_t slab = static_cast<size_t>(nx) * ny;
+    const size_t px = jb.px, slab = px * ny;
     // edges of every slab (microenvironment.mm:225-235)
     const uint32_t per = 2u * nx + 2u * ny;
     const size_t total = static_cast<size_t>(nz) * per;
@@ -331,12 +380,14 @@ __global__ void k_dirichlet(float* __restrict__ dens, const FaceJob* __restrict_
         else if (q < 2u * nx) { i = q - nx; j = ny - 1; }
         else if (q < 2u * nx + ny) { i = 0; j = q - 2u * nx; }
         else { i = nx - 1; j = q - 2u * nx - ny; }
-        base[k * slab + static_cast<size_t>(j) * nx + i] = jb.T;
+        base[k * slab + j * px + i] = jb.T;
     }
     if (nz > 1) {   // z faces (3-D rule)
-        for (size_t e = threadIdx.x; e < 2 * slab; e += blockDim.x) {
-            const size_t k = (e < slab) ? 0 : (nz - 1);
-            base[k * slab + (e % slab)] = jb.T;
+        const size_t plane = static_cast<size_t>(nx) * ny;
+        for (size_t e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
+            const size_t k = (e < plane) ? 0 : (nz - 1);
+            const size_t v = e % plane;
+            base[k * slab + (v / nx) * px + (v % nx)] = jb.T;
         }
     }
 }
@@ -347,28 +398,29 @@ __global__ void k_gradients(const float* __restrict__ dens, float* __restrict__ 
                             float* __restrict__ gz, const GradJob* __restrict__ jobs)
 {
     const GradJob jb = jobs[blockIdx.y];
-    const size_t nx = jb.nx, ny = jb.ny, nz = jb.nz, nv = nx * ny * nz;
+    const size_t nx = jb.nx, ny = jb.ny, nz = jb.nz, nv = nx * ny * nz, px = jb.px;
     const float* D = dens + jb.base;
     for (size_t n = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; n < nv;
          n += static_cast<size_t>(gridDim.x) * blockDim.x) {
         const size_t i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
-        const size_t o = jb.out_base + n;
+        const size_t a = (k * ny + j) * px + i;       // device offset of voxel n
+        const size_t o = jb.out_base + n;             // dense output
+        const size_t sy = px, sz = px * ny;
         double v;
         if (nx == 1) v = 0.0;
-        else if (i == 0) v = (static_cast<double>(D[n + 1]) - D[n]) * jb.inv_dx;
-        else if (i == nx - 1) v = (static_cast<double>(D[n]) - D[n - 1]) * jb.inv_dx;
-        else v = (static_cast<double>(D[n + 1]) - D[n - 1]) * 0.5 * jb.inv_dx;
+        else if (i == 0) v = (static_cast<double>(D[a + 1]) - D[a]) * jb.inv_dx;
+        else if (i == nx - 1) v = (static_cast<double>(D[a]) - D[a - 1]) * jb.inv_dx;
+        else v = (static_cast<double>(D[a + 1]) - D[a - 1]) * 0.5 * jb.inv_dx;
         if (gx) gx[o] = static_cast<float>(v);
         if (ny == 1) v = 0.0;
-        else if (j == 0) v = (static_cast<double>(D[n + nx]) - D[n]) * jb.inv_dy;
-        else if (j == ny - 1) v = (static_cast<double>(D[n]) - D[n - nx]) * jb.inv_dy;
-        else v = (static_cast<double>(D[n + nx]) - D[n - nx]) * 0.5 * jb.inv_dy;
+        else if (j == 0) v = (static_cast<double>(D[a + sy]) - D[a]) * jb.inv_dy;
+        else if (j == ny - 1) v = (static_cast<double>(D[a]) - D[a - sy]) * jb.inv_dy;
+        else v = (static_cast<double>(D[a + sy]) - D[a - sy]) * 0.5 * jb.inv_dy;
         if (gy) gy[o] = static_cast<float>(v);
         if (nz > 1) {
-            const size_t sz = nx * ny;
-            if (k == 0) v = (static_cast<double>(D[n + sz]) - D[n]) * jb.inv_dz;
-            else if (k == nz - 1) v = (static_cast<double>(D[n]) - D[n - sz]) * jb.inv_dz;
-            else v = (static_cast<double>(D[n + sz]) - D[n - sz]) * 0.5 * jb.inv_dz;
+            if (k == 0) v = (static_cast<double>(D[a + sz]) - D[a]) * jb.inv_dz;
+            else if (k == nz - 1) v = (static_cast<double>(D[a]) - D[a - sz]) * jb.inv_dz;
+            else v = (static_cast<double>(D[a + sz]) - D[a - sz]) * 0.5 * jb.inv_dz;
         } else {
             v = 0.0;
         }
@@ -378,67 +430,47 @@ __global__ void k_gradients(const float* __restrict__ dens, float* __restrict__ 
 
 // ------------------------------------------------------------- launchers
 
-template <int M>
-static int occ_x(int block)
+size_t sweep_tma_smem(int warps, int nstages, int stage_floats)
 {
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep_x<M>, block, 0) != cudaSuccess) return 0;
-    return b;
+    return kBarBytes + static_cast<size_t>(warps) * nstages * stage_floats * sizeof(float);
 }
-template <int M>
-static int occ_cols()
+
+static cudaError_t allow_max_smem(const void* fn)
 {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    return e;
+}
+
+int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats)
+{
+    const void* fn = rows ? reinterpret_cast<const void*>(k_sweep_tma<true>)
+                          : reinterpret_cast<const void*>(k_sweep_tma<false>);
+    if (warps < 1 || warps * nstages * 8 > kBarBytes || nstages < 3) return 0;
+    if (allow_max_smem(fn) != cudaSuccess) return 0;
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep_cols<M>, kColsWarps * 32, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, warps * 32, sweep_tma_smem(warps, nstages, stage_floats)) !=
+        cudaSuccess) {
+        cudaGetLastError();
         return 0;
+    }
     return b;
 }
 
-int sweep_x_occupancy(int nmax, int block)
-{
-    switch (x_chunk_template(static_cast<uint32_t>(nmax))) {
-        case 4: return occ_x<4>(block);
-        case 8: return occ_x<8>(block);
-        case 16: return occ_x<16>(block);
-        default: return 0;
-    }
-}
-
-int sweep_cols_occupancy(int nmax)
-{
-    switch (cols_chunk_template(static_cast<uint32_t>(nmax))) {
-        case 8: return occ_cols<8>();
-        case 16: return occ_cols<16>();
-        case 32: return occ_cols<32>();
-        default: return 0;
-    }
-}
-
-cudaError_t launch_sweep_x(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                           const LineRule* rules, const float2* tab, int nmax, const uint8_t* mask, RowsCfg cfg)
+cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
+                             const LineRule* rules, const float2* tab, int apply_faces, const uint8_t* mask,
+                             unsigned* status, TmaCfg cfg)
 {
     if (ntiles == 0) return cudaSuccess;
-    switch (x_chunk_template(static_cast<uint32_t>(nmax))) {
-        case 4: k_sweep_x<4><<<cfg.grid, cfg.block, 0, st>>>(dens, tiles, ntiles, rules, tab, mask); break;
-        case 8: k_sweep_x<8><<<cfg.grid, cfg.block, 0, st>>>(dens, tiles, ntiles, rules, tab, mask); break;
-        case 16: k_sweep_x<16><<<cfg.grid, cfg.block, 0, st>>>(dens, tiles, ntiles, rules, tab, mask); break;
-        default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_sweep_cols(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                              const LineRule* rules, const float2* tab, int nmax, int apply_faces,
-                              const uint8_t* mask, ColsCfg cfg)
-{
-    if (ntiles == 0) return cudaSuccess;
-    const int b = kColsWarps * 32;
-    switch (cols_chunk_template(static_cast<uint32_t>(nmax))) {
-        case 8: k_sweep_cols<8><<<cfg.grid, b, 0, st>>>(dens, tiles, ntiles, rules, tab, apply_faces, mask); break;
-        case 16: k_sweep_cols<16><<<cfg.grid, b, 0, st>>>(dens, tiles, ntiles, rules, tab, apply_faces, mask); break;
-        case 32: k_sweep_cols<32><<<cfg.grid, b, 0, st>>>(dens, tiles, ntiles, rules, tab, apply_faces, mask); break;
-        default: return cudaErrorInvalidValue;
-    }
+    const size_t smem = sweep_tma_smem(cfg.warps, cfg.stages, cfg.stage_floats);
+    if (rows)
+        k_sweep_tma<true><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, rules, tab, cfg.stage_floats,
+                                                                   cfg.stages, apply_faces, mask, status);
+    else
+        k_sweep_tma<false><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, rules, tab, cfg.stage_floats,
+                                                                    cfg.stages, apply_faces, mask, status);
     return cudaGetLastError();
 }
 

@@ -41,21 +41,24 @@ struct LineRule {
     uint32_t _pad;
 };
 
-// A tile of lines for one sweep launch.  Row tiles (x sweep): 'count'
-// contiguous lines of length n starting at element 'base', line stride n.
-// Column tiles (y and z sweeps): 'count' (<= 32) adjacent columns starting
-// at 'base', element stride 'rs' along the line.
+// A tile of lines for one sweep launch.  Row tiles (x sweep, TILE_ROWS):
+// 'count' (<= 32) lines of length n starting at element 'base', lines 'rs'
+// (the row pitch) apart.  Column tiles (y and z sweeps): 'count' (<= 32)
+// adjacent columns starting at 'base', element stride 'rs' along the line.
 struct SweepTile {
     uint64_t base;
     uint32_t rule;
     uint32_t count;
-    uint32_t rs;    // element stride along a line
+    uint32_t rs;    // row tiles: line pitch; column tiles: element stride along a line
     uint32_t i0;    // x index of the tile's first line (column tiles)
     uint32_t nx;    // the instance's nx
     uint32_t face;  // TILE_FACE: the Dirichlet reset is fused into this sweep;
                     // TILE_FACE_ALL: every line of the tile lies on a face
 };
-enum : uint32_t { TILE_FACE = 1u, TILE_FACE_ALL = 2u };
+enum : uint32_t { TILE_FACE = 1u, TILE_FACE_ALL = 2u, TILE_ROWS = 4u };
+
+// Device status word bits (a kernel that cannot finish records why and returns).
+enum : unsigned { PCG_DEV_TIMEOUT = 1u, PCG_DEV_ALIGN = 2u };
 
 // ---------------------------------------------------------------- cells
 
@@ -68,6 +71,8 @@ struct CellInst {
     float x_min, y_min, z_min, dt_mech;
     uint64_t dens_off;     // element offset of substrate 0 in the density arena
     uint64_t sub_pitch;    // elements between substrates
+    uint32_t px;           // row pitch (floats) of the density layout
+    uint32_t _pad_px;
     uint32_t vox_base;     // global diffusion-voxel key of voxel 0
     uint32_t cell_off;     // global index of the instance's first cell
     uint32_t n_cells;
@@ -87,53 +92,30 @@ enum : uint8_t { STEP_DIFFUSE = 1u, STEP_MECH = 2u };
 // ---------------------------------------------------------------- launchers
 // All launchers enqueue on 'st' and return the CUDA launch status.
 
-struct RowsCfg { int block; int grid; };    // x sweep: threads per CTA (one tile per warp), CTAs
-struct ColsCfg { int grid; };               // y/z sweeps: CTAs of 16 warps (one tile per CTA)
+// Pipelined TMA sweeps: 'warps' warps per CTA, each with 'stages' shared
+// memory stages of 'stage_floats' floats; 'grid' persistent CTAs.
+struct TmaCfg { int warps; int stages; int stage_floats; int grid; };
 
-// Chunking of a line, a function of its length only (so results do not
-// depend on what shares a launch).
-//   x:   S lanes of one warp per line (8, 16 or 32), chunks of ceil(n / S)
-//   y/z: chunks of max(4, ceil(n / 16)) rows, one per warp of the CTA
-__host__ __device__ inline uint32_t x_seg_lanes(uint32_t n) { return n <= 32 ? 8u : (n <= 64 ? 16u : 32u); }
-__host__ __device__ inline uint32_t x_lines_per_tile(uint32_t n) { return 32u / x_seg_lanes(n); }
-__host__ __device__ inline uint32_t cols_chunk(uint32_t n)
-{
-    const uint32_t c = (n + 15) / 16;
-    return c < 4 ? 4u : c;
-}
-// register chunk capacity (template) for the longest line of a launch; 0 =
-// too long for the chunked kernels (handled one thread per line)
-inline int x_chunk_template(uint32_t nmax)
-{
-    const uint32_t m = (nmax + x_seg_lanes(nmax) - 1) / x_seg_lanes(nmax);
-    return m <= 4 ? 4 : (m <= 8 ? 8 : (m <= 16 ? 16 : 0));
-}
-inline int cols_chunk_template(uint32_t nmax)
-{
-    const uint32_t m = cols_chunk(nmax);
-    return m <= 8 ? 8 : (m <= 16 ? 16 : (m <= 32 ? 32 : 0));
-}
-constexpr uint32_t kChunkedMaxN = 512;
+// Longest line staged in shared memory; longer lines take the one-thread-
+// per-line kernel.
+constexpr uint32_t kTmaMaxN = 512;
 
-int sweep_x_occupancy(int nmax, int block);   // resident CTAs per SM
-int sweep_cols_occupancy(int nmax);
-
-cudaError_t launch_sweep_x(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                           const LineRule* rules, const float2* tab, int nmax, const uint8_t* mask, RowsCfg cfg);
-cudaError_t launch_sweep_cols(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                              const LineRule* rules, const float2* tab, int nmax, int apply_faces,
-                              const uint8_t* mask, ColsCfg cfg);
+size_t sweep_tma_smem(int warps, int nstages, int stage_floats);
+int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats);   // CTAs per SM (0 = does not fit)
+cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
+                             const LineRule* rules, const float2* tab, int apply_faces, const uint8_t* mask,
+                             unsigned* status, TmaCfg cfg);
 // Any line length: one thread per line, d kept in place in global memory.
 cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
                                 const LineRule* rules, const float2* tab, int apply_faces, const uint8_t* mask,
                                 int grid);
 
 // applyDirichletBC over instances [0, n_inst): faces of Dirichlet substrates.
-struct FaceJob { uint64_t base; uint32_t nx, ny, nz; float T; };
+struct FaceJob { uint64_t base; uint32_t nx, ny, nz, px; float T; uint32_t _pad; };
 cudaError_t launch_dirichlet(cudaStream_t st, float* dens, const FaceJob* jobs, uint32_t njobs);
 
 // Central / one-sided gradients (microenvironment.mm:282-342).
-struct GradJob { uint64_t base; uint64_t out_base; uint32_t nx, ny, nz; float inv_dx, inv_dy, inv_dz; };
+struct GradJob { uint64_t base; uint64_t out_base; uint32_t nx, ny, nz, px; float inv_dx, inv_dy, inv_dz, _pad; };
 cudaError_t launch_gradients(cudaStream_t st, const float* dens, float* gx, float* gy, float* gz,
                              const GradJob* jobs, uint32_t njobs, uint64_t max_voxels);
 

@@ -159,7 +159,8 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
         if (d.subs.size() != g.n_substrates) return fail(ctx, PCG_ERR_INVALID, "substrate count mismatch");
         const uint64_t nv = d.nvox();
         if (nv > 0xFFFFFFFFull) return fail(ctx, PCG_ERR_INVALID, "grid larger than 2^32 voxels");
-        d.pitch = (nv + 31) / 32 * 32;
+        d.px = (g.nx + 3u) & ~3u;
+        d.pitch = (d.rows() * d.px + 31) / 32 * 32;
         d.dens_off = dens_elems;
         d.vox_base = static_cast<uint32_t>(total_vox);
         dens_elems += d.pitch * g.n_substrates;
@@ -216,6 +217,7 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
                 f.nx = g.nx;
                 f.ny = g.ny;
                 f.nz = g.nz;
+                f.px = d.px;
                 f.T = sp.target_value;
                 fj.push_back(f);
             }
@@ -239,9 +241,9 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
     return PCG_OK;
 }
 
-// Tile lists of one axis: lines up to kChunkedMaxN go to the chunked
-// kernels (x: x_lines_per_tile(n) lines per warp tile; y/z: 32 columns per
-// CTA tile), longer lines to the one-thread-per-line kernel.
+// Tile lists of one axis: lines up to kTmaMaxN go to the pipelined TMA
+// kernels (x: 32 lines per tile; y/z: 32 columns per tile), longer lines to
+// the one-thread-per-line kernel.
 int Diffusion::build_axis(int axis)
 {
     std::vector<SweepTile> fast_t, glob_t;
@@ -254,7 +256,7 @@ int Diffusion::build_axis(int axis)
         const int nd = d.ndim();
         if (axis == 2 && nd < 3) continue;
         const uint32_t n = axis_n(g, axis);
-        const bool fast = n <= kChunkedMaxN;
+        const bool fast = n <= kTmaMaxN;
         auto& out = fast ? fast_t : glob_t;
         int& nmax = fast ? fast_nmax : glob_nmax;
         uint64_t& nl = fast ? fast_lines : glob_lines;
@@ -265,23 +267,23 @@ int Diffusion::build_axis(int axis)
             const bool dir = d.subs[s].dirichlet_enabled != 0;
             const uint64_t sbase = d.dens_off + s * d.pitch;
             if (axis == 0) {
-                const uint64_t lines = static_cast<uint64_t>(g.ny) * g.nz;
-                const uint32_t L = fast ? x_lines_per_tile(n) : 32u;
-                for (uint64_t l0 = 0; l0 < lines; l0 += L) {
+                const uint64_t lines = d.rows();
+                for (uint64_t l0 = 0; l0 < lines; l0 += 32) {
                     SweepTile t{};
-                    t.base = sbase + l0 * g.nx;
+                    t.base = sbase + l0 * d.px;
                     t.rule = rule;
-                    t.count = static_cast<uint32_t>(std::min<uint64_t>(L, lines - l0));
-                    t.rs = 1;
+                    t.count = static_cast<uint32_t>(std::min<uint64_t>(32, lines - l0));
+                    t.rs = d.px;
                     t.nx = g.nx;
+                    t.face = TILE_ROWS;
                     out.push_back(t);
                 }
                 nl += lines;
             } else {
-                // y: families over (i, k), stride nx; z: families over (i, j), stride nx*ny
+                // y: families over (i, k), stride px; z: families over (i, j), stride ny*px
                 const uint32_t outer = axis == 1 ? g.nz : g.ny;
-                const uint64_t ostride = axis == 1 ? static_cast<uint64_t>(g.nx) * g.ny : g.nx;
-                const uint32_t rs = axis == 1 ? g.nx : g.nx * g.ny;
+                const uint64_t ostride = axis == 1 ? static_cast<uint64_t>(d.px) * g.ny : d.px;
+                const uint32_t rs = axis == 1 ? d.px : d.px * g.ny;
                 for (uint32_t o = 0; o < outer; ++o) {
                     for (uint32_t i0 = 0; i0 < g.nx; i0 += 32) {
                         SweepTile t{};
@@ -326,28 +328,46 @@ int Diffusion::build_axis(int axis)
     return PCG_OK;
 }
 
-// Launch shape of one list: 'param' is the x kernel's CTA size or the
-// y/z kernel's CTAs per SM (0 = as many as fit).
+// Launch shape of one TMA list.  'param' = warps * 16 + stages picks one
+// shape; 0 takes the shape that keeps the most bytes in flight per SM.
+static int tma_stage_floats(const SweepList& l)
+{
+    const int span = l.kind == 0 ? ((l.nmax + 3) & ~3) : l.nmax;   // x: pitch of the longest line
+    return (32 * span + 31) / 32 * 32;
+}
+
 int Diffusion::config_list(SweepList& l, int param)
 {
     if (l.n == 0) return PCG_OK;
-    if (l.kind == 0) {
-        const int block = param > 0 ? param : 256;
-        const int occ = sweep_x_occupancy(l.nmax, block);
-        if (occ <= 0) return fail(ctx, PCG_ERR_INVALID, "x sweep launch does not fit");
-        const uint64_t warps = static_cast<uint64_t>(block / 32);
-        const uint64_t ctas = (l.n + warps - 1) / warps;
-        l.rc.block = block;
-        l.rc.grid = static_cast<int>(std::min<uint64_t>(ctas, static_cast<uint64_t>(occ) * ctx->sms));
-    } else if (l.kind == 1) {
-        const int occ = sweep_cols_occupancy(l.nmax);
-        if (occ <= 0) return fail(ctx, PCG_ERR_INVALID, "column sweep launch does not fit");
-        const int per_sm = param > 0 ? std::min(param, occ) : occ;
-        l.cc.grid = static_cast<int>(std::min<uint64_t>(l.n, static_cast<uint64_t>(per_sm) * ctx->sms));
-    } else {
+    if (l.kind == 2) {
         const uint64_t ctas = (static_cast<uint64_t>(l.n) * 32 + 127) / 128;
         l.ggrid = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(ctas, 1), static_cast<uint64_t>(ctx->sms) * 16));
+        return PCG_OK;
     }
+    const bool rows = l.kind == 0;
+    const int sf = tma_stage_floats(l);
+    int best_w = 0, best_s = 0, best_occ = 0;
+    double best_flight = -1.0;
+    for (int w : {1, 2, 3, 4, 6, 8}) {
+        for (int st : {3, 4}) {
+            if (param && param != w * 16 + st) continue;
+            const int occ = sweep_tma_occupancy(rows, w, st, sf);
+            if (occ <= 0) continue;
+            const double flight = static_cast<double>(occ) * w * (st - 2) * sf;
+            if (flight > best_flight) {
+                best_flight = flight;
+                best_w = w;
+                best_s = st;
+                best_occ = occ;
+            }
+        }
+    }
+    if (best_w == 0) return fail(ctx, PCG_ERR_INVALID, "sweep tile does not fit shared memory");
+    l.tc.warps = best_w;
+    l.tc.stages = best_s;
+    l.tc.stage_floats = sf;
+    const uint64_t ctas = (l.n + best_w - 1) / best_w;
+    l.tc.grid = static_cast<int>(std::min<uint64_t>(ctas, static_cast<uint64_t>(best_occ) * ctx->sms));
     return PCG_OK;
 }
 
@@ -365,9 +385,8 @@ int Diffusion::launch_list(const SweepList& l, bool fuse, const uint8_t* mask)
     const LineRule* r = rules.as<LineRule>();
     const float2* tb = tab.as<float2>();
     cudaError_t e;
-    if (l.kind == 0) e = launch_sweep_x(ctx->stream, d, t, l.n, r, tb, l.nmax, mask, l.rc);
-    else if (l.kind == 1) e = launch_sweep_cols(ctx->stream, d, t, l.n, r, tb, l.nmax, fuse ? 1 : 0, mask, l.cc);
-    else e = launch_sweep_global(ctx->stream, d, t, l.n, r, tb, fuse ? 1 : 0, mask, l.ggrid);
+    if (l.kind == 2) e = launch_sweep_global(ctx->stream, d, t, l.n, r, tb, fuse ? 1 : 0, mask, l.ggrid);
+    else e = launch_sweep_tma(ctx->stream, l.kind == 0, d, t, l.n, r, tb, fuse ? 1 : 0, mask, ctx->status, l.tc);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep launch");
     ctx->launches++;
     return PCG_OK;
@@ -414,6 +433,7 @@ int Diffusion::gradients(float* gx, float* gy, float* gz)
             j.nx = d.g.nx;
             j.ny = d.g.ny;
             j.nz = d.g.nz;
+            j.px = d.px;
             j.inv_dx = 1.0f / d.g.dx;
             j.inv_dy = 1.0f / d.g.dy;
             j.inv_dz = 1.0f / d.g.dz;
@@ -435,13 +455,15 @@ int Diffusion::gradients(float* gx, float* gy, float* gz)
     return PCG_OK;
 }
 
+// Host arrays are dense [s][k][j][i]; device rows are px floats apart.
 int Diffusion::upload(uint32_t i, const float* host, bool async_pinned)
 {
     const DiffInstance& d = inst[i];
     const size_t nv = d.nvox();
     for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
         float* dst = dens.as<float>() + d.dens_off + s * d.pitch;
-        PCG_CU(ctx, cudaMemcpyAsync(dst, host + s * nv, nv * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        PCG_CU(ctx, cudaMemcpy2DAsync(dst, d.px * sizeof(float), host + s * nv, d.g.nx * sizeof(float),
+                                      d.g.nx * sizeof(float), d.rows(), cudaMemcpyHostToDevice, ctx->stream));
     }
     if (!async_pinned) PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
     return PCG_OK;
@@ -453,7 +475,8 @@ int Diffusion::download(uint32_t i, float* host, bool async_pinned)
     const size_t nv = d.nvox();
     for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
         const float* src = dens.as<float>() + d.dens_off + s * d.pitch;
-        PCG_CU(ctx, cudaMemcpyAsync(host + s * nv, src, nv * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        PCG_CU(ctx, cudaMemcpy2DAsync(host + s * nv, d.g.nx * sizeof(float), src, d.px * sizeof(float),
+                                      d.g.nx * sizeof(float), d.rows(), cudaMemcpyDeviceToHost, ctx->stream));
     }
     if (!async_pinned) PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
     return PCG_OK;
@@ -462,7 +485,7 @@ int Diffusion::download(uint32_t i, float* host, bool async_pinned)
 int Diffusion::fill(uint32_t i, const float* values)
 {
     const DiffInstance& d = inst[i];
-    std::vector<float> tmp(d.nvox());
+    std::vector<float> tmp(d.rows() * d.px);
     for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
         std::fill(tmp.begin(), tmp.end(), values[s]);
         float* dst = dens.as<float>() + d.dens_off + s * d.pitch;
@@ -487,8 +510,9 @@ std::string Diffusion::describe() const
         for (const auto& l : lists[a]) {
             if (l.n == 0) continue;
             o << ax[a] << ":";
-            if (l.kind == 0) o << "x-chunked(block=" << l.rc.block << ",grid=" << l.rc.grid;
-            else if (l.kind == 1) o << "cols-chunked(grid=" << l.cc.grid;
+            if (l.kind != 2)
+                o << (l.kind == 0 ? "x-tma(" : "cols-tma(") << "warps=" << l.tc.warps << ",stages=" << l.tc.stages
+                  << ",grid=" << l.tc.grid;
             else o << "global(grid=" << l.ggrid;
             o << ",tiles=" << l.n << ",nmax=" << l.nmax << ") ";
         }
@@ -532,7 +556,10 @@ int Diffusion::tune()
         int best = 0;
         if (!Tuner::get().lookup(key, &best)) {
             float best_ms = 1e30f;
-            const std::vector<int> cands = l.kind == 0 ? std::vector<int>{64, 128, 256} : std::vector<int>{1, 2, 3, 4, 0};
+            std::vector<int> cands;
+            for (int w : {1, 2, 3, 4, 6, 8})
+                for (int st : {3, 4})
+                    if (sweep_tma_occupancy(l.kind == 0, w, st, tma_stage_floats(l)) > 0) cands.push_back(w * 16 + st);
             for (int c : cands) {
                 rc = config_list(l, c);
                 if (rc != PCG_OK) break;
@@ -574,6 +601,7 @@ void fill_diff_inst(CellInst& ci, const DiffInstance& d)
     ci.z_min = d.g.z_min;
     ci.dens_off = d.dens_off;
     ci.sub_pitch = d.pitch;
+    ci.px = d.px;
     ci.vox_base = d.vox_base;
 }
 

@@ -20,6 +20,7 @@ struct pcg_ctx {
     int sms = 0;
     int smem_optin = 0;
     uint64_t launches = 0;
+    unsigned* status = nullptr;   // device status word (PCG_DEV_* bits)
 };
 
 namespace pcg {
@@ -100,18 +101,19 @@ struct DiffInstance {
     std::vector<pcg_substrate_params> subs;
     uint64_t dens_off = 0;
     uint64_t pitch = 0;       // elements between substrates (multiple of 32)
+    uint32_t px = 0;          // row pitch: nx rounded up to 4 floats (16-byte rows)
     uint32_t vox_base = 0;
     uint64_t nvox() const { return static_cast<uint64_t>(g.nx) * g.ny * g.nz; }
+    uint64_t rows() const { return static_cast<uint64_t>(g.ny) * g.nz; }
     int ndim() const { return g.nz > 1 ? 3 : 2; }
 };
 
 struct SweepList {
-    int kind = 0;              // 0 row tiles (SMEM), 1 column tiles (SMEM), 2 any length (global)
+    int kind = 0;              // 0 row tiles (TMA), 1 column tiles (TMA), 2 any length (global)
     int nmax = 0;
     uint32_t n = 0;
     DevBuf tiles;
-    RowsCfg rc{256, 1};
-    ColsCfg cc{1};
+    TmaCfg tc{4, 3, 0, 1};
     int ggrid = 1;
     uint64_t lines = 0;        // lines covered (for tuning keys)
 };
