@@ -31,6 +31,9 @@
 // Every value is read from HBM once and written once per sweep.  Waits are
 // bounded: a wait that runs out records PCG_DEV_TIMEOUT in the status word,
 // drains what it issued, and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "pcg_kernels.cuh"
 
 namespace pcg {
@@ -101,6 +104,21 @@ __device__ __forceinline__ void bulk_store(void* gdst, const void* smem_src, uin
                  "r"(bytes)
                  : "memory");
 }
+// 3-D tensor-map copies of a whole column tile (one instruction each way)
+__device__ __forceinline__ void tensor_load3(void* smem_dst, const void* tmap, int c0, int c1, int c2, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+            "r"(smem_u32(smem_dst)),
+        "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tensor_store3(const void* tmap, int c0, int c1, int c2, const void* smem_src)
+{
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tmap),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(smem_src))
+                 : "memory");
+}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory"); }
@@ -118,13 +136,31 @@ __device__ __forceinline__ bool aligned16(const void* p, uint32_t bytes)
 __device__ __forceinline__ uint32_t col_row_bytes(uint32_t count) { return ((count + 3u) & ~3u) * 4u; }
 
 // Issue the loads of 'tile' into stage 'st' (all lanes take part).
+// Tensor coordinates {x, y, z} of a column tile's box.
+__device__ __forceinline__ void tile_coords(const SweepTile& tile, int* c)
+{
+    c[0] = static_cast<int>(tile.i0);
+    c[1] = (tile.face & TILE_AXIS_Z) ? static_cast<int>(tile.outer) : 0;
+    c[2] = (tile.face & TILE_AXIS_Z) ? 0 : static_cast<int>(tile.outer);
+}
+
 template <bool kRows>
 __device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const LineRule* __restrict__ rules,
-                                                const float* __restrict__ dens, float* st, uint64_t* bar, int lane,
-                                                unsigned* status)
+                                                const float* __restrict__ dens, const void* tmaps, float* st,
+                                                uint64_t* bar, int lane, unsigned* status)
 {
     const uint32_t n = rules[tile.rule].n;
     const float* src = dens + tile.base;
+    if (!kRows && (tile.face & TILE_TENSOR)) {
+        if (lane == 0) {
+            int c[3];
+            tile_coords(tile, c);
+            mbar_arrive_expect_tx(bar, 32u * n * 4u);
+            tensor_load3(st, static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.rule) * 128, c[0],
+                         c[1], c[2], bar);
+        }
+        return true;
+    }
     if (kRows) {
         const uint32_t bytes = tile.count * tile.rs * 4u;     // count lines of pitch rs
         if (lane == 0) {
@@ -154,9 +190,19 @@ __device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const Lin
 
 template <bool kRows>
 __device__ __forceinline__ void issue_tile_store(const SweepTile& tile, const LineRule* __restrict__ rules,
-                                                 float* __restrict__ dens, const float* st, int lane)
+                                                 float* __restrict__ dens, const void* tmaps, const float* st, int lane)
 {
     float* dst = dens + tile.base;
+    if (!kRows && (tile.face & TILE_TENSOR)) {
+        if (lane == 0) {
+            int c[3];
+            tile_coords(tile, c);
+            tensor_store3(static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.rule) * 128, c[0], c[1],
+                          c[2], st);
+            bulk_commit();
+        }
+        return;
+    }
     if (kRows) {
         if (lane == 0) {
             bulk_store(dst, st, tile.count * tile.rs * 4u);
@@ -172,9 +218,66 @@ __device__ __forceinline__ void issue_tile_store(const SweepTile& tile, const Li
 
 // ------------------------------------------------------------------ solves in shared memory
 
-// x tile: lane t solves line t (if t < count) stored at st + t * px.  Steps
-// are skewed by the lane index so the lanes touch distinct banks
-// (px is a multiple of 4, so px - 1 and px + 1 are odd).
+// Interior positions 1..n-2 are p[0..m-1] with m = n - 2.  The Dirichlet
+// fold is added to the first and last interior value once, so the passes
+// are bare recurrences: forward d = fma(-c'_i, d, p_i / den_i), backward
+// x = fma(-c'_i, x, d_i).
+
+// Steps [k0, k1) of one pass at positions pos(k) (value at base[pos * stride],
+// table entry t[pos]).  Blocks of kU steps: the next block's values and table
+// entries are loaded before the current block's dependent FFMAs run, so the
+// loads never sit on the recurrence.
+constexpr int kU = 8;
+
+template <bool kForward, class Pos>
+__device__ __forceinline__ float chain(float* base, int stride, const float2* __restrict__ t, Pos pos, int k0, int k1,
+                                       float acc)
+{
+    int k = k0;
+    if (k1 - k0 >= kU) {
+        float v[kU];
+        float2 e[kU];
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+            const int i = pos(k + q);
+            v[q] = base[i * stride];
+            e[q] = __ldg(&t[i]);
+        }
+        for (; k + kU <= k1; k += kU) {
+            const int kn = (k + 2 * kU <= k1) ? k + kU : k;
+            float vn[kU];
+            float2 en[kU];
+#pragma unroll
+            for (int q = 0; q < kU; ++q) {
+                const int i = pos(kn + q);
+                vn[q] = base[i * stride];
+                en[q] = __ldg(&t[i]);
+            }
+#pragma unroll
+            for (int q = 0; q < kU; ++q) {
+                acc = kForward ? fmaf(-e[q].x, acc, v[q] * e[q].y) : fmaf(-e[q].x, acc, v[q]);
+                base[pos(k + q) * stride] = acc;
+            }
+#pragma unroll
+            for (int q = 0; q < kU; ++q) {
+                v[q] = vn[q];
+                e[q] = en[q];
+            }
+        }
+    }
+    for (; k < k1; ++k) {
+        const int i = pos(k);
+        const float2 e = __ldg(&t[i]);
+        acc = kForward ? fmaf(-e.x, acc, base[i * stride] * e.y) : fmaf(-e.x, acc, base[i * stride]);
+        base[i * stride] = acc;
+    }
+    return acc;
+}
+
+// x tile: lane t solves line t stored at st + t * px.  Lane t reaches
+// interior position i at step i + t, so at every step the 32 lanes touch 32
+// different banks (px is a multiple of 4, so px - 1 is odd).  Steps
+// [31, m) are taken by every lane and run pipelined without predicates.
 __device__ __forceinline__ void solve_rows(float* st, const SweepTile& tile, const LineRule& r,
                                            const float2* __restrict__ tb, int lane)
 {
@@ -182,24 +285,52 @@ __device__ __forceinline__ void solve_rows(float* st, const SweepTile& tile, con
     const int px = static_cast<int>(tile.rs);
     const bool act = lane < static_cast<int>(tile.count);
     float* row = st + lane * px;
-    const float f = r.fold;
     if (n >= 3) {
+        const int m = n - 2;
+        float* p = row + 1;
+        const float2* t = tb + 1;
+        if (act) {
+            p[0] += r.fold;
+            if (m > 1) p[m - 1] += r.fold;
+        }
+        // Steps [0, 31) and [max(m, 31), m + 31) are predicated; [31, m)
+        // (empty when m <= 31) is taken by every lane.
+        const int c_begin = m > 31 ? m : 31;
+        // forward: position k - lane at step k
         float d = 0.f;
-        for (int k = 0; k < n - 2 + 31; ++k) {
-            const int i = 1 + k - lane;   // this lane's interior position at step k
-            if (act && i >= 1 && i <= n - 2) {
-                const float2 e = __ldg(&tb[i]);
-                const float fi = (i == 1 || i == n - 2) ? f : 0.f;
-                d = fmaf(-e.x, d, (row[i] + fi) * e.y);
-                row[i] = d;
+        int k = 0;
+        for (; k < 31; ++k) {
+            const int i = k - lane;
+            if (i >= 0 && i < m) {
+                const float2 e = __ldg(&t[i]);
+                d = fmaf(-e.x, d, p[i] * e.y);
+                p[i] = d;
             }
         }
+        d = chain<true>(p, 1, t, [lane](int s) { return s - lane; }, 31, m, d);
+        for (k = c_begin; k < m + 31; ++k) {
+            const int i = k - lane;
+            if (i >= 0 && i < m) {
+                const float2 e = __ldg(&t[i]);
+                d = fmaf(-e.x, d, p[i] * e.y);
+                p[i] = d;
+            }
+        }
+        // backward: position m - 1 - (k - lane) at step k
         float x = 0.f;
-        for (int k = 0; k < n - 2 + 31; ++k) {
-            const int i = n - 2 - (k - lane);
-            if (act && i >= 1 && i <= n - 2) {
-                x = fmaf(-__ldg(&tb[i].x), x, row[i]);
-                row[i] = x;
+        for (k = 0; k < 31; ++k) {
+            const int i = m - 1 - (k - lane);
+            if (i >= 0 && i < m) {
+                x = fmaf(-__ldg(&t[i].x), x, p[i]);
+                p[i] = x;
+            }
+        }
+        x = chain<false>(p, 1, t, [lane, m](int s) { return m - 1 - (s - lane); }, 31, m, x);
+        for (k = c_begin; k < m + 31; ++k) {
+            const int i = m - 1 - (k - lane);
+            if (i >= 0 && i < m) {
+                x = fmaf(-__ldg(&t[i].x), x, p[i]);
+                p[i] = x;
             }
         }
     }
@@ -209,37 +340,29 @@ __device__ __forceinline__ void solve_rows(float* st, const SweepTile& tile, con
     }
 }
 
-// y/z tile: lane = column, rows at st + j * 32.
+// y/z tile: lane = column, rows at st + j * 32 (32 lanes, 32 banks).
 __device__ __forceinline__ void solve_cols(float* st, const SweepTile& tile, const LineRule& r,
                                            const float2* __restrict__ tb, int lane, bool apply_faces)
 {
     if (lane >= static_cast<int>(tile.count)) return;
     const int n = static_cast<int>(r.n);
-    float* col = st + lane;
+    float* c = st + lane;
     if (apply_faces && (tile.face & TILE_FACE) && on_face(tile, lane)) {
-        for (int j = 0; j < n; ++j) col[j * 32] = r.T;   // applyDirichletBC fused: the line lies on a face
+        for (int j = 0; j < n; ++j) c[j * 32] = r.T;   // applyDirichletBC fused: the line lies on a face
         return;
     }
     if (n >= 3) {
-        const float f = r.fold;
-        float d = 0.f;
-#pragma unroll 4
-        for (int j = 1; j <= n - 2; ++j) {
-            const float2 e = __ldg(&tb[j]);
-            const float fj = (j == 1 || j == n - 2) ? f : 0.f;
-            d = fmaf(-e.x, d, (col[j * 32] + fj) * e.y);
-            col[j * 32] = d;
-        }
-        float x = 0.f;
-#pragma unroll 4
-        for (int j = n - 2; j >= 1; --j) {
-            x = fmaf(-__ldg(&tb[j].x), x, col[j * 32]);
-            col[j * 32] = x;
-        }
+        const int m = n - 2;
+        float* p = c + 32;
+        const float2* t = tb + 1;
+        p[0] += r.fold;
+        if (m > 1) p[(m - 1) * 32] += r.fold;
+        chain<true>(p, 32, t, [](int s) { return s; }, 0, m, 0.f);
+        chain<false>(p, 32, t, [m](int s) { return m - 1 - s; }, 0, m, 0.f);
     }
     if (r.dir) {
-        col[0] = r.T;
-        col[(n - 1) * 32] = r.T;
+        c[0] = r.T;
+        c[(n - 1) * 32] = r.T;
     }
 }
 
@@ -252,9 +375,9 @@ constexpr int kBarBytes = 512;   // up to 16 warps x 4 stages
 template <bool kRows>
 __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
                                                    uint32_t ntiles, const LineRule* __restrict__ rules,
-                                                   const float2* __restrict__ tab, int stage_floats, int nstages,
-                                                   int apply_faces, const uint8_t* __restrict__ mask,
-                                                   unsigned* __restrict__ status)
+                                                   const float2* __restrict__ tab, const void* __restrict__ tmaps,
+                                                   int stage_floats, int nstages, int apply_faces,
+                                                   const uint8_t* __restrict__ mask, unsigned* __restrict__ status)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -267,21 +390,23 @@ __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, con
 
     const uint32_t gw = blockIdx.x * nwarps + warp, tw = gridDim.x * nwarps;
     const uint32_t ntw = gw < ntiles ? (ntiles - gw + tw - 1) / tw : 0u;
-    const int ahead = nstages - 2;   // loads in flight while one stage is solved and one drains
+    const int ahead = nstages - 1;   // loads in flight while one stage is solved
     uint32_t issued = 0;
     bool ok = true;
     for (; issued < ntw && static_cast<int>(issued) < ahead; ++issued) {
         const int s = static_cast<int>(issued % nstages);
-        issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, stages + s * stage_floats, &bars[s], lane, status);
+        issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, tmaps, stages + s * stage_floats, &bars[s], lane,
+                               status);
     }
     for (uint32_t k = 0; k < ntw; ++k) {
-        // refill: tile k + ahead goes to the stage last stored two tiles ago
+        // refill: tile k + ahead goes to the stage of tile k - 1, whose store
+        // (issued last) must have finished reading shared memory
         if (issued < ntw) {
-            bulk_wait_read<1>();
+            bulk_wait_read<0>();
             __syncwarp();
             const int s = static_cast<int>(issued % nstages);
-            issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, stages + s * stage_floats, &bars[s], lane,
-                                   status);
+            issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, tmaps, stages + s * stage_floats, &bars[s],
+                                   lane, status);
             ++issued;
         }
         const int s = static_cast<int>(k % nstages);
@@ -298,7 +423,7 @@ __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, con
         }
         fence_async_smem();
         __syncwarp();
-        issue_tile_store<kRows>(tile, rules, dens, st, lane);
+        issue_tile_store<kRows>(tile, rules, dens, tmaps, st, lane);
     }
     if (!ok) {
         // let every load this warp issued land before the CTA exits (bounded)
@@ -448,7 +573,7 @@ int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats)
 {
     const void* fn = rows ? reinterpret_cast<const void*>(k_sweep_tma<true>)
                           : reinterpret_cast<const void*>(k_sweep_tma<false>);
-    if (warps < 1 || warps * nstages * 8 > kBarBytes || nstages < 3) return 0;
+    if (warps < 1 || warps * nstages * 8 > kBarBytes || nstages < 2) return 0;
     if (allow_max_smem(fn) != cudaSuccess) return 0;
     int b = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, warps * 32, sweep_tma_smem(warps, nstages, stage_floats)) !=
@@ -460,18 +585,53 @@ int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats)
 }
 
 cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                             const LineRule* rules, const float2* tab, int apply_faces, const uint8_t* mask,
-                             unsigned* status, TmaCfg cfg)
+                             const LineRule* rules, const float2* tab, const void* tmaps, int apply_faces,
+                             const uint8_t* mask, unsigned* status, TmaCfg cfg)
 {
     if (ntiles == 0) return cudaSuccess;
     const size_t smem = sweep_tma_smem(cfg.warps, cfg.stages, cfg.stage_floats);
     if (rows)
-        k_sweep_tma<true><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, rules, tab, cfg.stage_floats,
-                                                                   cfg.stages, apply_faces, mask, status);
+        k_sweep_tma<true><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, rules, tab, tmaps,
+                                                                   cfg.stage_floats, cfg.stages, apply_faces, mask,
+                                                                   status);
     else
-        k_sweep_tma<false><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, rules, tab, cfg.stage_floats,
-                                                                    cfg.stages, apply_faces, mask, status);
+        k_sweep_tma<false><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, rules, tab, tmaps,
+                                                                    cfg.stage_floats, cfg.stages, apply_faces, mask,
+                                                                    status);
     return cudaGetLastError();
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link-time dependency on libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        cudaGetLastError();
+    }
+    return fn;
+}
+
+bool encode_column_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t px, int axis,
+                       uint32_t n)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn || n == 0 || n > kTensorMaxN || (px & 3u) || (reinterpret_cast<uintptr_t>(block) & 15u)) return false;
+    const cuuint64_t dims[3] = {nx, ny, nz};
+    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(px) * 4u, static_cast<cuuint64_t>(px) * ny * 4u};
+    const cuuint32_t box[3] = {32u, axis == 1 ? n : 1u, axis == 1 ? 1u : n};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    const CUresult r = fn(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, block, dims, strides,
+                          box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
 }
 
 cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,

@@ -53,9 +53,16 @@ struct SweepTile {
     uint32_t i0;    // x index of the tile's first line (column tiles)
     uint32_t nx;    // the instance's nx
     uint32_t face;  // TILE_FACE: the Dirichlet reset is fused into this sweep;
-                    // TILE_FACE_ALL: every line of the tile lies on a face
+                    // TILE_FACE_ALL: every line of the tile lies on a face;
+                    // TILE_ROWS: x tile; TILE_TENSOR: moved with the rule's
+                    // 3-D tensor map; TILE_AXIS_Z: z tile (else y)
+    uint32_t outer; // column tiles: the fixed coordinate (k for y, j for z)
+    uint32_t _pad[3];
 };
-enum : uint32_t { TILE_FACE = 1u, TILE_FACE_ALL = 2u, TILE_ROWS = 4u };
+enum : uint32_t { TILE_FACE = 1u, TILE_FACE_ALL = 2u, TILE_ROWS = 4u, TILE_TENSOR = 8u, TILE_AXIS_Z = 16u };
+
+// Longest line a tensor-map box can cover (box dimensions are <= 256).
+constexpr uint32_t kTensorMaxN = 256;
 
 // Device status word bits (a kernel that cannot finish records why and returns).
 enum : unsigned { PCG_DEV_TIMEOUT = 1u, PCG_DEV_ALIGN = 2u };
@@ -102,9 +109,16 @@ constexpr uint32_t kTmaMaxN = 512;
 
 size_t sweep_tma_smem(int warps, int nstages, int stage_floats);
 int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats);   // CTAs per SM (0 = does not fit)
+// tmaps: one 128-byte CUtensorMap per rule (64-byte aligned, global memory)
+// for the column tiles flagged TILE_TENSOR; may be null otherwise.
 cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                             const LineRule* rules, const float2* tab, int apply_faces, const uint8_t* mask,
-                             unsigned* status, TmaCfg cfg);
+                             const LineRule* rules, const float2* tab, const void* tmaps, int apply_faces,
+                             const uint8_t* mask, unsigned* status, TmaCfg cfg);
+// Encode the 3-D tensor map of one substrate block (dims nx, ny, nz; rows px
+// floats apart) with a box of 32 x n x 1 (y) or 32 x 1 x n (z); returns
+// false when the driver entry point is unavailable or rejects the map.
+bool encode_column_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t px, int axis,
+                       uint32_t n);
 // Any line length: one thread per line, d kept in place in global memory.
 cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
                                 const LineRule* rules, const float2* tab, int apply_faces, const uint8_t* mask,

@@ -231,6 +231,28 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
         PCG_CU(ctx, cudaMemcpy(rules.p, h_rules_.data(), h_rules_.size() * sizeof(LineRule), cudaMemcpyHostToDevice));
     if (!h_tab_.empty())
         PCG_CU(ctx, cudaMemcpy(tab.p, h_tab_.data(), h_tab_.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    // one 3-D tensor map per y/z rule short enough for a tensor box
+    tensor_ok_.assign(h_rules_.size(), 0);
+    {
+        std::vector<unsigned char> maps(std::max<size_t>(h_rules_.size(), 1) * 128, 0);
+        for (size_t i = 0; i < inst.size(); ++i) {
+            const DiffInstance& d = inst[i];
+            for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
+                for (int a = 1; a < 3; ++a) {
+                    if (a == 2 && d.ndim() < 3) continue;
+                    const uint32_t rule = rule_of(i, s, a);
+                    const uint32_t n = axis_n(d.g, a);
+                    if (n > kTensorMaxN) continue;
+                    float* block = dens.as<float>() + d.dens_off + s * d.pitch;
+                    if (encode_column_map(maps.data() + static_cast<size_t>(rule) * 128, block, d.g.nx, d.g.ny, d.g.nz,
+                                          d.px, a, n))
+                        tensor_ok_[rule] = 1;
+                }
+            }
+        }
+        PCG_CU(ctx, tmaps.alloc(maps.size()));
+        PCG_CU(ctx, cudaMemcpy(tmaps.p, maps.data(), maps.size(), cudaMemcpyHostToDevice));
+    }
     n_faces = static_cast<uint32_t>(fj.size());
     PCG_CU(ctx, faces.alloc(std::max<size_t>(fj.size(), 1) * sizeof(FaceJob)));
     if (!fj.empty()) PCG_CU(ctx, cudaMemcpy(faces.p, fj.data(), fj.size() * sizeof(FaceJob), cudaMemcpyHostToDevice));
@@ -293,8 +315,10 @@ int Diffusion::build_axis(int axis)
                         t.rs = rs;
                         t.i0 = i0;
                         t.nx = g.nx;
+                        t.outer = o;
+                        if (fast && tensor_ok_[rule]) t.face |= TILE_TENSOR | (axis == 2 ? TILE_AXIS_Z : 0u);
                         if (final_axis && dir) {
-                            t.face = TILE_FACE;
+                            t.face |= TILE_FACE;
                             if (axis == 2 && (o == 0 || o + 1 == g.ny)) t.face |= TILE_FACE_ALL;
                         }
                         out.push_back(t);
@@ -349,11 +373,12 @@ int Diffusion::config_list(SweepList& l, int param)
     int best_w = 0, best_s = 0, best_occ = 0;
     double best_flight = -1.0;
     for (int w : {1, 2, 3, 4, 6, 8}) {
-        for (int st : {3, 4}) {
+        for (int st : {2, 3, 4}) {
             if (param && param != w * 16 + st) continue;
             const int occ = sweep_tma_occupancy(rows, w, st, sf);
             if (occ <= 0) continue;
-            const double flight = static_cast<double>(occ) * w * (st - 2) * sf;
+            // warps computing per SM x tiles in flight per warp
+            const double flight = static_cast<double>(occ) * w * (st - 1) * sf + 0.5 * occ * w;
             if (flight > best_flight) {
                 best_flight = flight;
                 best_w = w;
@@ -386,7 +411,8 @@ int Diffusion::launch_list(const SweepList& l, bool fuse, const uint8_t* mask)
     const float2* tb = tab.as<float2>();
     cudaError_t e;
     if (l.kind == 2) e = launch_sweep_global(ctx->stream, d, t, l.n, r, tb, fuse ? 1 : 0, mask, l.ggrid);
-    else e = launch_sweep_tma(ctx->stream, l.kind == 0, d, t, l.n, r, tb, fuse ? 1 : 0, mask, ctx->status, l.tc);
+    else
+        e = launch_sweep_tma(ctx->stream, l.kind == 0, d, t, l.n, r, tb, tmaps.p, fuse ? 1 : 0, mask, ctx->status, l.tc);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep launch");
     ctx->launches++;
     return PCG_OK;
@@ -558,7 +584,7 @@ int Diffusion::tune()
             float best_ms = 1e30f;
             std::vector<int> cands;
             for (int w : {1, 2, 3, 4, 6, 8})
-                for (int st : {3, 4})
+                for (int st : {2, 3, 4})
                     if (sweep_tma_occupancy(l.kind == 0, w, st, tma_stage_floats(l)) > 0) cands.push_back(w * 16 + st);
             for (int c : cands) {
                 rc = config_list(l, c);

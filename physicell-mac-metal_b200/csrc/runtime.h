@@ -125,7 +125,7 @@ public:
     uint64_t dens_elems = 0;
     uint64_t total_vox = 0;        // sum nx*ny*nz
     uint64_t total_vox_sub = 0;    // sum nx*ny*nz*S
-    DevBuf dens, rules, tab, faces, grad_jobs;
+    DevBuf dens, rules, tab, faces, grad_jobs, tmaps;
     uint32_t n_faces = 0;
     std::vector<SweepList> lists[3];
     std::string shapes;
@@ -154,6 +154,7 @@ private:
     std::vector<LineRule> h_rules_;
     std::vector<float2> h_tab_;
     std::vector<uint32_t> rule_index_;   // (inst, s, axis) -> rule
+    std::vector<uint8_t> tensor_ok_;     // rule has a 3-D tensor map (column tiles)
     uint32_t rule_of(size_t i, uint32_t s, int axis) const;
 };
 
