@@ -191,6 +191,27 @@ pcg_status pcg_mech_set_diagnostics(pcg_mech* mech, int on);
 pcg_status pcg_mech_neighbor_stats(pcg_mech* mech, uint32_t* count, uint32_t* hash);
 uint32_t pcg_neighbor_hash(uint32_t cell);
 
+/* No reference counterpart.  The stable (key, value) radix sort that bins
+ * cells by mechanics voxel, run on caller-owned DEVICE buffers and making
+ * no device allocation: all scratch lives in one fixed 2.5 MiB array
+ * compiled into the library.  For callers that cannot allocate device
+ * memory at the point of the call (a server that partitioned the device up
+ * front and must not fail a request with out-of-memory, or host code that
+ * must avoid allocation calls because they can synchronise the device).
+ * - Sorts n pairs by the low key_bits (1..32) bits of the keys, equal keys
+ *   keeping their input order; enqueued on ctx's stream (pcg_sync waits).
+ * - n <= PCG_SORT_STATIC_MAX_PAIRS, else PCG_ERR_INVALID with a message;
+ *   outputs must not overlap the inputs or each other.
+ * - The first call on each device looks up the scratch array's address
+ *   (device set-up); make it, e.g. with n = 0, before the calls that
+ *   matter.  The scratch needs no initial contents.
+ * - One scratch array per device: calls on the same device must not
+ *   overlap in time (issue them on one stream, or order them with events);
+ *   overlapping calls race on the scratch and give wrong results. */
+#define PCG_SORT_STATIC_MAX_PAIRS (1u << 18)
+pcg_status pcg_sort_pairs_static(pcg_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in,
+                                 uint32_t* keys_out, uint32_t* vals_out, uint32_t n, int key_bits);
+
 /* ------------------------------------------------------------------------
  * Batch — many independent simulations of uneven grid and cell counts
  * advanced together: one CUDA graph per main-loop step, each phase one

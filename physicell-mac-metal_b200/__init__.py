@@ -138,6 +138,8 @@ _SIGS = [
     ("pcg_mech_set_diagnostics", C.c_int, [_P, C.c_int]),
     ("pcg_mech_neighbor_stats", C.c_int, [_P, _U32P, _U32P]),
     ("pcg_neighbor_hash", C.c_uint32, [C.c_uint32]),
+    ("pcg_sort_pairs_static", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                        C.c_int]),
     ("pcg_batch_create", C.c_int, [_P, C.POINTER(InstanceDesc), C.c_uint32, C.POINTER(BatchOptions),
                                    C.POINTER(_P)]),
     ("pcg_batch_destroy", C.c_int, [_P]),
