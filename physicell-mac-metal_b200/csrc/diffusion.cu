@@ -18,16 +18,19 @@
 // Data movement.  density is [s][k][j][i] FP32 with rows padded to a pitch
 // px = nx rounded up to 4 floats, so every row starts on 16 bytes.  Each
 // warp of a persistent CTA runs its own pipeline of shared-memory stages:
-// its lane 0 (x) or all lanes (y/z, one row each) issue 1-D TMA bulk copies
-// (cp.async.bulk) of the warp's next tiles into free stages, completion is
-// counted on one mbarrier per stage, the warp solves the current stage in
-// place and writes it back with bulk stores.  Two tiles per warp are in
-// flight while one is solved, so HBM sees a deep queue with few threads.
-//   x tile:   32 lines (one per lane) stored [line][px]; lanes walk their
-//             lines skewed by the lane index (lane t reaches position i at
-//             step i + t) so that the 32 lanes always hit 32 banks;
-//   y/z tile: 32 adjacent columns x n rows stored [row][32]; lane = column,
-//             each row one 128-byte bulk copy.
+// lane 0 issues one TMA tensor copy (cp.async.bulk.tensor) of the warp's
+// next tile into a free stage, completion is counted on one mbarrier per
+// stage, the warp solves the current stage in place and writes it back with
+// one tensor store.  Tiles are loaded while the previous one is solved, so
+// HBM sees a deep queue with few threads.
+//   x tile:   32 lines (one per lane) stored [line][P], P = row_smem_pitch(nx)
+//             (2-D map, box P x 32); all lanes walk their lines in step,
+//             4 values per 16-byte shared access, coefficients broadcast;
+//   y/z tile: 32 adjacent columns x n rows stored [row][32] (3-D map, box
+//             32 x n); lane = column.
+// Lines too long for a tensor box move with 1-D bulk copies (x: the whole
+// tile, lanes skewed by the lane index so 32 lanes hit 32 banks; y/z: one
+// 128-byte copy per row).
 // Every value is read from HBM once and written once per sweep.  Waits are
 // bounded: a wait that runs out records PCG_DEV_TIMEOUT in the status word,
 // drains what it issued, and returns.
@@ -113,6 +116,21 @@ __device__ __forceinline__ void tensor_load3(void* smem_dst, const void* tmap, i
         "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
         : "memory");
 }
+// 2-D tensor-map copies of a whole x tile
+__device__ __forceinline__ void tensor_load2(void* smem_dst, const void* tmap, int c0, int c1, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(smem_dst)),
+        "l"(tmap), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tensor_store2(const void* tmap, int c0, int c1, const void* smem_src)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(tmap), "r"(c0),
+                 "r"(c1), "r"(smem_u32(smem_src))
+                 : "memory");
+}
 __device__ __forceinline__ void tensor_store3(const void* tmap, int c0, int c1, int c2, const void* smem_src)
 {
     asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tmap),
@@ -151,13 +169,20 @@ __device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const Lin
 {
     const uint32_t n = rules[tile.rule].n;
     const float* src = dens + tile.base;
+    const void* map = static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.rule) * 128;
+    if (kRows && (tile.face & TILE_TENSOR)) {
+        if (lane == 0) {
+            mbar_arrive_expect_tx(bar, 32u * row_smem_pitch(n) * 4u);   // the whole box, fill included
+            tensor_load2(st, map, 0, static_cast<int>(tile.outer), bar);
+        }
+        return true;
+    }
     if (!kRows && (tile.face & TILE_TENSOR)) {
         if (lane == 0) {
             int c[3];
             tile_coords(tile, c);
             mbar_arrive_expect_tx(bar, 32u * n * 4u);
-            tensor_load3(st, static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.rule) * 128, c[0],
-                         c[1], c[2], bar);
+            tensor_load3(st, map, c[0], c[1], c[2], bar);
         }
         return true;
     }
@@ -193,6 +218,14 @@ __device__ __forceinline__ void issue_tile_store(const SweepTile& tile, const Li
                                                  float* __restrict__ dens, const void* tmaps, const float* st, int lane)
 {
     float* dst = dens + tile.base;
+    if (kRows && (tile.face & TILE_TENSOR)) {
+        if (lane == 0) {
+            tensor_store2(static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.rule) * 128, 0,
+                          static_cast<int>(tile.outer), st);
+            bulk_commit();
+        }
+        return;
+    }
     if (!kRows && (tile.face & TILE_TENSOR)) {
         if (lane == 0) {
             int c[3];
@@ -218,123 +251,141 @@ __device__ __forceinline__ void issue_tile_store(const SweepTile& tile, const Li
 
 // ------------------------------------------------------------------ solves in shared memory
 
-// Interior positions 1..n-2 are p[0..m-1] with m = n - 2.  The Dirichlet
-// fold is added to the first and last interior value once, so the passes
-// are bare recurrences: forward d = fma(-c'_i, d, p_i / den_i), backward
-// x = fma(-c'_i, x, d_i).
-
-// Steps [k0, k1) of one pass at positions pos(k) (value at base[pos * stride],
-// table entry t[pos]).  Blocks of kU steps: the next block's values and table
-// entries are loaded before the current block's dependent FFMAs run, so the
-// loads never sit on the recurrence.
-constexpr int kU = 8;
-
-template <bool kForward, class Pos>
-__device__ __forceinline__ float chain(float* base, int stride, const float2* __restrict__ t, Pos pos, int k0, int k1,
-                                       float acc)
+// Coefficient table of one rule: line positions in chunks of 4, each chunk
+// 8 floats {g[4], inv[4]} (32-byte aligned), g_i = c / den_i, inv_i = 1 / den_i;
+// zero at the end nodes.
+__device__ __forceinline__ float tab_g(const float* __restrict__ t, int i) { return __ldg(t + ((i >> 2) << 3) + (i & 3)); }
+__device__ __forceinline__ float tab_inv(const float* __restrict__ t, int i)
 {
-    int k = k0;
-    if (k1 - k0 >= kU) {
-        float v[kU];
-        float2 e[kU];
-#pragma unroll
-        for (int q = 0; q < kU; ++q) {
-            const int i = pos(k + q);
-            v[q] = base[i * stride];
-            e[q] = __ldg(&t[i]);
-        }
-        for (; k + kU <= k1; k += kU) {
-            const int kn = (k + 2 * kU <= k1) ? k + kU : k;
-            float vn[kU];
-            float2 en[kU];
-#pragma unroll
-            for (int q = 0; q < kU; ++q) {
-                const int i = pos(kn + q);
-                vn[q] = base[i * stride];
-                en[q] = __ldg(&t[i]);
-            }
-#pragma unroll
-            for (int q = 0; q < kU; ++q) {
-                acc = kForward ? fmaf(-e[q].x, acc, v[q] * e[q].y) : fmaf(-e[q].x, acc, v[q]);
-                base[pos(k + q) * stride] = acc;
-            }
-#pragma unroll
-            for (int q = 0; q < kU; ++q) {
-                v[q] = vn[q];
-                e[q] = en[q];
-            }
-        }
-    }
-    for (; k < k1; ++k) {
-        const int i = pos(k);
-        const float2 e = __ldg(&t[i]);
-        acc = kForward ? fmaf(-e.x, acc, base[i * stride] * e.y) : fmaf(-e.x, acc, base[i * stride]);
-        base[i * stride] = acc;
-    }
-    return acc;
+    return __ldg(t + ((i >> 2) << 3) + 4 + (i & 3));
+}
+__device__ __forceinline__ float4 tab_g4(const float* __restrict__ t, int q)
+{
+    return __ldg(reinterpret_cast<const float4*>(t + (q << 3)));
+}
+__device__ __forceinline__ float4 tab_inv4(const float* __restrict__ t, int q)
+{
+    return __ldg(reinterpret_cast<const float4*>(t + (q << 3) + 4));
 }
 
-// x tile: lane t solves line t stored at st + t * px.  Lane t reaches
-// interior position i at step i + t, so at every step the 32 lanes touch 32
-// different banks (px is a multiple of 4, so px - 1 is odd).  Steps
-// [31, m) are taken by every lane and run pipelined without predicates.
-__device__ __forceinline__ void solve_rows(float* st, const SweepTile& tile, const LineRule& r,
-                                           const float2* __restrict__ tb, int lane)
+// One block of 8 positions (two table chunks) of the forward / backward
+// pass: positions 8k + u for u in [lo, hi] (all eight when kFull).
+template <bool kFull>
+__device__ __forceinline__ float fwd8(float (&v)[8], const float4 (&g)[2], const float4 (&iv)[2], float d, int lo,
+                                      int hi)
 {
-    const int n = static_cast<int>(r.n);
-    const int px = static_cast<int>(tile.rs);
-    const bool act = lane < static_cast<int>(tile.count);
-    float* row = st + lane * px;
-    if (n >= 3) {
-        const int m = n - 2;
-        float* p = row + 1;
-        const float2* t = tb + 1;
-        if (act) {
-            p[0] += r.fold;
-            if (m > 1) p[m - 1] += r.fold;
-        }
-        // Steps [0, 31) and [max(m, 31), m + 31) are predicated; [31, m)
-        // (empty when m <= 31) is taken by every lane.
-        const int c_begin = m > 31 ? m : 31;
-        // forward: position k - lane at step k
-        float d = 0.f;
-        int k = 0;
-        for (; k < 31; ++k) {
-            const int i = k - lane;
-            if (i >= 0 && i < m) {
-                const float2 e = __ldg(&t[i]);
-                d = fmaf(-e.x, d, p[i] * e.y);
-                p[i] = d;
-            }
-        }
-        d = chain<true>(p, 1, t, [lane](int s) { return s - lane; }, 31, m, d);
-        for (k = c_begin; k < m + 31; ++k) {
-            const int i = k - lane;
-            if (i >= 0 && i < m) {
-                const float2 e = __ldg(&t[i]);
-                d = fmaf(-e.x, d, p[i] * e.y);
-                p[i] = d;
-            }
-        }
-        // backward: position m - 1 - (k - lane) at step k
-        float x = 0.f;
-        for (k = 0; k < 31; ++k) {
-            const int i = m - 1 - (k - lane);
-            if (i >= 0 && i < m) {
-                x = fmaf(-__ldg(&t[i].x), x, p[i]);
-                p[i] = x;
-            }
-        }
-        x = chain<false>(p, 1, t, [lane, m](int s) { return m - 1 - (s - lane); }, 31, m, x);
-        for (k = c_begin; k < m + 31; ++k) {
-            const int i = m - 1 - (k - lane);
-            if (i >= 0 && i < m) {
-                x = fmaf(-__ldg(&t[i].x), x, p[i]);
-                p[i] = x;
-            }
+    const float gg[8] = {g[0].x, g[0].y, g[0].z, g[0].w, g[1].x, g[1].y, g[1].z, g[1].w};
+    const float ii[8] = {iv[0].x, iv[0].y, iv[0].z, iv[0].w, iv[1].x, iv[1].y, iv[1].z, iv[1].w};
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        if (kFull || (u >= lo && u <= hi)) {
+            d = fmaf(gg[u], d, v[u] * ii[u]);
+            v[u] = d;
         }
     }
-    if (act && r.dir) {
+    return d;
+}
+template <bool kFull>
+__device__ __forceinline__ float bwd8(float (&v)[8], const float4 (&g)[2], float x, int lo, int hi)
+{
+    const float gg[8] = {g[0].x, g[0].y, g[0].z, g[0].w, g[1].x, g[1].y, g[1].z, g[1].w};
+#pragma unroll
+    for (int u = 7; u >= 0; --u) {
+        if (kFull || (u >= lo && u <= hi)) {
+            x = fmaf(gg[u], x, v[u]);
+            v[u] = x;
+        }
+    }
+    return x;
+}
+
+// Both passes of one line over positions 1..n-2 (n >= 3) in blocks of 8
+// positions; ld(q, p) / st(q, p) move the 4 positions of chunk q (4q..4q+3)
+// from / to p[0..3].  Two register sets alternate: the next block and its
+// coefficients are loaded into one while the other's dependent FFMAs run,
+// so no load sits on the recurrence and no register is copied.  Only chunks
+// up to the one holding position n - 2 are read or written; values past
+// n - 2 in that chunk are written back unchanged.
+template <class LD, class ST>
+__device__ __forceinline__ void thomas_line(const float* __restrict__ t, int n, LD ld, ST st)
+{
+    const int ql = (n - 2) >> 2;       // chunk of the last interior position
+    const int bl = ql >> 1;            // its block
+    const int hl = n - 2 - 8 * bl;     // its place in that block
+    float a[8], b[8];
+    float4 ga[2], ia[2], gb[2], ib[2];
+    auto load = [&](int k, float (&v)[8], float4 (&g)[2], float4 (&iv)[2], bool with_inv) {
+        ld(2 * k, v);
+        g[0] = tab_g4(t, 2 * k);
+        if (with_inv) iv[0] = tab_inv4(t, 2 * k);
+        if (2 * k + 1 <= ql) {
+            ld(2 * k + 1, v + 4);
+            g[1] = tab_g4(t, 2 * k + 1);
+            if (with_inv) iv[1] = tab_inv4(t, 2 * k + 1);
+        }
+    };
+    auto store = [&](int k, float (&v)[8]) {
+        st(2 * k, v);
+        if (2 * k + 1 <= ql) st(2 * k + 1, v + 4);
+    };
+    auto fwd = [&](int k, float (&v)[8], float4 (&g)[2], float4 (&iv)[2], float d) {
+        if (k > 0 && k < bl) return fwd8<true>(v, g, iv, d, 0, 7);
+        return fwd8<false>(v, g, iv, d, k == 0 ? 1 : 0, k == bl ? hl : 7);
+    };
+    auto bwd = [&](int k, float (&v)[8], float4 (&g)[2], float x) {
+        if (k > 0 && k < bl) return bwd8<true>(v, g, x, 0, 7);
+        return bwd8<false>(v, g, x, k == 0 ? 1 : 0, k == bl ? hl : 7);
+    };
+    float d = 0.f;
+    load(0, a, ga, ia, true);
+    for (int k = 0; k <= bl; k += 2) {
+        if (k + 1 <= bl) load(k + 1, b, gb, ib, true);
+        d = fwd(k, a, ga, ia, d);
+        store(k, a);
+        if (k + 1 > bl) break;
+        if (k + 2 <= bl) load(k + 2, a, ga, ia, true);
+        d = fwd(k + 1, b, gb, ib, d);
+        store(k + 1, b);
+    }
+    float x = 0.f;
+    load(bl, a, ga, ia, false);
+    for (int k = bl; k >= 0; k -= 2) {
+        if (k >= 1) load(k - 1, b, gb, ib, false);
+        x = bwd(k, a, ga, x);
+        store(k, a);
+        if (k < 1) break;
+        if (k >= 2) load(k - 2, a, ga, ia, false);
+        x = bwd(k - 1, b, gb, x);
+        store(k - 1, b);
+    }
+}
+
+// x tile through the row tensor map: lane t solves line t stored at
+// st + t * P, P = row_smem_pitch(n).  All lanes sit at the same position, so
+// the coefficients are one broadcast load, and each lane moves 4 values with
+// one 16-byte shared access; P / 4 is odd, so the 8 lanes of each quarter
+// warp hit 8 different 16-byte bank groups (no conflicts).
+__device__ __forceinline__ void solve_rows_vec(float* st, const LineRule& r, const float* __restrict__ t, int lane,
+                                               int count)
+{
+    if (lane >= count) return;
+    const int n = static_cast<int>(r.n);
+    float* row = st + lane * static_cast<int>(row_smem_pitch(r.n));
+    if (n >= 3) {
+        row[1] += r.fold;
+        if (n > 3) row[n - 2] += r.fold;
+        thomas_line(
+            t, n,
+            [row](int q, float* v) {
+                const float4 a = *reinterpret_cast<const float4*>(row + 4 * q);
+                v[0] = a.x;
+                v[1] = a.y;
+                v[2] = a.z;
+                v[3] = a.w;
+            },
+            [row](int q, const float* v) { *reinterpret_cast<float4*>(row + 4 * q) = make_float4(v[0], v[1], v[2], v[3]); });
+    }
+    if (r.dir) {
         row[0] = r.T;
         row[n - 1] = r.T;
     }
@@ -342,7 +393,7 @@ __device__ __forceinline__ void solve_rows(float* st, const SweepTile& tile, con
 
 // y/z tile: lane = column, rows at st + j * 32 (32 lanes, 32 banks).
 __device__ __forceinline__ void solve_cols(float* st, const SweepTile& tile, const LineRule& r,
-                                           const float2* __restrict__ tb, int lane, bool apply_faces)
+                                           const float* __restrict__ t, int lane, bool apply_faces)
 {
     if (lane >= static_cast<int>(tile.count)) return;
     const int n = static_cast<int>(r.n);
@@ -352,17 +403,83 @@ __device__ __forceinline__ void solve_cols(float* st, const SweepTile& tile, con
         return;
     }
     if (n >= 3) {
-        const int m = n - 2;
-        float* p = c + 32;
-        const float2* t = tb + 1;
-        p[0] += r.fold;
-        if (m > 1) p[(m - 1) * 32] += r.fold;
-        chain<true>(p, 32, t, [](int s) { return s; }, 0, m, 0.f);
-        chain<false>(p, 32, t, [m](int s) { return m - 1 - s; }, 0, m, 0.f);
+        c[32] += r.fold;
+        if (n > 3) c[(n - 2) * 32] += r.fold;
+        thomas_line(
+            t, n,
+            [c](int q, float* v) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) v[u] = c[(4 * q + u) * 32];
+            },
+            [c](int q, const float* v) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) c[(4 * q + u) * 32] = v[u];
+            });
     }
     if (r.dir) {
         c[0] = r.T;
         c[(n - 1) * 32] = r.T;
+    }
+}
+
+// x tile moved as one 1-D bulk copy (lines longer than a tensor box): lane t
+// solves line t stored at st + t * px.  Lane t reaches interior position i
+// at step i + t, so at every step the 32 lanes touch 32 different banks
+// (px is a multiple of 4, so px - 1 is odd).
+__device__ __forceinline__ void skew_step_fwd(float* p, const float* __restrict__ t, int i, float& d)
+{
+    d = fmaf(tab_g(t, i + 1), d, p[i] * tab_inv(t, i + 1));
+    p[i] = d;
+}
+__device__ __forceinline__ void skew_step_bwd(float* p, const float* __restrict__ t, int i, float& x)
+{
+    x = fmaf(tab_g(t, i + 1), x, p[i]);
+    p[i] = x;
+}
+
+__device__ __forceinline__ void solve_rows(float* st, const SweepTile& tile, const LineRule& r,
+                                           const float* __restrict__ t, int lane)
+{
+    const int n = static_cast<int>(r.n);
+    const int px = static_cast<int>(tile.rs);
+    const bool act = lane < static_cast<int>(tile.count);
+    float* row = st + lane * px;
+    if (n >= 3) {
+        const int m = n - 2;
+        float* p = row + 1;   // interior position i + 1 at p[i]
+        if (act) {
+            p[0] += r.fold;
+            if (m > 1) p[m - 1] += r.fold;
+        }
+        // steps [0, 31) and [max(m, 31), m + 31) are predicated, [31, m) is
+        // taken by every lane
+        const int c_begin = m > 31 ? m : 31;
+        float d = 0.f;
+        for (int k = 0; k < 31; ++k) {
+            const int i = k - lane;
+            if (i >= 0 && i < m) skew_step_fwd(p, t, i, d);
+        }
+#pragma unroll 4
+        for (int k = 31; k < m; ++k) skew_step_fwd(p, t, k - lane, d);
+        for (int k = c_begin; k < m + 31; ++k) {
+            const int i = k - lane;
+            if (i >= 0 && i < m) skew_step_fwd(p, t, i, d);
+        }
+        float x = 0.f;
+        for (int k = 0; k < 31; ++k) {
+            const int i = m - 1 - (k - lane);
+            if (i >= 0 && i < m) skew_step_bwd(p, t, i, x);
+        }
+#pragma unroll 4
+        for (int k = 31; k < m; ++k) skew_step_bwd(p, t, m - 1 - (k - lane), x);
+        for (int k = c_begin; k < m + 31; ++k) {
+            const int i = m - 1 - (k - lane);
+            if (i >= 0 && i < m) skew_step_bwd(p, t, i, x);
+        }
+    }
+    if (act && r.dir) {
+        row[0] = r.T;
+        row[n - 1] = r.T;
     }
 }
 
@@ -375,7 +492,7 @@ constexpr int kBarBytes = 512;   // up to 16 warps x 4 stages
 template <bool kRows>
 __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
                                                    uint32_t ntiles, const LineRule* __restrict__ rules,
-                                                   const float2* __restrict__ tab, const void* __restrict__ tmaps,
+                                                   const float* __restrict__ tab, const void* __restrict__ tmaps,
                                                    int stage_floats, int nstages, int apply_faces,
                                                    const uint8_t* __restrict__ mask, unsigned* __restrict__ status)
 {
@@ -418,8 +535,12 @@ __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, con
         const LineRule r = rules[tile.rule];
         float* st = stages + s * stage_floats;
         if (tile_on(r, mask)) {
-            if (kRows) solve_rows(st, tile, r, tab + r.tab, lane);
-            else solve_cols(st, tile, r, tab + r.tab, lane, apply_faces != 0);
+            if (kRows) {
+                if (tile.face & TILE_TENSOR) solve_rows_vec(st, r, tab + r.tab, lane, static_cast<int>(tile.count));
+                else solve_rows(st, tile, r, tab + r.tab, lane);
+            } else {
+                solve_cols(st, tile, r, tab + r.tab, lane, apply_faces != 0);
+            }
         }
         fence_async_smem();
         __syncwarp();
@@ -439,20 +560,19 @@ __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, con
 
 // Reference rule for a whole line held at s[m * st], sequentially (lines
 // longer than the shared-memory tiles).
-__device__ __forceinline__ void solve_line(float* s, size_t st, const LineRule& r, const float2* __restrict__ tb)
+__device__ __forceinline__ void solve_line(float* s, size_t st, const LineRule& r, const float* __restrict__ t)
 {
     const int n = static_cast<int>(r.n);
     if (n >= 3) {
         float d = 0.f;
         for (int i = 1; i <= n - 2; ++i) {
-            const float2 e = __ldg(&tb[i]);
             const float f = (i == 1 || i == n - 2) ? r.fold : 0.f;
-            d = fmaf(-e.x, d, (s[i * st] + f) * e.y);
+            d = fmaf(tab_g(t, i), d, (s[i * st] + f) * tab_inv(t, i));
             s[i * st] = d;
         }
         float x = 0.f;
         for (int i = n - 2; i >= 1; --i) {
-            x = fmaf(-__ldg(&tb[i].x), x, s[i * st]);
+            x = fmaf(tab_g(t, i), x, s[i * st]);
             s[i * st] = x;
         }
     }
@@ -464,7 +584,7 @@ __device__ __forceinline__ void solve_line(float* s, size_t st, const LineRule& 
 
 __global__ void __launch_bounds__(128) k_sweep_global(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
                                                       uint32_t ntiles, const LineRule* __restrict__ rules,
-                                                      const float2* __restrict__ tab, int apply_faces,
+                                                      const float* __restrict__ tab, int apply_faces,
                                                       const uint8_t* __restrict__ mask)
 {
     const int lane = threadIdx.x & 31;
@@ -585,7 +705,7 @@ int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats)
 }
 
 cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                             const LineRule* rules, const float2* tab, const void* tmaps, int apply_faces,
+                             const LineRule* rules, const float* tab, const void* tmaps, int apply_faces,
                              const uint8_t* mask, unsigned* status, TmaCfg cfg)
 {
     if (ntiles == 0) return cudaSuccess;
@@ -634,8 +754,25 @@ bool encode_column_map(void* map128, float* block, uint32_t nx, uint32_t ny, uin
     return r == CUDA_SUCCESS;
 }
 
+bool encode_row_map(void* map128, float* block, uint32_t nx, uint64_t rows, uint32_t px)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    const uint32_t P = row_smem_pitch(nx);
+    if (!fn || nx == 0 || nx > kRowTensorMaxN || rows == 0 || (px & 3u) || px < nx ||
+        (reinterpret_cast<uintptr_t>(block) & 15u))
+        return false;
+    const cuuint64_t dims[2] = {nx, rows};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(px) * 4u};
+    const cuuint32_t box[2] = {P, 32u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = fn(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, block, dims, strides,
+                          box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                                const LineRule* rules, const float2* tab, int apply_faces, const uint8_t* mask,
+                                const LineRule* rules, const float* tab, int apply_faces, const uint8_t* mask,
                                 int grid)
 {
     if (ntiles == 0) return cudaSuccess;

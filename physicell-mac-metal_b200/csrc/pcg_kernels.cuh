@@ -22,16 +22,18 @@ enum Field : int {
 // ---------------------------------------------------------------- diffusion
 
 // Thomas constants of one (instance, substrate, axis) line family.  Every
-// line of the family has the same matrix, so c'_i and 1/den_i are one
-// table (float2 {c'_i, 1/den_i} at tab[0..n-1]) built on the host in FP64
-// from the reference's recurrence (shaders/diffusion_2d.metal:86-148):
+// line of the family has the same matrix, so g_i = c / den_i and
+// inv_i = 1 / den_i are one table built on the host in FP64 from the
+// reference's recurrence (shaders/diffusion_2d.metal:86-148):
 //   forward   d_1 = (rho_1 + fold) / b_bnd
 //             d_i = (rho_i [+ fold at i = n-2] + c d_{i-1}) / den_i
 //   backward  rho_i = d_i - c'_i rho_{i+1}
-// with den_i = b + c c'_{i-1}, c'_i = -c / den_i; written as
-// d_i = fma(-c'_i, d_{i-1}, (rho_i + fold_i) * inv_i) since c/den_i = -c'_i.
+// with den_i = b + c c'_{i-1}, c'_i = -c / den_i = -g_i; written as
+// d_i = fma(g_i, d_{i-1}, (rho_i + fold_i) * inv_i), x_i = fma(g_i, x_{i+1}, d_i).
+// Table layout: line positions in chunks of 4, chunk q at tab + 8 q holds
+// {g[4q..4q+3], inv[4q..4q+3]} (32-byte aligned; zero at the end nodes).
 struct LineRule {
-    uint32_t tab;   // first table entry
+    uint32_t tab;   // first float of the rule's table (multiple of 8)
     uint32_t n;     // line length
     float c;        // D dt / h^2
     float fold;     // Dirichlet RHS fold: c T (2 c T when n == 3), 0 without Dirichlet
@@ -40,6 +42,9 @@ struct LineRule {
     uint32_t inst;  // instance index (step mask lookup)
     uint32_t _pad;
 };
+
+// Floats of table for a line of n positions.
+__host__ __device__ constexpr uint32_t tab_floats(uint32_t n) { return ((n + 3u) / 4u) * 8u; }
 
 // A tile of lines for one sweep launch.  Row tiles (x sweep, TILE_ROWS):
 // 'count' (<= 32) lines of length n starting at element 'base', lines 'rs'
@@ -56,13 +61,21 @@ struct SweepTile {
                     // TILE_FACE_ALL: every line of the tile lies on a face;
                     // TILE_ROWS: x tile; TILE_TENSOR: moved with the rule's
                     // 3-D tensor map; TILE_AXIS_Z: z tile (else y)
-    uint32_t outer; // column tiles: the fixed coordinate (k for y, j for z)
+    uint32_t outer; // column tiles: the fixed coordinate (k for y, j for z);
+                    // row tiles: index of the first line in the substrate block
     uint32_t _pad[3];
 };
 enum : uint32_t { TILE_FACE = 1u, TILE_FACE_ALL = 2u, TILE_ROWS = 4u, TILE_TENSOR = 8u, TILE_AXIS_Z = 16u };
 
 // Longest line a tensor-map box can cover (box dimensions are <= 256).
 constexpr uint32_t kTensorMaxN = 256;
+
+// x tiles moved with a 2-D tensor map land in shared memory as 32 rows of
+// row_smem_pitch(nx) floats: nx rounded up to 4 with an odd number of
+// 16-byte groups, so 16-byte accesses of the 32 rows are free of bank
+// conflicts.  The box must fit 256 floats.
+__host__ __device__ constexpr uint32_t row_smem_pitch(uint32_t n) { return (((n + 3u) / 4u) | 1u) * 4u; }
+constexpr uint32_t kRowTensorMaxN = 252;
 
 // Device status word bits (a kernel that cannot finish records why and returns).
 enum : unsigned { PCG_DEV_TIMEOUT = 1u, PCG_DEV_ALIGN = 2u };
@@ -104,24 +117,27 @@ enum : uint8_t { STEP_DIFFUSE = 1u, STEP_MECH = 2u };
 struct TmaCfg { int warps; int stages; int stage_floats; int grid; };
 
 // Longest line staged in shared memory; longer lines take the one-thread-
-// per-line kernel.
+// per-line kernel.  Tables are the chunked LineRule tables (float).
 constexpr uint32_t kTmaMaxN = 512;
 
 size_t sweep_tma_smem(int warps, int nstages, int stage_floats);
 int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats);   // CTAs per SM (0 = does not fit)
 // tmaps: one 128-byte CUtensorMap per rule (64-byte aligned, global memory)
-// for the column tiles flagged TILE_TENSOR; may be null otherwise.
+// for the tiles flagged TILE_TENSOR; may be null otherwise.
 cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                             const LineRule* rules, const float2* tab, const void* tmaps, int apply_faces,
+                             const LineRule* rules, const float* tab, const void* tmaps, int apply_faces,
                              const uint8_t* mask, unsigned* status, TmaCfg cfg);
 // Encode the 3-D tensor map of one substrate block (dims nx, ny, nz; rows px
 // floats apart) with a box of 32 x n x 1 (y) or 32 x 1 x n (z); returns
 // false when the driver entry point is unavailable or rejects the map.
 bool encode_column_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t px, int axis,
                        uint32_t n);
+// Encode the 2-D tensor map of one substrate block seen as rows x nx (rows
+// px floats apart) with a box of row_smem_pitch(nx) x 32 (x tiles).
+bool encode_row_map(void* map128, float* block, uint32_t nx, uint64_t rows, uint32_t px);
 // Any line length: one thread per line, d kept in place in global memory.
 cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                                const LineRule* rules, const float2* tab, int apply_faces, const uint8_t* mask,
+                                const LineRule* rules, const float* tab, int apply_faces, const uint8_t* mask,
                                 int grid);
 
 // applyDirichletBC over instances [0, n_inst): faces of Dirichlet substrates.

@@ -190,22 +190,27 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
                 r.T = sp.target_value;
                 r.dir = dir ? 1u : 0u;
                 r.inst = static_cast<uint32_t>(i);
-                h_tab_.resize(h_tab_.size() + std::max<uint32_t>(n, 2), make_float2(0.f, 0.f));
-                float2* tb = h_tab_.data() + r.tab;
+                h_tab_.resize(h_tab_.size() + tab_floats(std::max<uint32_t>(n, 1)), 0.f);
+                float* tb = h_tab_.data() + r.tab;
+                // position i: g_i = c / den_i = -c'_i and 1 / den_i (chunked layout)
+                auto put = [tb](uint32_t i, double g, double inv) {
+                    tb[(i / 4) * 8 + i % 4] = static_cast<float>(g);
+                    tb[(i / 4) * 8 + 4 + i % 4] = static_cast<float>(inv);
+                };
                 const double b_int = 1.0 + 2.0 * cc + hd, b_bnd = 1.0 + cc + hd;
                 if (n == 3) {
-                    tb[1] = make_float2(0.f, static_cast<float>(1.0 / b_int));
+                    put(1, 0.0, 1.0 / b_int);
                     r.fold = dir ? static_cast<float>(2.0 * cc * T) : 0.f;
                 } else if (n >= 4) {
                     double cp = -cc / b_bnd;
-                    tb[1] = make_float2(static_cast<float>(cp), static_cast<float>(1.0 / b_bnd));
+                    put(1, -cp, 1.0 / b_bnd);
                     for (uint32_t m = 2; m + 2 < n; ++m) {
                         const double den = b_int + cc * cp;
                         cp = -cc / den;
-                        tb[m] = make_float2(static_cast<float>(cp), static_cast<float>(1.0 / den));
+                        put(m, -cp, 1.0 / den);
                     }
                     const double den = b_bnd + cc * cp;
-                    tb[n - 2] = make_float2(static_cast<float>(-cc / den), static_cast<float>(1.0 / den));
+                    put(n - 2, cc / den, 1.0 / den);
                     r.fold = dir ? static_cast<float>(cc * T) : 0.f;
                 }
                 rule_index_.push_back(static_cast<uint32_t>(h_rules_.size()));
@@ -226,27 +231,29 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
     PCG_CU(ctx, dens.alloc(std::max<uint64_t>(dens_elems, 32) * sizeof(float)));
     PCG_CU(ctx, cudaMemsetAsync(dens.p, 0, dens.bytes, ctx->stream));
     PCG_CU(ctx, rules.alloc(std::max<size_t>(h_rules_.size(), 1) * sizeof(LineRule)));
-    PCG_CU(ctx, tab.alloc(std::max<size_t>(h_tab_.size(), 1) * sizeof(float2)));
+    PCG_CU(ctx, tab.alloc(std::max<size_t>(h_tab_.size(), 8) * sizeof(float)));
     if (!h_rules_.empty())
         PCG_CU(ctx, cudaMemcpy(rules.p, h_rules_.data(), h_rules_.size() * sizeof(LineRule), cudaMemcpyHostToDevice));
     if (!h_tab_.empty())
-        PCG_CU(ctx, cudaMemcpy(tab.p, h_tab_.data(), h_tab_.size() * sizeof(float2), cudaMemcpyHostToDevice));
-    // one 3-D tensor map per y/z rule short enough for a tensor box
+        PCG_CU(ctx, cudaMemcpy(tab.p, h_tab_.data(), h_tab_.size() * sizeof(float), cudaMemcpyHostToDevice));
+    // one tensor map per rule short enough for a tensor box: 2-D row maps
+    // for x, 3-D column maps for y and z
     tensor_ok_.assign(h_rules_.size(), 0);
     {
         std::vector<unsigned char> maps(std::max<size_t>(h_rules_.size(), 1) * 128, 0);
         for (size_t i = 0; i < inst.size(); ++i) {
             const DiffInstance& d = inst[i];
             for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
-                for (int a = 1; a < 3; ++a) {
+                float* block = dens.as<float>() + d.dens_off + s * d.pitch;
+                for (int a = 0; a < 3; ++a) {
                     if (a == 2 && d.ndim() < 3) continue;
                     const uint32_t rule = rule_of(i, s, a);
                     const uint32_t n = axis_n(d.g, a);
-                    if (n > kTensorMaxN) continue;
-                    float* block = dens.as<float>() + d.dens_off + s * d.pitch;
-                    if (encode_column_map(maps.data() + static_cast<size_t>(rule) * 128, block, d.g.nx, d.g.ny, d.g.nz,
-                                          d.px, a, n))
-                        tensor_ok_[rule] = 1;
+                    unsigned char* m = maps.data() + static_cast<size_t>(rule) * 128;
+                    const bool ok = a == 0 ? (n <= kRowTensorMaxN && encode_row_map(m, block, d.g.nx, d.rows(), d.px))
+                                           : (n <= kTensorMaxN &&
+                                              encode_column_map(m, block, d.g.nx, d.g.ny, d.g.nz, d.px, a, n));
+                    if (ok) tensor_ok_[rule] = 1;
                 }
             }
         }
@@ -297,7 +304,8 @@ int Diffusion::build_axis(int axis)
                     t.count = static_cast<uint32_t>(std::min<uint64_t>(32, lines - l0));
                     t.rs = d.px;
                     t.nx = g.nx;
-                    t.face = TILE_ROWS;
+                    t.outer = static_cast<uint32_t>(l0);
+                    t.face = TILE_ROWS | ((fast && tensor_ok_[rule]) ? TILE_TENSOR : 0u);
                     out.push_back(t);
                 }
                 nl += lines;
@@ -354,10 +362,15 @@ int Diffusion::build_axis(int axis)
 
 // Launch shape of one TMA list.  'param' = warps * 16 + stages picks one
 // shape; 0 takes the shape that keeps the most bytes in flight per SM.
+// Stage size: x tiles need 32 rows of the longest line's pitch (tensor
+// box or bulk copy); column tiles 32 x n rounded up to whole chunks of 4
+// rows, which the solve may read past the last row.
 static int tma_stage_floats(const SweepList& l)
 {
-    const int span = l.kind == 0 ? ((l.nmax + 3) & ~3) : l.nmax;   // x: pitch of the longest line
-    return (32 * span + 31) / 32 * 32;
+    const uint32_t n = static_cast<uint32_t>(l.nmax);
+    const uint32_t r4 = (n + 3u) & ~3u;
+    const uint32_t span = l.kind == 0 ? std::max(row_smem_pitch(std::min(n, kRowTensorMaxN)), r4) : r4;
+    return static_cast<int>(32u * span);
 }
 
 int Diffusion::config_list(SweepList& l, int param)
@@ -408,7 +421,7 @@ int Diffusion::launch_list(const SweepList& l, bool fuse, const uint8_t* mask)
     float* d = dens.as<float>();
     const SweepTile* t = l.tiles.as<SweepTile>();
     const LineRule* r = rules.as<LineRule>();
-    const float2* tb = tab.as<float2>();
+    const float* tb = tab.as<float>();
     cudaError_t e;
     if (l.kind == 2) e = launch_sweep_global(ctx->stream, d, t, l.n, r, tb, fuse ? 1 : 0, mask, l.ggrid);
     else

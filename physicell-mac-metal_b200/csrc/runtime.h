@@ -152,7 +152,7 @@ private:
     int config_list(SweepList& l, int param);
     int launch_list(const SweepList& l, bool fuse_faces, const uint8_t* mask);
     std::vector<LineRule> h_rules_;
-    std::vector<float2> h_tab_;
+    std::vector<float> h_tab_;
     std::vector<uint32_t> rule_index_;   // (inst, s, axis) -> rule
     std::vector<uint8_t> tensor_ok_;     // rule has a 3-D tensor map (column tiles)
     uint32_t rule_of(size_t i, uint32_t s, int axis) const;
