@@ -162,18 +162,24 @@ __device__ __forceinline__ void tile_coords(const SweepTile& tile, int* c)
     c[2] = (tile.face & TILE_AXIS_Z) ? 0 : static_cast<int>(tile.outer);
 }
 
+// Issue the loads of 'tile' into stage 'st' and of its rule's coefficient
+// table into 'stab' (the stage's table area), all counted on 'bar'.
 template <bool kRows>
 __device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const LineRule* __restrict__ rules,
-                                                const float* __restrict__ dens, const void* tmaps, float* st,
-                                                uint64_t* bar, int lane, unsigned* status)
+                                                const float* __restrict__ dens, const float* __restrict__ tab,
+                                                const void* tmaps, float* st, float* stab, uint64_t* bar, int lane,
+                                                unsigned* status)
 {
-    const uint32_t n = rules[tile.rule].n;
+    const LineRule& r = rules[tile.rule];
+    const uint32_t n = r.n;
+    const uint32_t tb = tab_floats(n) * 4u;    // 32-byte multiple, 32-byte aligned source
     const float* src = dens + tile.base;
     const void* map = static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.rule) * 128;
     if (kRows && (tile.face & TILE_TENSOR)) {
         if (lane == 0) {
-            mbar_arrive_expect_tx(bar, 32u * row_smem_pitch(n) * 4u);   // the whole box, fill included
+            mbar_arrive_expect_tx(bar, 32u * row_smem_pitch(n) * 4u + tb);   // the whole box, fill included
             tensor_load2(st, map, 0, static_cast<int>(tile.outer), bar);
+            bulk_load(stab, tab + r.tab, tb, bar);
         }
         return true;
     }
@@ -181,8 +187,9 @@ __device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const Lin
         if (lane == 0) {
             int c[3];
             tile_coords(tile, c);
-            mbar_arrive_expect_tx(bar, 32u * n * 4u);
+            mbar_arrive_expect_tx(bar, 32u * n * 4u + tb);
             tensor_load3(st, map, c[0], c[1], c[2], bar);
+            bulk_load(stab, tab + r.tab, tb, bar);
         }
         return true;
     }
@@ -194,8 +201,9 @@ __device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const Lin
                 mbar_arrive_expect_tx(bar, 0);
                 return false;
             }
-            mbar_arrive_expect_tx(bar, bytes);
+            mbar_arrive_expect_tx(bar, bytes + tb);
             bulk_load(st, src, bytes, bar);
+            bulk_load(stab, tab + r.tab, tb, bar);
         }
     } else {
         const uint32_t rb = col_row_bytes(tile.count);
@@ -206,7 +214,10 @@ __device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const Lin
             }
             return false;
         }
-        if (lane == 0) mbar_arrive_expect_tx(bar, rb * n);
+        if (lane == 0) {
+            mbar_arrive_expect_tx(bar, rb * n + tb);
+            bulk_load(stab, tab + r.tab, tb, bar);
+        }
         __syncwarp();
         for (uint32_t j = lane; j < n; j += 32) bulk_load(st + j * 32, src + static_cast<size_t>(j) * tile.rs, rb, bar);
     }
@@ -253,19 +264,14 @@ __device__ __forceinline__ void issue_tile_store(const SweepTile& tile, const Li
 
 // Coefficient table of one rule: line positions in chunks of 4, each chunk
 // 8 floats {g[4], inv[4]} (32-byte aligned), g_i = c / den_i, inv_i = 1 / den_i;
-// zero at the end nodes.
-__device__ __forceinline__ float tab_g(const float* __restrict__ t, int i) { return __ldg(t + ((i >> 2) << 3) + (i & 3)); }
-__device__ __forceinline__ float tab_inv(const float* __restrict__ t, int i)
+// zero at the end nodes.  The tile solves read the copy staged in shared
+// memory next to the tile.
+__device__ __forceinline__ float tab_g(const float* t, int i) { return t[((i >> 2) << 3) + (i & 3)]; }
+__device__ __forceinline__ float tab_inv(const float* t, int i) { return t[((i >> 2) << 3) + 4 + (i & 3)]; }
+__device__ __forceinline__ float4 tab_g4(const float* t, int q) { return *reinterpret_cast<const float4*>(t + (q << 3)); }
+__device__ __forceinline__ float4 tab_inv4(const float* t, int q)
 {
-    return __ldg(t + ((i >> 2) << 3) + 4 + (i & 3));
-}
-__device__ __forceinline__ float4 tab_g4(const float* __restrict__ t, int q)
-{
-    return __ldg(reinterpret_cast<const float4*>(t + (q << 3)));
-}
-__device__ __forceinline__ float4 tab_inv4(const float* __restrict__ t, int q)
-{
-    return __ldg(reinterpret_cast<const float4*>(t + (q << 3) + 4));
+    return *reinterpret_cast<const float4*>(t + (q << 3) + 4);
 }
 
 // One block of 8 positions (two table chunks) of the forward / backward
@@ -307,7 +313,7 @@ __device__ __forceinline__ float bwd8(float (&v)[8], const float4 (&g)[2], float
 // up to the one holding position n - 2 are read or written; values past
 // n - 2 in that chunk are written back unchanged.
 template <class LD, class ST>
-__device__ __forceinline__ void thomas_line(const float* __restrict__ t, int n, LD ld, ST st)
+__device__ __forceinline__ void thomas_line(const float* t, int n, LD ld, ST st)
 {
     const int ql = (n - 2) >> 2;       // chunk of the last interior position
     const int bl = ql >> 1;            // its block
@@ -365,7 +371,7 @@ __device__ __forceinline__ void thomas_line(const float* __restrict__ t, int n, 
 // the coefficients are one broadcast load, and each lane moves 4 values with
 // one 16-byte shared access; P / 4 is odd, so the 8 lanes of each quarter
 // warp hit 8 different 16-byte bank groups (no conflicts).
-__device__ __forceinline__ void solve_rows_vec(float* st, const LineRule& r, const float* __restrict__ t, int lane,
+__device__ __forceinline__ void solve_rows_vec(float* st, const LineRule& r, const float* t, int lane,
                                                int count)
 {
     if (lane >= count) return;
@@ -393,7 +399,7 @@ __device__ __forceinline__ void solve_rows_vec(float* st, const LineRule& r, con
 
 // y/z tile: lane = column, rows at st + j * 32 (32 lanes, 32 banks).
 __device__ __forceinline__ void solve_cols(float* st, const SweepTile& tile, const LineRule& r,
-                                           const float* __restrict__ t, int lane, bool apply_faces)
+                                           const float* t, int lane, bool apply_faces)
 {
     if (lane >= static_cast<int>(tile.count)) return;
     const int n = static_cast<int>(r.n);
@@ -426,19 +432,19 @@ __device__ __forceinline__ void solve_cols(float* st, const SweepTile& tile, con
 // solves line t stored at st + t * px.  Lane t reaches interior position i
 // at step i + t, so at every step the 32 lanes touch 32 different banks
 // (px is a multiple of 4, so px - 1 is odd).
-__device__ __forceinline__ void skew_step_fwd(float* p, const float* __restrict__ t, int i, float& d)
+__device__ __forceinline__ void skew_step_fwd(float* p, const float* t, int i, float& d)
 {
     d = fmaf(tab_g(t, i + 1), d, p[i] * tab_inv(t, i + 1));
     p[i] = d;
 }
-__device__ __forceinline__ void skew_step_bwd(float* p, const float* __restrict__ t, int i, float& x)
+__device__ __forceinline__ void skew_step_bwd(float* p, const float* t, int i, float& x)
 {
     x = fmaf(tab_g(t, i + 1), x, p[i]);
     p[i] = x;
 }
 
-__device__ __forceinline__ void solve_rows(float* st, const SweepTile& tile, const LineRule& r,
-                                           const float* __restrict__ t, int lane)
+__device__ __forceinline__ void solve_rows(float* st, const SweepTile& tile, const LineRule& r, const float* t,
+                                           int lane)
 {
     const int n = static_cast<int>(r.n);
     const int px = static_cast<int>(tile.rs);
@@ -493,9 +499,10 @@ template <bool kRows>
 __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
                                                    uint32_t ntiles, const LineRule* __restrict__ rules,
                                                    const float* __restrict__ tab, const void* __restrict__ tmaps,
-                                                   int stage_floats, int nstages, int apply_faces,
+                                                   int stage_floats, int nstages, int tab_area, int apply_faces,
                                                    const uint8_t* __restrict__ mask, unsigned* __restrict__ status)
 {
+    // stage: [tile data][tab_area floats of coefficient table]
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem) + warp * nstages;
@@ -512,8 +519,9 @@ __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, con
     bool ok = true;
     for (; issued < ntw && static_cast<int>(issued) < ahead; ++issued) {
         const int s = static_cast<int>(issued % nstages);
-        issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, tmaps, stages + s * stage_floats, &bars[s], lane,
-                               status);
+        float* st = stages + s * stage_floats;
+        issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, tab, tmaps, st, st + stage_floats - tab_area,
+                               &bars[s], lane, status);
     }
     for (uint32_t k = 0; k < ntw; ++k) {
         // refill: tile k + ahead goes to the stage of tile k - 1, whose store
@@ -522,8 +530,9 @@ __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, con
             bulk_wait_read<0>();
             __syncwarp();
             const int s = static_cast<int>(issued % nstages);
-            issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, tmaps, stages + s * stage_floats, &bars[s],
-                                   lane, status);
+            float* st = stages + s * stage_floats;
+            issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, tab, tmaps, st, st + stage_floats - tab_area,
+                                   &bars[s], lane, status);
             ++issued;
         }
         const int s = static_cast<int>(k % nstages);
@@ -534,12 +543,13 @@ __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, con
         const SweepTile tile = tiles[gw + k * tw];
         const LineRule r = rules[tile.rule];
         float* st = stages + s * stage_floats;
+        const float* t = st + stage_floats - tab_area;
         if (tile_on(r, mask)) {
             if (kRows) {
-                if (tile.face & TILE_TENSOR) solve_rows_vec(st, r, tab + r.tab, lane, static_cast<int>(tile.count));
-                else solve_rows(st, tile, r, tab + r.tab, lane);
+                if (tile.face & TILE_TENSOR) solve_rows_vec(st, r, t, lane, static_cast<int>(tile.count));
+                else solve_rows(st, tile, r, t, lane);
             } else {
-                solve_cols(st, tile, r, tab + r.tab, lane, apply_faces != 0);
+                solve_cols(st, tile, r, t, lane, apply_faces != 0);
             }
         }
         fence_async_smem();
@@ -567,12 +577,12 @@ __device__ __forceinline__ void solve_line(float* s, size_t st, const LineRule& 
         float d = 0.f;
         for (int i = 1; i <= n - 2; ++i) {
             const float f = (i == 1 || i == n - 2) ? r.fold : 0.f;
-            d = fmaf(tab_g(t, i), d, (s[i * st] + f) * tab_inv(t, i));
+            d = fmaf(__ldg(t + ((i >> 2) << 3) + (i & 3)), d, (s[i * st] + f) * __ldg(t + ((i >> 2) << 3) + 4 + (i & 3)));
             s[i * st] = d;
         }
         float x = 0.f;
         for (int i = n - 2; i >= 1; --i) {
-            x = fmaf(tab_g(t, i), x, s[i * st]);
+            x = fmaf(__ldg(t + ((i >> 2) << 3) + (i & 3)), x, s[i * st]);
             s[i * st] = x;
         }
     }
@@ -709,15 +719,18 @@ cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const Swee
                              const uint8_t* mask, unsigned* status, TmaCfg cfg)
 {
     if (ntiles == 0) return cudaSuccess;
+    // stages start 128-byte aligned (tensor copies), the table area on 32 bytes
+    if (cfg.stage_floats % 32 != 0 || cfg.tab_floats % 8 != 0 || cfg.tab_floats >= cfg.stage_floats)
+        return cudaErrorInvalidValue;
     const size_t smem = sweep_tma_smem(cfg.warps, cfg.stages, cfg.stage_floats);
     if (rows)
         k_sweep_tma<true><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, rules, tab, tmaps,
-                                                                   cfg.stage_floats, cfg.stages, apply_faces, mask,
-                                                                   status);
+                                                                   cfg.stage_floats, cfg.stages, cfg.tab_floats,
+                                                                   apply_faces, mask, status);
     else
         k_sweep_tma<false><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, rules, tab, tmaps,
-                                                                    cfg.stage_floats, cfg.stages, apply_faces, mask,
-                                                                    status);
+                                                                    cfg.stage_floats, cfg.stages, cfg.tab_floats,
+                                                                    apply_faces, mask, status);
     return cudaGetLastError();
 }
 

@@ -113,8 +113,9 @@ enum : uint8_t { STEP_DIFFUSE = 1u, STEP_MECH = 2u };
 // All launchers enqueue on 'st' and return the CUDA launch status.
 
 // Pipelined TMA sweeps: 'warps' warps per CTA, each with 'stages' shared
-// memory stages of 'stage_floats' floats; 'grid' persistent CTAs.
-struct TmaCfg { int warps; int stages; int stage_floats; int grid; };
+// memory stages of 'stage_floats' floats, the last 'tab_floats' of which
+// hold the tile's coefficient table; 'grid' persistent CTAs.
+struct TmaCfg { int warps; int stages; int stage_floats; int grid; int tab_floats; };
 
 // Longest line staged in shared memory; longer lines take the one-thread-
 // per-line kernel.  Tables are the chunked LineRule tables (float).

@@ -364,13 +364,17 @@ int Diffusion::build_axis(int axis)
 // shape; 0 takes the shape that keeps the most bytes in flight per SM.
 // Stage size: x tiles need 32 rows of the longest line's pitch (tensor
 // box or bulk copy); column tiles 32 x n rounded up to whole chunks of 4
-// rows, which the solve may read past the last row.
+// rows, which the solve may read past the last row; then the longest
+// line's coefficient table.
+static int tma_tab_floats(const SweepList& l) { return static_cast<int>(tab_floats(static_cast<uint32_t>(l.nmax))); }
 static int tma_stage_floats(const SweepList& l)
 {
     const uint32_t n = static_cast<uint32_t>(l.nmax);
     const uint32_t r4 = (n + 3u) & ~3u;
     const uint32_t span = l.kind == 0 ? std::max(row_smem_pitch(std::min(n, kRowTensorMaxN)), r4) : r4;
-    return static_cast<int>(32u * span);
+    // whole 128-byte units, so every stage starts 128-byte aligned (tensor
+    // copies need it); the table area then starts on 32 bytes
+    return static_cast<int>((32u * span + static_cast<uint32_t>(tma_tab_floats(l)) + 31u) / 32u * 32u);
 }
 
 int Diffusion::config_list(SweepList& l, int param)
@@ -404,6 +408,7 @@ int Diffusion::config_list(SweepList& l, int param)
     l.tc.warps = best_w;
     l.tc.stages = best_s;
     l.tc.stage_floats = sf;
+    l.tc.tab_floats = tma_tab_floats(l);
     const uint64_t ctas = (l.n + best_w - 1) / best_w;
     l.tc.grid = static_cast<int>(std::min<uint64_t>(ctas, static_cast<uint64_t>(best_occ) * ctx->sms));
     return PCG_OK;
