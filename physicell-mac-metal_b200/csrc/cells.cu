@@ -44,65 +44,110 @@ __global__ void k_sec_keys(const float* __restrict__ soa, uint32_t stride, uint3
     vals[g] = g;
 }
 
-// coef3[(rate index) * 3 + {0,1,2}] = {dt*ne/V_vox, ic*sec*sat, 1 + ic*(sec+upt)}
-// with ic = dt*V_cell/V_vox, exactly as processSecretion forms them.
-__global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, uint32_t n,
-                              const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
-                              const double* __restrict__ rates4, uint32_t n_rate, double dt,
-                              double* __restrict__ coef3)
+// Runs of the sorted order.  A run is the cells of one voxel (equal keys);
+// heads[p] = 1 at the first position of each run, sbeg[i] = first sorted
+// position of instance i's cells (valid keys form a prefix of the order and
+// instances occupy increasing key ranges).  heads has n + 1 entries.
+__global__ void k_sec_heads(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder, uint32_t n,
+                            const uint32_t* __restrict__ cell_inst, uint32_t invalid_key, uint32_t* __restrict__ heads,
+                            uint32_t* __restrict__ sbeg)
 {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    const CellInst& in = insts[cell_inst[g]];
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > n) return;
+    if (p == n) {
+        heads[n] = 0;
+        return;
+    }
+    const uint32_t key = skeys[p];
+    const bool valid = key < invalid_key;
+    heads[p] = (valid && (p == 0 || skeys[p - 1] != key)) ? 1u : 0u;
+    if (valid) {
+        const uint32_t ii = cell_inst[sorder[p]];
+        if (p == 0 || cell_inst[sorder[p - 1]] != ii) sbeg[ii] = p;
+    }
+}
+
+// rid = exclusive scan of heads: run r starts at run_start[r] and ends at
+// run_start[r + 1]; run_start[n_runs] is the first invalid position (or n).
+__global__ void k_sec_runs(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder, uint32_t n,
+                           const uint32_t* __restrict__ cell_inst, uint32_t invalid_key, const uint32_t* __restrict__ rid,
+                           uint32_t* __restrict__ run_start, uint32_t* __restrict__ run_inst)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > n) return;
+    const bool valid = p < n && skeys[p] < invalid_key;
+    if (valid && (p == 0 || skeys[p - 1] != skeys[p])) {
+        const uint32_t r = rid[p];
+        run_start[r] = p;
+        run_inst[r] = cell_inst[sorder[p]];
+    }
+    if (!valid && (p == 0 || skeys[p - 1] < invalid_key)) run_start[rid[p]] = p;
+}
+
+// Secretion constants in sorted order: cell sorder[q] of instance i goes to
+// rate slot in.rate_off + (q - sbeg[i]) * S (+ s), as
+// cs[3 * slot + {0,1,2}] = {dt*ne/V_vox, ic*sec*sat, 1 + ic*(sec+upt)} with
+// ic = dt*V_cell/V_vox, exactly as processSecretion forms them
+// (cell_phenotype.cpp:526-564).
+__global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, uint32_t n,
+                              const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder,
+                              const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
+                              const uint32_t* __restrict__ sbeg, uint32_t invalid_key,
+                              const double* __restrict__ rates4, uint32_t n_rate, double dt, double* __restrict__ cs)
+{
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n || skeys[q] >= invalid_key) return;
+    const uint32_t g = sorder[q];
+    const uint32_t ii = cell_inst[g];
+    const CellInst& in = insts[ii];
     const double V_vox = __dmul_rn(__dmul_rn(static_cast<double>(in.dx), static_cast<double>(in.dy)),
                                    static_cast<double>(in.dz));
     const double V_cell = static_cast<double>(soa[static_cast<size_t>(F_TOTAL_VOL) * stride + g]);
     const double ic = __ddiv_rn(__dmul_rn(dt, V_cell), V_vox);
-    const uint32_t base = in.rate_off + (g - in.cell_off) * in.S;
+    const uint32_t src = in.rate_off + (g - in.cell_off) * in.S;
+    const uint32_t dst = in.rate_off + (q - sbeg[ii]) * in.S;
     for (uint32_t s = 0; s < in.S; ++s) {
-        const uint32_t o = base + s;
+        const uint32_t o = src + s;
         const double sec = rates4[o], upt = rates4[n_rate + o], sat = rates4[2ull * n_rate + o],
                      ne = rates4[3ull * n_rate + o];
-        coef3[3ull * o + 0] = __ddiv_rn(__dmul_rn(dt, ne), V_vox);
-        coef3[3ull * o + 1] = __dmul_rn(__dmul_rn(ic, sec), sat);
-        coef3[3ull * o + 2] = __dadd_rn(1.0, __dmul_rn(ic, __dadd_rn(sec, upt)));
+        double* c = cs + 3ull * (dst + s);
+        c[0] = __ddiv_rn(__dmul_rn(dt, ne), V_vox);
+        c[1] = __dmul_rn(__dmul_rn(ic, sec), sat);
+        c[2] = __dadd_rn(1.0, __dmul_rn(ic, __dadd_rn(sec, upt)));
     }
 }
 
-// One thread per run of equal keys in the sorted order: applies the run's
-// cells to the voxel in ascending cell index, substrate by substrate.
+// One thread per (run, substrate = blockIdx.y): applies the run's cells to
+// the voxel in ascending cell index (the stable order), FP64 per cell with
+// the FP32 store after each cell.
 __global__ void k_secrete(float* __restrict__ dens, const uint32_t* __restrict__ skeys,
-                          const uint32_t* __restrict__ sorder, uint32_t n, const uint32_t* __restrict__ cell_inst,
-                          const CellInst* __restrict__ insts, const double* __restrict__ coef3, uint32_t invalid_key,
+                          const uint32_t* __restrict__ run_start, const uint32_t* __restrict__ run_inst,
+                          const uint32_t* __restrict__ n_runs, const CellInst* __restrict__ insts,
+                          const uint32_t* __restrict__ sbeg, const double* __restrict__ cs,
                           const uint8_t* __restrict__ mask)
 {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    const uint32_t key = skeys[p];
-    if (key >= invalid_key) return;
-    if (p > 0 && skeys[p - 1] == key) return;
-    uint32_t q_end = p + 1;
-    while (q_end < n && skeys[q_end] == key) ++q_end;
-    const uint32_t ii = cell_inst[sorder[p]];
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = blockIdx.y;
+    if (r >= *n_runs) return;
+    const uint32_t ii = run_inst[r];
     if (mask && !(mask[ii] & STEP_DIFFUSE)) return;
     const CellInst& in = insts[ii];
-    const uint32_t v = key - in.vox_base;
+    if (s >= in.S) return;
+    const uint32_t p0 = run_start[r], p1 = run_start[r + 1];
+    const uint32_t v = skeys[p0] - in.vox_base;
     // dense voxel index -> padded-row device offset
     const uint64_t off = static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
-    for (uint32_t s = 0; s < in.S; ++s) {
-        float* d = dens + in.dens_off + s * in.sub_pitch + off;
-        float rho32 = *d;
-        for (uint32_t q = p; q < q_end; ++q) {
-            const uint32_t g = sorder[q];
-            const double* c = coef3 + 3ull * (in.rate_off + (g - in.cell_off) * in.S + s);
-            double rho = static_cast<double>(rho32);
-            rho = __dadd_rn(rho, c[0]);
-            rho = __ddiv_rn(__dadd_rn(rho, c[1]), c[2]);
-            if (rho < 0.0) rho = 0.0;
-            rho32 = __double2float_rn(rho);
-        }
-        *d = rho32;
+    float* d = dens + in.dens_off + s * in.sub_pitch + off;
+    const double* c = cs + 3ull * (in.rate_off + (p0 - sbeg[ii]) * in.S + s);
+    float rho32 = *d;
+    for (uint32_t q = p0; q < p1; ++q, c += 3ull * in.S) {
+        double rho = static_cast<double>(rho32);
+        rho = __dadd_rn(rho, c[0]);
+        rho = __ddiv_rn(__dadd_rn(rho, c[1]), c[2]);
+        if (rho < 0.0) rho = 0.0;
+        rho32 = __double2float_rn(rho);
     }
+    *d = rho32;
 }
 
 // ------------------------------------------------------------------ mechanics
@@ -310,21 +355,38 @@ cudaError_t launch_sec_keys(cudaStream_t st, const float* soa, uint32_t stride, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
-                               const uint32_t* cell_inst, const CellInst* insts, const double* rates4, uint32_t n_rate,
-                               double dt, double* coef3)
+cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
+                            const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* heads_rid, uint32_t* sbeg,
+                            uint32_t* run_start, uint32_t* run_inst, void* scan_scratch)
 {
-    if (n == 0) return cudaSuccess;
-    k_sec_prepare<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, rates4, n_rate, dt, coef3);
+    k_sec_heads<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, sorder, n, cell_inst, invalid_key, heads_rid, sbeg);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = scan_exclusive(st, heads_rid, heads_rid, static_cast<uint64_t>(n) + 1, scan_scratch);
+    if (e != cudaSuccess) return e;
+    k_sec_runs<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, sorder, n, cell_inst, invalid_key, heads_rid, run_start,
+                                                         run_inst);
     return cudaGetLastError();
 }
 
-cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
-                           const uint32_t* cell_inst, const CellInst* insts, const double* coef3, uint32_t invalid_key,
-                           const uint8_t* mask)
+cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n, const uint32_t* skeys,
+                               const uint32_t* sorder, const uint32_t* cell_inst, const CellInst* insts,
+                               const uint32_t* sbeg, uint32_t invalid_key, const double* rates4, uint32_t n_rate,
+                               double dt, double* cs)
 {
     if (n == 0) return cudaSuccess;
-    k_secrete<<<blocks_for(n, 256), 256, 0, st>>>(dens, skeys, sorder, n, cell_inst, insts, coef3, invalid_key, mask);
+    k_sec_prepare<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, skeys, sorder, cell_inst, insts, sbeg,
+                                                       invalid_key, rates4, n_rate, dt, cs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, const uint32_t* run_start,
+                           const uint32_t* run_inst, const uint32_t* n_runs, uint32_t max_runs, uint32_t max_s,
+                           const CellInst* insts, const uint32_t* sbeg, const double* cs, const uint8_t* mask)
+{
+    if (max_runs == 0 || max_s == 0) return cudaSuccess;
+    dim3 grid(blocks_for(max_runs, 256), max_s);
+    k_secrete<<<grid, 256, 0, st>>>(dens, skeys, run_start, run_inst, n_runs, insts, sbeg, cs, mask);
     return cudaGetLastError();
 }
 

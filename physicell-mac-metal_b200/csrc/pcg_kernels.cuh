@@ -150,16 +150,25 @@ struct GradJob { uint64_t base; uint64_t out_base; uint32_t nx, ny, nz, px; floa
 cudaError_t launch_gradients(cudaStream_t st, const float* dens, float* gx, float* gy, float* gz,
                              const GradJob* jobs, uint32_t njobs, uint64_t max_voxels);
 
-// Secretion: keys / coefficient preparation / ordered application.
+// Secretion: keys, then (after the stable sort by key) the run list of the
+// sorted order, constants in sorted order and the ordered application.
 cudaError_t launch_sec_keys(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
                             const uint32_t* cell_inst, const CellInst* insts, const uint8_t* active,
                             uint32_t invalid_key, uint32_t* keys, uint32_t* vals);
-cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
-                               const uint32_t* cell_inst, const CellInst* insts, const double* rates4,
-                               uint32_t n_rate, double dt_override, double* coef3);
-cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, const uint32_t* sorder,
-                           uint32_t n, const uint32_t* cell_inst, const CellInst* insts,
-                           const double* coef3, uint32_t invalid_key, const uint8_t* mask);
+// heads_rid: n + 1 entries (run index of every position; [n] = run count);
+// run_start: n + 1 entries; run_inst: n; sbeg: one per instance;
+// scan_scratch: scan_scratch_bytes(n + 1).
+cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
+                            const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* heads_rid, uint32_t* sbeg,
+                            uint32_t* run_start, uint32_t* run_inst, void* scan_scratch);
+cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n, const uint32_t* skeys,
+                               const uint32_t* sorder, const uint32_t* cell_inst, const CellInst* insts,
+                               const uint32_t* sbeg, uint32_t invalid_key, const double* rates4, uint32_t n_rate,
+                               double dt, double* cs);
+// n_runs: device count (heads_rid[n]); max_runs >= it; max_s = largest S.
+cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, const uint32_t* run_start,
+                           const uint32_t* run_inst, const uint32_t* n_runs, uint32_t max_runs, uint32_t max_s,
+                           const CellInst* insts, const uint32_t* sbeg, const double* cs, const uint8_t* mask);
 
 // Mechanics.
 cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,

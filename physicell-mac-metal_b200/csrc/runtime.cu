@@ -684,8 +684,12 @@ int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_
     PCG_CU(ctx, coef.alloc(3 * rc * sizeof(double)));
     PCG_CU(ctx, active.alloc(max_cells));
     for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp})
-        PCG_CU(ctx, b->alloc(static_cast<size_t>(max_cells) * sizeof(uint32_t)));
+        PCG_CU(ctx, b->alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint32_t)));
     PCG_CU(ctx, sort_scr.alloc(radix_sort_scratch_bytes(max_cells, 32)));
+    PCG_CU(ctx, sbeg.alloc(h_inst.size() * sizeof(uint32_t)));
+    PCG_CU(ctx, cudaMemset(sbeg.p, 0, sbeg.bytes));
+    PCG_CU(ctx, run_scr.alloc(scan_scratch_bytes(static_cast<uint64_t>(max_cells) + 1)));
+    PCG_CU(ctx, cudaMemset(ktmp.p, 0, ktmp.bytes));   // run count 0 until the first order
     inst_dirty = coef_dirty = order_dirty = true;
     return PCG_OK;
 }
@@ -776,40 +780,55 @@ int Cells::build_order(uint64_t total_vox)
     e = radix_sort_pairs(ctx->stream, keys.as<uint32_t>(), vals.as<uint32_t>(), skeys.as<uint32_t>(),
                          sorder.as<uint32_t>(), ktmp.as<uint32_t>(), vtmp.as<uint32_t>(), n, key_bits, sort_scr.p);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion sort");
-    ctx->launches += 1 + radix_sort_launches(n, key_bits);
+    e = launch_sec_runs(ctx->stream, skeys.as<uint32_t>(), sorder.as<uint32_t>(), n, cell_inst.as<uint32_t>(),
+                        invalid_key, ktmp.as<uint32_t>(), sbeg.as<uint32_t>(), vals.as<uint32_t>(), vtmp.as<uint32_t>(),
+                        run_scr.p);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion runs");
+    ctx->launches += 1 + radix_sort_launches(n, key_bits) + 2 + scan_launches(static_cast<uint64_t>(n) + 1);
     order_dirty = false;
+    if (coef_dt >= 0.0) PCG_TRY(sorted_constants());   // constants follow the order
+    return PCG_OK;
+}
+
+int Cells::sorted_constants()
+{
+    const uint32_t cap = static_cast<uint32_t>(rates.bytes / (4 * sizeof(double)));
+    cudaError_t e = launch_sec_prepare(ctx->stream, soa.as<float>(), max_cells, n, skeys.as<uint32_t>(),
+                                       sorder.as<uint32_t>(), cell_inst.as<uint32_t>(), inst.as<CellInst>(),
+                                       sbeg.as<uint32_t>(), invalid_key, rates.as<double>(), cap, coef_dt,
+                                       coef.as<double>());
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion prepare");
+    if (n) ctx->launches++;
+    coef_dirty = false;
     return PCG_OK;
 }
 
 int Cells::prepare_secretion(double dt, uint64_t total_vox)
 {
     PCG_TRY(sync_inst());
-    if (coef_dirty || coef_dt != dt) {
-        const uint32_t cap = static_cast<uint32_t>(rates.bytes / (4 * sizeof(double)));
-        cudaError_t e = launch_sec_prepare(ctx->stream, soa.as<float>(), max_cells, n, cell_inst.as<uint32_t>(),
-                                           inst.as<CellInst>(), rates.as<double>(), cap, dt, coef.as<double>());
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion prepare");
-        ctx->launches++;
-        coef_dirty = false;
-        coef_dt = dt;
-    }
-    if (order_dirty || invalid_key != static_cast<uint32_t>(total_vox)) PCG_TRY(build_order(total_vox));
+    const bool stale = coef_dirty || coef_dt != dt;
+    coef_dt = dt;
+    if (order_dirty || invalid_key != static_cast<uint32_t>(total_vox)) return build_order(total_vox);
+    if (stale) return sorted_constants();
     return PCG_OK;
 }
 
 int Cells::secrete(Diffusion& d, const uint8_t* mask)
 {
-    cudaError_t e = launch_secrete(ctx->stream, d.dens.as<float>(), skeys.as<uint32_t>(), sorder.as<uint32_t>(), n,
-                                   cell_inst.as<uint32_t>(), inst.as<CellInst>(), coef.as<double>(), invalid_key, mask);
+    uint32_t max_s = 0;
+    for (const CellInst& ci : h_inst) max_s = std::max(max_s, ci.S);
+    cudaError_t e = launch_secrete(ctx->stream, d.dens.as<float>(), skeys.as<uint32_t>(), vals.as<uint32_t>(),
+                                   vtmp.as<uint32_t>(), ktmp.as<uint32_t>() + n, n, max_s, inst.as<CellInst>(),
+                                   sbeg.as<uint32_t>(), coef.as<double>(), mask);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion launch");
-    ctx->launches++;
+    if (n && max_s) ctx->launches++;
     return PCG_OK;
 }
 
 uint64_t Cells::device_bytes() const
 {
     return inst.bytes + soa.bytes + cell_inst.bytes + rates.bytes + coef.bytes + active.bytes + keys.bytes + vals.bytes +
-           skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes;
+           skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + sbeg.bytes + run_scr.bytes;
 }
 
 // ------------------------------------------------------------------ mechanics

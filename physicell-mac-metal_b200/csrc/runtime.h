@@ -171,8 +171,11 @@ public:
     bool has_active = false;
     bool inst_dirty = true, coef_dirty = true, order_dirty = true;
     double coef_dt = -1.0;
-    // secretion ordering
-    DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr;
+    // secretion ordering: keys/vals sort input, (skeys, sorder) the order;
+    // after the sort ktmp holds the run index of every position (+ count),
+    // vals the run starts and vtmp the run instances; coef the constants
+    // in sorted order
+    DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr, sbeg, run_scr;
     uint32_t invalid_key = 0;
     int key_bits = 0;
 
@@ -188,7 +191,8 @@ public:
     int set_cell_instances(const std::vector<uint32_t>& per_instance_counts);
     // Recompute secretion constants / ordering when stale.
     int prepare_secretion(double dt, uint64_t total_vox);
-    int build_order(uint64_t total_vox);
+    int build_order(uint64_t total_vox);   // order, runs and (once a dt is known) the constants
+    int sorted_constants();
     int secrete(Diffusion& d, const uint8_t* mask);
     uint64_t device_bytes() const;
 };
