@@ -186,8 +186,10 @@ __global__ void k_mech_gather(const float* __restrict__ soa, uint32_t stride, co
     const uint32_t g = sorder[p];
     spos[p] = make_float4(soa[static_cast<size_t>(F_POS_X) * stride + g], soa[static_cast<size_t>(F_POS_Y) * stride + g],
                           soa[static_cast<size_t>(F_POS_Z) * stride + g], soa[static_cast<size_t>(F_RADIUS) * stride + g]);
-    sprm[p] = make_float4(soa[static_cast<size_t>(F_REPULSION) * stride + g],
-                          soa[static_cast<size_t>(F_ADHESION) * stride + g],
+    // square roots of the (non-negative) strengths: the pair factors
+    // sqrt(rep_i rep_j), sqrt(adh_i adh_j) become one product each
+    sprm[p] = make_float4(sqrtf(soa[static_cast<size_t>(F_REPULSION) * stride + g]),
+                          sqrtf(soa[static_cast<size_t>(F_ADHESION) * stride + g]),
                           soa[static_cast<size_t>(F_REL_MAX_ADH) * stride + g], 0.0f);
 }
 
@@ -206,8 +208,27 @@ __device__ __forceinline__ uint32_t nbr_hash(uint32_t j)
 // one contiguous range of the sorted order covering di = -1..1, which the G
 // lanes stride through; partial sums are combined with a fixed xor-shuffle
 // tree, so the result does not depend on scheduling.
-template <int G>
-__global__ void __launch_bounds__(512) k_mech_forces(const float4* __restrict__ spos, const float4* __restrict__ sprm,
+// Distance from c to the mechanics-voxel slab [lo, lo + vs) along one axis,
+// slabs at the grid edge reaching to infinity (clamped cells), minus a
+// 0.01 um margin that covers FP32 rounding of positions and bounds.
+__device__ __forceinline__ float slab_gap(float c, float lo, float vs, int idx, int nidx)
+{
+    const float l = idx == 0 ? -INFINITY : lo;
+    const float h = idx == nidx - 1 ? INFINITY : lo + vs;
+    return fmaxf(fmaxf(l - c, c - h) - 0.01f, 0.0f);
+}
+
+// One thread per cell (sorted order p): candidates are visited in the
+// reference's order (dk, dj, di, then the voxel's cells in ascending index;
+// mechanics.metal:125-208) and summed sequentially.  The nine voxel rows'
+// ranges in the cell-start table are loaded up front; rows (and side voxels
+// of a row) that lie entirely beyond the interaction distance are skipped,
+// and the next candidate's position is loaded while the current one is
+// tested.  The neighbour test is the reference's FP32 one without
+// contraction (mechanics.metal:159-165), so neighbour sets are exact; the
+// force terms (mechanics.metal:167-208) use reciprocal / rsqrt forms and
+// per-cell square roots of the strengths (a few ulp per term).
+__global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ spos, const float4* __restrict__ sprm,
                                                      const uint32_t* __restrict__ skeys,
                                                      const uint32_t* __restrict__ sorder,
                                                      const uint32_t* __restrict__ start, uint32_t n,
@@ -217,89 +238,84 @@ __global__ void __launch_bounds__(512) k_mech_forces(const float4* __restrict__ 
                                                      uint32_t* __restrict__ diag_hash,
                                                      const uint8_t* __restrict__ mask)
 {
-    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t p = gid / G;
-    const int sub = static_cast<int>(gid % G);
-    bool valid = p < n;
-    float fx = 0.f, fy = 0.f, fz = 0.f, P = 0.f;
-    uint32_t cnt = 0, hsh = 0, g = 0;
-    if (valid) {
-        g = sorder[p];
-        const uint32_t ii = cell_inst[g];
-        if (mask && !(mask[ii] & STEP_MECH)) valid = false;
-    }
-    if (valid) {
-        const CellInst& in = insts[cell_inst[g]];
-        const float4 me = spos[p];
-        const float4 mp = sprm[p];
-        const uint32_t local = skeys[p] - in.mvox_base;
-        const int mnx = static_cast<int>(in.mnx), mny = static_cast<int>(in.mny), mnz = static_cast<int>(in.mnz);
-        const int ci = static_cast<int>(local % in.mnx);
-        const int cj = static_cast<int>((local / in.mnx) % in.mny);
-        const int ck = static_cast<int>(local / (in.mnx * in.mny));
-        const float maxd2 = __fmul_rn(in.maxd, in.maxd);
-        const int ilo = ci > 0 ? ci - 1 : 0, ihi = ci + 1 < mnx ? ci + 1 : mnx - 1;
-        const int dk0 = mnz > 1 ? -1 : 0, dk1 = mnz > 1 ? 1 : 0;
-        for (int dk = dk0; dk <= dk1; ++dk) {
-            const int nk = ck + dk;
-            if (nk < 0 || nk >= mnz) continue;
-            for (int dj = -1; dj <= 1; ++dj) {
-                const int nj = cj + dj;
-                if (nj < 0 || nj >= mny) continue;
-                const uint32_t row = in.mvox_base + static_cast<uint32_t>(nk * mny + nj) * static_cast<uint32_t>(mnx);
-                const uint32_t q0 = start[row + ilo], q1 = start[row + ihi + 1];
-                for (uint32_t q = q0 + sub; q < q1; q += G) {
-                    if (q == p) continue;
-                    const float4 o = spos[q];
-                    // neighbour test exactly as mechanics.metal:159-165 (no contraction)
-                    const float ddx = __fsub_rn(me.x, o.x), ddy = __fsub_rn(me.y, o.y), ddz = __fsub_rn(me.z, o.z);
-                    const float dsq = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
-                    if (dsq >= maxd2 || dsq < 1e-12f) continue;
-                    if (diag_cnt) {
-                        ++cnt;
-                        hsh += nbr_hash(sorder[q] - in.cell_off);
-                    }
-                    const float dist = sqrtf(dsq);
-                    const float inv = 1.0f / dist;
-                    const float R = me.w + o.w;
-                    float F = 0.f;
-                    if (dist < R) {
-                        const float4 op = sprm[q];
-                        const float ov = 1.0f - dist / R;
-                        F += ov * ov * sqrtf(mp.x * op.x);
-                        P += ov * ov / 0.027288820670331f;
-                    }
-                    const float A = mp.z * R;
-                    if (dist < A) {
-                        const float op_adh = sprm[q].y;
-                        const float t = 1.0f - dist / A;
-                        F -= t * t * sqrtf(mp.y * op_adh);
-                    }
-                    fx += F * (ddx * inv);
-                    fy += F * (ddy * inv);
-                    fz += F * (ddz * inv);
-                }
-            }
-        }
-    }
+    constexpr float kInvPressureScale = 1.0f / 0.027288820670331f;
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint32_t g = sorder[p];
+    const uint32_t ii = cell_inst[g];
+    if (mask && !(mask[ii] & STEP_MECH)) return;
+    const CellInst& in = insts[ii];
+    const float4 me = spos[p];
+    const float4 mp = sprm[p];
+    const uint32_t local = skeys[p] - in.mvox_base;
+    const int mnx = static_cast<int>(in.mnx), mny = static_cast<int>(in.mny), mnz = static_cast<int>(in.mnz);
+    const int ci = static_cast<int>(local % in.mnx);
+    const int cj = static_cast<int>((local / in.mnx) % in.mny);
+    const int ck = static_cast<int>(local / (in.mnx * in.mny));
+    const float vs = in.vs;
+    const float maxd2 = __fmul_rn(in.maxd, in.maxd);
+    const int ilo = ci > 0 ? ci - 1 : 0, ihi = ci + 1 < mnx ? ci + 1 : mnx - 1;
+    const float gxl = ci > 0 ? slab_gap(me.x, in.mx_min + (ci - 1) * vs, vs, ci - 1, mnx) : 0.f;
+    const float gxr = ci + 1 < mnx ? slab_gap(me.x, in.mx_min + (ci + 1) * vs, vs, ci + 1, mnx) : 0.f;
+    // row ranges [q0, q1) of the cell-start table, dk-major then dj
+    uint32_t rq0[9], rq1[9];
 #pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) {
-        fx += __shfl_xor_sync(0xffffffffu, fx, o);
-        fy += __shfl_xor_sync(0xffffffffu, fy, o);
-        fz += __shfl_xor_sync(0xffffffffu, fz, o);
-        P += __shfl_xor_sync(0xffffffffu, P, o);
-        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-        hsh += __shfl_xor_sync(0xffffffffu, hsh, o);
+    for (int r = 0; r < 9; ++r) {
+        const int dk = r / 3 - 1, dj = r % 3 - 1;
+        const int nk = ck + dk, nj = cj + dj;
+        rq0[r] = rq1[r] = 0;
+        if ((mnz == 1 && dk != 0) || nk < 0 || nk >= mnz || nj < 0 || nj >= mny) continue;
+        const float gz = mnz > 1 ? slab_gap(me.z, in.mz_min + nk * vs, vs, nk, mnz) : 0.f;
+        const float gy = slab_gap(me.y, in.my_min + nj * vs, vs, nj, mny);
+        const float gyz = gy * gy + gz * gz;
+        if (gyz >= maxd2) continue;   // the whole row is out of reach
+        const int i0 = (ilo < ci && gxl * gxl + gyz < maxd2) ? ilo : ci;
+        const int i1 = (ihi > ci && gxr * gxr + gyz < maxd2) ? ihi : ci;
+        const uint32_t row = in.mvox_base + static_cast<uint32_t>(nk * mny + nj) * static_cast<uint32_t>(mnx);
+        rq0[r] = start[row + i0];
+        rq1[r] = start[row + i1 + 1];
     }
-    if (valid && sub == 0) {
-        soa[static_cast<size_t>(F_VEL_X) * stride + g] = fx;
-        soa[static_cast<size_t>(F_VEL_Y) * stride + g] = fy;
-        soa[static_cast<size_t>(F_VEL_Z) * stride + g] = fz;
-        soa[static_cast<size_t>(F_PRESSURE) * stride + g] = P;
-        if (diag_cnt) {
-            diag_cnt[g] = cnt;
-            diag_hash[g] = hsh;
+    float fx = 0.f, fy = 0.f, fz = 0.f, P = 0.f;
+    uint32_t cnt = 0, hsh = 0;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        uint32_t q = rq0[r];
+        const uint32_t q1 = rq1[r];
+        float4 o = q < q1 ? spos[q] : me;
+        for (; q < q1; ++q) {
+            const float4 cur = o;
+            if (q + 1 < q1) o = spos[q + 1];   // next candidate in flight
+            if (q == p) continue;
+            // neighbour test exactly as mechanics.metal:159-165 (no contraction)
+            const float ddx = __fsub_rn(me.x, cur.x), ddy = __fsub_rn(me.y, cur.y), ddz = __fsub_rn(me.z, cur.z);
+            const float dsq = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
+            if (dsq >= maxd2 || dsq < 1e-12f) continue;
+            if (diag_cnt) {
+                ++cnt;
+                hsh += nbr_hash(sorder[q] - in.cell_off);
+            }
+            const float inv = rsqrtf(dsq);
+            const float dist = dsq * inv;
+            const float R = me.w + cur.w;
+            const float4 op = sprm[q];
+            const float ov = fmaxf(1.0f - __fdividef(dist, R), 0.0f);         // repulsion overlap
+            const float t = fmaxf(1.0f - __fdividef(dist, mp.z * R), 0.0f);    // adhesion reach
+            const float ov2 = ov * ov;
+            const float F = ov2 * (mp.x * op.x) - t * t * (mp.y * op.y);
+            P += ov2 * kInvPressureScale;
+            const float Fi = F * inv;
+            fx += Fi * ddx;
+            fy += Fi * ddy;
+            fz += Fi * ddz;
         }
+    }
+    soa[static_cast<size_t>(F_VEL_X) * stride + g] = fx;
+    soa[static_cast<size_t>(F_VEL_Y) * stride + g] = fy;
+    soa[static_cast<size_t>(F_VEL_Z) * stride + g] = fz;
+    soa[static_cast<size_t>(F_PRESSURE) * stride + g] = P;
+    if (diag_cnt) {
+        diag_cnt[g] = cnt;
+        diag_hash[g] = hsh;
     }
 }
 
@@ -414,8 +430,8 @@ cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4
 {
     if (n == 0) return cudaSuccess;
     const unsigned grid = blocks_for(static_cast<uint64_t>(n) * kForceLanes, block);
-    k_mech_forces<kForceLanes><<<grid, block, 0, st>>>(spos, sprm, skeys, sorder, start, n, cell_inst, insts, soa,
-                                                        stride, diag_cnt, diag_hash, mask);
+    k_mech_forces<<<grid, block, 0, st>>>(spos, sprm, skeys, sorder, start, n, cell_inst, insts, soa, stride, diag_cnt,
+                                          diag_hash, mask);
     return cudaGetLastError();
 }
 

@@ -184,9 +184,10 @@ cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4
 cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
                                   const uint32_t* cell_inst, const CellInst* insts, float dt_override,
                                   const uint8_t* mask);
-// Lanes per cell in the force pass; fixed so that a cell's summation order
-// never depends on what else is in the batch.
-constexpr int kForceLanes = 8;
+// Threads per cell in the force pass: one, summing in the reference's
+// candidate order, so a cell's result never depends on what else is in the
+// batch.
+constexpr int kForceLanes = 1;
 
 // Radix sort of (key, value) pairs, stable, 'bits' significant key bits.
 // Scratch from radix_sort_scratch_bytes().  Result lands in (k_out, v_out).
