@@ -19,6 +19,9 @@ Reports (one JSON line on rank 0):
   cpu_baseline     the multi-threaded FP32 CPU port on a bounded sample
   plain            the same instances advanced one at a time through the
                    single-simulation API (Microenvironment / CellMechanics)
+  serving          config 4 on a bounded horizon: Poisson request arrivals
+                   served by continuous batching; p50/p99 time-to-result
+                   and aggregate voxel-steps/s, cell-steps/s
 Multi-GPU: one process per GPU, each rank runs its own 64-instance batch
 (seed offset by rank, no collective on the data path): weak scaling.
 --impl reference times the CPU port alone (the reference's shaders exist
@@ -68,6 +71,8 @@ def traffic_summary():
 
 
 class ClockSampler:
+    """nvidia-smi samples (50 ms) taken by a reader thread, each stamped on
+    arrival; only the samples inside [begin(), end()] are summarised."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -75,27 +80,48 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.lines = []
+        self.t0 = self.t1 = None
 
     def start(self):
+        import threading
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return
+        def reader():
+            for line in self.proc.stdout:
+                self.lines.append((time.monotonic(), line))
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+        deadline = time.monotonic() + 10.0   # wait until the sampler is producing
+        while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
+            time.sleep(0.02)
+
+    def begin(self):
+        self.t0 = time.monotonic()
+
+    def end(self):
+        self.t1 = time.monotonic()
 
     def stop(self):
         if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-            out = ""
+        t0 = self.t0 if self.t0 is not None else float("-inf")
+        t1 = self.t1 if self.t1 is not None else float("inf")
         sm, smax, reasons = [], [], set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for line in out.strip().splitlines():
+        for t, line in list(self.lines):
+            if not (t0 <= t <= t1):
+                continue
             p = [x.strip() for x in line.split(",")]
             if len(p) < 9:
                 continue
@@ -277,16 +303,51 @@ def plain_path(pcg, ctx, insts, periods):
     return secs
 
 
+def serving_leg(pcg, ctx, horizon_s):
+    """Config 4 on a bounded horizon: Poisson arrivals (20 req/s, seeded) of
+    mixed 2-D / 3-D parameter-sweep requests submitted in real time to the
+    continuous-batching server (150 GB budget); runs until every request is
+    done.  Time-to-result = submit -> results on the host."""
+    from pcg import workloads
+    reqs = workloads.serving_requests(horizon_s=horizon_s)
+    srv = pcg.Server(ctx, budget_bytes=150e9, steps_per_tick=100)
+    ids = []
+    i = 0
+    t0 = time.perf_counter()
+    peak_running = 0
+    while True:
+        now = time.perf_counter() - t0
+        while i < len(reqs) and reqs[i][0] <= now:
+            ids.append(srv.submit(reqs[i][1], reqs[i][2]))
+            i += 1
+        running, queued, _ = srv.tick()
+        peak_running = max(peak_running, running)
+        if running == 0 and queued == 0:
+            if i == len(reqs):
+                break
+            time.sleep(max(0.0, min(0.01, reqs[i][0] - (time.perf_counter() - t0))))
+    wall = time.perf_counter() - t0
+    lat = np.array([srv.times(r)[0] for r in ids])
+    vox, cells, _ = srv.totals()
+    srv.close()
+    return {"requests": len(ids), "horizon_s": horizon_s, "arrival_rate_per_s": 20.0, "wall_s": wall,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "voxel_steps_per_s": vox / wall, "cell_steps_per_s": cells / wall, "peak_running": peak_running,
+            "budget_bytes": 150e9}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tune-cache", default=None, help="JSON file of autotuned launch shapes (read and updated)")
+    ap.add_argument("--serve-horizon", type=float, default=10.0,
+                    help="seconds of request arrivals for the serving leg (0 = skip)")
     args = ap.parse_args()
     rank, world, local, dist = setup_dist(args.gpus)
     if args.impl == "reference":
@@ -313,7 +374,9 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     launches0 = ctx.launches
+    clocks.begin()
     secs = time_steps(ctx, period, args.steps)
+    clocks.end()
     launches = ctx.launches - launches0
     clk = clocks.stop()
     secs_max = dist_max(dist, local, secs)
@@ -377,6 +440,10 @@ def main():
                          f"{cb['cells']} cells), one mechanics period each",
                "cell_steps_per_s": cb["cells"] / cb["seconds"]}
 
+    serving = None
+    if args.serve_horizon > 0 and rank == 0 and world == 1:
+        serving = serving_leg(pcg, ctx, args.serve_horizon)
+
     if rank == 0:
         line = {
             "metric": "voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world,
@@ -399,6 +466,7 @@ def main():
                          "avg_launch_ms": sweep_ms,
                          "phase_ms_per_substep": {k: v / max(nst, 1) for k, v in ph.items()}},
             "cpu_baseline": cpu,
+            "serving": serving,
             "gpu_launches": launches,
             "clocks": clk,
         }

@@ -43,6 +43,7 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
 {
     ctx = c;
     masked = masked_steps;
+    AllocStream pool_scope(ctx->stream);   // buffers come from (and return to) the device pool
     auto from = [&](uint32_t i) -> const DevSource* {
         return (src && i < src->size() && (*src)[i].batch) ? &(*src)[i] : nullptr;
     };

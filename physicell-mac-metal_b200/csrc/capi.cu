@@ -133,7 +133,9 @@ static pcg_status create_ctx(int device, void* stream, pcg_ctx** out)
         }
         c->own_stream = true;
     }
-    if (cudaMalloc(&c->status, sizeof(unsigned)) != cudaSuccess || cudaMemset(c->status, 0, sizeof(unsigned)) != cudaSuccess) {
+    if (cudaMalloc(&c->status, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
         g_create_err = "status word allocation failed";
         if (c->own_stream) cudaStreamDestroy(c->stream);
         delete c;
@@ -165,7 +167,8 @@ pcg_status pcg_sync(pcg_ctx* ctx)
     unsigned st = 0;
     PCG_CU(ctx, cudaMemcpy(&st, ctx->status, sizeof st, cudaMemcpyDeviceToHost));
     if (st) {
-        PCG_CU(ctx, cudaMemset(ctx->status, 0, sizeof st));
+        PCG_CU(ctx, cudaMemsetAsync(ctx->status, 0, sizeof st, ctx->stream));
+        PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
         return fail(ctx, PCG_ERR_DEVICE, std::string("a kernel stopped early:") + ((st & PCG_DEV_TIMEOUT) ? " wait limit reached" : "") +
                                               ((st & PCG_DEV_ALIGN) ? " unaligned bulk copy refused" : ""));
     }
@@ -199,6 +202,7 @@ pcg_status pcg_host_free(void* p)
 pcg_status pcg_me_create(pcg_ctx* ctx, const pcg_grid_params* grid, const pcg_substrate_params* subs, pcg_me** out)
 {
     if (!ctx || !out) return PCG_ERR_INVALID;
+    AllocStream pool_scope(ctx->stream);
     *out = nullptr;
     PCG_TRY(check_grid(ctx, grid, subs));
     pcg_me* me = new (std::nothrow) pcg_me();
@@ -290,13 +294,16 @@ pcg_status pcg_me_gradients(pcg_me* me, float* gx, float* gy, float* gz, size_t 
 {
     if (!me) return PCG_ERR_INVALID;
     if (n != me->d.total_vox_sub) return bad(me->ctx, "gradient size mismatch");
+    AllocStream pool_scope(me->ctx->stream);
     DevBuf buf;
     PCG_CU(me->ctx, buf.alloc(3 * n * sizeof(float) + 16));
     float* b = buf.as<float>();
     PCG_TRY(me->d.gradients(gx ? b : nullptr, gy ? b + n : nullptr, gz ? b + 2 * n : nullptr));
     float* outs[3] = {gx, gy, gz};
     for (int q = 0; q < 3; ++q)
-        if (outs[q]) PCG_CU(me->ctx, cudaMemcpy(outs[q], b + q * n, n * sizeof(float), cudaMemcpyDeviceToHost));
+        if (outs[q])
+            PCG_CU(me->ctx, cudaMemcpyAsync(outs[q], b + q * n, n * sizeof(float), cudaMemcpyDeviceToHost, me->ctx->stream));
+    PCG_CU(me->ctx, cudaStreamSynchronize(me->ctx->stream));
     return PCG_OK;
 }
 
@@ -314,6 +321,7 @@ pcg_status pcg_me_device_density(pcg_me* me, float** dptr, size_t* row_pitch, si
 pcg_status pcg_cells_create(pcg_ctx* ctx, uint32_t max_cells, uint32_t S, pcg_cells** out)
 {
     if (!ctx || !out) return PCG_ERR_INVALID;
+    AllocStream pool_scope(ctx->stream);
     *out = nullptr;
     if (max_cells == 0) return bad(ctx, "max_cells must be >= 1");
     pcg_cells* c = new (std::nothrow) pcg_cells();
@@ -418,6 +426,7 @@ pcg_status pcg_mech_create(pcg_ctx* ctx, const pcg_mechanics_params* p, float x_
                            uint32_t max_cells, pcg_mech** out)
 {
     if (!ctx || !out) return PCG_ERR_INVALID;
+    AllocStream pool_scope(ctx->stream);
     *out = nullptr;
     PCG_TRY(check_mech(ctx, p));
     pcg_mech* m = new (std::nothrow) pcg_mech();

@@ -24,24 +24,158 @@ int cuda_fail(pcg_ctx* ctx, cudaError_t e, const char* what)
     return e == cudaErrorMemoryAllocation ? PCG_ERR_OOM : PCG_ERR_CUDA;
 }
 
+// ------------------------------------------------------------------ device pool
+//
+// Stream-ordered caching of device blocks.  A block released by a DevBuf
+// that was allocated under an AllocStream goes back to the pool with an
+// event recorded on that stream; it is handed out again only once the event
+// has completed, so no kernel still using it can see it reused, and nothing
+// synchronises the device (cudaFree would).  Blocks are reused best-fit
+// within 1/8 (+ 1 MiB) of the request.  On an allocation failure the idle
+// blocks are returned to the driver and the allocation is retried.  The
+// pool lives until process exit (never destroyed, so no CUDA call runs
+// during static destruction).
+
+namespace {
+
+thread_local cudaStream_t tl_alloc_stream = nullptr;
+
+struct PoolBlock {
+    void* p;
+    int device;
+    cudaEvent_t ev;
+};
+
+class DevicePool {
+public:
+    static DevicePool& get()
+    {
+        static DevicePool* pool = new DevicePool();
+        return *pool;
+    }
+    cudaError_t take(size_t want, void** out, size_t* got, int* device)
+    {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        *device = dev;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            const size_t limit = want + want / 8 + (1u << 20);
+            for (auto it = free_.lower_bound(want); it != free_.end() && it->first <= limit; ++it) {
+                if (it->second.device != dev) continue;
+                const cudaError_t q = cudaEventQuery(it->second.ev);
+                if (q == cudaErrorNotReady) continue;
+                if (q != cudaSuccess) cudaGetLastError();
+                *out = it->second.p;
+                *got = it->first;
+                cudaEventDestroy(it->second.ev);
+                free_.erase(it);
+                return cudaSuccess;
+            }
+        }
+        const size_t b = round_up(want);
+        e = cudaMalloc(out, b);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            trim(dev);
+            e = cudaMalloc(out, b);
+        }
+        if (e != cudaSuccess) {
+            *out = nullptr;
+            return e;
+        }
+        *got = b;
+        return cudaSuccess;
+    }
+    // false: the caller frees the block itself (no event could be recorded)
+    bool give(void* p, size_t bytes, cudaStream_t st, int dev)
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+            cudaGetLastError();
+            return false;
+        }
+        cudaEvent_t ev = nullptr;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        if (cudaEventRecord(ev, st) != cudaSuccess) {
+            cudaGetLastError();
+            cudaEventDestroy(ev);
+            return false;
+        }
+        std::lock_guard<std::mutex> lk(mu_);
+        free_.emplace(bytes, PoolBlock{p, dev, ev});
+        return true;
+    }
+    void trim(int dev)
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (auto it = free_.begin(); it != free_.end();) {
+            if (it->second.device == dev && cudaEventQuery(it->second.ev) == cudaSuccess) {
+                cudaEventDestroy(it->second.ev);
+                cudaFree(it->second.p);
+                it = free_.erase(it);
+            } else {
+                cudaGetLastError();
+                ++it;
+            }
+        }
+    }
+
+private:
+    static size_t round_up(size_t b)
+    {
+        const size_t g = b >= (1u << 20) ? (1u << 20) : 512;
+        return (b + g - 1) / g * g;
+    }
+    std::mutex mu_;
+    std::multimap<size_t, PoolBlock> free_;
+};
+
+}  // namespace
+
+AllocStream::AllocStream(cudaStream_t s) : prev_(tl_alloc_stream) { tl_alloc_stream = s; }
+AllocStream::~AllocStream() { tl_alloc_stream = prev_; }
+
 cudaError_t DevBuf::alloc(size_t b)
 {
     release();
     if (b == 0) return cudaSuccess;
+    if (tl_alloc_stream) {
+        size_t got = 0;
+        const cudaError_t e = DevicePool::get().take(b, &p, &got, &dev_);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return e;
+        }
+        bytes = b;
+        cap_ = got;
+        stream_ = tl_alloc_stream;
+        return cudaSuccess;
+    }
     cudaError_t e = cudaMalloc(&p, b);
     if (e != cudaSuccess) {
         p = nullptr;
         return e;
     }
     bytes = b;
+    cap_ = 0;
+    stream_ = nullptr;
     return cudaSuccess;
 }
 
 void DevBuf::release()
 {
-    if (p) cudaFree(p);
+    if (p) {
+        if (!(stream_ && cap_ && DevicePool::get().give(p, cap_, stream_, dev_))) cudaFree(p);
+    }
     p = nullptr;
     bytes = 0;
+    cap_ = 0;
+    stream_ = nullptr;
 }
 
 cudaError_t HostBuf::alloc(size_t b)
@@ -233,9 +367,9 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
     PCG_CU(ctx, rules.alloc(std::max<size_t>(h_rules_.size(), 1) * sizeof(LineRule)));
     PCG_CU(ctx, tab.alloc(std::max<size_t>(h_tab_.size(), 8) * sizeof(float)));
     if (!h_rules_.empty())
-        PCG_CU(ctx, cudaMemcpy(rules.p, h_rules_.data(), h_rules_.size() * sizeof(LineRule), cudaMemcpyHostToDevice));
+        PCG_CU(ctx, cudaMemcpyAsync(rules.p, h_rules_.data(), h_rules_.size() * sizeof(LineRule), cudaMemcpyHostToDevice, ctx->stream));
     if (!h_tab_.empty())
-        PCG_CU(ctx, cudaMemcpy(tab.p, h_tab_.data(), h_tab_.size() * sizeof(float), cudaMemcpyHostToDevice));
+        PCG_CU(ctx, cudaMemcpyAsync(tab.p, h_tab_.data(), h_tab_.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     // one tensor map per rule short enough for a tensor box: 2-D row maps
     // for x, 3-D column maps for y and z
     tensor_ok_.assign(h_rules_.size(), 0);
@@ -258,11 +392,11 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
             }
         }
         PCG_CU(ctx, tmaps.alloc(maps.size()));
-        PCG_CU(ctx, cudaMemcpy(tmaps.p, maps.data(), maps.size(), cudaMemcpyHostToDevice));
+        PCG_CU(ctx, cudaMemcpyAsync(tmaps.p, maps.data(), maps.size(), cudaMemcpyHostToDevice, ctx->stream));
     }
     n_faces = static_cast<uint32_t>(fj.size());
     PCG_CU(ctx, faces.alloc(std::max<size_t>(fj.size(), 1) * sizeof(FaceJob)));
-    if (!fj.empty()) PCG_CU(ctx, cudaMemcpy(faces.p, fj.data(), fj.size() * sizeof(FaceJob), cudaMemcpyHostToDevice));
+    if (!fj.empty()) PCG_CU(ctx, cudaMemcpyAsync(faces.p, fj.data(), fj.size() * sizeof(FaceJob), cudaMemcpyHostToDevice, ctx->stream));
     for (int a = 0; a < 3; ++a) {
         PCG_TRY(build_axis(a));
         PCG_TRY(default_configs(a));
@@ -355,7 +489,7 @@ int Diffusion::build_axis(int axis)
         const auto& v = q == 0 ? fast_t : glob_t;
         PCG_CU(ctx, ls[q].tiles.alloc(std::max<size_t>(v.size(), 1) * sizeof(SweepTile)));
         if (!v.empty())
-            PCG_CU(ctx, cudaMemcpy(ls[q].tiles.p, v.data(), v.size() * sizeof(SweepTile), cudaMemcpyHostToDevice));
+            PCG_CU(ctx, cudaMemcpyAsync(ls[q].tiles.p, v.data(), v.size() * sizeof(SweepTile), cudaMemcpyHostToDevice, ctx->stream));
     }
     return PCG_OK;
 }
@@ -533,7 +667,7 @@ int Diffusion::fill(uint32_t i, const float* values)
     for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
         std::fill(tmp.begin(), tmp.end(), values[s]);
         float* dst = dens.as<float>() + d.dens_off + s * d.pitch;
-        PCG_CU(ctx, cudaMemcpy(dst, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice));
+        PCG_CU(ctx, cudaMemcpyAsync(dst, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     }
     return PCG_OK;
 }
@@ -675,21 +809,21 @@ int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_
     h_inst.assign(std::max<uint32_t>(n_instances, 1), CellInst{});
     PCG_CU(ctx, inst.alloc(h_inst.size() * sizeof(CellInst)));
     PCG_CU(ctx, soa.alloc(static_cast<size_t>(NUM_FIELDS) * max_cells * sizeof(float)));
-    PCG_CU(ctx, cudaMemset(soa.p, 0, soa.bytes));
+    PCG_CU(ctx, cudaMemsetAsync(soa.p, 0, soa.bytes, ctx->stream));
     PCG_CU(ctx, cell_inst.alloc(static_cast<size_t>(max_cells) * sizeof(uint32_t)));
-    PCG_CU(ctx, cudaMemset(cell_inst.p, 0, cell_inst.bytes));
+    PCG_CU(ctx, cudaMemsetAsync(cell_inst.p, 0, cell_inst.bytes, ctx->stream));
     const size_t rc = std::max<uint32_t>(rate_capacity, 1);
     PCG_CU(ctx, rates.alloc(4 * rc * sizeof(double)));
-    PCG_CU(ctx, cudaMemset(rates.p, 0, rates.bytes));
+    PCG_CU(ctx, cudaMemsetAsync(rates.p, 0, rates.bytes, ctx->stream));
     PCG_CU(ctx, coef.alloc(3 * rc * sizeof(double)));
     PCG_CU(ctx, active.alloc(max_cells));
     for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp})
         PCG_CU(ctx, b->alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint32_t)));
     PCG_CU(ctx, sort_scr.alloc(radix_sort_scratch_bytes(max_cells, 32)));
     PCG_CU(ctx, sbeg.alloc(h_inst.size() * sizeof(uint32_t)));
-    PCG_CU(ctx, cudaMemset(sbeg.p, 0, sbeg.bytes));
+    PCG_CU(ctx, cudaMemsetAsync(sbeg.p, 0, sbeg.bytes, ctx->stream));
     PCG_CU(ctx, run_scr.alloc(scan_scratch_bytes(static_cast<uint64_t>(max_cells) + 1)));
-    PCG_CU(ctx, cudaMemset(ktmp.p, 0, ktmp.bytes));   // run count 0 until the first order
+    PCG_CU(ctx, cudaMemsetAsync(ktmp.p, 0, ktmp.bytes, ctx->stream));   // run count 0 until the first order
     inst_dirty = coef_dirty = order_dirty = true;
     return PCG_OK;
 }
@@ -750,10 +884,11 @@ int Cells::set_rates(uint32_t off, uint32_t count, const double* sec, const doub
 int Cells::set_active(uint32_t off, uint32_t count, const uint8_t* act)
 {
     if (act) {
-        PCG_CU(ctx, cudaMemcpy(active.as<uint8_t>() + off, act, count, cudaMemcpyHostToDevice));
+        PCG_CU(ctx, cudaMemcpyAsync(active.as<uint8_t>() + off, act, count, cudaMemcpyHostToDevice, ctx->stream));
+        PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));   // the caller may reuse 'act' on return
         has_active = true;
     } else {
-        PCG_CU(ctx, cudaMemset(active.as<uint8_t>() + off, 1, count));
+        PCG_CU(ctx, cudaMemsetAsync(active.as<uint8_t>() + off, 1, count, ctx->stream));
     }
     order_dirty = true;
     return PCG_OK;
@@ -764,7 +899,7 @@ int Cells::set_cell_instances(const std::vector<uint32_t>& counts)
     std::vector<uint32_t> ci;
     for (size_t i = 0; i < counts.size(); ++i) ci.insert(ci.end(), counts[i], static_cast<uint32_t>(i));
     if (ci.size() > max_cells) return fail(ctx, PCG_ERR_INVALID, "more cells than capacity");
-    if (!ci.empty()) PCG_CU(ctx, cudaMemcpy(cell_inst.p, ci.data(), ci.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (!ci.empty()) PCG_CU(ctx, cudaMemcpyAsync(cell_inst.p, ci.data(), ci.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     return PCG_OK;
 }
 
@@ -844,7 +979,7 @@ int Mechanics::create(pcg_ctx* c, uint32_t tmv, uint32_t maxc)
     PCG_CU(ctx, sort_scr.alloc(radix_sort_scratch_bytes(cap, key_bits)));
     PCG_CU(ctx, counts.alloc((static_cast<size_t>(tmv) + 1) * sizeof(uint32_t)));
     PCG_CU(ctx, start.alloc((static_cast<size_t>(tmv) + 1) * sizeof(uint32_t)));
-    PCG_CU(ctx, cudaMemset(start.p, 0, start.bytes));
+    PCG_CU(ctx, cudaMemsetAsync(start.p, 0, start.bytes, ctx->stream));
     PCG_CU(ctx, scan_scr.alloc(scan_scratch_bytes(static_cast<uint64_t>(tmv) + 1)));
     PCG_CU(ctx, spos.alloc(static_cast<size_t>(cap) * sizeof(float4)));
     PCG_CU(ctx, sprm.alloc(static_cast<size_t>(cap) * sizeof(float4)));

@@ -39,6 +39,19 @@ int cuda_fail(pcg_ctx* ctx, cudaError_t e, const char* what);
         if (r_ != PCG_OK) return r_;  \
     } while (0)
 
+// Allocations made while an AllocStream is alive (on this thread) come
+// from the stream-ordered device pool and go back to it on release, tied to
+// that stream; without one, DevBuf uses cudaMalloc / cudaFree.
+class AllocStream {
+public:
+    explicit AllocStream(cudaStream_t s);
+    ~AllocStream();
+    AllocStream(const AllocStream&) = delete;
+    AllocStream& operator=(const AllocStream&) = delete;
+private:
+    cudaStream_t prev_;
+};
+
 // Device allocation owned by the library.
 struct DevBuf {
     void* p = nullptr;
@@ -46,15 +59,26 @@ struct DevBuf {
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes), cap_(o.cap_), stream_(o.stream_), dev_(o.dev_)
+    {
+        o.p = nullptr;
+        o.bytes = 0;
+        o.cap_ = 0;
+        o.stream_ = nullptr;
+    }
     DevBuf& operator=(DevBuf&& o) noexcept
     {
         if (this != &o) {
             release();
             p = o.p;
             bytes = o.bytes;
+            cap_ = o.cap_;
+            stream_ = o.stream_;
+            dev_ = o.dev_;
             o.p = nullptr;
             o.bytes = 0;
+            o.cap_ = 0;
+            o.stream_ = nullptr;
         }
         return *this;
     }
@@ -63,6 +87,10 @@ struct DevBuf {
     void release();
     template <class T>
     T* as() const { return static_cast<T*>(p); }
+private:
+    size_t cap_ = 0;                   // pool block size (0: cudaMalloc)
+    cudaStream_t stream_ = nullptr;    // stream the pool block is ordered on
+    int dev_ = 0;                      // device of the pool block
 };
 
 // Page-locked host allocation (staging for end-to-end copies).

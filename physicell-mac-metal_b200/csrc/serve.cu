@@ -231,11 +231,12 @@ pcg_status pcg_serve_tick(pcg_server* s, uint32_t* n_running, uint32_t* n_queued
         changed = true;
     }
     if (changed) PCG_TRY(rebuild(s));
-    // 3. advance
+    // 3. advance: every running request takes min(steps_per_tick, remaining)
+    // steps; one that finishes inside the tick is masked out of the rest
     if (!s->running.empty()) {
         Batch& b = *s->batch;
-        uint32_t k = s->opt.steps_per_tick;
-        for (Request* r : s->running) k = std::min(k, r->n_steps - r->done);
+        uint32_t k = 0;
+        for (Request* r : s->running) k = std::max(k, std::min(s->opt.steps_per_tick, r->n_steps - r->done));
         const size_t n = s->running.size();
         if (s->masks.bytes < static_cast<size_t>(k) * n) PCG_CU(s->ctx, s->masks.alloc(static_cast<size_t>(k) * n));
         uint8_t* m = s->masks.as<uint8_t>();
@@ -243,6 +244,10 @@ pcg_status pcg_serve_tick(pcg_server* s, uint32_t* n_running, uint32_t* n_queued
             bool any = false;
             for (size_t i = 0; i < n; ++i) {
                 Request* r = s->running[i];
+                if (r->done + st >= r->n_steps) {
+                    m[st * n + i] = 0;
+                    continue;
+                }
                 const double dtd = r->desc.grid.dt;
                 const double dtm = r->desc.dt_mechanics > 0.f ? r->desc.dt_mechanics : r->desc.mech.dt;
                 r->accum += dtd;
@@ -258,8 +263,9 @@ pcg_status pcg_serve_tick(pcg_server* s, uint32_t* n_running, uint32_t* n_queued
         }
         PCG_CU(s->ctx, cudaStreamSynchronize(s->ctx->stream));
         for (Request* r : s->running) {
-            r->done += k;
-            s->voxel_steps += static_cast<uint64_t>(r->desc.grid.nx) * r->desc.grid.ny * r->desc.grid.nz * k;
+            const uint32_t taken = std::min(k, r->n_steps - r->done);
+            r->done += taken;
+            s->voxel_steps += static_cast<uint64_t>(r->desc.grid.nx) * r->desc.grid.ny * r->desc.grid.nz * taken;
             if (r->done >= r->n_steps) {
                 PCG_TRY(finish(s, r));
                 ++finished;
