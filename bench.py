@@ -22,8 +22,10 @@ Reports (one JSON line on rank 0):
   serving          config 4 on a bounded horizon: Poisson request arrivals
                    served by continuous batching; p50/p99 time-to-result
                    and aggregate voxel-steps/s, cell-steps/s
-Multi-GPU: one process per GPU, each rank runs its own 64-instance batch
-(seed offset by rank, no collective on the data path): weak scaling.
+Multi-GPU: one process per GPU; 64 x N instances are split across the N
+ranks by predicted bytes (greedy packing, computed identically on every
+rank) and each rank runs its shard as one batch, with no collective on the
+data path: weak scaling.
 --impl reference times the CPU port alone (the reference's shaders exist
 only for Apple Metal).
 """
@@ -137,7 +139,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def setup_dist(gpus):
+def setup_dist(gpus, backend="nccl"):
+    """One process per GPU (torchrun): rank, world size, local rank and the
+    process group (None when alone).  The group only carries the barrier and
+    the max / sum of timings; no simulation data crosses GPUs."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -146,28 +151,38 @@ def setup_dist(gpus):
         import datetime
         import torch
         import torch.distributed as td
-        torch.cuda.set_device(local)
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        td.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         dist = td
     return rank, world, local, dist
 
 
-def dist_max(dist, local, x):
+def _reduce(dist, local, x, op):
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def dist_max(dist, local, x):
+    return _reduce(dist, local, x, dist.ReduceOp.MAX if dist is not None else None)
 
 
 def dist_sum(dist, local, x):
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(dist, local, x, dist.ReduceOp.SUM if dist is not None else None)
+
+
+def rank_shard(n_per_gpu, rank, world, seed=1237):
+    """Weak scaling: world * n_per_gpu batched 3-D instances, split across
+    ranks by predicted bytes (physicell-mac-metal_b200/sharding.py); rank
+    'rank' gets its shard's indices."""
+    from pcg import sharding, workloads
+    work = workloads.batched_3d_work(n_instances=n_per_gpu * world, seed=seed)
+    return sharding.partition(work, world)[rank]
 
 
 def barrier(dist):
@@ -361,7 +376,8 @@ def main():
     from pcg import workloads
     torch.cuda.set_device(local)
     ctx = pcg.Context(local)
-    insts = workloads.batched_3d(n_instances=args.instances, seed=1237 + 1000 * rank)
+    shard = rank_shard(args.instances, rank, world)
+    insts = workloads.batched_3d(n_instances=args.instances * world, seed=1237, only=shard)
     batch = pcg.Batch(ctx, insts, tune_cache=args.tune_cache)
     voxels, voxel_subs, cells = batch.totals()
 
@@ -450,8 +466,9 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)",
-            "config": {"workload": f"batched_3d: {len(insts)} instances per GPU, side U{{40..120}}, S=2, "
-                                   f"1k-100k cells; step = 10 diffusion sub-steps + 1 mechanics step",
+            "config": {"workload": f"batched_3d: {args.instances} instances per GPU ({args.instances * world} in all, "
+                                   f"sharded by predicted bytes), side U{{40..120}}, S=2, 1k-100k cells; "
+                                   f"step = 10 diffusion sub-steps + 1 mechanics step",
                        "voxels_per_gpu": voxels, "voxel_substrates_per_gpu": voxel_subs, "cells_per_gpu": cells,
                        "l2": f"inputs larger than L2 ({voxel_subs * 4 / 1e6:.0f} MB density per GPU)",
                        "launch_shapes": batch.describe()},

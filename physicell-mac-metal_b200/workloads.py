@@ -149,17 +149,41 @@ def batched_2d(n_instances=256, seed=1236, max_cells=20_000, min_cells=100):
     return out
 
 
-def batched_3d(n_instances=64, seed=1237, min_cells=1_000, max_cells=100_000, side_range=(40, 120)):
+def _batched_3d_spec(i, seed, min_cells, max_cells, side_range):
+    """Scalar parameters of batched_3d instance i and its generator (the
+    per-cell arrays are drawn from the same generator afterwards)."""
+    rng = np.random.default_rng(seed + i)
+    side = int(rng.integers(side_range[0], side_range[1] + 1))
+    drug_D = float(np.exp(rng.uniform(np.log(1e3), np.log(5e4))))
+    drug_lam = float(rng.uniform(0, 0.5))
+    target = float(rng.uniform(0, 10))
+    n = int(rng.integers(min_cells, max_cells + 1))
+    return rng, side, drug_D, drug_lam, target, n
+
+
+def batched_3d_work(n_instances=64, seed=1237, min_cells=1_000, max_cells=100_000, side_range=(40, 120)):
+    """Algorithmic bytes of one mechanics period (10 diffusion sub-steps + 1
+    mechanics step) per batched_3d instance, from its parameters alone:
+    3 sweeps x 8 B per voxel-substrate, secretion 8 + 24 S B per cell, per
+    sub-step; mechanics 136 B per cell.  Used to shard instances across GPUs
+    without drawing their cells."""
     out = []
     for i in range(n_instances):
-        rng = np.random.default_rng(seed + i)
-        side = int(rng.integers(side_range[0], side_range[1] + 1))
+        _, side, _, _, _, n = _batched_3d_spec(i, seed, min_cells, max_cells, side_range)
+        S = 2
+        out.append(10 * (24 * S * side ** 3 + (8 + 24 * S) * n) + 136 * n)
+    return out
+
+
+def batched_3d(n_instances=64, seed=1237, min_cells=1_000, max_cells=100_000, side_range=(40, 120), only=None):
+    """The batched 3-D configuration; 'only' restricts it to the given
+    instance indices (a shard), each drawn exactly as in the full set."""
+    out = []
+    for i in (range(n_instances) if only is None else only):
+        rng, side, drug_D, drug_lam, target, n = _batched_3d_spec(i, seed, min_cells, max_cells, side_range)
         L = side * 20.0
         grid = make_grid(side, side, side, 2, dx=20.0, dt=DT_DIFF)
-        drug_D = float(np.exp(rng.uniform(np.log(1e3), np.log(5e4))))
-        drug_lam = float(rng.uniform(0, 0.5))
-        subs = [(1e5, 0.1, True, 38.0), (drug_D, drug_lam, True, float(rng.uniform(0, 10)))]
-        n = int(rng.integers(min_cells, max_cells + 1))
+        subs = [(1e5, 0.1, True, 38.0), (drug_D, drug_lam, True, target)]
         pos = _ball(rng, n, 0.4 * L, (L / 2, L / 2, L / 2))
         radius = np.clip(rng.normal(8.4, 0.5, n), 5.0, 12.0).astype(np.float32)
         rep = float(rng.uniform(5, 20))
