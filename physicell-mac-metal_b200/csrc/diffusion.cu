@@ -46,11 +46,21 @@ __device__ __forceinline__ bool tile_on(const LineRule& r, const uint8_t* __rest
     return mask == nullptr || (mask[r.inst] & STEP_DIFFUSE);
 }
 
+// Column tile lane -> (slab, column).
+__device__ __forceinline__ uint32_t lane_slab(const SweepTile& tile, int lane) { return static_cast<uint32_t>(lane) / tile.width; }
+__device__ __forceinline__ uint32_t lane_col(const SweepTile& tile, int lane) { return static_cast<uint32_t>(lane) % tile.width; }
+
+// The lane's line lies on a face of the block (3-D: x faces and, for z
+// lines, y faces; 2-D y lines: x faces).
 __device__ __forceinline__ bool on_face(const SweepTile& tile, int lane)
 {
-    if (tile.face & TILE_FACE_ALL) return true;
-    const uint32_t i = tile.i0 + static_cast<uint32_t>(lane);
-    return i == 0u || i + 1u == tile.nx;
+    const uint32_t i = tile.i0 + lane_col(tile, lane);
+    if (i == 0u || i + 1u == tile.nx) return true;
+    if (tile.face & TILE_AXIS_Z) {
+        const uint32_t j = tile.outer + lane_slab(tile, lane);
+        return j == 0u || j + 1u == tile.outer_n;
+    }
+    return false;
 }
 
 // ------------------------------------------------------------------ TMA / mbarrier helpers
@@ -154,12 +164,12 @@ __device__ __forceinline__ bool aligned16(const void* p, uint32_t bytes)
 __device__ __forceinline__ uint32_t col_row_bytes(uint32_t count) { return ((count + 3u) & ~3u) * 4u; }
 
 // Issue the loads of 'tile' into stage 'st' (all lanes take part).
-// Tensor coordinates {x, y, z} of a column tile's box.
+// Tensor coordinates of a column tile's box: (x, slab, line position).
 __device__ __forceinline__ void tile_coords(const SweepTile& tile, int* c)
 {
     c[0] = static_cast<int>(tile.i0);
-    c[1] = (tile.face & TILE_AXIS_Z) ? static_cast<int>(tile.outer) : 0;
-    c[2] = (tile.face & TILE_AXIS_Z) ? 0 : static_cast<int>(tile.outer);
+    c[1] = static_cast<int>(tile.outer);
+    c[2] = 0;
 }
 
 // Issue the loads of 'tile' into stage 'st' and of its rule's coefficient
@@ -174,7 +184,7 @@ __device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const Lin
     const uint32_t n = r.n;
     const uint32_t tb = tab_floats(n) * 4u;    // 32-byte multiple, 32-byte aligned source
     const float* src = dens + tile.base;
-    const void* map = static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.rule) * 128;
+    const void* map = static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.map) * 128;
     if (kRows && (tile.face & TILE_TENSOR)) {
         if (lane == 0) {
             mbar_arrive_expect_tx(bar, 32u * row_smem_pitch(n) * 4u + tb);   // the whole box, fill included
@@ -231,7 +241,7 @@ __device__ __forceinline__ void issue_tile_store(const SweepTile& tile, const Li
     float* dst = dens + tile.base;
     if (kRows && (tile.face & TILE_TENSOR)) {
         if (lane == 0) {
-            tensor_store2(static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.rule) * 128, 0,
+            tensor_store2(static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.map) * 128, 0,
                           static_cast<int>(tile.outer), st);
             bulk_commit();
         }
@@ -241,7 +251,7 @@ __device__ __forceinline__ void issue_tile_store(const SweepTile& tile, const Li
         if (lane == 0) {
             int c[3];
             tile_coords(tile, c);
-            tensor_store3(static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.rule) * 128, c[0], c[1],
+            tensor_store3(static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(tile.map) * 128, c[0], c[1],
                           c[2], st);
             bulk_commit();
         }
@@ -401,7 +411,7 @@ __device__ __forceinline__ void solve_rows_vec(float* st, const LineRule& r, con
 __device__ __forceinline__ void solve_cols(float* st, const SweepTile& tile, const LineRule& r,
                                            const float* t, int lane, bool apply_faces)
 {
-    if (lane >= static_cast<int>(tile.count)) return;
+    if (lane_col(tile, lane) >= tile.count || lane_slab(tile, lane) >= tile.nslab) return;
     const int n = static_cast<int>(r.n);
     float* c = st + lane;
     if (apply_faces && (tile.face & TILE_FACE) && on_face(tile, lane)) {
@@ -753,13 +763,16 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 }
 
 bool encode_column_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t px, int axis,
-                       uint32_t n)
+                       uint32_t n, uint32_t width)
 {
     PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
     if (!fn || n == 0 || n > kTensorMaxN || (px & 3u) || (reinterpret_cast<uintptr_t>(block) & 15u)) return false;
-    const cuuint64_t dims[3] = {nx, ny, nz};
-    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(px) * 4u, static_cast<cuuint64_t>(px) * ny * 4u};
-    const cuuint32_t box[3] = {32u, axis == 1 ? n : 1u, axis == 1 ? 1u : n};
+    if (width != 32u && width != 16u && width != 8u) return false;
+    const cuuint64_t row = static_cast<cuuint64_t>(px) * 4u, slab = row * ny;
+    // y lines: (x, z, y); z lines: (x, y, z) -- the line runs along the last dimension
+    const cuuint64_t dims[3] = {nx, axis == 1 ? nz : ny, axis == 1 ? ny : nz};
+    const cuuint64_t strides[2] = {axis == 1 ? slab : row, axis == 1 ? row : slab};
+    const cuuint32_t box[3] = {width, 32u / width, n};
     const cuuint32_t estr[3] = {1u, 1u, 1u};
     const CUresult r = fn(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, block, dims, strides,
                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

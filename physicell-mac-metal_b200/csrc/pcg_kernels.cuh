@@ -48,27 +48,34 @@ __host__ __device__ constexpr uint32_t tab_floats(uint32_t n) { return ((n + 3u)
 
 // A tile of lines for one sweep launch.  Row tiles (x sweep, TILE_ROWS):
 // 'count' (<= 32) lines of length n starting at element 'base', lines 'rs'
-// (the row pitch) apart.  Column tiles (y and z sweeps): 'count' (<= 32)
-// adjacent columns starting at 'base', element stride 'rs' along the line.
+// (the row pitch) apart.  Column tiles (y and z sweeps): 'nslab' adjacent
+// slabs (outer coordinates outer .. outer + nslab - 1) of 'count' (<= width)
+// adjacent columns from x = i0, width * nslab <= 32; lane = slab * width +
+// column.  Without a tensor map a column tile has width 32 and one slab, and
+// its lines start at 'base' with element stride 'rs'.
 struct SweepTile {
     uint64_t base;
     uint32_t rule;
     uint32_t count;
-    uint32_t rs;    // row tiles: line pitch; column tiles: element stride along a line
-    uint32_t i0;    // x index of the tile's first line (column tiles)
-    uint32_t nx;    // the instance's nx
-    uint32_t face;  // TILE_FACE: the Dirichlet reset is fused into this sweep;
-                    // TILE_FACE_ALL: every line of the tile lies on a face;
-                    // TILE_ROWS: x tile; TILE_TENSOR: moved with the rule's
-                    // 3-D tensor map; TILE_AXIS_Z: z tile (else y)
-    uint32_t outer; // column tiles: the fixed coordinate (k for y, j for z);
-                    // row tiles: index of the first line in the substrate block
-    uint32_t _pad[3];
+    uint32_t rs;       // row tiles: line pitch; column tiles: element stride along a line
+    uint32_t i0;       // x index of the tile's first column (column tiles)
+    uint32_t nx;       // the instance's nx
+    uint32_t face;     // TILE_FACE: the Dirichlet reset is fused into this sweep;
+                       // TILE_ROWS: x tile; TILE_TENSOR: moved with tensor map 'map';
+                       // TILE_AXIS_Z: z tile (else y)
+    uint32_t outer;    // column tiles: first slab (k for y, j for z); row tiles: first line
+    uint32_t map;      // index of the 128-byte tensor map
+    uint16_t width;    // columns per slab (column tiles): 32, 16 or 8
+    uint16_t nslab;    // slabs in the tile
+    uint32_t outer_n;  // number of slabs (nz for y, ny for z)
 };
-enum : uint32_t { TILE_FACE = 1u, TILE_FACE_ALL = 2u, TILE_ROWS = 4u, TILE_TENSOR = 8u, TILE_AXIS_Z = 16u };
+enum : uint32_t { TILE_FACE = 1u, TILE_ROWS = 4u, TILE_TENSOR = 8u, TILE_AXIS_Z = 16u };
 
 // Longest line a tensor-map box can cover (box dimensions are <= 256).
 constexpr uint32_t kTensorMaxN = 256;
+// Tensor-map slots per rule: x rules use slot 0, y / z rules one per
+// column-tile width (32, 16, 8).
+constexpr uint32_t kMapsPerRule = 3;
 
 // x tiles moved with a 2-D tensor map land in shared memory as 32 rows of
 // row_smem_pitch(nx) floats: nx rounded up to 4 with an odd number of
@@ -128,11 +135,13 @@ int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats);   
 cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
                              const LineRule* rules, const float* tab, const void* tmaps, int apply_faces,
                              const uint8_t* mask, unsigned* status, TmaCfg cfg);
-// Encode the 3-D tensor map of one substrate block (dims nx, ny, nz; rows px
-// floats apart) with a box of 32 x n x 1 (y) or 32 x 1 x n (z); returns
-// false when the driver entry point is unavailable or rejects the map.
+// Encode the 3-D tensor map of one substrate block (rows px floats apart)
+// for column tiles of 'width' columns x 32/width slabs x n line positions:
+// y sweep dims (x, z, y), z sweep dims (x, y, z), box {width, 32/width, n},
+// so a tile lands in shared memory as [n][32].  Returns false when the
+// driver entry point is unavailable or rejects the map.
 bool encode_column_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t px, int axis,
-                       uint32_t n);
+                       uint32_t n, uint32_t width);
 // Encode the 2-D tensor map of one substrate block seen as rows x nx (rows
 // px floats apart) with a box of row_smem_pitch(nx) x 32 (x tiles).
 bool encode_row_map(void* map128, float* block, uint32_t nx, uint64_t rows, uint32_t px);

@@ -370,11 +370,12 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
         PCG_CU(ctx, cudaMemcpyAsync(rules.p, h_rules_.data(), h_rules_.size() * sizeof(LineRule), cudaMemcpyHostToDevice, ctx->stream));
     if (!h_tab_.empty())
         PCG_CU(ctx, cudaMemcpyAsync(tab.p, h_tab_.data(), h_tab_.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    // one tensor map per rule short enough for a tensor box: 2-D row maps
-    // for x, 3-D column maps for y and z
+    // tensor maps, three 128-byte slots per rule (kMapsPerRule): x rules use
+    // slot 0 (2-D row map); y / z rules one 3-D column map per tile width
+    // (32, 16, 8 columns).  tensor_ok_ bit w: the slot-w map exists.
     tensor_ok_.assign(h_rules_.size(), 0);
     {
-        std::vector<unsigned char> maps(std::max<size_t>(h_rules_.size(), 1) * 128, 0);
+        std::vector<unsigned char> maps(std::max<size_t>(h_rules_.size(), 1) * kMapsPerRule * 128, 0);
         for (size_t i = 0; i < inst.size(); ++i) {
             const DiffInstance& d = inst[i];
             for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
@@ -383,11 +384,15 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
                     if (a == 2 && d.ndim() < 3) continue;
                     const uint32_t rule = rule_of(i, s, a);
                     const uint32_t n = axis_n(d.g, a);
-                    unsigned char* m = maps.data() + static_cast<size_t>(rule) * 128;
-                    const bool ok = a == 0 ? (n <= kRowTensorMaxN && encode_row_map(m, block, d.g.nx, d.rows(), d.px))
-                                           : (n <= kTensorMaxN &&
-                                              encode_column_map(m, block, d.g.nx, d.g.ny, d.g.nz, d.px, a, n));
-                    if (ok) tensor_ok_[rule] = 1;
+                    unsigned char* m = maps.data() + static_cast<size_t>(rule) * kMapsPerRule * 128;
+                    if (a == 0) {
+                        if (n <= kRowTensorMaxN && encode_row_map(m, block, d.g.nx, d.rows(), d.px)) tensor_ok_[rule] = 1;
+                        continue;
+                    }
+                    if (n > kTensorMaxN) continue;
+                    for (int w = 0; w < 3; ++w)
+                        if (encode_column_map(m + w * 128, block, d.g.nx, d.g.ny, d.g.nz, d.px, a, n, 32u >> w))
+                            tensor_ok_[rule] |= static_cast<uint8_t>(1u << w);
                 }
             }
         }
@@ -439,30 +444,49 @@ int Diffusion::build_axis(int axis)
                     t.rs = d.px;
                     t.nx = g.nx;
                     t.outer = static_cast<uint32_t>(l0);
+                    t.map = rule * kMapsPerRule;
+                    t.width = 32;
+                    t.nslab = 1;
                     t.face = TILE_ROWS | ((fast && tensor_ok_[rule]) ? TILE_TENSOR : 0u);
                     out.push_back(t);
                 }
                 nl += lines;
             } else {
-                // y: families over (i, k), stride px; z: families over (i, j), stride ny*px
+                // y: families over (i, k), stride px; z: families over (i, j), stride ny*px.
+                // With tensor maps, the last (narrow) tile of each slab takes
+                // 16 or 8 columns from 2 or 4 adjacent slabs, so its lanes are
+                // not left idle.
                 const uint32_t outer = axis == 1 ? g.nz : g.ny;
                 const uint64_t ostride = axis == 1 ? static_cast<uint64_t>(d.px) * g.ny : d.px;
                 const uint32_t rs = axis == 1 ? d.px : d.px * g.ny;
-                for (uint32_t o = 0; o < outer; ++o) {
-                    for (uint32_t i0 = 0; i0 < g.nx; i0 += 32) {
+                for (uint32_t i0 = 0; i0 < g.nx; i0 += 32) {
+                    const uint32_t cnt = std::min<uint32_t>(32, g.nx - i0);
+                    int w = 0;
+                    if (fast && tensor_ok_[rule]) {
+                        if (cnt <= 8 && (tensor_ok_[rule] & 4u)) w = 2;
+                        else if (cnt <= 16 && (tensor_ok_[rule] & 2u)) w = 1;
+                        if (!(tensor_ok_[rule] & (1u << w))) w = -1;
+                    } else {
+                        w = -1;
+                    }
+                    const uint32_t width = w < 0 ? 32u : (32u >> w);
+                    const uint32_t group = 32u / width;
+                    for (uint32_t o = 0; o < outer; o += group) {
                         SweepTile t{};
                         t.base = sbase + o * ostride + i0;
                         t.rule = rule;
-                        t.count = std::min<uint32_t>(32, g.nx - i0);
+                        t.count = cnt;
                         t.rs = rs;
                         t.i0 = i0;
                         t.nx = g.nx;
                         t.outer = o;
-                        if (fast && tensor_ok_[rule]) t.face |= TILE_TENSOR | (axis == 2 ? TILE_AXIS_Z : 0u);
-                        if (final_axis && dir) {
-                            t.face |= TILE_FACE;
-                            if (axis == 2 && (o == 0 || o + 1 == g.ny)) t.face |= TILE_FACE_ALL;
-                        }
+                        t.outer_n = outer;
+                        t.width = static_cast<uint16_t>(width);
+                        t.nslab = static_cast<uint16_t>(std::min(group, outer - o));
+                        t.map = rule * kMapsPerRule + static_cast<uint32_t>(w < 0 ? 0 : w);
+                        if (w >= 0) t.face |= TILE_TENSOR;
+                        if (axis == 2) t.face |= TILE_AXIS_Z;
+                        if (final_axis && dir) t.face |= TILE_FACE;
                         out.push_back(t);
                     }
                 }
