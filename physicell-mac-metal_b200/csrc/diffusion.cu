@@ -41,6 +41,21 @@
 
 namespace pcg {
 
+// The LineRule a tile descriptor carries.
+__device__ __forceinline__ LineRule rule_of(const SweepTile& t)
+{
+    LineRule r;
+    r.tab = t.tab;
+    r.n = t.n;
+    r.c = 0.f;
+    r.fold = t.fold;
+    r.T = t.T;
+    r.dir = t.inst >> 31;
+    r.inst = t.inst & 0x7fffffffu;
+    r._pad = 0;
+    return r;
+}
+
 __device__ __forceinline__ bool tile_on(const LineRule& r, const uint8_t* __restrict__ mask)
 {
     return mask == nullptr || (mask[r.inst] & STEP_DIFFUSE);
@@ -175,12 +190,11 @@ __device__ __forceinline__ void tile_coords(const SweepTile& tile, int* c)
 // Issue the loads of 'tile' into stage 'st' and of its rule's coefficient
 // table into 'stab' (the stage's table area), all counted on 'bar'.
 template <bool kRows>
-__device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const LineRule* __restrict__ rules,
-                                                const float* __restrict__ dens, const float* __restrict__ tab,
-                                                const void* tmaps, float* st, float* stab, uint64_t* bar, int lane,
-                                                unsigned* status)
+__device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const float* __restrict__ dens,
+                                                const float* __restrict__ tab, const void* tmaps, float* st,
+                                                float* stab, uint64_t* bar, int lane, unsigned* status)
 {
-    const LineRule& r = rules[tile.rule];
+    const LineRule r = rule_of(tile);
     const uint32_t n = r.n;
     const uint32_t tb = tab_floats(n) * 4u;    // 32-byte multiple, 32-byte aligned source
     const float* src = dens + tile.base;
@@ -235,8 +249,7 @@ __device__ __forceinline__ bool issue_tile_load(const SweepTile& tile, const Lin
 }
 
 template <bool kRows>
-__device__ __forceinline__ void issue_tile_store(const SweepTile& tile, const LineRule* __restrict__ rules,
-                                                 float* __restrict__ dens, const void* tmaps, const float* st, int lane)
+__device__ __forceinline__ void issue_tile_store(const SweepTile& tile, float* __restrict__ dens, const void* tmaps, const float* st, int lane)
 {
     float* dst = dens + tile.base;
     if (kRows && (tile.face & TILE_TENSOR)) {
@@ -263,7 +276,7 @@ __device__ __forceinline__ void issue_tile_store(const SweepTile& tile, const Li
             bulk_commit();
         }
     } else {
-        const uint32_t n = rules[tile.rule].n;
+        const uint32_t n = tile.n;
         const uint32_t rb = col_row_bytes(tile.count);
         for (uint32_t j = lane; j < n; j += 32) bulk_store(dst + static_cast<size_t>(j) * tile.rs, st + j * 32, rb);
         bulk_commit();
@@ -502,21 +515,32 @@ __device__ __forceinline__ void solve_rows(float* st, const SweepTile& tile, con
 // ------------------------------------------------------------------ pipelined kernel
 
 // Shared memory: kBarBytes of mbarriers ([warp][stage]), then the stages
-// ([warp][stage][stage_floats], 128-byte aligned).
-constexpr int kBarBytes = 512;   // up to 16 warps x 4 stages
+// ([warp][stage][stage_floats], 128-byte aligned).  Between them, one tile
+// descriptor per stage ([warp][stage], 64 bytes): the descriptor of the tile
+// a stage holds, stashed when its load is issued.  Both regions are sized
+// for the launch shape and rounded to 128 bytes.
+constexpr int kBarBytes = 512;    // at most 16 warps x 4 stages
+__host__ __device__ constexpr int round128(int b) { return (b + 127) & ~127; }
+__host__ __device__ constexpr int sweep_bar_bytes(int warps, int nstages) { return round128(warps * nstages * 8); }
+__host__ __device__ constexpr int sweep_header_bytes(int warps, int nstages)
+{
+    return sweep_bar_bytes(warps, nstages) + round128(warps * nstages * 64);
+}
 
 template <bool kRows>
 __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
-                                                   uint32_t ntiles, const LineRule* __restrict__ rules,
-                                                   const float* __restrict__ tab, const void* __restrict__ tmaps,
-                                                   int stage_floats, int nstages, int tab_area, int apply_faces,
+                                                   uint32_t ntiles, const float* __restrict__ tab,
+                                                   const void* __restrict__ tmaps, int stage_floats, int nstages,
+                                                   int tab_area, int apply_faces,
                                                    const uint8_t* __restrict__ mask, unsigned* __restrict__ status)
 {
     // stage: [tile data][tab_area floats of coefficient table]
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem) + warp * nstages;
-    float* stages = reinterpret_cast<float*>(smem + kBarBytes) + static_cast<size_t>(warp) * nstages * stage_floats;
+    SweepTile* descs = reinterpret_cast<SweepTile*>(smem + sweep_bar_bytes(nwarps, nstages)) + warp * nstages;
+    float* stages = reinterpret_cast<float*>(smem + sweep_header_bytes(nwarps, nstages)) +
+                    static_cast<size_t>(warp) * nstages * stage_floats;
     if (lane == 0)
         for (int s = 0; s < nstages; ++s) mbar_init(&bars[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -527,31 +551,35 @@ __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, con
     const int ahead = nstages - 1;   // loads in flight while one stage is solved
     uint32_t issued = 0;
     bool ok = true;
-    for (; issued < ntw && static_cast<int>(issued) < ahead; ++issued) {
+    // 'nd' is the descriptor of the next tile to issue, loaded one tile
+    // ahead so its latency hides behind the current solve
+    SweepTile nd{};
+    if (ntw) nd = tiles[gw];
+    auto issue = [&]() {
         const int s = static_cast<int>(issued % nstages);
         float* st = stages + s * stage_floats;
-        issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, tab, tmaps, st, st + stage_floats - tab_area,
-                               &bars[s], lane, status);
-    }
+        issue_tile_load<kRows>(nd, dens, tab, tmaps, st, st + stage_floats - tab_area, &bars[s], lane, status);
+        if (lane == 0) descs[s] = nd;
+        ++issued;
+        if (issued < ntw) nd = tiles[gw + issued * tw];
+    };
+    while (issued < ntw && static_cast<int>(issued) < ahead) issue();
     for (uint32_t k = 0; k < ntw; ++k) {
         // refill: tile k + ahead goes to the stage of tile k - 1, whose store
         // (issued last) must have finished reading shared memory
         if (issued < ntw) {
             bulk_wait_read<0>();
             __syncwarp();
-            const int s = static_cast<int>(issued % nstages);
-            float* st = stages + s * stage_floats;
-            issue_tile_load<kRows>(tiles[gw + issued * tw], rules, dens, tab, tmaps, st, st + stage_floats - tab_area,
-                                   &bars[s], lane, status);
-            ++issued;
+            issue();
         }
         const int s = static_cast<int>(k % nstages);
         if (!mbar_wait(&bars[s], (k / nstages) & 1u, status)) {
             ok = false;
             break;
         }
-        const SweepTile tile = tiles[gw + k * tw];
-        const LineRule r = rules[tile.rule];
+        __syncwarp();
+        const SweepTile tile = descs[s];
+        const LineRule r = rule_of(tile);
         float* st = stages + s * stage_floats;
         const float* t = st + stage_floats - tab_area;
         if (tile_on(r, mask)) {
@@ -564,7 +592,7 @@ __global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, con
         }
         fence_async_smem();
         __syncwarp();
-        issue_tile_store<kRows>(tile, rules, dens, tmaps, st, lane);
+        issue_tile_store<kRows>(tile, dens, tmaps, st, lane);
     }
     if (!ok) {
         // let every load this warp issued land before the CTA exits (bounded)
@@ -603,7 +631,7 @@ __device__ __forceinline__ void solve_line(float* s, size_t st, const LineRule& 
 }
 
 __global__ void __launch_bounds__(128) k_sweep_global(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
-                                                      uint32_t ntiles, const LineRule* __restrict__ rules,
+                                                      uint32_t ntiles,
                                                       const float* __restrict__ tab, int apply_faces,
                                                       const uint8_t* __restrict__ mask)
 {
@@ -613,7 +641,7 @@ __global__ void __launch_bounds__(128) k_sweep_global(float* __restrict__ dens, 
     for (uint32_t t = gw; t < ntiles; t += nw) {
         const SweepTile tile = tiles[t];
         if (static_cast<uint32_t>(lane) >= tile.count) continue;
-        const LineRule r = rules[tile.rule];
+        const LineRule r = rule_of(tile);
         if (!tile_on(r, mask)) continue;
         const bool rows = (tile.face & TILE_ROWS) != 0;
         // row tiles: lines tile.rs apart, unit stride; column tiles: adjacent lines, stride tile.rs
@@ -697,7 +725,8 @@ __global__ void k_gradients(const float* __restrict__ dens, float* __restrict__ 
 
 size_t sweep_tma_smem(int warps, int nstages, int stage_floats)
 {
-    return kBarBytes + static_cast<size_t>(warps) * nstages * stage_floats * sizeof(float);
+    return static_cast<size_t>(sweep_header_bytes(warps, nstages)) +
+           static_cast<size_t>(warps) * nstages * stage_floats * sizeof(float);
 }
 
 static cudaError_t allow_max_smem(const void* fn)
@@ -725,7 +754,7 @@ int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats)
 }
 
 cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                             const LineRule* rules, const float* tab, const void* tmaps, int apply_faces,
+                             const float* tab, const void* tmaps, int apply_faces,
                              const uint8_t* mask, unsigned* status, TmaCfg cfg)
 {
     if (ntiles == 0) return cudaSuccess;
@@ -734,11 +763,11 @@ cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const Swee
         return cudaErrorInvalidValue;
     const size_t smem = sweep_tma_smem(cfg.warps, cfg.stages, cfg.stage_floats);
     if (rows)
-        k_sweep_tma<true><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, rules, tab, tmaps,
+        k_sweep_tma<true><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, tab, tmaps,
                                                                    cfg.stage_floats, cfg.stages, cfg.tab_floats,
                                                                    apply_faces, mask, status);
     else
-        k_sweep_tma<false><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, rules, tab, tmaps,
+        k_sweep_tma<false><<<cfg.grid, cfg.warps * 32, smem, st>>>(dens, tiles, ntiles, tab, tmaps,
                                                                     cfg.stage_floats, cfg.stages, cfg.tab_floats,
                                                                     apply_faces, mask, status);
     return cudaGetLastError();
@@ -798,11 +827,11 @@ bool encode_row_map(void* map128, float* block, uint32_t nx, uint64_t rows, uint
 }
 
 cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                                const LineRule* rules, const float* tab, int apply_faces, const uint8_t* mask,
+                                const float* tab, int apply_faces, const uint8_t* mask,
                                 int grid)
 {
     if (ntiles == 0) return cudaSuccess;
-    k_sweep_global<<<grid, 128, 0, st>>>(dens, tiles, ntiles, rules, tab, apply_faces, mask);
+    k_sweep_global<<<grid, 128, 0, st>>>(dens, tiles, ntiles, tab, apply_faces, mask);
     return cudaGetLastError();
 }
 

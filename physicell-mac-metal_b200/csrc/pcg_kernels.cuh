@@ -55,7 +55,6 @@ __host__ __device__ constexpr uint32_t tab_floats(uint32_t n) { return ((n + 3u)
 // its lines start at 'base' with element stride 'rs'.
 struct SweepTile {
     uint64_t base;
-    uint32_t rule;
     uint32_t count;
     uint32_t rs;       // row tiles: line pitch; column tiles: element stride along a line
     uint32_t i0;       // x index of the tile's first column (column tiles)
@@ -68,7 +67,15 @@ struct SweepTile {
     uint16_t width;    // columns per slab (column tiles): 32, 16 or 8
     uint16_t nslab;    // slabs in the tile
     uint32_t outer_n;  // number of slabs (nz for y, ny for z)
+    // the tile's line rule (LineRule), carried in the descriptor so that a
+    // tile costs one descriptor load
+    uint32_t n;        // line length
+    uint32_t tab;      // first float of the coefficient table
+    float fold;        // Dirichlet RHS fold
+    float T;           // Dirichlet target
+    uint32_t inst;     // instance index; bit 31 set: Dirichlet
 };
+static_assert(sizeof(SweepTile) == 64, "one 64-byte descriptor per tile");
 enum : uint32_t { TILE_FACE = 1u, TILE_ROWS = 4u, TILE_TENSOR = 8u, TILE_AXIS_Z = 16u };
 
 // Longest line a tensor-map box can cover (box dimensions are <= 256).
@@ -133,7 +140,7 @@ int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats);   
 // tmaps: one 128-byte CUtensorMap per rule (64-byte aligned, global memory)
 // for the tiles flagged TILE_TENSOR; may be null otherwise.
 cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                             const LineRule* rules, const float* tab, const void* tmaps, int apply_faces,
+                             const float* tab, const void* tmaps, int apply_faces,
                              const uint8_t* mask, unsigned* status, TmaCfg cfg);
 // Encode the 3-D tensor map of one substrate block (rows px floats apart)
 // for column tiles of 'width' columns x 32/width slabs x n line positions:
@@ -147,7 +154,7 @@ bool encode_column_map(void* map128, float* block, uint32_t nx, uint32_t ny, uin
 bool encode_row_map(void* map128, float* block, uint32_t nx, uint64_t rows, uint32_t px);
 // Any line length: one thread per line, d kept in place in global memory.
 cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,
-                                const LineRule* rules, const float* tab, int apply_faces, const uint8_t* mask,
+                                const float* tab, int apply_faces, const uint8_t* mask,
                                 int grid);
 
 // applyDirichletBC over instances [0, n_inst): faces of Dirichlet substrates.

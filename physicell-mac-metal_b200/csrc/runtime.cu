@@ -409,6 +409,16 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
     return PCG_OK;
 }
 
+// Copy a line rule into a tile descriptor.
+static void fill_rule(SweepTile& t, const LineRule& r)
+{
+    t.n = r.n;
+    t.tab = r.tab;
+    t.fold = r.fold;
+    t.T = r.T;
+    t.inst = r.inst | (r.dir ? 0x80000000u : 0u);
+}
+
 // Tile lists of one axis: lines up to kTmaMaxN go to the pipelined TMA
 // kernels (x: 32 lines per tile; y/z: 32 columns per tile), longer lines to
 // the one-thread-per-line kernel.
@@ -439,7 +449,7 @@ int Diffusion::build_axis(int axis)
                 for (uint64_t l0 = 0; l0 < lines; l0 += 32) {
                     SweepTile t{};
                     t.base = sbase + l0 * d.px;
-                    t.rule = rule;
+                    fill_rule(t, h_rules_[rule]);
                     t.count = static_cast<uint32_t>(std::min<uint64_t>(32, lines - l0));
                     t.rs = d.px;
                     t.nx = g.nx;
@@ -474,7 +484,7 @@ int Diffusion::build_axis(int axis)
                     for (uint32_t o = 0; o < outer; o += group) {
                         SweepTile t{};
                         t.base = sbase + o * ostride + i0;
-                        t.rule = rule;
+                        fill_rule(t, h_rules_[rule]);
                         t.count = cnt;
                         t.rs = rs;
                         t.i0 = i0;
@@ -495,7 +505,7 @@ int Diffusion::build_axis(int axis)
         }
     }
     // larger lines first so the persistent loop ends evenly
-    auto by_n = [&](const SweepTile& a, const SweepTile& b) { return h_rules_[a.rule].n > h_rules_[b.rule].n; };
+    auto by_n = [](const SweepTile& a, const SweepTile& b) { return a.n > b.n; };
     std::stable_sort(fast_t.begin(), fast_t.end(), by_n);
     std::stable_sort(glob_t.begin(), glob_t.end(), by_n);
     std::vector<SweepList>& ls = lists[axis];
@@ -583,12 +593,11 @@ int Diffusion::launch_list(const SweepList& l, bool fuse, const uint8_t* mask)
     if (l.n == 0) return PCG_OK;
     float* d = dens.as<float>();
     const SweepTile* t = l.tiles.as<SweepTile>();
-    const LineRule* r = rules.as<LineRule>();
     const float* tb = tab.as<float>();
     cudaError_t e;
-    if (l.kind == 2) e = launch_sweep_global(ctx->stream, d, t, l.n, r, tb, fuse ? 1 : 0, mask, l.ggrid);
+    if (l.kind == 2) e = launch_sweep_global(ctx->stream, d, t, l.n, tb, fuse ? 1 : 0, mask, l.ggrid);
     else
-        e = launch_sweep_tma(ctx->stream, l.kind == 0, d, t, l.n, r, tb, tmaps.p, fuse ? 1 : 0, mask, ctx->status, l.tc);
+        e = launch_sweep_tma(ctx->stream, l.kind == 0, d, t, l.n, tb, tmaps.p, fuse ? 1 : 0, mask, ctx->status, l.tc);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep launch");
     ctx->launches++;
     return PCG_OK;
