@@ -92,13 +92,18 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+// One bounded try: the thread may be suspended for up to kSuspendNs while
+// the phase is incomplete, so a waiting warp does not spin on the issue
+// slots of the warps that are computing.
+constexpr uint32_t kSuspendNs = 20000;
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 {
     uint32_t done;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
         : "memory");
     return done != 0;
 }
@@ -297,95 +302,133 @@ __device__ __forceinline__ float4 tab_inv4(const float* t, int q)
     return *reinterpret_cast<const float4*>(t + (q << 3) + 4);
 }
 
-// One block of 8 positions (two table chunks) of the forward / backward
-// pass: positions 8k + u for u in [lo, hi] (all eight when kFull).
-template <bool kFull>
-__device__ __forceinline__ float fwd8(float (&v)[8], const float4 (&g)[2], const float4 (&iv)[2], float d, int lo,
-                                      int hi)
+// One chunk of the forward / backward pass (positions 4q..4q+3): all four,
+// or those with place u in [lo, hi] at the ends of the line.
+__device__ __forceinline__ float fwd1(float g, float iv, float d, float& v)
 {
-    const float gg[8] = {g[0].x, g[0].y, g[0].z, g[0].w, g[1].x, g[1].y, g[1].z, g[1].w};
-    const float ii[8] = {iv[0].x, iv[0].y, iv[0].z, iv[0].w, iv[1].x, iv[1].y, iv[1].z, iv[1].w};
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-        if (kFull || (u >= lo && u <= hi)) {
-            d = fmaf(gg[u], d, v[u] * ii[u]);
-            v[u] = d;
-        }
-    }
+    d = fmaf(g, d, v * iv);
+    v = d;
     return d;
 }
-template <bool kFull>
-__device__ __forceinline__ float bwd8(float (&v)[8], const float4 (&g)[2], float x, int lo, int hi)
+__device__ __forceinline__ float bwd1(float g, float x, float& v)
 {
-    const float gg[8] = {g[0].x, g[0].y, g[0].z, g[0].w, g[1].x, g[1].y, g[1].z, g[1].w};
-#pragma unroll
-    for (int u = 7; u >= 0; --u) {
-        if (kFull || (u >= lo && u <= hi)) {
-            x = fmaf(gg[u], x, v[u]);
-            v[u] = x;
-        }
-    }
+    x = fmaf(g, x, v);
+    v = x;
+    return x;
+}
+__device__ __forceinline__ float fwd4(float4& v, float4 g, float4 iv, float d)
+{
+    d = fwd1(g.x, iv.x, d, v.x);
+    d = fwd1(g.y, iv.y, d, v.y);
+    d = fwd1(g.z, iv.z, d, v.z);
+    return fwd1(g.w, iv.w, d, v.w);
+}
+__device__ __forceinline__ float bwd4(float4& v, float4 g, float x)
+{
+    x = bwd1(g.w, x, v.w);
+    x = bwd1(g.z, x, v.z);
+    x = bwd1(g.y, x, v.y);
+    return bwd1(g.x, x, v.x);
+}
+__device__ __forceinline__ float fwd4p(float4& v, float4 g, float4 iv, float d, int lo, int hi)
+{
+    if (lo <= 0 && 0 <= hi) d = fwd1(g.x, iv.x, d, v.x);
+    if (lo <= 1 && 1 <= hi) d = fwd1(g.y, iv.y, d, v.y);
+    if (lo <= 2 && 2 <= hi) d = fwd1(g.z, iv.z, d, v.z);
+    if (lo <= 3 && 3 <= hi) d = fwd1(g.w, iv.w, d, v.w);
+    return d;
+}
+__device__ __forceinline__ float bwd4p(float4& v, float4 g, float x, int lo, int hi)
+{
+    if (lo <= 3 && 3 <= hi) x = bwd1(g.w, x, v.w);
+    if (lo <= 2 && 2 <= hi) x = bwd1(g.z, x, v.z);
+    if (lo <= 1 && 1 <= hi) x = bwd1(g.y, x, v.y);
+    if (lo <= 0 && 0 <= hi) x = bwd1(g.x, x, v.x);
     return x;
 }
 
-// Both passes of one line over positions 1..n-2 (n >= 3) in blocks of 8
-// positions; ld(q, p) / st(q, p) move the 4 positions of chunk q (4q..4q+3)
-// from / to p[0..3].  Two register sets alternate: the next block and its
-// coefficients are loaded into one while the other's dependent FFMAs run,
-// so no load sits on the recurrence and no register is copied.  Only chunks
-// up to the one holding position n - 2 are read or written; values past
-// n - 2 in that chunk are written back unchanged.
+// Both passes of one line over positions 1..n-2 (n >= 3), chunk by chunk:
+// ld(q) returns chunk q (positions 4q..4q+3) from shared memory and st(q, v)
+// writes it back.  The two end chunks are peeled off, so the main loops run
+// over whole chunks with no per-position tests; each loop keeps the next
+// chunk and its coefficients loaded while the current chunk's dependent
+// FFMAs run.  Only chunks up to the one holding position n - 2 are touched;
+// places past the line's end in that chunk are written back unchanged.
 template <class LD, class ST>
 __device__ __forceinline__ void thomas_line(const float* t, int n, LD ld, ST st)
 {
-    const int ql = (n - 2) >> 2;       // chunk of the last interior position
-    const int bl = ql >> 1;            // its block
-    const int hl = n - 2 - 8 * bl;     // its place in that block
-    float a[8], b[8];
-    float4 ga[2], ia[2], gb[2], ib[2];
-    auto load = [&](int k, float (&v)[8], float4 (&g)[2], float4 (&iv)[2], bool with_inv) {
-        ld(2 * k, v);
-        g[0] = tab_g4(t, 2 * k);
-        if (with_inv) iv[0] = tab_inv4(t, 2 * k);
-        if (2 * k + 1 <= ql) {
-            ld(2 * k + 1, v + 4);
-            g[1] = tab_g4(t, 2 * k + 1);
-            if (with_inv) iv[1] = tab_inv4(t, 2 * k + 1);
-        }
-    };
-    auto store = [&](int k, float (&v)[8]) {
-        st(2 * k, v);
-        if (2 * k + 1 <= ql) st(2 * k + 1, v + 4);
-    };
-    auto fwd = [&](int k, float (&v)[8], float4 (&g)[2], float4 (&iv)[2], float d) {
-        if (k > 0 && k < bl) return fwd8<true>(v, g, iv, d, 0, 7);
-        return fwd8<false>(v, g, iv, d, k == 0 ? 1 : 0, k == bl ? hl : 7);
-    };
-    auto bwd = [&](int k, float (&v)[8], float4 (&g)[2], float x) {
-        if (k > 0 && k < bl) return bwd8<true>(v, g, x, 0, 7);
-        return bwd8<false>(v, g, x, k == 0 ? 1 : 0, k == bl ? hl : 7);
-    };
+    const int ql = (n - 2) >> 2;      // chunk of position n - 2
+    const int hl = n - 2 - 4 * ql;    // its place in that chunk
+    // forward: chunk 0 (from position 1), whole chunks 1..ql-1, chunk ql
     float d = 0.f;
-    load(0, a, ga, ia, true);
-    for (int k = 0; k <= bl; k += 2) {
-        if (k + 1 <= bl) load(k + 1, b, gb, ib, true);
-        d = fwd(k, a, ga, ia, d);
-        store(k, a);
-        if (k + 1 > bl) break;
-        if (k + 2 <= bl) load(k + 2, a, ga, ia, true);
-        d = fwd(k + 1, b, gb, ib, d);
-        store(k + 1, b);
+    {
+        float4 v0 = ld(0);
+        if (ql == 0) {
+            d = fwd4p(v0, tab_g4(t, 0), tab_inv4(t, 0), d, 1, hl);
+            st(0, v0);
+        } else {
+            float4 a = ld(1), ga = tab_g4(t, 1), ia = tab_inv4(t, 1);
+            d = fwd4p(v0, tab_g4(t, 0), tab_inv4(t, 0), d, 1, 3);
+            st(0, v0);
+            int q = 1;   // a holds chunk q
+            for (; q + 1 < ql; q += 2) {
+                float4 b = ld(q + 1), gb = tab_g4(t, q + 1), ib = tab_inv4(t, q + 1);
+                d = fwd4(a, ga, ia, d);
+                st(q, a);
+                a = ld(q + 2);
+                ga = tab_g4(t, q + 2);
+                ia = tab_inv4(t, q + 2);
+                d = fwd4(b, gb, ib, d);
+                st(q + 1, b);
+            }
+            if (q < ql) {   // q == ql - 1: one whole chunk, then chunk ql
+                float4 b = ld(ql), gb = tab_g4(t, ql), ib = tab_inv4(t, ql);
+                d = fwd4(a, ga, ia, d);
+                st(q, a);
+                d = fwd4p(b, gb, ib, d, 0, hl);
+                st(ql, b);
+            } else {        // a holds chunk ql
+                d = fwd4p(a, ga, ia, d, 0, hl);
+                st(ql, a);
+            }
+        }
     }
+    // backward: chunk ql, whole chunks ql-1..1, chunk 0 (down to position 1)
     float x = 0.f;
-    load(bl, a, ga, ia, false);
-    for (int k = bl; k >= 0; k -= 2) {
-        if (k >= 1) load(k - 1, b, gb, ib, false);
-        x = bwd(k, a, ga, x);
-        store(k, a);
-        if (k < 1) break;
-        if (k >= 2) load(k - 2, a, ga, ia, false);
-        x = bwd(k - 1, b, gb, x);
-        store(k - 1, b);
+    if (ql == 0) {
+        float4 w = ld(0);
+        x = bwd4p(w, tab_g4(t, 0), x, 1, hl);
+        st(0, w);
+        return;
+    }
+    float4 a = ld(ql), ga = tab_g4(t, ql);
+    int q = ql;
+    {
+        float4 b = ld(q - 1), gb = tab_g4(t, q - 1);
+        x = bwd4p(a, ga, x, 0, hl);
+        st(q, a);
+        a = b;
+        ga = gb;
+        --q;
+    }
+    for (; q - 1 >= 1; q -= 2) {   // a holds whole chunk q
+        float4 b = ld(q - 1), gb = tab_g4(t, q - 1);
+        x = bwd4(a, ga, x);
+        st(q, a);
+        a = ld(q - 2);
+        ga = tab_g4(t, q - 2);
+        x = bwd4(b, gb, x);
+        st(q - 1, b);
+    }
+    if (q >= 1) {   // q == 1
+        float4 b = ld(0), gb = tab_g4(t, 0);
+        x = bwd4(a, ga, x);
+        st(1, a);
+        x = bwd4p(b, gb, x, 1, 3);
+        st(0, b);
+    } else {        // a holds chunk 0
+        x = bwd4p(a, ga, x, 1, 3);
+        st(0, a);
     }
 }
 
@@ -404,15 +447,8 @@ __device__ __forceinline__ void solve_rows_vec(float* st, const LineRule& r, con
         row[1] += r.fold;
         if (n > 3) row[n - 2] += r.fold;
         thomas_line(
-            t, n,
-            [row](int q, float* v) {
-                const float4 a = *reinterpret_cast<const float4*>(row + 4 * q);
-                v[0] = a.x;
-                v[1] = a.y;
-                v[2] = a.z;
-                v[3] = a.w;
-            },
-            [row](int q, const float* v) { *reinterpret_cast<float4*>(row + 4 * q) = make_float4(v[0], v[1], v[2], v[3]); });
+            t, n, [row](int q) { return *reinterpret_cast<const float4*>(row + 4 * q); },
+            [row](int q, float4 v) { *reinterpret_cast<float4*>(row + 4 * q) = v; });
     }
     if (r.dir) {
         row[0] = r.T;
@@ -436,13 +472,14 @@ __device__ __forceinline__ void solve_cols(float* st, const SweepTile& tile, con
         if (n > 3) c[(n - 2) * 32] += r.fold;
         thomas_line(
             t, n,
-            [c](int q, float* v) {
-#pragma unroll
-                for (int u = 0; u < 4; ++u) v[u] = c[(4 * q + u) * 32];
+            [c](int q) {
+                return make_float4(c[(4 * q) * 32], c[(4 * q + 1) * 32], c[(4 * q + 2) * 32], c[(4 * q + 3) * 32]);
             },
-            [c](int q, const float* v) {
-#pragma unroll
-                for (int u = 0; u < 4; ++u) c[(4 * q + u) * 32] = v[u];
+            [c](int q, float4 v) {
+                c[(4 * q) * 32] = v.x;
+                c[(4 * q + 1) * 32] = v.y;
+                c[(4 * q + 2) * 32] = v.z;
+                c[(4 * q + 3) * 32] = v.w;
             });
     }
     if (r.dir) {
@@ -528,7 +565,7 @@ __host__ __device__ constexpr int sweep_header_bytes(int warps, int nstages)
 }
 
 template <bool kRows>
-__global__ void __launch_bounds__(512) k_sweep_tma(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
+__global__ void __launch_bounds__(256, 1) k_sweep_tma(float* __restrict__ dens, const SweepTile* __restrict__ tiles,
                                                    uint32_t ntiles, const float* __restrict__ tab,
                                                    const void* __restrict__ tmaps, int stage_floats, int nstages,
                                                    int tab_area, int apply_faces,
