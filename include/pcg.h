@@ -79,6 +79,7 @@ typedef struct pcg_ctx pcg_ctx;
 typedef struct pcg_me pcg_me;
 typedef struct pcg_cells pcg_cells;
 typedef struct pcg_mech pcg_mech;
+typedef struct pcg_motility pcg_motility;
 typedef struct pcg_batch pcg_batch;
 typedef struct pcg_server pcg_server;
 
@@ -190,6 +191,44 @@ uint32_t pcg_mech_total_voxels(const pcg_mech* mech);
 pcg_status pcg_mech_set_diagnostics(pcg_mech* mech, int on);
 pcg_status pcg_mech_neighbor_stats(pcg_mech* mech, uint32_t* count, uint32_t* hash);
 uint32_t pcg_neighbor_hash(uint32_t cell);
+
+/* ------------------------------------------------------------------------
+ * Motility — updateMotility (src/motility.cpp:179-293) on the device: the
+ * persistent random walk with chemotaxis bias that main.mm:379-387 runs
+ * between CellMechanics::computeForces and integratePositions.  State is
+ * MotilityData (src/motility.h:10-50), resident on the device.
+ *
+ * Random draws: the reference uses an unseeded std::mt19937; here draw k of
+ * cell i at step `step` is a counter-based uniform of (seed, i, step, k)
+ * (k = 0 resample test, 1 theta, 2 phi), so a run is reproducible and the
+ * CPU oracle computes the same draws.
+ * Gradient read: layout PCG_MOT_REFERENCE reads the density as
+ * motility.cpp:68-74 does (linear index voxel * n_substrates + s into the
+ * substrate-major buffer); PCG_MOT_SUBSTRATE_MAJOR reads substrate s of the
+ * voxel.  They agree for one substrate.
+ * ---------------------------------------------------------------------- */
+enum { PCG_MOT_REFERENCE = 0, PCG_MOT_SUBSTRATE_MAJOR = 1 };
+
+/* MotilityData::allocate / allocateSubstrate (motility.cpp:91-113);
+ * n_substrates = 0: the single-substrate chemotaxis rule only. */
+pcg_status pcg_motility_create(pcg_ctx* ctx, uint32_t max_cells, uint32_t n_substrates, pcg_motility** out);
+pcg_status pcg_motility_destroy(pcg_motility* mot);
+/* Host -> device state of cells [0, n_cells): persistence_time, elapsed,
+ * bias, vec (three arrays of n_cells: x, y, z), is_motile, restrict_to_2D,
+ * chemotaxis_index, chemotaxis_direction, sensitivity (n_cells *
+ * n_substrates, cell-major; may be NULL when created with 0 substrates). */
+pcg_status pcg_motility_upload(pcg_motility* mot, uint32_t n_cells, const double* persistence_time,
+                               const double* elapsed, const double* bias, const double* vec,
+                               const uint32_t* is_motile, const uint32_t* restrict_2d,
+                               const int32_t* chemotaxis_index, const int32_t* chemotaxis_direction,
+                               const double* sensitivity);
+/* Device -> host of what updateMotility changes: elapsed and vec. */
+pcg_status pcg_motility_download(pcg_motility* mot, double* elapsed, double* vec);
+/* updateMotility(cells, mot, density, grid, dt): adds each living motile
+ * cell's motility vector to its velocity (fields 3-5, written by the force
+ * pass); me supplies the density and grid for the chemotaxis gradient. */
+pcg_status pcg_motility_update(pcg_motility* mot, pcg_cells* cells, const pcg_me* me, double dt, uint64_t seed,
+                               uint64_t step, int layout);
 
 /* No reference counterpart.  The stable (key, value) radix sort that bins
  * cells by mechanics voxel, run on caller-owned DEVICE buffers and making

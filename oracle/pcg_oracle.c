@@ -458,6 +458,156 @@ void or_voxel_refresh(float* soa, uint32_t max_cells, uint32_t n_cells, const or
 /* Whole step (main.mm:341-391)                                         */
 /* ------------------------------------------------------------------ */
 
+/* ------------------------------------------------------------------ motility */
+
+#define OR_PI 3.14159265358979323846
+
+static uint64_t or_mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+double or_uniform(uint64_t seed, uint64_t cell, uint64_t step, uint32_t k)
+{
+    uint64_t h = or_mix64(seed ^ 0x9e3779b97f4a7c15ULL);
+    h = or_mix64(h ^ cell);
+    h = or_mix64(h ^ step);
+    h = or_mix64(h ^ (uint64_t)k);
+    return (double)(h >> 11) * 0x1.0p-53;
+}
+
+/* The density value at the clamped voxel (i, j, k) for substrate s, read as
+ * the reference reads it (layout OR_MOT_REF) or substrate-major. */
+static double or_mot_density(const float* density, const or_grid* g, int i, int j, int k, int s, int layout)
+{
+    const int nx = (int)g->nx, ny = (int)g->ny, nz = (int)g->nz;
+    i = i < 0 ? 0 : (i > nx - 1 ? nx - 1 : i);
+    j = j < 0 ? 0 : (j > ny - 1 ? ny - 1 : j);
+    k = k < 0 ? 0 : (k > nz - 1 ? nz - 1 : k);
+    const size_t v = ((size_t)k * ny + j) * nx + i;
+    const size_t nvox = (size_t)g->nx * g->ny * g->nz;
+    return (double)density[layout == OR_MOT_REF ? v * g->n_substrates + (size_t)s : (size_t)s * nvox + v];
+}
+
+/* computeGradient (motility.cpp:46-87): voxel by FP32 subtract and divide,
+ * truncation, clamp; central differences with clamped neighbours. */
+static void or_mot_gradient(const float* density, const or_grid* g, float px, float py, float pz, int s,
+                            int layout, double* gx, double* gy, double* gz)
+{
+    if (s < 0 || s >= (int)g->n_substrates) {   /* undefined in the reference: no gradient */
+        *gx = *gy = *gz = 0.0;
+        return;
+    }
+    const int nx = (int)g->nx, ny = (int)g->ny, nz = (int)g->nz;
+    int ix = (int)((px - g->x_min) / g->dx);
+    int iy = (int)((py - g->y_min) / g->dy);
+    int iz = (int)((pz - g->z_min) / g->dz);
+    ix = ix < 0 ? 0 : (ix > nx - 1 ? nx - 1 : ix);
+    iy = iy < 0 ? 0 : (iy > ny - 1 ? ny - 1 : iy);
+    iz = iz < 0 ? 0 : (iz > nz - 1 ? nz - 1 : iz);
+    *gx = (or_mot_density(density, g, ix + 1, iy, iz, s, layout) - or_mot_density(density, g, ix - 1, iy, iz, s, layout)) /
+          (2.0 * g->dx);
+    *gy = (or_mot_density(density, g, ix, iy + 1, iz, s, layout) - or_mot_density(density, g, ix, iy - 1, iz, s, layout)) /
+          (2.0 * g->dy);
+    *gz = 0.0;
+    if (nz > 1)
+        *gz = (or_mot_density(density, g, ix, iy, iz + 1, s, layout) -
+               or_mot_density(density, g, ix, iy, iz - 1, s, layout)) /
+              (2.0 * g->dz);
+}
+
+void or_motility_update(float* soa, uint32_t max_cells, uint32_t n_cells, const float* density,
+                        const or_grid* g, or_motility* m, double dt, uint64_t seed, uint64_t step, int layout)
+{
+    float* px = soa + (size_t)0 * max_cells;
+    float* py = soa + (size_t)1 * max_cells;
+    float* pz = soa + (size_t)2 * max_cells;
+    float* vx = soa + (size_t)3 * max_cells;
+    float* vy = soa + (size_t)4 * max_cells;
+    float* vz = soa + (size_t)5 * max_cells;
+    const float* speed = soa + (size_t)16 * max_cells;
+    const float* alive = soa + (size_t)25 * max_cells;
+    double* mvx = m->vec;
+    double* mvy = m->vec + n_cells;
+    double* mvz = m->vec + 2 * (size_t)n_cells;
+    for (uint32_t i = 0; i < n_cells; i++) {
+        uint32_t is_alive;
+        memcpy(&is_alive, &alive[i], sizeof is_alive);
+        if (is_alive == 0) continue;
+        if (m->is_motile[i] == 0) {
+            mvx[i] = mvy[i] = mvz[i] = 0.0;
+            continue;
+        }
+        m->elapsed[i] += dt;
+        const double pt = m->persistence_time[i];
+        const int resample = (pt < dt) || (or_uniform(seed, i, step, 0) < dt / pt);
+        if (resample) {
+            m->elapsed[i] = 0.0;
+            double rx, ry, rz;
+            if (m->restrict_2d[i]) {
+                const double theta = 2.0 * OR_PI * or_uniform(seed, i, step, 1);
+                rx = cos(theta);
+                ry = sin(theta);
+                rz = 0.0;
+            } else {
+                const double theta = 2.0 * OR_PI * or_uniform(seed, i, step, 1);
+                const double phi = OR_PI * or_uniform(seed, i, step, 2);
+                const double sin_phi = sin(phi);
+                rx = sin_phi * cos(theta);
+                ry = sin_phi * sin(theta);
+                rz = cos(phi);
+            }
+            double bx = 0.0, by = 0.0, bz = 0.0;
+            const double bias = m->bias[i];
+            if (bias > 0.0 && density != NULL) {
+                if (m->sensitivity && m->n_sens > 0) {
+                    for (uint32_t s = 0; s < m->n_sens; s++) {
+                        const double sens = m->sensitivity[(size_t)i * m->n_sens + s];
+                        if (fabs(sens) < 1e-16) continue;
+                        double gx, gy, gz;
+                        or_mot_gradient(density, g, px[i], py[i], pz[i], (int)s, layout, &gx, &gy, &gz);
+                        bx += sens * gx;
+                        by += sens * gy;
+                        bz += sens * gz;
+                    }
+                } else {
+                    double gx, gy, gz;
+                    or_mot_gradient(density, g, px[i], py[i], pz[i], m->chemotaxis_index[i], layout, &gx, &gy, &gz);
+                    const int dir = m->chemotaxis_direction[i];
+                    bx = dir * gx;
+                    by = dir * gy;
+                    bz = dir * gz;
+                }
+                const double bmag = sqrt(bx * bx + by * by + bz * bz);
+                if (bmag > 1e-16) {
+                    bx /= bmag;
+                    by /= bmag;
+                    bz /= bmag;
+                }
+            }
+            const double omb = 1.0 - bias;
+            double mx = omb * rx + bias * bx;
+            double my = omb * ry + bias * by;
+            double mz = omb * rz + bias * bz;
+            const double mag = sqrt(mx * mx + my * my + mz * mz);
+            if (mag > 1e-16) {
+                mx /= mag;
+                my /= mag;
+                mz /= mag;
+            }
+            const double sp = (double)speed[i];
+            mvx[i] = mx * sp;
+            mvy[i] = my * sp;
+            mvz[i] = mz * sp;
+        }
+        vx[i] += (float)mvx[i];
+        vy[i] += (float)mvy[i];
+        vz[i] += (float)mvz[i];
+    }
+}
+
 void or_run(const or_sim* sim, float* density, float* soa, uint32_t max_cells, uint32_t n_cells,
             const double* secretion, const double* uptake, const double* saturation,
             const double* net_export, const uint8_t* active,

@@ -161,6 +161,50 @@ typedef struct {
     int refresh_voxels;           /* recompute voxel_index after integrate */
 } or_sim;
 
+/* ---------------------------------------------------------------- motility
+ *
+ * updateMotility (src/motility.cpp:179-293): persistent random walk with a
+ * chemotaxis bias, added to the velocity the force pass wrote.  The
+ * reference draws from a std::mt19937 seeded by std::random_device, which
+ * cannot be reproduced; here every draw is or_uniform(seed, cell, step, k)
+ * with k = 0 (resample test), 1 (theta), 2 (phi), a counter-based
+ * generator the device uses too.  Parity with the reference itself is
+ * pinned where its result does not depend on the draws: bias 1 with
+ * persistence below dt makes every motile cell's vector the normalised
+ * gradient times its speed.
+ *
+ * Gradient read (motility.cpp:46-87): the reference indexes the density as
+ * density[voxel * n_substrates + s] although the buffer is substrate-major;
+ * layout OR_MOT_REF reproduces that, OR_MOT_SUBSTRATE_MAJOR reads
+ * density[s * n_voxels + voxel].  The two agree for one substrate. */
+enum { OR_MOT_REF = 0, OR_MOT_SUBSTRATE_MAJOR = 1 };
+
+/* Per-cell motility state (src/motility.h:10-50), arrays of n_cells; vec is
+ * three arrays of n_cells (x, y, z).  sensitivity: n_cells * n_sens doubles
+ * or NULL for the single-substrate rule (chemotaxis_index / direction). */
+typedef struct {
+    double* persistence_time;
+    double* elapsed;
+    const double* bias;
+    double* vec;
+    const uint32_t* is_motile;
+    const uint32_t* restrict_2d;
+    const int32_t* chemotaxis_index;
+    const int32_t* chemotaxis_direction;
+    const double* sensitivity;
+    uint32_t n_sens;
+} or_motility;
+
+/* Uniform double in [0, 1) of draw k for (seed, cell, step): three rounds
+ * of the SplitMix64 finaliser (Steele, Lea and Flood, 2014), 53 bits. */
+double or_uniform(uint64_t seed, uint64_t cell, uint64_t step, uint32_t k);
+
+/* soa: 28-field SoA (velocity fields 3-5 updated, speed field 16 and
+ * is_alive field 25 read); density: substrate-major FP32 of grid g. */
+void or_motility_update(float* soa, uint32_t max_cells, uint32_t n_cells, const float* density,
+                        const or_grid* g, or_motility* mot, double dt, uint64_t seed, uint64_t step,
+                        int layout);
+
 /* Runs n_diffusion_steps of: sweeps -> Dirichlet -> secretion ->
  * [mech accumulator: bin/sort -> forces -> integrate].  mech_accum carries
  * the accumulator between calls (start at 0). */

@@ -318,3 +318,67 @@ def ref_integrate(soa, max_cells, n, m, origin, dt):
     mg = Grid(m.mech_grid_nx, m.mech_grid_ny, m.mech_grid_nz, 0, m.mechanics_voxel_size,
               m.mechanics_voxel_size, m.mechanics_voxel_size, 0.0, origin[0], origin[1], origin[2], 0.0)
     ref().ref_integrate(_p(soa, _F32), _U32(max_cells), _U32(n), C.byref(mg), _F32(dt))
+
+
+# ---------------------------------------------------------------- motility
+
+MOT_REF, MOT_SUBSTRATE_MAJOR = 0, 1
+
+
+class MotilityState(C.Structure):
+    """or_motility: pointers into the arrays of a motility state dict."""
+    _fields_ = [("persistence_time", C.POINTER(C.c_double)), ("elapsed", C.POINTER(C.c_double)),
+                ("bias", C.POINTER(C.c_double)), ("vec", C.POINTER(C.c_double)),
+                ("is_motile", C.POINTER(C.c_uint32)), ("restrict_2d", C.POINTER(C.c_uint32)),
+                ("chemotaxis_index", C.POINTER(C.c_int32)), ("chemotaxis_direction", C.POINTER(C.c_int32)),
+                ("sensitivity", C.POINTER(C.c_double)), ("n_sens", C.c_uint32)]
+
+
+def motility_state(n, n_sens=0):
+    """A zeroed motility state (src/motility.cpp:133-152 defaults): persistence
+    15, bias 0.5, not motile, 2-D, chemotaxis up the first substrate."""
+    st = {"persistence_time": np.full(n, 15.0), "elapsed": np.zeros(n), "bias": np.full(n, 0.5),
+          "vec": np.zeros(3 * n), "is_motile": np.zeros(n, np.uint32), "restrict_2d": np.ones(n, np.uint32),
+          "chemotaxis_index": np.zeros(n, np.int32), "chemotaxis_direction": np.ones(n, np.int32),
+          "sensitivity": np.zeros(n * n_sens) if n_sens else None, "n_sens": n_sens}
+    return st
+
+
+def _mot_struct(st):
+    m = MotilityState()
+    m.persistence_time = _p(st["persistence_time"], C.c_double)
+    m.elapsed = _p(st["elapsed"], C.c_double)
+    m.bias = _p(st["bias"], C.c_double)
+    m.vec = _p(st["vec"], C.c_double)
+    m.is_motile = _p(st["is_motile"], C.c_uint32)
+    m.restrict_2d = _p(st["restrict_2d"], C.c_uint32)
+    m.chemotaxis_index = _p(st["chemotaxis_index"], C.c_int32)
+    m.chemotaxis_direction = _p(st["chemotaxis_direction"], C.c_int32)
+    m.sensitivity = _p(st["sensitivity"], C.c_double) if st["sensitivity"] is not None else None
+    m.n_sens = st["n_sens"] if st["sensitivity"] is not None else 0
+    return m
+
+
+def uniform(seed, cell, step, k):
+    lib = oracle()
+    lib.or_uniform.restype = C.c_double
+    return lib.or_uniform(C.c_uint64(seed), C.c_uint64(cell), C.c_uint64(step), C.c_uint32(k))
+
+
+def motility_update(soa, max_cells, n, density, grid, st, dt, seed, step, layout=MOT_REF):
+    m = _mot_struct(st)
+    oracle().or_motility_update(_p(soa, _F32), _U32(max_cells), _U32(n),
+                                _p(density, _F32) if density is not None else None, C.byref(grid), C.byref(m),
+                                _F64(dt), C.c_uint64(seed), C.c_uint64(step), C.c_int(layout))
+
+
+def ref_motility_update(soa, max_cells, n, density, grid, st, dt):
+    s = st["sensitivity"]
+    ref().ref_update_motility(_p(soa, _F32), _U32(max_cells), _U32(n),
+                              _p(density, _F32) if density is not None else None, C.byref(grid),
+                              _p(st["persistence_time"], C.c_double), _p(st["elapsed"], C.c_double),
+                              _p(st["bias"], C.c_double), _p(st["vec"], C.c_double),
+                              _p(st["is_motile"], C.c_uint32), _p(st["restrict_2d"], C.c_uint32),
+                              _p(st["chemotaxis_index"], C.c_int32), _p(st["chemotaxis_direction"], C.c_int32),
+                              _p(s, C.c_double) if s is not None else None, _U32(st["n_sens"] if s is not None else 0),
+                              _F64(dt))

@@ -8,7 +8,7 @@
  *     (through metal_shim.h; one call per Metal thread id, ascending, so the
  *     spatial-hash slot order is ascending cell index)
  *   src/cell_phenotype.cpp (processSecretion), src/cell_data.cpp,
- *   src/cell_definitions.cpp
+ *   src/cell_definitions.cpp, src/motility.cpp (updateMotility)
  * The host-side steps that live in Objective-C++ files and cannot be
  * compiled here are restated below with their citations:
  *   ThomasCoeffs set-up   src/microenvironment.mm:171-177
@@ -23,6 +23,7 @@
 #include "types.h"
 #include "cell_data.h"
 #include "cell_phenotype.h"
+#include "motility.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -148,6 +149,49 @@ void ref_compute_forces(float* soa, uint32_t max_cells, uint32_t n_cells, const 
 void ref_integrate(float* soa, uint32_t max_cells, uint32_t n_cells, const GridParams* mech_grid, float dt)
 {
     for (uint32_t t = 0; t < n_cells; t++) integrate_positions(soa, *mech_grid, dt, n_cells, max_cells, t);
+}
+
+/* updateMotility (motility.cpp:179-293) on a 28-field SoA block and the
+ * MotilityData arrays (vec: three arrays of n_cells).  Its random draws come
+ * from the reference's own unseeded generator, so only results that do not
+ * depend on them are comparable (bias 1 with persistence below dt). */
+void ref_update_motility(float* soa, uint32_t max_cells, uint32_t n_cells, const float* density, const GridParams* g,
+                         double* persistence, double* elapsed, const double* bias, double* vec,
+                         const uint32_t* is_motile, const uint32_t* restrict_2d, const int32_t* chem_index,
+                         const int32_t* chem_dir, const double* sens, uint32_t n_sens, double dt)
+{
+    CellData cells(max_cells ? max_cells : 1);
+    std::vector<float> block(cells.gpuBufferSize() / sizeof(float), 0.0f);
+    std::memcpy(block.data(), soa, (size_t)NUM_CELL_FIELDS * max_cells * sizeof(float));
+    cells.setGPUBufferBase(block.data());
+    cells.num_cells = n_cells;
+    MotilityData mot;
+    mot.allocate(max_cells ? max_cells : 1);
+    if (sens && n_sens) mot.allocateSubstrate(n_sens);
+    for (uint32_t i = 0; i < n_cells; i++) {
+        mot.persistence_time[i] = persistence[i];
+        mot.motility_elapsed[i] = elapsed[i];
+        mot.motility_bias[i] = bias[i];
+        mot.motility_vec_x[i] = vec[i];
+        mot.motility_vec_y[i] = vec[n_cells + i];
+        mot.motility_vec_z[i] = vec[2 * (size_t)n_cells + i];
+        mot.is_motile[i] = is_motile[i];
+        mot.restrict_to_2D[i] = restrict_2d[i];
+        mot.chemotaxis_index[i] = chem_index[i];
+        mot.chemotaxis_direction[i] = chem_dir[i];
+        for (uint32_t s = 0; sens && s < n_sens; s++)
+            mot.chemotactic_sensitivity[(size_t)i * n_sens + s] = sens[(size_t)i * n_sens + s];
+    }
+    updateMotility(cells, mot, density, *g, dt);
+    std::memcpy(soa, block.data(), (size_t)NUM_CELL_FIELDS * max_cells * sizeof(float));
+    for (uint32_t i = 0; i < n_cells; i++) {
+        persistence[i] = mot.persistence_time[i];
+        elapsed[i] = mot.motility_elapsed[i];
+        vec[i] = mot.motility_vec_x[i];
+        vec[n_cells + i] = mot.motility_vec_y[i];
+        vec[2 * (size_t)n_cells + i] = mot.motility_vec_z[i];
+    }
+    mot.free_all();
 }
 
 }  // extern "C"

@@ -11,6 +11,8 @@ read like the reference's own code:
     CellMechanics      src/cell_mechanics.h:15-87
         computeForces, integratePositions, update, syncHashPointers ->
         voxelCellCount / voxelCells
+    Motility           MotilityData + updateMotility (src/motility.h,
+                       src/motility.cpp:179-293)
     Batch, Server      many simulations at once; continuous batching
 
 Every call goes through the C ABI of include/pcg.h.  There is no CPU
@@ -71,6 +73,7 @@ _F32P = C.POINTER(C.c_float)
 _F64P = C.POINTER(C.c_double)
 _U32P = C.POINTER(C.c_uint32)
 _U8P = C.POINTER(C.c_uint8)
+_I32P = C.POINTER(C.c_int32)
 
 
 class InstanceDesc(C.Structure):
@@ -138,6 +141,12 @@ _SIGS = [
     ("pcg_mech_set_diagnostics", C.c_int, [_P, C.c_int]),
     ("pcg_mech_neighbor_stats", C.c_int, [_P, _U32P, _U32P]),
     ("pcg_neighbor_hash", C.c_uint32, [C.c_uint32]),
+    ("pcg_motility_create", C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
+    ("pcg_motility_destroy", C.c_int, [_P]),
+    ("pcg_motility_upload", C.c_int, [_P, C.c_uint32, _F64P, _F64P, _F64P, _F64P, _U32P, _U32P, _I32P, _I32P,
+                                      _F64P]),
+    ("pcg_motility_download", C.c_int, [_P, _F64P, _F64P]),
+    ("pcg_motility_update", C.c_int, [_P, _P, _P, C.c_double, C.c_uint64, C.c_uint64, C.c_int]),
     ("pcg_sort_pairs_static", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                         C.c_int]),
     ("pcg_batch_create", C.c_int, [_P, C.POINTER(InstanceDesc), C.c_uint32, C.POINTER(BatchOptions),
@@ -398,6 +407,61 @@ class Cells:
     def close(self):
         if getattr(self, "h", None):
             lib().pcg_cells_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+MOT_REFERENCE, MOT_SUBSTRATE_MAJOR = 0, 1
+
+
+class Motility:
+    """MotilityData (src/motility.h:10-50) resident on the device, with
+    updateMotility (src/motility.cpp:179-293).  'state' is a dict of the
+    per-cell arrays: persistence_time, elapsed, bias, vec (3 * n: x, y, z),
+    is_motile, restrict_2d, chemotaxis_index, chemotaxis_direction and
+    sensitivity (n * S, or None for the single-substrate rule)."""
+
+    def __init__(self, ctx, max_cells, n_substrates=0):
+        self.ctx = ctx
+        self.S = n_substrates
+        h = _P()
+        ctx.check(lib().pcg_motility_create(ctx.h, max_cells, n_substrates, C.byref(h)))
+        self.h = h
+        self.n = 0
+
+    def upload(self, state):
+        n = len(state["persistence_time"])
+        f64 = lambda k: np.ascontiguousarray(state[k], np.float64)
+        arrs = [f64("persistence_time"), f64("elapsed"), f64("bias"), f64("vec"),
+                np.ascontiguousarray(state["is_motile"], np.uint32),
+                np.ascontiguousarray(state["restrict_2d"], np.uint32),
+                np.ascontiguousarray(state["chemotaxis_index"], np.int32),
+                np.ascontiguousarray(state["chemotaxis_direction"], np.int32)]
+        sens = state.get("sensitivity")
+        sens = None if sens is None else np.ascontiguousarray(sens, np.float64)
+        ptrs = [_f64(arrs[0]), _f64(arrs[1]), _f64(arrs[2]), _f64(arrs[3]), _u32(arrs[4]), _u32(arrs[5]),
+                arrs[6].ctypes.data_as(_I32P), arrs[7].ctypes.data_as(_I32P), _f64(sens) if sens is not None else None]
+        self.ctx.check(lib().pcg_motility_upload(self.h, n, *ptrs))
+        self.n = n
+
+    def download(self):
+        el = np.zeros(max(self.n, 1))
+        vec = np.zeros(max(3 * self.n, 3))
+        self.ctx.check(lib().pcg_motility_download(self.h, _f64(el), _f64(vec)))
+        return el[:self.n], vec[:3 * self.n]
+
+    def update(self, cells, me, dt, seed, step, layout=MOT_REFERENCE):
+        self.ctx.check(lib().pcg_motility_update(self.h, cells.h, me.h if me is not None else None, dt,
+                                                 C.c_uint64(seed), C.c_uint64(step), layout))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().pcg_motility_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -7,29 +7,10 @@
 #include <string>
 #include <vector>
 
-#include "runtime.h"
+#include "capi.h"
 
 using namespace pcg;
 
-struct pcg_me {
-    pcg_ctx* ctx = nullptr;
-    Diffusion d;
-};
-
-struct pcg_cells {
-    pcg_ctx* ctx = nullptr;
-    Cells c;
-    uint32_t S = 0;
-    const pcg_me* bound_me = nullptr;
-    const pcg_mech* bound_mech = nullptr;
-};
-
-struct pcg_mech {
-    pcg_ctx* ctx = nullptr;
-    Mechanics m;
-    pcg_mechanics_params p{};
-    float ox = 0, oy = 0, oz = 0;
-};
 
 namespace {
 

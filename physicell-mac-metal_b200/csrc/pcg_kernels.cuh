@@ -14,8 +14,8 @@ enum Field : int {
     F_VEL_X = 3, F_VEL_Y = 4, F_VEL_Z = 5,
     F_PREV_VX = 6, F_PREV_VY = 7, F_PREV_VZ = 8,
     F_RADIUS = 9, F_TOTAL_VOL = 11,
-    F_REPULSION = 13, F_ADHESION = 14, F_REL_MAX_ADH = 15,
-    F_PRESSURE = 22, F_VOXEL_IDX = 26, F_MECH_VOXEL = 27,
+    F_REPULSION = 13, F_ADHESION = 14, F_REL_MAX_ADH = 15, F_MOT_SPEED = 16,
+    F_PRESSURE = 22, F_IS_ALIVE = 25, F_VOXEL_IDX = 26, F_MECH_VOXEL = 27,
     NUM_FIELDS = 28
 };
 

@@ -105,10 +105,51 @@ def gen_mechanics():
                         mech=np.array([m.mech_grid_nx, m.mech_grid_ny, m.mech_grid_nz], np.uint32))
 
 
+def motility_case(rng, two_d, S, multi, n=300, mc=320):
+    """Inputs for updateMotility where the result does not depend on the
+    reference's unseeded draws: bias 1, persistence below dt."""
+    nx, ny, nz = 20, 16, (1 if two_d else 12)
+    grid = np.array([nx, ny, nz, S], np.uint32)
+    geo = np.array([20.0, 20.0, 20.0, 0.01, -200.0, -160.0, -10.0 if two_d else -120.0], np.float32)
+    dens = rng.uniform(0, 40, nx * ny * nz * S).astype(np.float32)
+    soa = np.zeros(28 * mc, np.float32)
+    soa[0:n] = rng.uniform(-210, 210, n)
+    soa[mc:mc + n] = rng.uniform(-170, 170, n)
+    soa[2 * mc:2 * mc + n] = 0 if two_d else rng.uniform(-130, 130, n)
+    soa[3 * mc:6 * mc] = rng.normal(0, 1, 3 * mc)
+    soa[16 * mc:16 * mc + n] = rng.uniform(0.5, 2, n)
+    soa[25 * mc:25 * mc + n] = np.where(rng.random(n) < 0.9, 1, 0).astype(np.uint32).view(np.float32)
+    st = po.motility_state(n, S if multi else 0)
+    st["is_motile"][:] = rng.random(n) < 0.8
+    st["persistence_time"][:] = 0.001
+    st["bias"][:] = 1.0
+    st["restrict_2d"][:] = 1 if two_d else 0
+    st["vec"][:] = rng.normal(0, 1, 3 * n)
+    st["chemotaxis_index"][:] = rng.integers(0, S, n)
+    st["chemotaxis_direction"][:] = np.where(rng.random(n) < 0.5, 1, -1)
+    if multi:
+        st["sensitivity"][:] = rng.uniform(-1, 1, n * S)
+    return grid, geo, dens, soa, st, n, mc
+
+
+def gen_motility():
+    rng = np.random.default_rng(41)
+    for name, two_d, S, multi in (("motility_2d_legacy", True, 1, False), ("motility_3d_multi", False, 2, True)):
+        grid, geo, dens, soa0, st, n, mc = motility_case(rng, two_d, S, multi)
+        g = po.Grid(*[int(x) for x in grid], *[float(x) for x in geo[:4]], *[float(x) for x in geo[4:]], 0.0)
+        soa = soa0.copy()
+        st0 = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+        po.ref_motility_update(soa, mc, n, dens, g, st, 0.1)
+        arrays = {k: v for k, v in st0.items() if isinstance(v, np.ndarray)}
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), grid=grid, geo=geo, density=dens, soa0=soa0, n=n,
+                            max_cells=mc, n_sens=st0["n_sens"], soa_out=soa, vec_out=st["vec"],
+                            elapsed_out=st["elapsed"], **{"in_" + k: v for k, v in arrays.items()})
+
+
 if __name__ == "__main__":
     if not po.ref_available():
         sys.exit("oracle/_ref/libpcg_ref.so not built (make -C oracle with the reference tree present)")
-    gen_diffusion()
-    gen_secretion()
-    gen_mechanics()
+    which = sys.argv[1:] or ["diffusion", "secretion", "mechanics", "motility"]
+    for w in which:
+        globals()["gen_" + w]()
     print("golden vectors written to", OUT)

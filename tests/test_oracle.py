@@ -263,3 +263,86 @@ def test_live_reference_random_shapes(po):
         po.sweeps(b, g, subs, po.OR_FP32_REF)
         po.dirichlet(b, g, subs)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (nx, ny, S)
+
+
+# ---------------------------------------------------------------- motility
+
+def _motility_fixture(po, path):
+    f = np.load(path)
+    grid, geo = f["grid"], f["geo"]
+    g = po.Grid(*[int(x) for x in grid], *[float(x) for x in geo[:4]], *[float(x) for x in geo[4:]], 0.0)
+    n, mc, n_sens = int(f["n"]), int(f["max_cells"]), int(f["n_sens"])
+    st = po.motility_state(n, n_sens)
+    for k in st:
+        if isinstance(st[k], np.ndarray):
+            st[k] = f["in_" + k].copy()
+    return f, g, n, mc, st
+
+
+@pytest.mark.parametrize("name", ["motility_2d_legacy", "motility_3d_multi"])
+def test_motility_matches_reference_golden(po, name):
+    """updateMotility (motility.cpp:179-293) with bias 1 and persistence
+    below dt: every motile cell's vector is its normalised chemotaxis
+    direction times its speed, independent of the random draws; the oracle
+    reproduces the reference's output bit for bit (reference density
+    indexing, dead and non-motile cells, the single- and multi-substrate
+    rules)."""
+    f, g, n, mc, st = _motility_fixture(po, os.path.join(GOLDEN, name + ".npz"))
+    soa = f["soa0"].copy()
+    po.motility_update(soa, mc, n, f["density"], g, st, 0.1, seed=123, step=9)
+    assert np.array_equal(st["vec"], f["vec_out"])
+    assert np.array_equal(st["elapsed"], f["elapsed_out"])
+    assert np.array_equal(soa, f["soa_out"])
+
+
+def test_motility_draws_are_counter_based(po):
+    """Draw k of (seed, cell, step) is a pure function: repeatable, distinct
+    across keys, uniform in [0, 1)."""
+    u = [po.uniform(5, c, s, k) for c in range(50) for s in range(4) for k in range(3)]
+    assert u == [po.uniform(5, c, s, k) for c in range(50) for s in range(4) for k in range(3)]
+    assert len(set(u)) == len(u) and min(u) >= 0.0 and max(u) < 1.0
+    big = np.array([po.uniform(9, c, 0, 0) for c in range(4000)])
+    assert abs(big.mean() - 0.5) < 0.02 and abs(big.var() - 1 / 12) < 0.01
+
+
+def test_motility_random_walk_unit_speed_and_persistence(po):
+    """bias 0: the vector is a unit direction scaled by the speed; with a
+    long persistence most cells keep their vector (no resample)."""
+    rng = np.random.default_rng(3)
+    n, mc = 400, 400
+    g = po.Grid(10, 10, 10, 1, 20.0, 20.0, 20.0, 0.01, 0.0, 0.0, 0.0, 0.0)
+    dens = np.zeros(1000, np.float32)
+    soa = np.zeros(28 * mc, np.float32)
+    soa[16 * mc:17 * mc] = 1.5
+    soa[25 * mc:26 * mc] = np.ones(mc, np.uint32).view(np.float32)
+    st = po.motility_state(n)
+    st["is_motile"][:] = 1
+    st["bias"][:] = 0.0
+    st["restrict_2d"][:] = 0
+    st["persistence_time"][:] = 0.001
+    po.motility_update(soa, mc, n, dens, g, st, 0.1, seed=1, step=0)
+    v = st["vec"].reshape(3, n)
+    assert np.allclose(np.linalg.norm(v, axis=0), 1.5, rtol=1e-12)
+    prev = st["vec"].copy()
+    st["persistence_time"][:] = 1e6          # resample probability 1e-7
+    po.motility_update(soa, mc, n, dens, g, st, 0.1, seed=1, step=1)
+    assert np.array_equal(st["vec"], prev)
+    assert np.allclose(st["elapsed"], 0.1)
+
+
+def test_motility_live_reference_when_present(po):
+    if not po.ref_available():
+        pytest.skip("reference library not built here")
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("gen_golden", os.path.join(GOLDEN, "gen_golden.py"))
+    gg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gg)
+    rng = np.random.default_rng(77)
+    for two_d, S, multi in ((True, 2, True), (False, 1, False), (False, 3, True)):
+        grid, geo, dens, soa0, st, n, mc = gg.motility_case(rng, two_d, S, multi)
+        g = po.Grid(*[int(x) for x in grid], *[float(x) for x in geo[:4]], *[float(x) for x in geo[4:]], 0.0)
+        a, b = soa0.copy(), soa0.copy()
+        sa = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+        po.motility_update(a, mc, n, dens, g, sa, 0.1, seed=0, step=0)
+        po.ref_motility_update(b, mc, n, dens, g, st, 0.1)
+        assert np.array_equal(a, b) and np.array_equal(sa["vec"], st["vec"])
