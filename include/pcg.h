@@ -80,6 +80,7 @@ typedef struct pcg_me pcg_me;
 typedef struct pcg_cells pcg_cells;
 typedef struct pcg_mech pcg_mech;
 typedef struct pcg_motility pcg_motility;
+typedef struct pcg_snapshot pcg_snapshot;
 typedef struct pcg_batch pcg_batch;
 typedef struct pcg_server pcg_server;
 
@@ -229,6 +230,32 @@ pcg_status pcg_motility_download(pcg_motility* mot, double* elapsed, double* vec
  * pass); me supplies the density and grid for the chemotaxis gradient. */
 pcg_status pcg_motility_update(pcg_motility* mot, pcg_cells* cells, const pcg_me* me, double dt, uint64_t seed,
                                uint64_t step, int layout);
+
+/* ------------------------------------------------------------------------
+ * Snapshots — writeMatlabSnapshots (src/output_writer.cpp:295-452) with
+ * write_matlab4 (src/matlab_writer.cpp:5-49): MATLAB v4 files of one full
+ * double matrix, byte-identical to the reference writer's.  Asynchronous:
+ * the matrix is built on the device after the work queued so far on the
+ * context (later work on the context waits only for that build), then
+ * copied and written by a host callback while the simulation goes on.
+ * Cell columns come from the 28-field SoA and the secretion rates; the
+ * columns the reference takes from CPU-side phenotype arrays get the values
+ * it writes when those arrays are absent.
+ * ---------------------------------------------------------------------- */
+pcg_status pcg_snapshot_create(pcg_ctx* ctx, pcg_snapshot** out);
+/* Waits for every pending write; reports a file that could not be written. */
+pcg_status pcg_snapshot_wait(pcg_snapshot* snap);
+pcg_status pcg_snapshot_destroy(pcg_snapshot* snap);
+/* "multiscale_microenvironment": (4 + S) x voxels, rows x, y, z, voxel
+ * volume, densities. */
+pcg_status pcg_snapshot_microenvironment(pcg_snapshot* snap, const pcg_me* me, const char* path);
+/* "cells": (71 + 7 * types + 8 * S) x cells; n_cell_types 0 counts as 1. */
+pcg_status pcg_snapshot_cells(pcg_snapshot* snap, const pcg_cells* cells, uint32_t n_cell_types, const char* path);
+/* Both files of one output frame, named as the reference names them:
+ * folder/output%08d_cells.mat and folder/output%08d_microenvironment0.mat
+ * (either object may be NULL). */
+pcg_status pcg_snapshot_frame(pcg_snapshot* snap, const pcg_me* me, const pcg_cells* cells, uint32_t n_cell_types,
+                              const char* folder, int frame);
 
 /* No reference counterpart.  The stable (key, value) radix sort that bins
  * cells by mechanics voxel, run on caller-owned DEVICE buffers and making

@@ -382,3 +382,23 @@ def ref_motility_update(soa, max_cells, n, density, grid, st, dt):
                               _p(st["chemotaxis_index"], C.c_int32), _p(st["chemotaxis_direction"], C.c_int32),
                               _p(s, C.c_double) if s is not None else None, _U32(st["n_sens"] if s is not None else 0),
                               _F64(dt))
+
+
+# ---------------------------------------------------------------- .mat snapshots
+
+def ref_write_matlab(soa, max_cells, n, n_types, sec, upt, sat, ne, density, grid, frame, folder):
+    sec, upt, sat, ne = (np.ascontiguousarray(a, np.float64) for a in (sec, upt, sat, ne))
+    ref().ref_write_matlab(_p(soa, _F32), _U32(max_cells), _U32(n), _U32(n_types), _p(sec, _F64), _p(upt, _F64),
+                           _p(sat, _F64), _p(ne, _F64), _p(density, _F32), C.byref(grid), C.c_int(frame),
+                           C.c_char_p(folder.encode()))
+
+
+def read_mat4(path):
+    """(name, matrix rows x cols) of a MATLAB v4 file of one full double matrix."""
+    raw = open(path, "rb").read()
+    typ, rows, cols, imag, nlen = np.frombuffer(raw[:20], np.uint32)
+    assert typ == 0 and imag == 0
+    name = raw[20:20 + nlen - 1].decode()
+    data = np.frombuffer(raw[20 + nlen:], np.float64)
+    assert data.size == rows * cols
+    return name, data.reshape(cols, rows).T

@@ -8,7 +8,8 @@
  *     (through metal_shim.h; one call per Metal thread id, ascending, so the
  *     spatial-hash slot order is ascending cell index)
  *   src/cell_phenotype.cpp (processSecretion), src/cell_data.cpp,
- *   src/cell_definitions.cpp, src/motility.cpp (updateMotility)
+ *   src/cell_definitions.cpp, src/motility.cpp (updateMotility),
+ *   src/output_writer.cpp + src/matlab_writer.cpp (writeMatlabSnapshots)
  * The host-side steps that live in Objective-C++ files and cannot be
  * compiled here are restated below with their citations:
  *   ThomasCoeffs set-up   src/microenvironment.mm:171-177
@@ -24,6 +25,7 @@
 #include "cell_data.h"
 #include "cell_phenotype.h"
 #include "motility.h"
+#include "output_writer.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -192,6 +194,30 @@ void ref_update_motility(float* soa, uint32_t max_cells, uint32_t n_cells, const
         vec[2 * (size_t)n_cells + i] = mot.motility_vec_z[i];
     }
     mot.free_all();
+}
+
+/* writeMatlabSnapshots (output_writer.cpp:295-452) of a CellData holding
+ * the 28-field SoA block and the secretion rates only (its CPU-side
+ * phenotype arrays absent, so the writer uses its defaults for them), and a
+ * substrate-major density; files output%08d_cells.mat and
+ * output%08d_microenvironment0.mat in 'folder'. */
+void ref_write_matlab(const float* soa, uint32_t max_cells, uint32_t n_cells, uint32_t n_cell_types,
+                      const double* sec, const double* upt, const double* sat, const double* ne,
+                      const float* density, const GridParams* g, int frame, const char* folder)
+{
+    CellData cells(max_cells ? max_cells : 1);
+    std::vector<float> block(cells.gpuBufferSize() / sizeof(float), 0.0f);
+    std::memcpy(block.data(), soa, (size_t)NUM_CELL_FIELDS * max_cells * sizeof(float));
+    cells.setGPUBufferBase(block.data());
+    cells.num_cells = n_cells;
+    cells.num_cell_types = n_cell_types;
+    cells.allocateSubstrateBuffers(g->n_substrates);
+    const size_t nS = (size_t)n_cells * g->n_substrates;
+    std::memcpy(cells.secretion_rate, sec, nS * sizeof(double));
+    std::memcpy(cells.uptake_rate, upt, nS * sizeof(double));
+    std::memcpy(cells.saturation_density, sat, nS * sizeof(double));
+    std::memcpy(cells.net_export_rate, ne, nS * sizeof(double));
+    writeMatlabSnapshots(cells, density, *g, frame, folder);
 }
 
 }  // extern "C"

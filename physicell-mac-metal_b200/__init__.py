@@ -147,6 +147,12 @@ _SIGS = [
                                       _F64P]),
     ("pcg_motility_download", C.c_int, [_P, _F64P, _F64P]),
     ("pcg_motility_update", C.c_int, [_P, _P, _P, C.c_double, C.c_uint64, C.c_uint64, C.c_int]),
+    ("pcg_snapshot_create", C.c_int, [_P, C.POINTER(_P)]),
+    ("pcg_snapshot_wait", C.c_int, [_P]),
+    ("pcg_snapshot_destroy", C.c_int, [_P]),
+    ("pcg_snapshot_microenvironment", C.c_int, [_P, _P, C.c_char_p]),
+    ("pcg_snapshot_cells", C.c_int, [_P, _P, C.c_uint32, C.c_char_p]),
+    ("pcg_snapshot_frame", C.c_int, [_P, _P, _P, C.c_uint32, C.c_char_p, C.c_int]),
     ("pcg_sort_pairs_static", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                         C.c_int]),
     ("pcg_batch_create", C.c_int, [_P, C.POINTER(InstanceDesc), C.c_uint32, C.POINTER(BatchOptions),
@@ -462,6 +468,42 @@ class Motility:
     def close(self):
         if getattr(self, "h", None):
             lib().pcg_motility_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Snapshot:
+    """Asynchronous .mat snapshots (writeMatlabSnapshots,
+    src/output_writer.cpp:295-452)."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        h = _P()
+        ctx.check(lib().pcg_snapshot_create(ctx.h, C.byref(h)))
+        self.h = h
+
+    def microenvironment(self, me, path):
+        self.ctx.check(lib().pcg_snapshot_microenvironment(self.h, me.h, str(path).encode()))
+
+    def cells(self, cells, path, n_cell_types=1):
+        self.ctx.check(lib().pcg_snapshot_cells(self.h, cells.h, n_cell_types, str(path).encode()))
+
+    def frame(self, me, cells, folder, frame, n_cell_types=1):
+        self.ctx.check(lib().pcg_snapshot_frame(self.h, me.h if me is not None else None,
+                                                cells.h if cells is not None else None, n_cell_types,
+                                                str(folder).encode(), frame))
+
+    def wait(self):
+        self.ctx.check(lib().pcg_snapshot_wait(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().pcg_snapshot_destroy(self.h)
             self.h = None
 
     def __del__(self):

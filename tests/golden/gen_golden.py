@@ -146,10 +146,42 @@ def gen_motility():
                             elapsed_out=st["elapsed"], **{"in_" + k: v for k, v in arrays.items()})
 
 
+def matlab_case(rng, two_d, S, n=40, mc=48, n_types=2):
+    """Inputs for writeMatlabSnapshots: a small grid and cells whose 28-field
+    SoA columns all carry values."""
+    nx, ny, nz = (12, 10, 1) if two_d else (6, 5, 4)
+    grid = np.array([nx, ny, nz, S], np.uint32)
+    geo = np.array([20.0, 20.0, 20.0, 0.01, -120.0, -100.0, -10.0 if two_d else -40.0], np.float32)
+    dens = rng.uniform(0, 40, nx * ny * nz * S).astype(np.float32)
+    soa = np.zeros(28 * mc, np.float32)
+    for f in range(23):
+        soa[f * mc:f * mc + n] = rng.normal(0, 50, n)
+    for f, hi in ((23, n_types), (24, 6), (25, 2)):
+        soa[f * mc:f * mc + n] = rng.integers(0, hi, n).astype(np.uint32).view(np.float32)
+    soa[26 * mc:28 * mc] = rng.integers(0, 100, 2 * mc).astype(np.uint32).view(np.float32)
+    rates = [rng.uniform(0, 10, n * S) for _ in range(4)]
+    return grid, geo, dens, soa, rates, n, mc, n_types
+
+
+def gen_matlab():
+    import tempfile
+    rng = np.random.default_rng(51)
+    for name, two_d, S in (("matlab_2d", True, 2), ("matlab_3d", False, 1)):
+        grid, geo, dens, soa, rates, n, mc, n_types = matlab_case(rng, two_d, S)
+        g = po.Grid(*[int(x) for x in grid], *[float(x) for x in geo[:4]], *[float(x) for x in geo[4:]], 0.0)
+        with tempfile.TemporaryDirectory() as d:
+            po.ref_write_matlab(soa, mc, n, n_types, *rates, dens, g, 3, d)
+            cells_mat = np.frombuffer(open(os.path.join(d, "output00000003_cells.mat"), "rb").read(), np.uint8)
+            env_mat = np.frombuffer(open(os.path.join(d, "output00000003_microenvironment0.mat"), "rb").read(), np.uint8)
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), grid=grid, geo=geo, density=dens, soa=soa, n=n,
+                            max_cells=mc, n_types=n_types, sec=rates[0], upt=rates[1], sat=rates[2], ne=rates[3],
+                            cells_mat=cells_mat, env_mat=env_mat)
+
+
 if __name__ == "__main__":
     if not po.ref_available():
         sys.exit("oracle/_ref/libpcg_ref.so not built (make -C oracle with the reference tree present)")
-    which = sys.argv[1:] or ["diffusion", "secretion", "mechanics", "motility"]
+    which = sys.argv[1:] or ["diffusion", "secretion", "mechanics", "motility", "matlab"]
     for w in which:
         globals()["gen_" + w]()
     print("golden vectors written to", OUT)

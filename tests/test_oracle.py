@@ -346,3 +346,33 @@ def test_motility_live_reference_when_present(po):
         po.motility_update(a, mc, n, dens, g, sa, 0.1, seed=0, step=0)
         po.ref_motility_update(b, mc, n, dens, g, st, 0.1)
         assert np.array_equal(a, b) and np.array_equal(sa["vec"], st["vec"])
+
+
+# ---------------------------------------------------------------- .mat snapshots
+
+@pytest.mark.parametrize("name", ["matlab_2d", "matlab_3d"])
+def test_matlab_golden_layout(po, name, tmp_path):
+    """The golden files are MATLAB v4 full double matrices with the
+    reference's shapes: cells (71 + 7 T + 8 S) x n, microenvironment
+    (4 + S) x voxels with FP32 voxel centres; regenerated byte-identical by
+    the reference writer when it is built here."""
+    f = np.load(os.path.join(GOLDEN, name + ".npz"))
+    S, T, n = int(f["grid"][3]), int(f["n_types"]), int(f["n"])
+    nx, ny, nz = (int(x) for x in f["grid"][:3])
+    (tmp_path / "c.mat").write_bytes(f["cells_mat"].tobytes())
+    (tmp_path / "e.mat").write_bytes(f["env_mat"].tobytes())
+    cname, cm = po.read_mat4(str(tmp_path / "c.mat"))
+    ename, em = po.read_mat4(str(tmp_path / "e.mat"))
+    assert cname == "cells" and cm.shape == (71 + 7 * T + 8 * S, n)
+    assert ename == "multiscale_microenvironment" and em.shape == (4 + S, nx * ny * nz)
+    geo = f["geo"]
+    ix = np.arange(nx * ny * nz) % nx
+    xc = (np.float32(geo[4]) + (ix.astype(np.float32) + np.float32(0.5)) * np.float32(geo[0])).astype(np.float64)
+    assert np.array_equal(em[0], xc)
+    assert np.array_equal(cm[0], np.arange(n, dtype=np.float64))
+    if po.ref_available():
+        g = po.Grid(nx, ny, nz, S, *[float(x) for x in geo[:4]], *[float(x) for x in geo[4:]], 0.0)
+        po.ref_write_matlab(f["soa"], int(f["max_cells"]), n, T, f["sec"], f["upt"], f["sat"], f["ne"], f["density"],
+                            g, 3, str(tmp_path))
+        assert (tmp_path / "output00000003_cells.mat").read_bytes() == f["cells_mat"].tobytes()
+        assert (tmp_path / "output00000003_microenvironment0.mat").read_bytes() == f["env_mat"].tobytes()
