@@ -117,9 +117,10 @@ __global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, ui
     }
 }
 
-// One thread per (run, substrate = blockIdx.y): applies the run's cells to
-// the voxel in ascending cell index (the stable order), FP64 per cell with
-// the FP32 store after each cell.
+// One thread per run: applies the run's cells to its voxel in ascending
+// cell index (the stable order), substrate by substrate, FP64 per cell with
+// the FP32 store after each cell.  The run's metadata is read once and each
+// cell's constants for all substrates are contiguous.
 __global__ void k_secrete(float* __restrict__ dens, const uint32_t* __restrict__ skeys,
                           const uint32_t* __restrict__ run_start, const uint32_t* __restrict__ run_inst,
                           const uint32_t* __restrict__ n_runs, const CellInst* __restrict__ insts,
@@ -127,27 +128,28 @@ __global__ void k_secrete(float* __restrict__ dens, const uint32_t* __restrict__
                           const uint8_t* __restrict__ mask)
 {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t s = blockIdx.y;
     if (r >= *n_runs) return;
     const uint32_t ii = run_inst[r];
     if (mask && !(mask[ii] & STEP_DIFFUSE)) return;
     const CellInst& in = insts[ii];
-    if (s >= in.S) return;
+    const uint32_t S = in.S;
     const uint32_t p0 = run_start[r], p1 = run_start[r + 1];
     const uint32_t v = skeys[p0] - in.vox_base;
     // dense voxel index -> padded-row device offset
-    const uint64_t off = static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
-    float* d = dens + in.dens_off + s * in.sub_pitch + off;
-    const double* c = cs + 3ull * (in.rate_off + (p0 - sbeg[ii]) * in.S + s);
-    float rho32 = *d;
-    for (uint32_t q = p0; q < p1; ++q, c += 3ull * in.S) {
-        double rho = static_cast<double>(rho32);
-        rho = __dadd_rn(rho, c[0]);
-        rho = __ddiv_rn(__dadd_rn(rho, c[1]), c[2]);
-        if (rho < 0.0) rho = 0.0;
-        rho32 = __double2float_rn(rho);
+    float* d = dens + in.dens_off + static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
+    const double* c0 = cs + 3ull * (in.rate_off + static_cast<uint64_t>(p0 - sbeg[ii]) * S);
+    for (uint32_t s = 0; s < S; ++s, d += in.sub_pitch) {
+        float rho32 = *d;
+        const double* c = c0 + 3ull * s;
+        for (uint32_t q = p0; q < p1; ++q, c += 3ull * S) {
+            double rho = static_cast<double>(rho32);
+            rho = __dadd_rn(rho, c[0]);
+            rho = __ddiv_rn(__dadd_rn(rho, c[1]), c[2]);
+            if (rho < 0.0) rho = 0.0;
+            rho32 = __double2float_rn(rho);
+        }
+        *d = rho32;
     }
-    *d = rho32;
 }
 
 // ------------------------------------------------------------------ mechanics
@@ -401,8 +403,8 @@ cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, 
                            const CellInst* insts, const uint32_t* sbeg, const double* cs, const uint8_t* mask)
 {
     if (max_runs == 0 || max_s == 0) return cudaSuccess;
-    dim3 grid(blocks_for(max_runs, 256), max_s);
-    k_secrete<<<grid, 256, 0, st>>>(dens, skeys, run_start, run_inst, n_runs, insts, sbeg, cs, mask);
+    k_secrete<<<blocks_for(max_runs, 256), 256, 0, st>>>(dens, skeys, run_start, run_inst, n_runs, insts, sbeg, cs,
+                                                          mask);
     return cudaGetLastError();
 }
 
