@@ -121,7 +121,7 @@ __global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, ui
 // cell index (the stable order), substrate by substrate, FP64 per cell with
 // the FP32 store after each cell.  The run's metadata is read once and each
 // cell's constants for all substrates are contiguous.
-__global__ void k_secrete(float* __restrict__ dens, const uint32_t* __restrict__ skeys,
+__global__ void __launch_bounds__(256, 8) k_secrete(float* __restrict__ dens, const uint32_t* __restrict__ skeys,
                           const uint32_t* __restrict__ run_start, const uint32_t* __restrict__ run_inst,
                           const uint32_t* __restrict__ n_runs, const CellInst* __restrict__ insts,
                           const uint32_t* __restrict__ sbeg, const double* __restrict__ cs,
@@ -287,8 +287,8 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
         for (; q < q1; ++q) {
             const float4 cur = o;
             if (q + 1 < q1) o = spos[q + 1];   // next candidate in flight
-            if (q == p) continue;
-            // neighbour test exactly as mechanics.metal:159-165 (no contraction)
+            // neighbour test exactly as mechanics.metal:159-165 (no contraction);
+            // the cell itself (q == p, distance 0) fails it like any coincident cell
             const float ddx = __fsub_rn(me.x, cur.x), ddy = __fsub_rn(me.y, cur.y), ddz = __fsub_rn(me.z, cur.z);
             const float dsq = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
             if (dsq >= maxd2 || dsq < 1e-12f) continue;
