@@ -283,10 +283,10 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
     for (int r = 0; r < 9; ++r) {
         uint32_t q = rq0[r];
         const uint32_t q1 = rq1[r];
-        float4 o = q < q1 ? spos[q] : me;
+        float4 o = spos[q];   // q <= n: in bounds even for an empty row
         for (; q < q1; ++q) {
             const float4 cur = o;
-            if (q + 1 < q1) o = spos[q + 1];   // next candidate in flight
+            o = spos[q + 1];   // next candidate in flight (spos has one spare element)
             // neighbour test exactly as mechanics.metal:159-165 (no contraction);
             // the cell itself (q == p, distance 0) fails it like any coincident cell
             const float ddx = __fsub_rn(me.x, cur.x), ddy = __fsub_rn(me.y, cur.y), ddz = __fsub_rn(me.z, cur.z);

@@ -1014,8 +1014,9 @@ int Mechanics::create(pcg_ctx* c, uint32_t tmv, uint32_t maxc)
     PCG_CU(ctx, start.alloc((static_cast<size_t>(tmv) + 1) * sizeof(uint32_t)));
     PCG_CU(ctx, cudaMemsetAsync(start.p, 0, start.bytes, ctx->stream));
     PCG_CU(ctx, scan_scr.alloc(scan_scratch_bytes(static_cast<uint64_t>(tmv) + 1)));
-    PCG_CU(ctx, spos.alloc(static_cast<size_t>(cap) * sizeof(float4)));
-    PCG_CU(ctx, sprm.alloc(static_cast<size_t>(cap) * sizeof(float4)));
+    // one spare element: the force loop loads the next candidate without a bounds test
+    PCG_CU(ctx, spos.alloc((static_cast<size_t>(cap) + 1) * sizeof(float4)));
+    PCG_CU(ctx, sprm.alloc((static_cast<size_t>(cap) + 1) * sizeof(float4)));
     return PCG_OK;
 }
 
