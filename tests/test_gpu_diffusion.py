@@ -42,6 +42,10 @@ CASES = [
     ("long_y_global", 5, 600, 1, [O2]),
     ("long_z_global", 6, 4, 530, [(1e4, 0.1, True, 3.0)]),
     ("wide_y", 70, 3, 1, [(1e5, 0.0, True, 0.0)]),
+    ("x_bulk_300", 300, 7, 1, [O2]),                     # x lines past a tensor box: one bulk copy per tile
+    ("y_bulk_400", 9, 400, 1, [O2, (2e3, 0.2, False, 0.0)]),   # column tiles by per-row bulk copies
+    ("z_bulk_270", 5, 6, 270, [(1e4, 0.1, True, 3.0)]),
+    ("3d_w16_groups", 44, 13, 9, [O2, (4e3, 0.3, True, 2.0)]),  # 12-column remainder: 16-wide, 2-slab tiles
 ]
 
 
