@@ -613,6 +613,16 @@ void or_run(const or_sim* sim, float* density, float* soa, uint32_t max_cells, u
             const double* net_export, const uint8_t* active,
             int n_diffusion_steps, double* mech_accum)
 {
+    or_run_motile(sim, density, soa, max_cells, n_cells, secretion, uptake, saturation, net_export, active,
+                  n_diffusion_steps, mech_accum, NULL, 0, NULL, 0);
+}
+
+void or_run_motile(const or_sim* sim, float* density, float* soa, uint32_t max_cells, uint32_t n_cells,
+                   const double* secretion, const double* uptake, const double* saturation,
+                   const double* net_export, const uint8_t* active,
+                   int n_diffusion_steps, double* mech_accum,
+                   or_motility* mot, uint64_t seed, uint64_t* mot_step, int layout)
+{
     const or_grid* g = &sim->grid;
     const or_mech* m = &sim->mech;
     const uint32_t V = m->mech_grid_nx * m->mech_grid_ny * m->mech_grid_nz;
@@ -636,6 +646,10 @@ void or_run(const or_sim* sim, float* density, float* soa, uint32_t max_cells, u
                 or_mech_bin(soa, max_cells, n_cells, m, g->x_min, g->y_min, g->z_min, key);
                 or_mech_sort(key, n_cells, V, order, start);
                 or_mech_forces(soa, max_cells, n_cells, m, key, order, start, NULL, NULL, NULL);
+                if (mot) {
+                    or_motility_update(soa, max_cells, n_cells, density, g, mot, dt_mech, seed, *mot_step, layout);
+                    ++*mot_step;
+                }
                 or_mech_integrate(soa, max_cells, n_cells, m, g->x_min, g->y_min, g->z_min,
                                   (float)dt_mech);
                 if (sim->refresh_voxels) or_voxel_refresh(soa, max_cells, n_cells, g);

@@ -213,6 +213,15 @@ void or_run(const or_sim* sim, float* density, float* soa, uint32_t max_cells, u
             const double* net_export, const uint8_t* active,
             int n_diffusion_steps, double* mech_accum);
 
+/* or_run with the motility phase of main.mm:379-387: forces -> motility
+ * update (dt = dt_mechanics, draw step *mot_step, then *mot_step + 1) ->
+ * integrate.  mot = NULL is or_run. */
+void or_run_motile(const or_sim* sim, float* density, float* soa, uint32_t max_cells, uint32_t n_cells,
+                   const double* secretion, const double* uptake, const double* saturation,
+                   const double* net_export, const uint8_t* active,
+                   int n_diffusion_steps, double* mech_accum,
+                   or_motility* mot, uint64_t seed, uint64_t* mot_step, int layout);
+
 #ifdef __cplusplus
 }
 #endif

@@ -227,15 +227,24 @@ def nbr_hash(j):
 
 
 def run(grid, subs, mech, dt_mech, density, soa, max_cells, n, sec, upt, sat, ne, active, steps,
-        accum=0.0, refresh=False):
+        accum=0.0, refresh=False, motility=None, seed=0, mot_step=0, layout=0):
+    """The main loop (or_run).  With a motility state (motility_state), the
+    motility phase runs between forces and integrate and the state is
+    updated in place; returns (accumulator, next motility step) then."""
     sim = Sim(grid, C.cast(subs, C.POINTER(Substrate)), mech, dt_mech, 1 if refresh else 0)
     acc = C.c_double(accum)
     sec, upt, sat, ne = (np.ascontiguousarray(a, np.float64) for a in (sec, upt, sat, ne))
     act = None if active is None else np.ascontiguousarray(active, np.uint8)
-    oracle().or_run(C.byref(sim), _p(density, _F32), _p(soa, _F32), _U32(max_cells), _U32(n),
-                    _p(sec, _F64), _p(upt, _F64), _p(sat, _F64), _p(ne, _F64),
-                    None if act is None else _p(act, _U8), C.c_int(steps), C.byref(acc))
-    return acc.value
+    args = (C.byref(sim), _p(density, _F32), _p(soa, _F32), _U32(max_cells), _U32(n),
+            _p(sec, _F64), _p(upt, _F64), _p(sat, _F64), _p(ne, _F64),
+            None if act is None else _p(act, _U8), C.c_int(steps), C.byref(acc))
+    if motility is None:
+        oracle().or_run(*args)
+        return acc.value
+    m = _mot_struct(motility)
+    ms = C.c_uint64(mot_step)
+    oracle().or_run_motile(*args, C.byref(m), C.c_uint64(seed), C.byref(ms), C.c_int(layout))
+    return acc.value, ms.value
 
 
 # ---------------------------------------------------------------- FP32 port

@@ -1,6 +1,7 @@
 // pcg_host.cpp — non-template members of the host drop-ins (see pcg_host.h).
 #include "pcg_host.h"
 
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -32,7 +33,14 @@ Context::Context(int device)
     if (st != PCG_OK) throw Error(st, std::string("pcg_create: ") + pcg_last_error_string(nullptr));
 }
 
-Context::~Context() { pcg_destroy(ctx_); }
+void release_stores(const Context* ctx);
+
+Context::~Context()
+{
+    while (!motility_.empty()) motility_.back()->release();   // release() unregisters
+    release_stores(this);
+    pcg_destroy(ctx_);
+}
 
 void Context::waitForCompletion() { check(pcg_sync(ctx_)); }
 
@@ -56,6 +64,19 @@ pcg_cells* device_store(Context* ctx, const void* host_block, uint32_t max_cells
     ctx->check(pcg_cells_create(ctx->get(), max_cells, n_substrates, &c));
     g_stores[key] = c;
     return c;
+}
+
+void release_stores(const Context* ctx)
+{
+    std::lock_guard<std::mutex> lk(g_store_mu);
+    for (auto it = g_stores.begin(); it != g_stores.end();) {
+        if (it->first.first == ctx) {
+            pcg_cells_destroy(it->second);
+            it = g_stores.erase(it);
+        } else {
+            ++it;
+        }
+    }
 }
 
 // ------------------------------------------------------------------ Microenvironment
@@ -185,5 +206,109 @@ const uint32_t* CellMechanics::voxelCells(uint32_t v) const
     if (start_.empty() || v >= total_) return nullptr;
     return sorted_.data() + start_[v];
 }
+
+// ------------------------------------------------------------------ MotilityData
+
+MotilityData::~MotilityData() { release(); }
+
+void MotilityData::release()
+{
+    if (!dev_) return;
+    pcg_motility_destroy(dev_);
+    auto& reg = dev_ctx_->motility_;
+    reg.erase(std::remove(reg.begin(), reg.end(), this), reg.end());
+    dev_ = nullptr;
+    dev_ctx_ = nullptr;
+}
+
+void MotilityData::allocate(uint32_t max_c)
+{
+    release();
+    max_cells = max_c;
+    num_cells = 0;
+    n_substrates = 0;
+    for (auto* v : {&persistence_time, &motility_elapsed, &motility_bias, &motility_vec_x, &motility_vec_y,
+                    &motility_vec_z})
+        v->assign(max_c, 0.0);
+    is_motile.assign(max_c, 0);
+    restrict_to_2D.assign(max_c, 0);
+    chemotaxis_index.assign(max_c, 0);
+    chemotaxis_direction.assign(max_c, 0);
+    chemotactic_sensitivity.clear();
+}
+
+void MotilityData::allocateSubstrate(uint32_t nsubs)
+{
+    release();
+    n_substrates = nsubs;
+    chemotactic_sensitivity.assign(static_cast<size_t>(max_cells) * nsubs, 0.0);
+}
+
+void MotilityData::free_all()
+{
+    release();
+    for (auto* v : {&persistence_time, &motility_elapsed, &motility_bias, &motility_vec_x, &motility_vec_y,
+                    &motility_vec_z, &chemotactic_sensitivity})
+        v->clear();
+    is_motile.clear();
+    restrict_to_2D.clear();
+    chemotaxis_index.clear();
+    chemotaxis_direction.clear();
+    n_substrates = 0;
+}
+
+void MotilityData::setDefaults(uint32_t i)
+{
+    if (i >= max_cells) throw Error(PCG_ERR_INVALID, "MotilityData::setDefaults: index out of range");
+    // PhysiCell's defaults: 15 min persistence, bias 0.5, not motile, 2-D,
+    // chemotaxis up the first substrate, no per-substrate sensitivity
+    persistence_time[i] = 15.0;
+    motility_elapsed[i] = 0.0;
+    motility_bias[i] = 0.5;
+    motility_vec_x[i] = motility_vec_y[i] = motility_vec_z[i] = 0.0;
+    is_motile[i] = 0;
+    restrict_to_2D[i] = 1;
+    chemotaxis_index[i] = 0;
+    chemotaxis_direction[i] = 1;
+    if (n_substrates)
+        std::fill_n(chemotactic_sensitivity.begin() + static_cast<size_t>(i) * n_substrates, n_substrates, 0.0);
+}
+
+void MotilityData::swapRemove(uint32_t i, uint32_t last)
+{
+    if (i == last) return;
+    for (auto* v : {&persistence_time, &motility_elapsed, &motility_bias, &motility_vec_x, &motility_vec_y,
+                    &motility_vec_z})
+        (*v)[i] = (*v)[last];
+    is_motile[i] = is_motile[last];
+    restrict_to_2D[i] = restrict_to_2D[last];
+    chemotaxis_index[i] = chemotaxis_index[last];
+    chemotaxis_direction[i] = chemotaxis_direction[last];
+    if (n_substrates)
+        std::copy_n(chemotactic_sensitivity.begin() + static_cast<size_t>(last) * n_substrates, n_substrates,
+                    chemotactic_sensitivity.begin() + static_cast<size_t>(i) * n_substrates);
+}
+
+pcg_motility* MotilityData::device(Context* ctx)
+{
+    if (dev_ && dev_ctx_ != ctx) release();
+    if (!dev_) {
+        ctx->check(pcg_motility_create(ctx->get(), max_cells, n_substrates, &dev_));
+        dev_ctx_ = ctx;
+        ctx->motility_.push_back(this);
+    }
+    return dev_;
+}
+
+// ------------------------------------------------------------------ SnapshotWriter
+
+SnapshotWriter::SnapshotWriter(Context* ctx) : ctx_(ctx)
+{
+    ctx_->check(pcg_snapshot_create(ctx_->get(), &snap_));
+}
+
+SnapshotWriter::~SnapshotWriter() { pcg_snapshot_destroy(snap_); }
+
+void SnapshotWriter::wait() { ctx_->check(pcg_snapshot_wait(snap_)); }
 
 }  // namespace pcg

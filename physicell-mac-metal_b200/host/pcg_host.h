@@ -1,6 +1,8 @@
 // pcg_host.h — C++ drop-ins for the reference's Microenvironment and
 // CellMechanics classes (src/microenvironment.h:17-83,
-// src/cell_mechanics.h:15-87), implemented over the C ABI of include/pcg.h.
+// src/cell_mechanics.h:15-87), for MotilityData / updateMotility
+// (src/motility.h:20-81) and for writeMatlabSnapshots
+// (src/output_writer.h:51-53), implemented over the C ABI of include/pcg.h.
 //
 // The public methods keep the reference's names, arguments and meaning.
 // The configuration and cell store are template parameters so that the
@@ -50,6 +52,7 @@ struct CellStore {
     uint32_t num_cells = 0;
     uint32_t max_cells = 0;
     uint32_t n_substrates = 0;
+    uint32_t num_cell_types = 1;
     std::vector<float> block;        // [field * max_cells + cell]
     float* position_x = nullptr;     // == block.data(), as in CellData
     std::vector<double> secretion_rate, uptake_rate, saturation_density, net_export_rate;
@@ -64,7 +67,11 @@ public:
     int status;
 };
 
-// Replaces MetalContext (src/metal_context.h:14-100).
+struct MotilityData;
+
+// Replaces MetalContext (src/metal_context.h:14-100).  Device state made
+// for host-side objects that may outlive it (MotilityData's device copy, the
+// device cell stores) is released when the Context goes.
 class Context {
 public:
     explicit Context(int device = 0);
@@ -75,7 +82,9 @@ public:
     void waitForCompletion();
     void check(int status) const;
 private:
+    friend struct MotilityData;
     pcg_ctx* ctx_ = nullptr;
+    std::vector<MotilityData*> motility_;
 };
 
 class Microenvironment {
@@ -107,6 +116,7 @@ public:
     uint32_t numVoxels() const { return grid_.nx * grid_.ny * grid_.nz; }
     uint32_t voxelIndex(float x, float y, float z) const;   // microenvironment.mm:261-269
     pcg_grid_params getGridParams() const { return grid_; }
+    Context* context() const { return ctx_; }
 
     void computeGradients();
     void getGradient(uint32_t voxel_index, uint32_t substrate_index, float& gx, float& gy, float& gz) const;
@@ -171,6 +181,80 @@ private:
     float ox_ = 0, oy_ = 0, oz_ = 0;
     uint32_t total_ = 0, max_cells_ = 0, n_substrates_ = 0;
     std::vector<uint32_t> start_, sorted_;
+};
+
+// MotilityData (src/motility.h:20-66): the same members, indexed as the
+// reference indexes its arrays, held in host vectors.  updateMotility keeps
+// a device copy in step with them.
+struct MotilityData {
+    uint32_t max_cells = 0;
+    uint32_t num_cells = 0;
+    std::vector<double> persistence_time, motility_elapsed, motility_bias;
+    std::vector<double> motility_vec_x, motility_vec_y, motility_vec_z;
+    std::vector<uint32_t> is_motile, restrict_to_2D;
+    std::vector<int32_t> chemotaxis_index, chemotaxis_direction;
+    std::vector<double> chemotactic_sensitivity;   // [cell * n_substrates + s]
+    uint32_t n_substrates = 0;
+    // The reference draws from an unseeded generator.  Here draw k of cell i
+    // in update number `step` is a counter-based uniform of (seed, i, step, k);
+    // updateMotility advances step by one per call.
+    uint64_t seed = 0;
+    uint64_t step = 0;
+
+    MotilityData() = default;
+    ~MotilityData();
+    MotilityData(const MotilityData&) = delete;
+    MotilityData& operator=(const MotilityData&) = delete;
+
+    void allocate(uint32_t max_cells);               // motility.cpp:91-107
+    void allocateSubstrate(uint32_t n_substrates);   // motility.cpp:109-116
+    void free_all();                                 // motility.cpp:118-131
+    void setDefaults(uint32_t index);                // motility.cpp:133-152
+    void swapRemove(uint32_t index, uint32_t last);  // motility.cpp:154-175
+
+    // the device state for this context, made on first use and again after
+    // allocate / allocateSubstrate change the sizes
+    pcg_motility* device(Context* ctx);
+private:
+    friend class Context;
+    void release();
+    pcg_motility* dev_ = nullptr;
+    Context* dev_ctx_ = nullptr;
+};
+
+// updateMotility(cells, mot, density, grid, dt) (motility.cpp:179-293): the
+// density and grid are the Microenvironment's, read on the device.  Adds the
+// motility vector of each living motile cell to its velocity and writes back
+// motility_elapsed and motility_vec_*.  layout PCG_MOT_REFERENCE reads the
+// gradient as the reference does (see include/pcg.h).
+template <class Cells>
+void updateMotility(Cells& cells, MotilityData& mot, Microenvironment& micro, double dt,
+                    int layout = PCG_MOT_REFERENCE);
+
+// writeMatlabSnapshots(cells, density, grid, frame, folder)
+// (output_writer.cpp:295-452): output%08d_cells.mat and
+// output%08d_microenvironment0.mat in output_folder, written before the call
+// returns, byte-identical to the reference writer's files.
+template <class Cells>
+void writeMatlabSnapshots(const Cells& cells, Microenvironment& micro, int frame_index,
+                          const std::string& output_folder);
+
+// The asynchronous form: frame() builds the matrices on the device behind the
+// work already queued and returns; a host thread writes the files while the
+// simulation goes on.  wait() blocks until every queued file is written and
+// throws for one that could not be.
+class SnapshotWriter {
+public:
+    explicit SnapshotWriter(Context* ctx);
+    ~SnapshotWriter();
+    SnapshotWriter(const SnapshotWriter&) = delete;
+    SnapshotWriter& operator=(const SnapshotWriter&) = delete;
+    template <class Cells>
+    void frame(const Cells& cells, Microenvironment& micro, int frame_index, const std::string& output_folder);
+    void wait();
+private:
+    Context* ctx_ = nullptr;
+    pcg_snapshot* snap_ = nullptr;
 };
 
 }  // namespace pcg

@@ -46,19 +46,29 @@ void Microenvironment::initialize(const Config& config, Context* ctx)
     mirror_valid_ = mirror_dirty_ = false;
 }
 
+// The CPU owns the cell block: refresh the device copy of the 28 fields and,
+// with rates, of the per-substrate secretion rates and the live mask.
+template <class Cells>
+pcg_cells* sync_cells(Context* ctx, const Cells& cells, uint32_t n_substrates, bool rates)
+{
+    pcg_cells* dc = device_store(ctx, block_of(cells), cells.max_cells, n_substrates);
+    ctx->check(pcg_cells_upload(dc, block_of(cells), cells.num_cells, cells.max_cells));
+    if (rates) {
+        std::vector<uint8_t> active(cells.num_cells, 1);
+        for (uint32_t i = 0; i < cells.num_cells && i < cells.current_death_model.size(); ++i)
+            active[i] = cells.current_death_model[i] == 0 ? 1 : 0;   // main.mm:360
+        ctx->check(pcg_cells_set_secretion(dc, cells.secretion_rate.data(), cells.uptake_rate.data(),
+                                           cells.saturation_density.data(), cells.net_export_rate.data(),
+                                           active.data()));
+    }
+    return dc;
+}
+
 template <class Cells>
 void Microenvironment::secreteAll(Cells& cells, double dt)
 {
     push_host_writes();
-    pcg_cells* dc = device_store(ctx_, block_of(cells), cells.max_cells, grid_.n_substrates);
-    // the CPU owns the cell block: refresh the device copy and the rates
-    ctx_->check(pcg_cells_upload(dc, block_of(cells), cells.num_cells, cells.max_cells));
-    std::vector<uint8_t> active(cells.num_cells, 1);
-    for (uint32_t i = 0; i < cells.num_cells && i < cells.current_death_model.size(); ++i)
-        active[i] = cells.current_death_model[i] == 0 ? 1 : 0;   // main.mm:360
-    ctx_->check(pcg_cells_set_secretion(dc, cells.secretion_rate.data(), cells.uptake_rate.data(),
-                                        cells.saturation_density.data(), cells.net_export_rate.data(),
-                                        active.data()));
+    pcg_cells* dc = sync_cells(ctx_, cells, grid_.n_substrates, true);
     ctx_->check(pcg_me_secrete(me_, dc, dt));
     mirror_valid_ = false;
 }
@@ -133,6 +143,57 @@ void CellMechanics::update(Cells& cells, float dt)
     push(cells);
     ctx_->check(pcg_mech_update(mech_, cells_, dt));
     pull(cells);
+}
+
+template <class Cells>
+void updateMotility(Cells& cells, MotilityData& mot, Microenvironment& micro, double dt, int layout)
+{
+    const uint32_t n = cells.num_cells;
+    if (n == 0) return;
+    if (n > mot.max_cells) throw Error(PCG_ERR_INVALID, "updateMotility: more cells than MotilityData::allocate'd");
+    Context* ctx = micro.context();
+    micro.push_host_writes();
+    mot.num_cells = n;
+    pcg_motility* dm = mot.device(ctx);
+    std::vector<double> vec(3 * static_cast<size_t>(n));
+    std::copy_n(mot.motility_vec_x.begin(), n, vec.begin());
+    std::copy_n(mot.motility_vec_y.begin(), n, vec.begin() + n);
+    std::copy_n(mot.motility_vec_z.begin(), n, vec.begin() + 2 * static_cast<size_t>(n));
+    ctx->check(pcg_motility_upload(dm, n, mot.persistence_time.data(), mot.motility_elapsed.data(),
+                                   mot.motility_bias.data(), vec.data(), mot.is_motile.data(),
+                                   mot.restrict_to_2D.data(), mot.chemotaxis_index.data(),
+                                   mot.chemotaxis_direction.data(),
+                                   mot.n_substrates ? mot.chemotactic_sensitivity.data() : nullptr));
+    pcg_cells* dc = sync_cells(ctx, cells, micro.getGridParams().n_substrates, false);
+    ctx->check(pcg_motility_update(dm, dc, micro.handle(), dt, mot.seed, mot.step, layout));
+    ++mot.step;
+    ctx->check(pcg_motility_download(dm, mot.motility_elapsed.data(), vec.data()));
+    std::copy_n(vec.begin(), n, mot.motility_vec_x.begin());
+    std::copy_n(vec.begin() + n, n, mot.motility_vec_y.begin());
+    std::copy_n(vec.begin() + 2 * static_cast<size_t>(n), n, mot.motility_vec_z.begin());
+    ctx->check(pcg_cells_download(dc, const_cast<float*>(block_of(cells)), cells.max_cells));
+}
+
+template <class Cells>
+uint32_t cell_types_of(const Cells& cells) { return cells.num_cell_types; }
+
+template <class Cells>
+void SnapshotWriter::frame(const Cells& cells, Microenvironment& micro, int frame_index,
+                           const std::string& output_folder)
+{
+    micro.push_host_writes();
+    pcg_cells* dc = sync_cells(ctx_, cells, micro.getGridParams().n_substrates, true);
+    ctx_->check(pcg_snapshot_frame(snap_, micro.handle(), dc, cell_types_of(cells), output_folder.c_str(),
+                                   frame_index));
+}
+
+template <class Cells>
+void writeMatlabSnapshots(const Cells& cells, Microenvironment& micro, int frame_index,
+                          const std::string& output_folder)
+{
+    SnapshotWriter w(micro.context());
+    w.frame(cells, micro, frame_index, output_folder);
+    w.wait();
 }
 
 }  // namespace pcg

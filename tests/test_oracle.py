@@ -348,6 +348,38 @@ def test_motility_live_reference_when_present(po):
         assert np.array_equal(a, b) and np.array_equal(sa["vec"], st["vec"])
 
 
+def test_main_loop_motility_phase(po, pcg):
+    """or_run_motile: no motile cell leaves the loop as or_run has it; with
+    motile cells, the phase runs once per mechanics step, between forces and
+    integrate (main.mm:379-387)."""
+    from pcg import workloads
+    inst = workloads.plain_2d(seed=5, n_cells=120)
+    n = inst.n_cells
+    g = inst.grid
+    og = po.make_grid(g.nx, g.ny, g.nz, 1, dx=g.dx, dt=g.dt, x_min=g.x_min, y_min=g.y_min, z_min=g.z_min)
+    om = po.mech_params(-500, 500, -500, 500, -10, 10, True, 0.1)
+    subs = po.make_subs([(1e5, 0.1, True, 38.0)])
+    soa = inst.soa.astype(np.float32).copy()
+    soa[16 * n:17 * n] = 1.0                    # motility speed
+    soa.view(np.uint32)[25 * n:26 * n] = 1      # is_alive
+    runs = []
+    for motile in (False, None, True):
+        d, s = np.full(2500, 38.0, np.float32), soa.copy()
+        st = po.motility_state(n)
+        st["is_motile"][:] = bool(motile)
+        if motile is None:
+            po.run(og, subs, om, 0.1, d, s, n, n, *inst.rates, None, 25)
+        else:
+            _, nxt = po.run(og, subs, om, 0.1, d, s, n, n, *inst.rates, None, 25, motility=st, seed=3)
+            assert nxt == 2
+        runs.append((d, s, st))
+    assert np.array_equal(runs[0][0], runs[1][0]) and np.array_equal(runs[0][1], runs[1][1])
+    moved = runs[2][1][:2 * n] - runs[1][1][:2 * n]
+    el = runs[2][2]["elapsed"]    # float dt_mechanics; 0 or 0.1 where an update resampled
+    assert np.abs(moved).max() > 0 and np.all((np.abs(el - 0.2) < 1e-6) | (np.abs(el - 0.1) < 1e-6) | (el == 0))
+    assert np.sum(np.abs(el - 0.2) < 1e-6) > n // 2
+
+
 # ---------------------------------------------------------------- .mat snapshots
 
 @pytest.mark.parametrize("name", ["matlab_2d", "matlab_3d"])
