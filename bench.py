@@ -361,6 +361,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tune-cache", default=None, help="JSON file of autotuned launch shapes (read and updated)")
+    ap.add_argument("--pin-x", type=int, default=0,
+                    help="x-sweep launch shape warps*16 + stages instead of the tuned one")
+    ap.add_argument("--pin-cols", type=int, default=0, help="the same for the y and z sweeps")
     ap.add_argument("--serve-horizon", type=float, default=10.0,
                     help="seconds of request arrivals for the serving leg (0 = skip)")
     args = ap.parse_args()
@@ -378,7 +381,7 @@ def main():
     ctx = pcg.Context(local)
     shard = rank_shard(args.instances, rank, world)
     insts = workloads.batched_3d(n_instances=args.instances * world, seed=1237, only=shard)
-    batch = pcg.Batch(ctx, insts, tune_cache=args.tune_cache)
+    batch = pcg.Batch(ctx, insts, tune_cache=args.tune_cache, pin_x=args.pin_x, pin_cols=args.pin_cols)
     voxels, voxel_subs, cells = batch.totals()
 
     def period():

@@ -308,6 +308,8 @@ typedef struct {
     int autotune;          /* pick tile shapes / block sizes by measurement (default 1) */
     const char* tune_cache;/* JSON cache path for autotuned choices, or NULL */
     int profile_phases;    /* record CUDA events around phases (default 0) */
+    int pin_x;             /* launch shape of the x sweeps instead of the tuned one: */
+    int pin_cols;          /* warps * 16 + stages (y and z sweeps: pin_cols); 0 = tuned */
 } pcg_batch_options;
 
 pcg_status pcg_batch_create(pcg_ctx* ctx, const pcg_instance_desc* instances, uint32_t n_instances,

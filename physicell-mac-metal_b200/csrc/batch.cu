@@ -157,6 +157,10 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
         PCG_TRY(d.tune());
         if (!tune_cache.empty()) Tuner::get().save(tune_cache);
     }
+    if (opt) {
+        PCG_TRY(d.pin(0, opt->pin_x));
+        PCG_TRY(d.pin(1, opt->pin_cols));
+    }
     for (int q = 0; q < 8; ++q) PCG_CU(ctx, cudaEventCreate(&ev[q]));
     if (masked) {
         PCG_CU(ctx, mask_d.alloc(n));

@@ -582,6 +582,17 @@ int Diffusion::config_list(SweepList& l, int param)
     return PCG_OK;
 }
 
+int Diffusion::pin(int kind, int param)
+{
+    if (!param) return PCG_OK;
+    if ((param & 15) < 2 || (param & 15) > 4 || (param >> 4) < 1 || (param >> 4) > 8)
+        return fail(ctx, PCG_ERR_INVALID, "bad pinned launch shape");
+    for (int a = 0; a < 3; ++a)
+        for (auto& l : lists[a])
+            if (l.kind == kind && l.n) PCG_TRY(config_list(l, param));
+    return PCG_OK;
+}
+
 int Diffusion::default_configs(int axis)
 {
     for (auto& l : lists[axis]) PCG_TRY(config_list(l, 0));

@@ -163,6 +163,7 @@ public:
     // initialised first when tuning, see tune()).
     int build(pcg_ctx* c, std::vector<DiffInstance> instances);
     int tune();                                    // restore-safe: density is saved and put back
+    int pin(int kind, int param);                  // one shape for every TMA list of a kind (0 x, 1 columns)
     int sweep(int axis, bool fuse_faces, const uint8_t* mask);
     int sweeps(bool fuse_faces, const uint8_t* mask);
     int dirichlet();

@@ -61,6 +61,23 @@ def test_graphs_equal_direct_launches(ctx, pcg):
         assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32))
 
 
+@pytest.mark.parametrize("pins", [(18, 18), (50, 35), (36, 52), (34, 66)])
+def test_pinned_launch_shapes_give_identical_results(ctx, pcg, pins):
+    """Warps per CTA and pipeline stages change only the schedule: every
+    shape gives the same bits."""
+    insts = small_mix(pcg, seed=9)[:4]
+    ref = run_batch(pcg, ctx, insts, 13, autotune=False)
+    got = run_batch(pcg, ctx, insts, 13, autotune=False, pin_x=pins[0], pin_cols=pins[1])
+    for (da, ca), (db, cb) in zip(ref, got):
+        assert np.array_equal(da.view(np.uint32), db.view(np.uint32))
+        assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32))
+
+
+def test_bad_pinned_shape_is_refused(ctx, pcg):
+    with pytest.raises(pcg.PcgError):
+        pcg.Batch(ctx, small_mix(pcg, seed=9)[:1], autotune=False, pin_x=17 * 16 + 2)
+
+
 def test_batch_instance_matches_oracle(ctx, pcg, po):
     insts = small_mix(pcg, seed=7)
     steps = 31
