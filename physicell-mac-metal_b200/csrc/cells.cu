@@ -1,5 +1,5 @@
 // cells.cu — per-cell kernels (sm_100a): secretion/uptake, spatial binning,
-// sorted-SoA gather, neighbour forces and the Adams-Bashforth update.
+// sorted SoA, neighbour forces and the Adams-Bashforth update.
 //
 // Reference semantics:
 //   secretion  src/cell_phenotype.cpp:526-564 (processSecretion), FP64 per
@@ -93,10 +93,13 @@ __global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, ui
                               const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder,
                               const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
                               const uint32_t* __restrict__ sbeg, uint32_t invalid_key,
-                              const double* __restrict__ rates4, uint32_t n_rate, double dt, double* __restrict__ cs)
+                              const double* __restrict__ rates4, uint32_t n_rate, double dt, double* __restrict__ cs,
+                              uint32_t* __restrict__ flags)
 {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n || skeys[q] >= invalid_key) return;
+    const bool live = q < n && skeys[q] < invalid_key;
+    const unsigned live_lanes = __ballot_sync(0xFFFFFFFFu, live);   // blocks are whole warps
+    if (!live) return;
     const uint32_t g = sorder[q];
     const uint32_t ii = cell_inst[g];
     const CellInst& in = insts[ii];
@@ -106,26 +109,49 @@ __global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, ui
     const double ic = __ddiv_rn(__dmul_rn(dt, V_cell), V_vox);
     const uint32_t src = in.rate_off + (g - in.cell_off) * in.S;
     const uint32_t dst = in.rate_off + (q - sbeg[ii]) * in.S;
+    uint32_t f = 0;
     for (uint32_t s = 0; s < in.S; ++s) {
         const uint32_t o = src + s;
         const double sec = rates4[o], upt = rates4[n_rate + o], sat = rates4[2ull * n_rate + o],
                      ne = rates4[3ull * n_rate + o];
-        double* c = cs + 3ull * (dst + s);
-        c[0] = __ddiv_rn(__dmul_rn(dt, ne), V_vox);
-        c[1] = __dmul_rn(__dmul_rn(ic, sec), sat);
-        c[2] = __dadd_rn(1.0, __dmul_rn(ic, __dadd_rn(sec, upt)));
+        const double c0 = __ddiv_rn(__dmul_rn(dt, ne), V_vox);
+        const double c1 = __dmul_rn(__dmul_rn(ic, sec), sat);
+        cs[dst + s] = c0;
+        cs[n_rate + dst + s] = c1;
+        cs[2ull * n_rate + dst + s] = __dadd_rn(1.0, __dmul_rn(ic, __dadd_rn(sec, upt)));
+        f |= (__double_as_longlong(c0) != 0 ? 1u : 0u) | (__double_as_longlong(c1) != 0 ? 2u : 0u);
     }
+    // per instance: does any cell have an export (bit 0) or a secretion
+    // (bit 1) term other than +0?  Cells of a warp mostly share the instance.
+    const unsigned grp = __match_any_sync(live_lanes, ii);
+    f = __reduce_or_sync(grp, f);
+    if (f && (threadIdx.x & 31) == static_cast<unsigned>(__ffs(grp) - 1)) atomicOr(&flags[ii], f);
+}
+
+// One cell's processSecretion on one substrate (cell_phenotype.cpp:526-564):
+// rho += c0; rho = (rho + c1) / c2; clamp at 0; FP32 store.  A term the
+// instance never has (flags) is exactly +0 and is added as the constant.
+__device__ __forceinline__ float secrete_cell(float rho32, const double* __restrict__ cs, uint64_t o, uint64_t cap,
+                                              uint32_t f)
+{
+    double rho = static_cast<double>(rho32);
+    rho = __dadd_rn(rho, (f & 1u) ? cs[o] : 0.0);
+    rho = __dadd_rn(rho, (f & 2u) ? cs[cap + o] : 0.0);
+    rho = __ddiv_rn(rho, cs[2 * cap + o]);
+    if (rho < 0.0) rho = 0.0;
+    return __double2float_rn(rho);
 }
 
 // One thread per run: applies the run's cells to its voxel in ascending
-// cell index (the stable order), substrate by substrate, FP64 per cell with
-// the FP32 store after each cell.  The run's metadata is read once and each
-// cell's constants for all substrates are contiguous.
-__global__ void __launch_bounds__(256, 8) k_secrete(float* __restrict__ dens, const uint32_t* __restrict__ skeys,
+// cell index (the stable order), FP64 per cell with the FP32 store after
+// each cell.  The run's metadata is read once; with one or two substrates
+// both are held in registers and advanced together.  Constants: three
+// arrays of cap (c0, c1, c2), entry (cell in sorted order, substrate).
+__global__ void __launch_bounds__(256, 6) k_secrete(float* __restrict__ dens, const uint32_t* __restrict__ skeys,
                           const uint32_t* __restrict__ run_start, const uint32_t* __restrict__ run_inst,
                           const uint32_t* __restrict__ n_runs, const CellInst* __restrict__ insts,
-                          const uint32_t* __restrict__ sbeg, const double* __restrict__ cs,
-                          const uint8_t* __restrict__ mask)
+                          const uint32_t* __restrict__ sbeg, const double* __restrict__ cs, uint64_t cap,
+                          const uint32_t* __restrict__ flags, const uint8_t* __restrict__ mask)
 {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= *n_runs) return;
@@ -137,17 +163,23 @@ __global__ void __launch_bounds__(256, 8) k_secrete(float* __restrict__ dens, co
     const uint32_t v = skeys[p0] - in.vox_base;
     // dense voxel index -> padded-row device offset
     float* d = dens + in.dens_off + static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
-    const double* c0 = cs + 3ull * (in.rate_off + static_cast<uint64_t>(p0 - sbeg[ii]) * S);
+    const uint64_t base = in.rate_off + static_cast<uint64_t>(p0 - sbeg[ii]) * S;
+    const uint32_t f = flags[ii];
+    if (S <= 2) {
+        float r0 = d[0], r1 = S > 1 ? d[in.sub_pitch] : 0.f;
+        for (uint32_t q = p0; q < p1; ++q) {
+            const uint64_t o = base + static_cast<uint64_t>(q - p0) * S;
+            r0 = secrete_cell(r0, cs, o, cap, f);
+            if (S > 1) r1 = secrete_cell(r1, cs, o + 1, cap, f);
+        }
+        d[0] = r0;
+        if (S > 1) d[in.sub_pitch] = r1;
+        return;
+    }
     for (uint32_t s = 0; s < S; ++s, d += in.sub_pitch) {
         float rho32 = *d;
-        const double* c = c0 + 3ull * s;
-        for (uint32_t q = p0; q < p1; ++q, c += 3ull * S) {
-            double rho = static_cast<double>(rho32);
-            rho = __dadd_rn(rho, c[0]);
-            rho = __ddiv_rn(__dadd_rn(rho, c[1]), c[2]);
-            if (rho < 0.0) rho = 0.0;
-            rho32 = __double2float_rn(rho);
-        }
+        for (uint32_t q = p0; q < p1; ++q)
+            rho32 = secrete_cell(rho32, cs, base + static_cast<uint64_t>(q - p0) * S + s, cap, f);
         *d = rho32;
     }
 }
@@ -180,12 +212,20 @@ __global__ void k_mech_bin(float* __restrict__ soa, uint32_t stride, uint32_t n,
     atomicAdd(&counts[key], 1u);
 }
 
-__global__ void k_mech_gather(const float* __restrict__ soa, uint32_t stride, const uint32_t* __restrict__ sorder,
-                              uint32_t n, float4* __restrict__ spos, float4* __restrict__ sprm)
+// Sorted SoA: rank[g] = place of cell g in the sorted order, then each cell
+// reads its own fields (coalesced) and writes them to its place.
+__global__ void k_mech_rank(const uint32_t* __restrict__ sorder, uint32_t n, uint32_t* __restrict__ rank)
 {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    const uint32_t g = sorder[p];
+    if (p < n) rank[sorder[p]] = p;
+}
+
+__global__ void k_mech_sorted_soa(const float* __restrict__ soa, uint32_t stride, const uint32_t* __restrict__ rank,
+                                  uint32_t n, float4* __restrict__ spos, float4* __restrict__ sprm)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t p = rank[g];
     spos[p] = make_float4(soa[static_cast<size_t>(F_POS_X) * stride + g], soa[static_cast<size_t>(F_POS_Y) * stride + g],
                           soa[static_cast<size_t>(F_POS_Z) * stride + g], soa[static_cast<size_t>(F_RADIUS) * stride + g]);
     // square roots of the (non-negative) strengths: the pair factors
@@ -390,21 +430,24 @@ cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, const uint32
 cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n, const uint32_t* skeys,
                                const uint32_t* sorder, const uint32_t* cell_inst, const CellInst* insts,
                                const uint32_t* sbeg, uint32_t invalid_key, const double* rates4, uint32_t n_rate,
-                               double dt, double* cs)
+                               double dt, double* cs, uint32_t* flags, uint32_t n_inst)
 {
     if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(flags, 0, static_cast<size_t>(n_inst) * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
     k_sec_prepare<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, skeys, sorder, cell_inst, insts, sbeg,
-                                                       invalid_key, rates4, n_rate, dt, cs);
+                                                       invalid_key, rates4, n_rate, dt, cs, flags);
     return cudaGetLastError();
 }
 
 cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, const uint32_t* run_start,
                            const uint32_t* run_inst, const uint32_t* n_runs, uint32_t max_runs, uint32_t max_s,
-                           const CellInst* insts, const uint32_t* sbeg, const double* cs, const uint8_t* mask)
+                           const CellInst* insts, const uint32_t* sbeg, const double* cs, uint32_t cap,
+                           const uint32_t* flags, const uint8_t* mask)
 {
     if (max_runs == 0 || max_s == 0) return cudaSuccess;
     k_secrete<<<blocks_for(max_runs, 256), 256, 0, st>>>(dens, skeys, run_start, run_inst, n_runs, insts, sbeg, cs,
-                                                          mask);
+                                                          cap, flags, mask);
     return cudaGetLastError();
 }
 
@@ -417,11 +460,14 @@ cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32
     return cudaGetLastError();
 }
 
-cudaError_t launch_mech_gather(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* sorder, uint32_t n,
-                               float4* spos, float4* sprm)
+cudaError_t launch_mech_sorted_soa(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* sorder,
+                                   uint32_t n, uint32_t* rank, float4* spos, float4* sprm)
 {
     if (n == 0) return cudaSuccess;
-    k_mech_gather<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, sorder, n, spos, sprm);
+    k_mech_rank<<<blocks_for(n, 256), 256, 0, st>>>(sorder, n, rank);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_mech_sorted_soa<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, rank, n, spos, sprm);
     return cudaGetLastError();
 }
 

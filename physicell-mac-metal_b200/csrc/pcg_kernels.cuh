@@ -180,18 +180,22 @@ cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, const uint32
 cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n, const uint32_t* skeys,
                                const uint32_t* sorder, const uint32_t* cell_inst, const CellInst* insts,
                                const uint32_t* sbeg, uint32_t invalid_key, const double* rates4, uint32_t n_rate,
-                               double dt, double* cs);
+                               double dt, double* cs, uint32_t* flags, uint32_t n_inst);
 // n_runs: device count (heads_rid[n]); max_runs >= it; max_s = largest S.
+// cs: constants c0, c1, c2 as three arrays of cap; flags: per instance, bit 0
+// some c0 not +0, bit 1 some c1 not +0 (written by launch_sec_prepare).
 cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, const uint32_t* run_start,
                            const uint32_t* run_inst, const uint32_t* n_runs, uint32_t max_runs, uint32_t max_s,
-                           const CellInst* insts, const uint32_t* sbeg, const double* cs, const uint8_t* mask);
+                           const CellInst* insts, const uint32_t* sbeg, const double* cs, uint32_t cap,
+                           const uint32_t* flags, const uint8_t* mask);
 
 // Mechanics.
 cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
                             const uint32_t* cell_inst, const CellInst* insts,
                             uint32_t* keys, uint32_t* vals, uint32_t* counts, const uint8_t* mask);
-cudaError_t launch_mech_gather(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* sorder,
-                               uint32_t n, float4* spos, float4* sprm);
+// Positions / radii and strengths in sorted order (rank: n scratch words).
+cudaError_t launch_mech_sorted_soa(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* sorder,
+                                   uint32_t n, uint32_t* rank, float4* spos, float4* sprm);
 cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* skeys,
                                const uint32_t* sorder, const uint32_t* start, uint32_t n,
                                const uint32_t* cell_inst, const CellInst* insts, float* soa, uint32_t stride,

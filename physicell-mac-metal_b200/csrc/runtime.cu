@@ -860,6 +860,8 @@ int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_
     PCG_CU(ctx, rates.alloc(4 * rc * sizeof(double)));
     PCG_CU(ctx, cudaMemsetAsync(rates.p, 0, rates.bytes, ctx->stream));
     PCG_CU(ctx, coef.alloc(3 * rc * sizeof(double)));
+    PCG_CU(ctx, coef_flags.alloc(h_inst.size() * sizeof(uint32_t)));
+    PCG_CU(ctx, cudaMemsetAsync(coef_flags.p, 0xFF, coef_flags.bytes, ctx->stream));   // all terms until prepared
     PCG_CU(ctx, active.alloc(max_cells));
     for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp})
         PCG_CU(ctx, b->alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint32_t)));
@@ -975,7 +977,8 @@ int Cells::sorted_constants()
     cudaError_t e = launch_sec_prepare(ctx->stream, soa.as<float>(), max_cells, n, skeys.as<uint32_t>(),
                                        sorder.as<uint32_t>(), cell_inst.as<uint32_t>(), inst.as<CellInst>(),
                                        sbeg.as<uint32_t>(), invalid_key, rates.as<double>(), cap, coef_dt,
-                                       coef.as<double>());
+                                       coef.as<double>(), coef_flags.as<uint32_t>(),
+                                       static_cast<uint32_t>(h_inst.size()));
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion prepare");
     if (n) ctx->launches++;
     coef_dirty = false;
@@ -998,7 +1001,9 @@ int Cells::secrete(Diffusion& d, const uint8_t* mask)
     for (const CellInst& ci : h_inst) max_s = std::max(max_s, ci.S);
     cudaError_t e = launch_secrete(ctx->stream, d.dens.as<float>(), skeys.as<uint32_t>(), vals.as<uint32_t>(),
                                    vtmp.as<uint32_t>(), ktmp.as<uint32_t>() + n, n, max_s, inst.as<CellInst>(),
-                                   sbeg.as<uint32_t>(), coef.as<double>(), mask);
+                                   sbeg.as<uint32_t>(), coef.as<double>(),
+                                   static_cast<uint32_t>(rates.bytes / (4 * sizeof(double))),
+                                   coef_flags.as<uint32_t>(), mask);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion launch");
     if (n && max_s) ctx->launches++;
     return PCG_OK;
@@ -1006,7 +1011,8 @@ int Cells::secrete(Diffusion& d, const uint8_t* mask)
 
 uint64_t Cells::device_bytes() const
 {
-    return inst.bytes + soa.bytes + cell_inst.bytes + rates.bytes + coef.bytes + active.bytes + keys.bytes + vals.bytes +
+    return inst.bytes + soa.bytes + cell_inst.bytes + rates.bytes + coef.bytes + coef_flags.bytes + active.bytes +
+           keys.bytes + vals.bytes +
            skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + sbeg.bytes + run_scr.bytes;
 }
 
@@ -1033,8 +1039,8 @@ int Mechanics::create(pcg_ctx* c, uint32_t tmv, uint32_t maxc)
 
 int Mechanics::launches_forces(uint32_t n) const
 {
-    return 1 /*memset*/ + 1 /*bin*/ + radix_sort_launches(n, key_bits) + scan_launches(total_mvox + 1ull) + 1 /*gather*/ +
-           1 /*forces*/;
+    return 1 /*memset*/ + 1 /*bin*/ + radix_sort_launches(n, key_bits) + scan_launches(total_mvox + 1ull) +
+           2 /*rank, sorted SoA*/ + 1 /*forces*/;
 }
 
 // computeForces: bin -> stable radix sort -> cell-start table -> sorted SoA -> forces
@@ -1059,9 +1065,9 @@ int Mechanics::binsort(Cells& c, const uint8_t* mask)
     if (e != cudaSuccess) return cuda_fail(ctx, e, "radix sort");
     e = scan_exclusive(st, counts.as<uint32_t>(), start.as<uint32_t>(), static_cast<uint64_t>(total_mvox) + 1, scan_scr.p);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "start-table scan");
-    e = launch_mech_gather(st, c.soa.as<float>(), c.max_cells, sorder.as<uint32_t>(), c.n, spos.as<float4>(),
-                           sprm.as<float4>());
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "gather launch");
+    e = launch_mech_sorted_soa(st, c.soa.as<float>(), c.max_cells, sorder.as<uint32_t>(), c.n, ktmp.as<uint32_t>(),
+                               spos.as<float4>(), sprm.as<float4>());
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sorted SoA launch");
     ctx->launches += launches_forces(c.n) - 2;   // the memset is not a kernel; forces counted below
     return PCG_OK;
 }

@@ -196,14 +196,15 @@ public:
     uint32_t n = 0;
     uint32_t n_rate = 0;          // sum over instances of n_cells * S
     std::vector<CellInst> h_inst;
-    DevBuf inst, soa, cell_inst, rates, coef, active;
+    DevBuf inst, soa, cell_inst, rates, coef, coef_flags, active;
     bool has_active = false;
     bool inst_dirty = true, coef_dirty = true, order_dirty = true;
     double coef_dt = -1.0;
     // secretion ordering: keys/vals sort input, (skeys, sorder) the order;
     // after the sort ktmp holds the run index of every position (+ count),
     // vals the run starts and vtmp the run instances; coef the constants
-    // in sorted order
+    // in sorted order (c0, c1, c2 arrays) and coef_flags which of c0 / c1
+    // each instance has
     DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr, sbeg, run_scr;
     uint32_t invalid_key = 0;
     int key_bits = 0;

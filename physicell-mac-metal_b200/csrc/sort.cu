@@ -9,8 +9,10 @@
 //   k_radix_scatter  each warp ranks its contiguous 256 keys with
 //                    __match_any_sync (peers with the same digit) and a
 //                    per-warp running count, warps are combined in warp
-//                    order, and every key goes to
-//                    offset[digit][tile] + warp prefix + rank.
+//                    order; the tile is laid out in shared memory in digit
+//                    order and written back so that consecutive threads
+//                    store consecutive elements of one digit's run at
+//                    offset[digit][tile] + place in the run.
 // Ranks follow input order within a warp, warps follow tile order and
 // tiles follow the scanned histogram, so each pass is stable.
 #include "pcg_kernels.cuh"
@@ -51,6 +53,9 @@ __global__ void __launch_bounds__(kThreads) k_radix_scatter(const uint32_t* __re
 {
     __shared__ uint32_t wcnt[kWarps][kRadix];
     __shared__ uint32_t gbase[kRadix];
+    __shared__ uint32_t tbase[kRadix];      // first place of each digit in the tile
+    __shared__ uint32_t wtot[kWarps];
+    __shared__ uint32_t sk[kTile], sv[kTile];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&wcnt[0][0])[i] = 0;
     __syncthreads();
@@ -72,7 +77,9 @@ __global__ void __launch_bounds__(kThreads) k_radix_scatter(const uint32_t* __re
         __syncwarp();
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < kRadix; d += kThreads) {
+    static_assert(kThreads == kRadix, "one thread per digit");
+    {
+        const int d = threadIdx.x;
         uint32_t sum = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) {
@@ -81,15 +88,36 @@ __global__ void __launch_bounds__(kThreads) k_radix_scatter(const uint32_t* __re
             sum += c;
         }
         gbase[d] = offsets[d * ntiles + blockIdx.x];
+        // exclusive scan of the digit totals across the block
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wtot[warp] = incl;
+        __syncthreads();
+        uint32_t before = 0;
+        for (int w = 0; w < warp; ++w) before += wtot[w];
+        tbase[d] = before + incl - sum;
     }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kItems; ++r) {
         if (dg[r] < kRadix) {
-            const uint32_t dst = gbase[dg[r]] + wcnt[warp][dg[r]] + rk[r];
-            kout[dst] = kk[r];
-            vout[dst] = vv[r];
+            const uint32_t t = tbase[dg[r]] + wcnt[warp][dg[r]] + rk[r];
+            sk[t] = kk[r];
+            sv[t] = vv[r];
         }
+    }
+    __syncthreads();
+    const uint32_t count = min(static_cast<uint32_t>(kTile), n - blockIdx.x * kTile);
+    for (uint32_t t = threadIdx.x; t < count; t += kThreads) {
+        const uint32_t k = sk[t];
+        const int d = static_cast<int>((k >> shift) & kMask);
+        const uint32_t dst = gbase[d] + (t - tbase[d]);
+        kout[dst] = k;
+        vout[dst] = sv[t];
     }
 }
 
