@@ -310,6 +310,8 @@ typedef struct {
     int profile_phases;    /* record CUDA events around phases (default 0) */
     int pin_x;             /* launch shape of the x sweeps instead of the tuned one: */
     int pin_cols;          /* warps * 16 + stages (y and z sweeps: pin_cols); 0 = tuned */
+    int disable_planes;    /* 1: x and y sweeps as separate tile passes even where an x-y plane
+                              fits shared memory (same results; 0 = one pass per plane) */
 } pcg_batch_options;
 
 pcg_status pcg_batch_create(pcg_ctx* ctx, const pcg_instance_desc* instances, uint32_t n_instances,

@@ -77,6 +77,7 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
     }
     if (cells_total > 0xFFFFFFF0ull || rates_total > 0xFFFFFFF0ull || mvox_total > 0xFFFFFFF0ull)
         return fail(ctx, PCG_ERR_INVALID, "batch too large for 32-bit indices");
+    d.use_planes = !(opt && opt->disable_planes);
     PCG_TRY(d.build(ctx, std::move(di)));
     for (uint32_t i = 0; i < n; ++i) {
         if (const DevSource* ds = from(i)) {

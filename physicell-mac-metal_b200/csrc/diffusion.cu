@@ -437,12 +437,9 @@ __device__ __forceinline__ void thomas_line(const float* t, int n, LD ld, ST st)
 // the coefficients are one broadcast load, and each lane moves 4 values with
 // one 16-byte shared access; P / 4 is odd, so the 8 lanes of each quarter
 // warp hit 8 different 16-byte bank groups (no conflicts).
-__device__ __forceinline__ void solve_rows_vec(float* st, const LineRule& r, const float* t, int lane,
-                                               int count)
+__device__ __forceinline__ void row_line(float* row, const LineRule& r, const float* t)
 {
-    if (lane >= count) return;
     const int n = static_cast<int>(r.n);
-    float* row = st + lane * static_cast<int>(row_smem_pitch(r.n));
     if (n >= 3) {
         row[1] += r.fold;
         if (n > 3) row[n - 2] += r.fold;
@@ -454,6 +451,13 @@ __device__ __forceinline__ void solve_rows_vec(float* st, const LineRule& r, con
         row[0] = r.T;
         row[n - 1] = r.T;
     }
+}
+
+__device__ __forceinline__ void solve_rows_vec(float* st, const LineRule& r, const float* t, int lane,
+                                               int count)
+{
+    if (lane >= count) return;
+    row_line(st + lane * static_cast<int>(row_smem_pitch(r.n)), r, t);
 }
 
 // y/z tile: lane = column, rows at st + j * 32 (32 lanes, 32 banks).
@@ -639,6 +643,105 @@ __global__ void __launch_bounds__(256, 1) k_sweep_tma(float* __restrict__ dens, 
         }
     }
     bulk_wait_all();
+}
+
+// ------------------------------------------------------- fused x + y sweeps of a plane
+
+// Column line of a plane in shared memory (rows P floats apart): the steps
+// of solve_cols with row stride P.  'face': the line lies on an x face of a
+// 2-D block whose last sweep this is, so applyDirichletBC sets it to T.
+__device__ __forceinline__ void plane_col(float* c, int P, const LineRule& r, const float* t, bool face)
+{
+    const int n = static_cast<int>(r.n);
+    if (face) {
+        for (int j = 0; j < n; ++j) c[j * P] = r.T;
+        return;
+    }
+    if (n >= 3) {
+        c[P] += r.fold;
+        if (n > 3) c[(n - 2) * P] += r.fold;
+        thomas_line(
+            t, n,
+            [c, P](int q) {
+                return make_float4(c[(4 * q) * P], c[(4 * q + 1) * P], c[(4 * q + 2) * P], c[(4 * q + 3) * P]);
+            },
+            [c, P](int q, float4 v) {
+                c[(4 * q) * P] = v.x;
+                c[(4 * q + 1) * P] = v.y;
+                c[(4 * q + 2) * P] = v.z;
+                c[(4 * q + 3) * P] = v.w;
+            });
+    }
+    if (r.dir) {
+        c[0] = r.T;
+        c[(n - 1) * P] = r.T;
+    }
+}
+
+// One CTA per x-y plane (one z slab of one instance-substrate): the plane
+// (rows of pitch P = row_smem_pitch(nx), zero-filled past nx) and both
+// rules' tables come in with one tensor box and two bulk copies; every row
+// is solved (x sweep), then every column (y sweep), and the plane goes back
+// with one tensor store.  The steps on each line are those of the x and y
+// tile kernels, so the result is the same bits, but the plane crosses HBM
+// once for both sweeps.  Several CTAs per SM overlap one plane's copies
+// with another's solves.
+__global__ void __launch_bounds__(kPlaneThreads) k_sweep_planes(const PlaneJob* __restrict__ jobs,
+                                                                const float* __restrict__ tab,
+                                                                const void* __restrict__ tmaps, int apply_faces,
+                                                                const uint8_t* __restrict__ mask,
+                                                                unsigned* __restrict__ status)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+    float* pl = reinterpret_cast<float*>(smem + 128);
+    const PlaneJob jb = jobs[blockIdx.x];
+    const uint32_t ii = jb.inst & kPlaneInstMask;
+    if (mask && !(mask[ii] & STEP_DIFFUSE)) return;   // the whole CTA leaves together
+    const uint32_t nx = jb.nx, ny = jb.ny, P = row_smem_pitch(nx);
+    float* tx = pl + plane_data_floats(nx, ny);
+    float* ty = tx + tab_floats(nx);
+    const void* map = static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(jb.map) * 128;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t tbx = tab_floats(nx) * 4u, tby = tab_floats(ny) * 4u;
+        mbar_arrive_expect_tx(bar, P * ny * 4u + tbx + tby);   // the whole box, fill included
+        tensor_load2(pl, map, 0, static_cast<int>(jb.row0), bar);
+        bulk_load(tx, tab + jb.tab_x, tbx, bar);
+        bulk_load(ty, tab + jb.tab_y, tby, bar);
+    }
+    const bool got = mbar_wait(bar, 0, status);
+    if (!__syncthreads_and(got)) {
+        // a wait ran out: one more bounded wait for the copies before the
+        // CTA releases its shared memory
+        if (threadIdx.x == 0 && !got) mbar_wait(bar, 0, status);
+        return;
+    }
+    LineRule rx{}, ry{};
+    rx.n = nx;
+    rx.fold = jb.fold_x;
+    rx.T = jb.T_x;
+    rx.dir = (jb.inst & kPlaneDirX) ? 1u : 0u;
+    ry.n = ny;
+    ry.fold = jb.fold_y;
+    ry.T = jb.T_y;
+    ry.dir = (jb.inst & kPlaneDirY) ? 1u : 0u;
+    for (uint32_t r = threadIdx.x; r < ny; r += blockDim.x) row_line(pl + r * P, rx, tx);
+    __syncthreads();
+    const bool faces = apply_faces && (jb.inst & kPlaneFaces) != 0;
+    for (uint32_t c = threadIdx.x; c < nx; c += blockDim.x)
+        plane_col(pl + c, static_cast<int>(P), ry, ty, faces && (c == 0u || c + 1u == nx));
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tensor_store2(map, 0, static_cast<int>(jb.row0), pl);
+        bulk_commit();
+        bulk_wait_all();
+    }
 }
 
 // ------------------------------------------------------- any line length
@@ -861,6 +964,40 @@ bool encode_row_map(void* map128, float* block, uint32_t nx, uint64_t rows, uint
                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
+}
+
+bool encode_plane_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint64_t rows, uint32_t px)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    const uint32_t P = row_smem_pitch(nx);
+    if (!fn || nx == 0 || nx > kRowTensorMaxN || ny == 0 || ny > 256 || rows == 0 || (px & 3u) || px < nx ||
+        (reinterpret_cast<uintptr_t>(block) & 15u))
+        return false;
+    const cuuint64_t dims[2] = {nx, rows};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(px) * 4u};
+    const cuuint32_t box[2] = {P, ny};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = fn(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, block, dims, strides,
+                          box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+size_t sweep_planes_smem(uint32_t floats) { return 128 + static_cast<size_t>(floats) * sizeof(float); }
+
+cudaError_t sweep_planes_prepare()
+{
+    return allow_max_smem(reinterpret_cast<const void*>(k_sweep_planes));
+}
+
+cudaError_t launch_sweep_planes(cudaStream_t st, const PlaneJob* jobs, uint32_t njobs, const float* tab,
+                                const void* tmaps, uint32_t floats, int apply_faces, const uint8_t* mask,
+                                unsigned* status)
+{
+    if (njobs == 0) return cudaSuccess;
+    k_sweep_planes<<<njobs, kPlaneThreads, sweep_planes_smem(floats), st>>>(jobs, tab, tmaps, apply_faces, mask,
+                                                                            status);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* tiles, uint32_t ntiles,

@@ -129,6 +129,33 @@ enum : uint8_t { STEP_DIFFUSE = 1u, STEP_MECH = 2u };
 // Pipelined TMA sweeps: 'warps' warps per CTA, each with 'stages' shared
 // memory stages of 'stage_floats' floats, the last 'tab_floats' of which
 // hold the tile's coefficient table; 'grid' persistent CTAs.
+// One x-y plane (z slab k of one instance-substrate) for the fused x + y
+// sweep kernel: the plane tensor map (box row_smem_pitch(nx) x ny, slot 1
+// of the x rule), its first row k * ny, and both rules.
+struct PlaneJob {
+    uint32_t map;
+    uint32_t row0;
+    uint32_t nx, ny;
+    uint32_t tab_x, tab_y;   // table offsets (floats)
+    float fold_x, T_x, fold_y, T_y;
+    uint32_t inst;           // instance | kPlaneDirX | kPlaneDirY | kPlaneFaces
+    uint32_t _pad[5];
+};
+static_assert(sizeof(PlaneJob) == 64, "PlaneJob is 64 bytes");
+constexpr uint32_t kPlaneDirX = 1u << 31, kPlaneDirY = 1u << 30, kPlaneFaces = 1u << 29;
+constexpr uint32_t kPlaneInstMask = (1u << 29) - 1u;
+constexpr uint32_t kPlaneThreads = 128;
+// Shared floats of a plane's data (rows rounded up to a whole chunk of 4,
+// which the column solve may touch; 128-byte multiple) and with both tables.
+__host__ __device__ constexpr uint32_t plane_data_floats(uint32_t nx, uint32_t ny)
+{
+    return (row_smem_pitch(nx) * ((ny + 3u) & ~3u) + 31u) / 32u * 32u;
+}
+__host__ __device__ constexpr uint32_t plane_floats(uint32_t nx, uint32_t ny)
+{
+    return plane_data_floats(nx, ny) + tab_floats(nx) + tab_floats(ny);
+}
+
 struct TmaCfg { int warps; int stages; int stage_floats; int grid; int tab_floats; };
 
 // Longest line staged in shared memory; longer lines take the one-thread-
@@ -139,6 +166,16 @@ size_t sweep_tma_smem(int warps, int nstages, int stage_floats);
 int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats);   // CTAs per SM (0 = does not fit)
 // tmaps: one 128-byte CUtensorMap per rule (64-byte aligned, global memory)
 // for the tiles flagged TILE_TENSOR; may be null otherwise.
+// Fused x + y sweeps, one CTA per plane; 'floats' = the largest
+// plane_floats of the jobs.
+cudaError_t launch_sweep_planes(cudaStream_t st, const PlaneJob* jobs, uint32_t njobs, const float* tab,
+                                const void* tmaps, uint32_t floats, int apply_faces, const uint8_t* mask,
+                                unsigned* status);
+// Lets the plane kernel use the opt-in shared memory (current device; once
+// per device, outside stream capture).
+cudaError_t sweep_planes_prepare();
+size_t sweep_planes_smem(uint32_t floats);
+bool encode_plane_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint64_t rows, uint32_t px);
 cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
                              const float* tab, const void* tmaps, int apply_faces,
                              const uint8_t* mask, unsigned* status, TmaCfg cfg);

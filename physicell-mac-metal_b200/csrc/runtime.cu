@@ -265,6 +265,10 @@ void Tuner::save(const std::string& path)
 
 // ------------------------------------------------------------------ diffusion
 
+// Largest plane (with its tables) the fused x + y kernel takes: two CTAs
+// per SM fit the 227 KB of shared memory.
+static constexpr size_t kPlaneMaxSmem = 112 * 1024;
+
 
 static uint32_t axis_n(const pcg_grid_params& g, int a) { return a == 0 ? g.nx : (a == 1 ? g.ny : g.nz); }
 static float axis_h(const pcg_grid_params& g, int a) { return a == 0 ? g.dx : (a == 1 ? g.dy : g.dz); }
@@ -396,6 +400,24 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
                 }
             }
         }
+        // plane maps (slot 1 of each x rule) for the instances whose x-y
+        // planes fit the plane kernel's shared memory
+        plane_inst_.assign(inst.size(), 0);
+        for (size_t i = 0; use_planes && i < inst.size(); ++i) {
+            const DiffInstance& d = inst[i];
+            const uint32_t nx = d.g.nx, ny = d.g.ny;
+            if (d.g.n_substrates == 0 || nx > kRowTensorMaxN || ny > 256 ||
+                sweep_planes_smem(plane_floats(nx, ny)) > kPlaneMaxSmem)
+                continue;
+            bool ok = true;
+            for (uint32_t s = 0; s < d.g.n_substrates && ok; ++s) {
+                const uint32_t rule = rule_of(i, s, 0);
+                unsigned char* m = maps.data() + static_cast<size_t>(rule) * kMapsPerRule * 128;
+                ok = (tensor_ok_[rule] & 1u) &&
+                     encode_plane_map(m + 128, dens.as<float>() + d.dens_off + s * d.pitch, nx, ny, d.rows(), d.px);
+            }
+            plane_inst_[i] = ok ? 1 : 0;
+        }
         PCG_CU(ctx, tmaps.alloc(maps.size()));
         PCG_CU(ctx, cudaMemcpyAsync(tmaps.p, maps.data(), maps.size(), cudaMemcpyHostToDevice, ctx->stream));
     }
@@ -403,9 +425,76 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
     PCG_CU(ctx, faces.alloc(std::max<size_t>(fj.size(), 1) * sizeof(FaceJob)));
     if (!fj.empty()) PCG_CU(ctx, cudaMemcpyAsync(faces.p, fj.data(), fj.size() * sizeof(FaceJob), cudaMemcpyHostToDevice, ctx->stream));
     for (int a = 0; a < 3; ++a) {
-        PCG_TRY(build_axis(a));
+        PCG_TRY(build_axis(a, nullptr, lists[a]));
         PCG_TRY(default_configs(a));
     }
+    return build_planes();
+}
+
+// Plane jobs (one per z slab of each substrate of each plane instance),
+// grouped by shared-memory size so small planes are not charged the
+// largest plane's footprint, and the x / y tiles of the other instances.
+int Diffusion::build_planes()
+{
+    planes.clear();
+    for (auto& r : rest) r.clear();
+    bool any = false;
+    for (uint8_t v : plane_inst_) any = any || v;
+    if (!any) return PCG_OK;
+    constexpr int kClasses = 3;
+    const size_t bounds[kClasses] = {28 * 1024, 56 * 1024, kPlaneMaxSmem};
+    std::vector<PlaneJob> jobs[kClasses];
+    uint32_t fl[kClasses] = {0, 0, 0};
+    uint64_t un[kClasses] = {0, 0, 0};
+    for (size_t i = 0; i < inst.size(); ++i) {
+        if (!plane_inst_[i]) continue;
+        const DiffInstance& d = inst[i];
+        const uint32_t nx = d.g.nx, ny = d.g.ny, pf = plane_floats(nx, ny);
+        int c = 0;
+        while (c + 1 < kClasses && sweep_planes_smem(pf) > bounds[c]) ++c;
+        for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
+            const uint32_t rx_i = rule_of(i, s, 0);
+            const LineRule& rx = h_rules_[rx_i];
+            const LineRule& ry = h_rules_[rule_of(i, s, 1)];
+            for (uint32_t k = 0; k < d.g.nz; ++k) {
+                PlaneJob j{};
+                j.map = rx_i * kMapsPerRule + 1;
+                j.row0 = k * ny;
+                j.nx = nx;
+                j.ny = ny;
+                j.tab_x = rx.tab;
+                j.tab_y = ry.tab;
+                j.fold_x = rx.fold;
+                j.T_x = rx.T;
+                j.fold_y = ry.fold;
+                j.T_y = ry.T;
+                j.inst = static_cast<uint32_t>(i) | (rx.dir ? kPlaneDirX : 0u) | (ry.dir ? kPlaneDirY : 0u) |
+                         ((d.ndim() == 2 && ry.dir) ? kPlaneFaces : 0u);
+                jobs[c].push_back(j);
+            }
+        }
+        fl[c] = std::max(fl[c], pf);
+        un[c] += d.nvox() * d.g.n_substrates;
+    }
+    int nl = 0;
+    for (int c = 0; c < kClasses; ++c) nl += jobs[c].empty() ? 0 : 1;
+    planes.resize(nl);
+    int q = 0;
+    for (int c = kClasses - 1; c >= 0; --c) {   // largest planes first
+        if (jobs[c].empty()) continue;
+        PlaneList& pl = planes[q++];
+        pl.n = static_cast<uint32_t>(jobs[c].size());
+        pl.floats = fl[c];
+        pl.units = un[c];
+        PCG_CU(ctx, pl.jobs.alloc(jobs[c].size() * sizeof(PlaneJob)));
+        PCG_CU(ctx, cudaMemcpyAsync(pl.jobs.p, jobs[c].data(), jobs[c].size() * sizeof(PlaneJob),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+    }
+    for (int a = 0; a < 2; ++a) {
+        PCG_TRY(build_axis(a, &plane_inst_, rest[a]));
+        for (auto& l : rest[a]) PCG_TRY(config_list(l, 0));
+    }
+    PCG_CU(ctx, sweep_planes_prepare());
     return PCG_OK;
 }
 
@@ -422,13 +511,14 @@ static void fill_rule(SweepTile& t, const LineRule& r)
 // Tile lists of one axis: lines up to kTmaMaxN go to the pipelined TMA
 // kernels (x: 32 lines per tile; y/z: 32 columns per tile), longer lines to
 // the one-thread-per-line kernel.
-int Diffusion::build_axis(int axis)
+int Diffusion::build_axis(int axis, const std::vector<uint8_t>* skip, std::vector<SweepList>& ls)
 {
     std::vector<SweepTile> fast_t, glob_t;
     int fast_nmax = 0, glob_nmax = 0;
-    uint64_t fast_lines = 0, glob_lines = 0;
+    uint64_t fast_lines = 0, glob_lines = 0, fast_units = 0, glob_units = 0;
     const int kind_fast = axis == 0 ? 0 : 1;
     for (size_t i = 0; i < inst.size(); ++i) {
+        if (skip && (*skip)[i]) continue;
         const DiffInstance& d = inst[i];
         const pcg_grid_params& g = d.g;
         const int nd = d.ndim();
@@ -438,6 +528,7 @@ int Diffusion::build_axis(int axis)
         auto& out = fast ? fast_t : glob_t;
         int& nmax = fast ? fast_nmax : glob_nmax;
         uint64_t& nl = fast ? fast_lines : glob_lines;
+        (fast ? fast_units : glob_units) += d.nvox() * g.n_substrates;
         nmax = std::max<int>(nmax, static_cast<int>(n));
         const bool final_axis = axis == nd - 1;
         for (uint32_t s = 0; s < g.n_substrates; ++s) {
@@ -508,17 +599,18 @@ int Diffusion::build_axis(int axis)
     auto by_n = [](const SweepTile& a, const SweepTile& b) { return a.n > b.n; };
     std::stable_sort(fast_t.begin(), fast_t.end(), by_n);
     std::stable_sort(glob_t.begin(), glob_t.end(), by_n);
-    std::vector<SweepList>& ls = lists[axis];
     ls.clear();
     ls.resize(2);
     ls[0].kind = kind_fast;
     ls[0].nmax = fast_nmax;
     ls[0].n = static_cast<uint32_t>(fast_t.size());
     ls[0].lines = fast_lines;
+    ls[0].units = fast_units;
     ls[1].kind = 2;
     ls[1].nmax = glob_nmax;
     ls[1].n = static_cast<uint32_t>(glob_t.size());
     ls[1].lines = glob_lines;
+    ls[1].units = glob_units;
     for (int q = 0; q < 2; ++q) {
         const auto& v = q == 0 ? fast_t : glob_t;
         PCG_CU(ctx, ls[q].tiles.alloc(std::max<size_t>(v.size(), 1) * sizeof(SweepTile)));
@@ -590,6 +682,9 @@ int Diffusion::pin(int kind, int param)
     for (int a = 0; a < 3; ++a)
         for (auto& l : lists[a])
             if (l.kind == kind && l.n) PCG_TRY(config_list(l, param));
+    for (int a = 0; a < 2; ++a)
+        for (auto& l : rest[a])
+            if (l.kind == kind && l.n) PCG_TRY(config_list(l, param));
     return PCG_OK;
 }
 
@@ -616,8 +711,34 @@ int Diffusion::launch_list(const SweepList& l, bool fuse, const uint8_t* mask)
 
 int Diffusion::sweep(int axis, bool fuse, const uint8_t* mask)
 {
+    if (!planes.empty() && axis < 2) {
+        if (axis == 0)
+            for (const auto& pl : planes) {
+                cudaError_t e = launch_sweep_planes(ctx->stream, pl.jobs.as<PlaneJob>(), pl.n, tab.as<float>(),
+                                                    tmaps.p, pl.floats, fuse ? 1 : 0, mask, ctx->status);
+                if (e != cudaSuccess) return cuda_fail(ctx, e, "plane sweep launch");
+                ctx->launches++;
+            }
+        for (const auto& l : rest[axis]) PCG_TRY(launch_list(l, fuse, mask));
+        return PCG_OK;
+    }
     for (const auto& l : lists[axis]) PCG_TRY(launch_list(l, fuse, mask));
     return PCG_OK;
+}
+
+uint64_t Diffusion::sweep_units_per_step() const
+{
+    uint64_t u = 0;
+    for (int a = 0; a < 3; ++a) {
+        if (!planes.empty() && a < 2) {
+            if (a == 0)
+                for (const auto& pl : planes) u += pl.units;
+            for (const auto& l : rest[a]) u += l.units;
+        } else {
+            for (const auto& l : lists[a]) u += l.units;
+        }
+    }
+    return u;
 }
 
 int Diffusion::sweeps(bool fuse, const uint8_t* mask)
@@ -629,8 +750,14 @@ int Diffusion::sweeps(bool fuse, const uint8_t* mask)
 int Diffusion::launches_per_step(bool) const
 {
     int k = 0;
-    for (int a = 0; a < 3; ++a)
-        for (const auto& l : lists[a]) k += l.n > 0 ? 1 : 0;
+    for (int a = 0; a < 3; ++a) {
+        if (!planes.empty() && a < 2) {
+            if (a == 0) k += static_cast<int>(planes.size());
+            for (const auto& l : rest[a]) k += l.n > 0 ? 1 : 0;
+        } else {
+            for (const auto& l : lists[a]) k += l.n > 0 ? 1 : 0;
+        }
+    }
     return k;
 }
 
@@ -721,6 +848,9 @@ uint64_t Diffusion::device_bytes() const
     uint64_t b = dens.bytes + rules.bytes + tab.bytes + faces.bytes;
     for (int a = 0; a < 3; ++a)
         for (const auto& l : lists[a]) b += l.tiles.bytes;
+    for (int a = 0; a < 2; ++a)
+        for (const auto& l : rest[a]) b += l.tiles.bytes;
+    for (const auto& pl : planes) b += pl.jobs.bytes;
     return b;
 }
 
@@ -728,8 +858,9 @@ std::string Diffusion::describe() const
 {
     std::ostringstream o;
     const char* ax = "xyz";
+    for (const auto& pl : planes) o << "xy:planes(jobs=" << pl.n << ",smem=" << sweep_planes_smem(pl.floats) << ") ";
     for (int a = 0; a < 3; ++a)
-        for (const auto& l : lists[a]) {
+        for (const auto& l : (!planes.empty() && a < 2) ? rest[a] : lists[a]) {
             if (l.n == 0) continue;
             o << ax[a] << ":";
             if (l.kind != 2)
@@ -771,7 +902,10 @@ int Diffusion::tune()
     };
     int rc = PCG_OK;
     for (int a = 0; a < 3 && rc == PCG_OK; ++a) {
-        SweepList& l = lists[a][0];
+        // the lists a sub-step launches
+        std::vector<SweepList>& la = (!planes.empty() && a < 2) ? rest[a] : lists[a];
+        if (la.empty()) continue;
+        SweepList& l = la[0];
         if (l.n == 0) continue;
         const std::string key = std::string(l.kind == 0 ? "x" : "cols") + ":n" + std::to_string(l.nmax) + ":l" +
                                 std::to_string(bucket(l.lines));

@@ -136,6 +136,14 @@ struct DiffInstance {
     int ndim() const { return g.nz > 1 ? 3 : 2; }
 };
 
+// Fused x + y plane jobs launched together (one shared-memory size).
+struct PlaneList {
+    DevBuf jobs;
+    uint32_t n = 0;
+    uint32_t floats = 0;       // largest plane_floats of the jobs
+    uint64_t units = 0;        // voxel-substrates covered
+};
+
 struct SweepList {
     int kind = 0;              // 0 row tiles (TMA), 1 column tiles (TMA), 2 any length (global)
     int nmax = 0;
@@ -144,6 +152,7 @@ struct SweepList {
     TmaCfg tc{4, 3, 0, 1};
     int ggrid = 1;
     uint64_t lines = 0;        // lines covered (for tuning keys)
+    uint64_t units = 0;        // voxel-substrates covered
 };
 
 class Diffusion {
@@ -156,6 +165,12 @@ public:
     DevBuf dens, rules, tab, faces, grad_jobs, tmaps;
     uint32_t n_faces = 0;
     std::vector<SweepList> lists[3];
+    // Instances whose x-y planes fit shared memory run their x and y sweeps
+    // as one plane pass (planes); rest[0] / rest[1] hold the x / y tiles of
+    // the others.  sweep(0) then launches planes + rest[0], sweep(1) rest[1].
+    std::vector<PlaneList> planes;
+    std::vector<SweepList> rest[2];
+    bool use_planes = true;            // set before build()
     std::string shapes;
 
     // Lays out the density arena, builds the Thomas tables and the tile
@@ -172,11 +187,16 @@ public:
     int download(uint32_t i, float* host, bool async_pinned = false);
     int fill(uint32_t i, const float* values);
     int launches_per_step(bool three_d_only = false) const;
+    // Voxel-substrates the sweep launches of one sub-step cover, summed over
+    // launches (each moves 8 bytes per unit: one read, one write).
+    uint64_t sweep_units_per_step() const;
     uint64_t device_bytes() const;
     std::string describe() const;
 
 private:
-    int build_axis(int axis);
+    int build_axis(int axis, const std::vector<uint8_t>* skip, std::vector<SweepList>& ls);
+    int build_planes();
+    std::vector<uint8_t> plane_inst_;    // instance's x + y sweeps run as planes
     int default_configs(int axis);
     int config_list(SweepList& l, int param);
     int launch_list(const SweepList& l, bool fuse_faces, const uint8_t* mask);

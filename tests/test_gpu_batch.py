@@ -73,6 +73,32 @@ def test_pinned_launch_shapes_give_identical_results(ctx, pcg, pins):
         assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32))
 
 
+def test_plane_pass_equals_separate_sweeps(ctx, pcg):
+    """Instances whose x-y planes fit shared memory run the x and y sweeps
+    as one pass per plane; the result is the same bits as the separate
+    passes, for 2-D (faces in the y pass) and 3-D instances, mixed with
+    instances too wide for a plane."""
+    from pcg import workloads
+    insts = small_mix(pcg, seed=10)
+    rng = np.random.default_rng(3)
+    for nx, ny, nz in ((300, 40, 1), (260, 30, 12)):       # rows longer than a plane row: tile passes
+        g = pcg.make_grid(nx, ny, nz, 2, dx=20.0, dt=0.01, z_min=-10.0 if nz == 1 else 0.0)
+        n = 400
+        L = np.array([nx, ny, nz]) * 20.0
+        pos = (rng.uniform(0.2, 0.8, (n, 3)) * L).astype(np.float32)
+        if nz == 1:
+            pos[:, 2] = 0.0
+        insts.append(workloads.instance(g, [(1e5, 0.1, True, 38.0), (3e3, 0.2, False, 0.0)], pos,
+                                        np.full(n, 8.41, np.float32), 10.0, 0.4, 1.25,
+                                        sec=rng.uniform(0, 5, 2 * n), upt=rng.uniform(0, 10, 2 * n),
+                                        sat=rng.uniform(0, 40, 2 * n), two_d=nz == 1))
+    a = run_batch(pcg, ctx, insts, 23, planes=True)
+    b = run_batch(pcg, ctx, insts, 23, planes=False)
+    for i, ((da, ca), (db, cb)) in enumerate(zip(a, b)):
+        assert np.array_equal(da.view(np.uint32), db.view(np.uint32)), f"density {i}"
+        assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32)), f"cells {i}"
+
+
 def test_bad_pinned_shape_is_refused(ctx, pcg):
     with pytest.raises(pcg.PcgError):
         pcg.Batch(ctx, small_mix(pcg, seed=9)[:1], autotune=False, pin_x=17 * 16 + 2)
