@@ -169,6 +169,7 @@ _SIGS = [
     ("pcg_batch_density_layout", C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                            C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_batch_totals", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("pcg_batch_sweep_units", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_batch_step_launches", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_batch_phase_times", C.c_int, [_P, _F32P, C.POINTER(C.c_uint64), C.c_int]),
     ("pcg_batch_set_profile", C.c_int, [_P, C.c_int]),
@@ -647,6 +648,13 @@ class Batch:
         v, vs, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
         self.ctx.check(lib().pcg_batch_totals(self.h, C.byref(v), C.byref(vs), C.byref(c)))
         return v.value, vs.value, c.value
+
+    def sweep_units(self):
+        """(plane_units, all_units): voxel-substrates one sub-step's fused
+        x + y plane launches / all sweep launches cover (8 bytes each)."""
+        pu, au = C.c_uint64(), C.c_uint64()
+        self.ctx.check(lib().pcg_batch_sweep_units(self.h, C.byref(pu), C.byref(au)))
+        return pu.value, au.value
 
     def layout(self, i):
         """(offset, row_pitch, substrate_pitch, arena_floats) of instance i's density on the device."""

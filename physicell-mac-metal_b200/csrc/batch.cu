@@ -419,6 +419,16 @@ pcg_status pcg_batch_totals(pcg_batch* b, uint64_t* voxels, uint64_t* vs, uint64
     return PCG_OK;
 }
 
+pcg_status pcg_batch_sweep_units(pcg_batch* b, uint64_t* plane_units, uint64_t* all_units)
+{
+    if (!b) return PCG_ERR_INVALID;
+    uint64_t pu = 0;
+    for (const auto& pl : b->b.d.planes) pu += pl.units;
+    if (plane_units) *plane_units = pu;
+    if (all_units) *all_units = b->b.d.sweep_units_per_step();
+    return PCG_OK;
+}
+
 pcg_status pcg_batch_step_launches(pcg_batch* b, uint64_t* ld, uint64_t* lm)
 {
     if (!b) return PCG_ERR_INVALID;

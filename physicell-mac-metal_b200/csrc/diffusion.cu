@@ -660,17 +660,16 @@ __device__ __forceinline__ void plane_col(float* c, int P, const LineRule& r, co
     if (n >= 3) {
         c[P] += r.fold;
         if (n > 3) c[(n - 2) * P] += r.fold;
-        thomas_line(
-            t, n,
-            [c, P](int q) {
-                return make_float4(c[(4 * q) * P], c[(4 * q + 1) * P], c[(4 * q + 2) * P], c[(4 * q + 3) * P]);
-            },
-            [c, P](int q, float4 v) {
-                c[(4 * q) * P] = v.x;
-                c[(4 * q + 1) * P] = v.y;
-                c[(4 * q + 2) * P] = v.z;
-                c[(4 * q + 3) * P] = v.w;
-            });
+        auto ld = [c, P](int q) {
+            return make_float4(c[(4 * q) * P], c[(4 * q + 1) * P], c[(4 * q + 2) * P], c[(4 * q + 3) * P]);
+        };
+        auto st4 = [c, P](int q, float4 v) {
+            c[(4 * q) * P] = v.x;
+            c[(4 * q + 1) * P] = v.y;
+            c[(4 * q + 2) * P] = v.z;
+            c[(4 * q + 3) * P] = v.w;
+        };
+        thomas_line(t, n, ld, st4);
     }
     if (r.dir) {
         c[0] = r.T;
@@ -740,7 +739,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_sweep_planes(const PlaneJob* 
     if (threadIdx.x == 0) {
         tensor_store2(map, 0, static_cast<int>(jb.row0), pl);
         bulk_commit();
-        bulk_wait_all();
+        bulk_wait_read<0>();   // shared memory may be released once the store has read it
     }
 }
 
