@@ -46,6 +46,8 @@ CASES = [
     ("y_bulk_400", 9, 400, 1, [O2, (2e3, 0.2, False, 0.0)]),   # column tiles by per-row bulk copies
     ("z_bulk_270", 5, 6, 270, [(1e4, 0.1, True, 3.0)]),
     ("3d_w16_groups", 44, 13, 9, [O2, (4e3, 0.3, True, 2.0)]),  # 12-column remainder: 16-wide, 2-slab tiles
+    ("3d_x70", 70, 9, 12, [O2, (4e3, 0.3, True, 2.0)]),         # z: 32-wide tiles + a 6-column remainder
+    ("3d_x130", 130, 6, 8, [(2e4, 0.1, True, 5.0)]),            # x rows past 128, z remainder of 2 columns
 ]
 
 
