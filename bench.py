@@ -277,7 +277,8 @@ def run_reference_arm(args, rank, world):
 
 
 def time_steps(ctx, fn, k):
-    """CUDA events on the library's stream, synchronised on both sides."""
+    """CUDA events on the library's stream, synchronised on both sides; the
+    closing event also follows the library's host copies (pcg_join)."""
     import torch
     st = torch.cuda.ExternalStream(ctx.stream)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -287,6 +288,7 @@ def time_steps(ctx, fn, k):
     e0.record(st)
     for _ in range(k):
         fn()
+    ctx.join()
     e1.record(st)
     ctx.sync()
     torch.cuda.synchronize()

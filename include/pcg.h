@@ -97,6 +97,10 @@ pcg_status pcg_destroy(pcg_ctx* ctx);
  * PCG_ERR_DEVICE when a kernel stopped early since the last sync. */
 pcg_status pcg_sync(pcg_ctx* ctx);
 void* pcg_stream(pcg_ctx* ctx);
+/* Orders the context's stream after every host copy issued so far by the
+ * whole-batch transfers (which run on copy streams of their own, beside the
+ * kernels), without waiting on the host; pcg_sync waits for them as well. */
+pcg_status pcg_join(pcg_ctx* ctx);
 const char* pcg_last_error_string(const pcg_ctx* ctx);
 /* Number of kernel launches this context has issued (graph launches count
  * their kernel nodes). */
@@ -328,8 +332,11 @@ pcg_status pcg_batch_upload_cells(pcg_batch* batch, uint32_t instance, const flo
  * should come from pcg_host_alloc).  Cells: one SoA of all instances' cells
  * in instance order, field stride = total cells (28 * total floats).
  * Density: the device arena as is (pcg_batch_density_layout gives each
- * instance's offset and substrate pitch).  Neither waits for completion;
- * pcg_sync does. */
+ * instance's offset and substrate pitch).  The host copies run on copy
+ * streams through device staging buffers, so they overlap the kernels of
+ * other steps: an upload is taken by the next step, a download is the state
+ * at the call.  None waits for completion; pcg_sync does (pcg_join orders
+ * the context stream after them). */
 pcg_status pcg_batch_upload_all_cells(pcg_batch* batch, const float* soa, uint64_t n_floats);
 pcg_status pcg_batch_download_all_cells(pcg_batch* batch, float* soa, uint64_t n_floats);
 pcg_status pcg_batch_download_all_density(pcg_batch* batch, float* host, uint64_t n_floats);

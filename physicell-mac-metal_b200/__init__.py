@@ -168,6 +168,7 @@ _SIGS = [
     ("pcg_batch_download_all_density", C.c_int, [_P, _F32P, C.c_uint64]),
     ("pcg_batch_density_layout", C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                            C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("pcg_join", C.c_int, [_P]),
     ("pcg_batch_totals", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_batch_sweep_units", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_batch_step_launches", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
@@ -270,6 +271,10 @@ class Context:
 
     def sync(self):
         self.check(lib().pcg_sync(self.h))
+
+    def join(self):
+        """Order the context stream after the whole-batch host copies issued so far."""
+        self.check(lib().pcg_join(self.h))
 
     @property
     def stream(self):

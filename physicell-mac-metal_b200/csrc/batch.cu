@@ -180,6 +180,13 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
 
 Batch::~Batch()
 {
+    if (ctx && (stage_in.p || stage_cells.p || stage_dens.p)) {   // copies may still read or write them
+        if (ctx->h2d) cudaStreamSynchronize(ctx->h2d);
+        if (ctx->d2h) cudaStreamSynchronize(ctx->d2h);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    for (cudaEvent_t e : {ev_in_done, ev_in_used, ev_cells_ready, ev_cells_done, ev_dens_ready, ev_dens_done})
+        if (e) cudaEventDestroy(e);
     if (g_diff) cudaGraphExecDestroy(g_diff);
     if (g_mech) cudaGraphExecDestroy(g_mech);
     for (int q = 0; q < 8; ++q)
@@ -371,32 +378,105 @@ pcg_status pcg_batch_upload_cells(pcg_batch* b, uint32_t i, const float* soa, ui
     return PCG_OK;
 }
 
+namespace {
+
+int ensure_copy_streams(pcg_ctx* ctx)
+{
+    if (ctx->h2d) return PCG_OK;
+    PCG_CU(ctx, cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
+    PCG_CU(ctx, cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
+    for (auto& e : ctx->copy_ev) PCG_CU(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return PCG_OK;
+}
+
+// An event recorded once on the context stream when made, so that the first
+// wait on it passes.
+int ensure_event(pcg_ctx* ctx, cudaEvent_t* e)
+{
+    if (*e) return PCG_OK;
+    PCG_CU(ctx, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    PCG_CU(ctx, cudaEventRecord(*e, ctx->stream));
+    return PCG_OK;
+}
+
+int ensure_stage(pcg_ctx* ctx, DevBuf& b, size_t bytes)
+{
+    if (b.bytes >= bytes) return PCG_OK;
+    PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->h2d) PCG_CU(ctx, cudaStreamSynchronize(ctx->h2d));
+    if (ctx->d2h) PCG_CU(ctx, cudaStreamSynchronize(ctx->d2h));
+    b.release();
+    PCG_CU(ctx, b.alloc(bytes));
+    return PCG_OK;
+}
+
+// device -> staging on the context stream, then staging -> host on the
+// copy stream; 'done' gates the next reuse of the staging buffer
+int staged_download(pcg_ctx* ctx, DevBuf& stage, cudaEvent_t* ready, cudaEvent_t* done, void* host,
+                    const void* src, size_t spitch, size_t width, size_t rows)
+{
+    PCG_TRY(ensure_copy_streams(ctx));
+    PCG_TRY(ensure_stage(ctx, stage, width * rows));
+    PCG_TRY(ensure_event(ctx, ready));
+    PCG_TRY(ensure_event(ctx, done));
+    PCG_CU(ctx, cudaStreamWaitEvent(ctx->stream, *done, 0));
+    PCG_CU(ctx, cudaMemcpy2DAsync(stage.p, width, src, spitch, width, rows, cudaMemcpyDeviceToDevice, ctx->stream));
+    PCG_CU(ctx, cudaEventRecord(*ready, ctx->stream));
+    PCG_CU(ctx, cudaStreamWaitEvent(ctx->d2h, *ready, 0));
+    PCG_CU(ctx, cudaMemcpyAsync(host, stage.p, width * rows, cudaMemcpyDeviceToHost, ctx->d2h));
+    PCG_CU(ctx, cudaEventRecord(*done, ctx->d2h));
+    return PCG_OK;
+}
+
+}  // namespace
+
 pcg_status pcg_batch_upload_all_cells(pcg_batch* b, const float* soa, uint64_t n_floats)
 {
     if (!b || !soa) return PCG_ERR_INVALID;
-    Cells& c = b->b.c_;
-    if (n_floats != static_cast<uint64_t>(NUM_FIELDS) * c.n) return fail(b->b.ctx, PCG_ERR_INVALID, "size mismatch");
+    Batch& B = b->b;
+    Cells& c = B.c_;
+    pcg_ctx* ctx = B.ctx;
+    if (n_floats != static_cast<uint64_t>(NUM_FIELDS) * c.n) return fail(ctx, PCG_ERR_INVALID, "size mismatch");
     if (c.n == 0) return PCG_OK;
-    PCG_TRY(c.upload_soa(0, c.n, soa, c.n, 0, NUM_FIELDS));
-    PCG_TRY(c.prepare_secretion(b->b.dt_diff, b->b.d.total_vox));
+    // host -> staging on the copy stream (once the previous upload has left
+    // the staging buffer), then staging -> the cell SoA on the context stream
+    const size_t row = static_cast<size_t>(c.n) * sizeof(float);
+    PCG_TRY(ensure_copy_streams(ctx));
+    PCG_TRY(ensure_stage(ctx, B.stage_in, row * NUM_FIELDS));
+    PCG_TRY(ensure_event(ctx, &B.ev_in_done));
+    PCG_TRY(ensure_event(ctx, &B.ev_in_used));
+    PCG_CU(ctx, cudaStreamWaitEvent(ctx->h2d, B.ev_in_used, 0));
+    PCG_CU(ctx, cudaMemcpyAsync(B.stage_in.p, soa, row * NUM_FIELDS, cudaMemcpyHostToDevice, ctx->h2d));
+    PCG_CU(ctx, cudaEventRecord(B.ev_in_done, ctx->h2d));
+    PCG_CU(ctx, cudaStreamWaitEvent(ctx->stream, B.ev_in_done, 0));
+    PCG_CU(ctx, cudaMemcpy2DAsync(c.soa.p, static_cast<size_t>(c.max_cells) * sizeof(float), B.stage_in.p, row, row,
+                                  NUM_FIELDS, cudaMemcpyDeviceToDevice, ctx->stream));
+    PCG_CU(ctx, cudaEventRecord(B.ev_in_used, ctx->stream));
+    c.coef_dirty = c.order_dirty = true;   // volumes and voxel indices came with the fields
+    PCG_TRY(c.prepare_secretion(B.dt_diff, B.d.total_vox));
     return PCG_OK;
 }
 
 pcg_status pcg_batch_download_all_cells(pcg_batch* b, float* soa, uint64_t n_floats)
 {
     if (!b || !soa) return PCG_ERR_INVALID;
-    Cells& c = b->b.c_;
-    if (n_floats != static_cast<uint64_t>(NUM_FIELDS) * c.n) return fail(b->b.ctx, PCG_ERR_INVALID, "size mismatch");
-    return c.download_soa(0, c.n, soa, c.n, 0, NUM_FIELDS);
+    Batch& B = b->b;
+    Cells& c = B.c_;
+    if (n_floats != static_cast<uint64_t>(NUM_FIELDS) * c.n) return fail(B.ctx, PCG_ERR_INVALID, "size mismatch");
+    if (c.n == 0) return PCG_OK;
+    return staged_download(B.ctx, B.stage_cells, &B.ev_cells_ready, &B.ev_cells_done, soa, c.soa.p,
+                           static_cast<size_t>(c.max_cells) * sizeof(float), static_cast<size_t>(c.n) * sizeof(float),
+                           NUM_FIELDS);
 }
 
 pcg_status pcg_batch_download_all_density(pcg_batch* b, float* host, uint64_t n_floats)
 {
     if (!b || !host) return PCG_ERR_INVALID;
-    if (n_floats != b->b.d.dens_elems) return fail(b->b.ctx, PCG_ERR_INVALID, "size mismatch");
-    PCG_CU(b->b.ctx, cudaMemcpyAsync(host, b->b.d.dens.p, n_floats * sizeof(float), cudaMemcpyDeviceToHost,
-                                     b->b.ctx->stream));
-    return PCG_OK;
+    Batch& B = b->b;
+    if (n_floats != B.d.dens_elems) return fail(B.ctx, PCG_ERR_INVALID, "size mismatch");
+    if (n_floats == 0) return PCG_OK;
+    const size_t bytes = n_floats * sizeof(float);
+    return staged_download(B.ctx, B.stage_dens, &B.ev_dens_ready, &B.ev_dens_done, host, B.d.dens.p, bytes, bytes, 1);
 }
 
 pcg_status pcg_batch_density_layout(pcg_batch* b, uint32_t i, uint64_t* off, uint64_t* row_pitch, uint64_t* pitch,

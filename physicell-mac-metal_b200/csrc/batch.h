@@ -32,6 +32,12 @@ public:
     cudaGraphExec_t g_diff = nullptr, g_mech = nullptr;
     uint64_t launches_diff = 0, launches_mech = 0;
     cudaEvent_t ev[8] = {};
+    // Staging of the whole-batch transfers (made on first use): host copies
+    // run on the context's copy streams, device-to-device copies on its
+    // stream; *_done / in_used mark when a staging buffer may be reused.
+    DevBuf stage_in, stage_cells, stage_dens;
+    cudaEvent_t ev_in_done = nullptr, ev_in_used = nullptr, ev_cells_ready = nullptr, ev_cells_done = nullptr,
+                ev_dens_ready = nullptr, ev_dens_done = nullptr;
     double phase_ms[PCG_N_PHASES] = {};
     uint64_t sweep_steps = 0, diff_steps = 0, mech_steps = 0;
 

@@ -135,9 +135,28 @@ pcg_status pcg_destroy(pcg_ctx* ctx)
     if (!ctx) return PCG_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (cudaStream_t c : {ctx->h2d, ctx->d2h})
+        if (c) {
+            cudaStreamSynchronize(c);
+            cudaStreamDestroy(c);
+        }
+    for (cudaEvent_t e : ctx->copy_ev)
+        if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->status) cudaFree(ctx->status);
     delete ctx;
+    return PCG_OK;
+}
+
+pcg_status pcg_join(pcg_ctx* ctx)
+{
+    if (!ctx) return PCG_ERR_INVALID;
+    const cudaStream_t cs[2] = {ctx->h2d, ctx->d2h};
+    for (int q = 0; q < 2; ++q) {
+        if (!cs[q]) continue;
+        PCG_CU(ctx, cudaEventRecord(ctx->copy_ev[q], cs[q]));
+        PCG_CU(ctx, cudaStreamWaitEvent(ctx->stream, ctx->copy_ev[q], 0));
+    }
     return PCG_OK;
 }
 
@@ -145,6 +164,8 @@ pcg_status pcg_sync(pcg_ctx* ctx)
 {
     if (!ctx) return PCG_ERR_INVALID;
     PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    for (cudaStream_t c : {ctx->h2d, ctx->d2h})
+        if (c) PCG_CU(ctx, cudaStreamSynchronize(c));
     unsigned st = 0;
     PCG_CU(ctx, cudaMemcpy(&st, ctx->status, sizeof st, cudaMemcpyDeviceToHost));
     if (st) {

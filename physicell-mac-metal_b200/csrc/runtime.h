@@ -21,6 +21,10 @@ struct pcg_ctx {
     int smem_optin = 0;
     uint64_t launches = 0;
     unsigned* status = nullptr;   // device status word (PCG_DEV_* bits)
+    // copy streams of the whole-batch transfers (made on first use): host
+    // copies run there, beside the kernels on 'stream'
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t copy_ev[2] = {};
 };
 
 namespace pcg {

@@ -99,6 +99,44 @@ def test_plane_pass_equals_separate_sweeps(ctx, pcg):
         assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32)), f"cells {i}"
 
 
+def test_whole_batch_transfers_pipelined(ctx, pcg):
+    """The whole-batch copies run on copy streams through staging buffers:
+    three rounds of upload -> steps -> download with no host wait between
+    calls give the same bits as with a wait after every call, and the cell
+    download is the per-instance downloads side by side."""
+    insts = small_mix(pcg, seed=13)
+    n_tot = sum(i.n_cells for i in insts)
+    runs = []
+    for wait in (False, True):
+        b = pcg.Batch(ctx, insts)
+        arena = b.layout(0)[3]
+        up = pcg.PinnedArray((28 * n_tot,))
+        outs = [(pcg.PinnedArray((28 * n_tot,)), pcg.PinnedArray((arena,))) for _ in range(3)]
+        b.download_all_cells(up.array)
+        ctx.sync()
+        up.array[3 * n_tot:4 * n_tot] += 0.25          # a host-side velocity change every round
+        for k in range(3):
+            for call in (lambda: b.upload_all_cells(up.array), lambda: b.step(6 + k),
+                         lambda: b.download_all_cells(outs[k][0].array),
+                         lambda: b.download_all_density(outs[k][1].array)):
+                call()
+                if wait:
+                    ctx.sync()
+        ctx.sync()
+        res = [(c.array.copy(), d.array.copy()) for c, d in outs]
+        if wait:
+            per = [b.cells(i) for i in range(len(insts))]
+            whole = np.concatenate([p.reshape(28, -1) for p in per], axis=1).ravel()
+            assert np.array_equal(whole.view(np.uint32), res[2][0].view(np.uint32))
+        runs.append(res)
+        for a in [up] + [x for o in outs for x in o]:
+            a.free()
+        b.close()
+    for k, ((ca, da), (cb, db)) in enumerate(zip(*runs)):
+        assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32)), f"cells round {k}"
+        assert np.array_equal(da.view(np.uint32), db.view(np.uint32)), f"density round {k}"
+
+
 def test_sweep_units_count_the_passes(ctx, pcg):
     """pcg_batch_sweep_units: with planes a 3-D instance's sub-step moves
     each voxel-substrate twice (x + y pass, z pass) and a 2-D one once;
