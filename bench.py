@@ -438,15 +438,15 @@ def main():
     ctx.sync()
     ph, nst = batch.phase_times(reset=True)
     batch.set_profile(False)
-    # dominant kernel: the fused x + y plane pass when the instances have
-    # planes (8 bytes per voxel-substrate it covers), else the three tile
-    # sweeps; "sweeps" adds the z pass (and any tile passes) of a sub-step
+    # dominant kernel: the plane kernel when every sweep launch of a sub-step
+    # is a plane pass (x + y planes, x-z planes; 8 bytes per voxel-substrate
+    # each covers), else all the sweep launches together
     plane_units, all_units = batch.sweep_units()
     sweep_ms = (ph["x_sweep"] + ph["y_sweep"] + ph["z_sweep"]) / max(nst, 1)
-    if plane_units:
-        kname = "k_sweep_planes (fused x+y Thomas pass)"
+    if plane_units and plane_units == all_units:
+        kname = "k_sweep_planes (x+y plane pass and z plane pass)"
         kbytes = 8 * plane_units
-        kms = ph["x_sweep"] / max(nst, 1)
+        kms = sweep_ms
     else:
         kname = "Thomas sweeps (x/y/z)"
         kbytes = 8 * all_units

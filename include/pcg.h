@@ -346,7 +346,8 @@ pcg_status pcg_batch_density_layout(pcg_batch* batch, uint32_t instance, uint64_
 pcg_status pcg_batch_totals(pcg_batch* batch, uint64_t* voxels, uint64_t* voxel_substrates, uint64_t* cells);
 /* Voxel-substrates the sweep launches of one sub-step cover, summed over the
  * launches (each launch reads and writes every value it covers once, 8
- * bytes): those of the fused x + y plane launches, and of all sweeps. */
+ * bytes): those of the plane launches (fused x + y planes, x-z planes of z
+ * lines), and of all sweeps. */
 pcg_status pcg_batch_sweep_units(pcg_batch* batch, uint64_t* plane_units, uint64_t* all_units);
 /* Kernel launches one main-loop sub-step issues: without / with a
  * mechanics step. */

@@ -655,8 +655,8 @@ class Batch:
         return v.value, vs.value, c.value
 
     def sweep_units(self):
-        """(plane_units, all_units): voxel-substrates one sub-step's fused
-        x + y plane launches / all sweep launches cover (8 bytes each)."""
+        """(plane_units, all_units): voxel-substrates one sub-step's plane
+        launches / all sweep launches cover (8 bytes each)."""
         pu, au = C.c_uint64(), C.c_uint64()
         self.ctx.check(lib().pcg_batch_sweep_units(self.h, C.byref(pu), C.byref(au)))
         return pu.value, au.value

@@ -504,6 +504,7 @@ pcg_status pcg_batch_sweep_units(pcg_batch* b, uint64_t* plane_units, uint64_t* 
     if (!b) return PCG_ERR_INVALID;
     uint64_t pu = 0;
     for (const auto& pl : b->b.d.planes) pu += pl.units;
+    for (const auto& pl : b->b.d.zplanes) pu += pl.units;
     if (plane_units) *plane_units = pu;
     if (all_units) *all_units = b->b.d.sweep_units_per_step();
     return PCG_OK;

@@ -697,9 +697,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_sweep_planes(const PlaneJob* 
     const PlaneJob jb = jobs[blockIdx.x];
     const uint32_t ii = jb.inst & kPlaneInstMask;
     if (mask && !(mask[ii] & STEP_DIFFUSE)) return;   // the whole CTA leaves together
-    const uint32_t nx = jb.nx, ny = jb.ny, P = row_smem_pitch(nx);
-    float* tx = pl + plane_data_floats(nx, ny);
-    float* ty = tx + tab_floats(nx);
+    const bool zk = (jb.inst & kPlaneZ) != 0;
+    const uint32_t nx = jb.nx, ny = jb.ny, P = plane_pitch(nx, zk);
+    float* tx = pl + plane_data_floats(nx, ny, zk);
+    float* ty = zk ? tx : tx + tab_floats(nx);
     const void* map = static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(jb.map) * 128;
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
@@ -707,10 +708,14 @@ __global__ void __launch_bounds__(kPlaneThreads) k_sweep_planes(const PlaneJob* 
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const uint32_t tbx = tab_floats(nx) * 4u, tby = tab_floats(ny) * 4u;
+        const uint32_t tbx = zk ? 0u : tab_floats(nx) * 4u, tby = tab_floats(ny) * 4u;
         mbar_arrive_expect_tx(bar, P * ny * 4u + tbx + tby);   // the whole box, fill included
-        tensor_load2(pl, map, 0, static_cast<int>(jb.row0), bar);
-        bulk_load(tx, tab + jb.tab_x, tbx, bar);
+        if (zk) {
+            tensor_load3(pl, map, 0, static_cast<int>(jb.row0), 0, bar);
+        } else {
+            tensor_load2(pl, map, 0, static_cast<int>(jb.row0), bar);
+            bulk_load(tx, tab + jb.tab_x, tbx, bar);
+        }
         bulk_load(ty, tab + jb.tab_y, tby, bar);
     }
     const bool got = mbar_wait(bar, 0, status);
@@ -729,15 +734,21 @@ __global__ void __launch_bounds__(kPlaneThreads) k_sweep_planes(const PlaneJob* 
     ry.fold = jb.fold_y;
     ry.T = jb.T_y;
     ry.dir = (jb.inst & kPlaneDirY) ? 1u : 0u;
-    for (uint32_t r = threadIdx.x; r < ny; r += blockDim.x) row_line(pl + r * P, rx, tx);
-    __syncthreads();
+    if (!zk) {
+        for (uint32_t r = threadIdx.x; r < ny; r += blockDim.x) row_line(pl + r * P, rx, tx);
+        __syncthreads();
+    }
+    // faces of the block's last sweep (2-D: y, 3-D: z): x faces, and a whole
+    // z plane on a y face
     const bool faces = apply_faces && (jb.inst & kPlaneFaces) != 0;
+    const bool slab_face = (jb.inst & kPlaneSlabFace) != 0;
     for (uint32_t c = threadIdx.x; c < nx; c += blockDim.x)
-        plane_col(pl + c, static_cast<int>(P), ry, ty, faces && (c == 0u || c + 1u == nx));
+        plane_col(pl + c, static_cast<int>(P), ry, ty, faces && (slab_face || c == 0u || c + 1u == nx));
     fence_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
-        tensor_store2(map, 0, static_cast<int>(jb.row0), pl);
+        if (zk) tensor_store3(map, 0, static_cast<int>(jb.row0), 0, pl);
+        else tensor_store2(map, 0, static_cast<int>(jb.row0), pl);
         bulk_commit();
         bulk_wait_read<0>();   // shared memory may be released once the store has read it
     }
@@ -977,6 +988,26 @@ bool encode_plane_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint
     const cuuint32_t box[2] = {P, ny};
     const cuuint32_t estr[2] = {1u, 1u};
     const CUresult r = fn(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, block, dims, strides,
+                          box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// x-z planes of one instance-substrate for the z lines: dims (x, y, z), box
+// round4(nx) x 1 x nz (the full x extent, one y, every z).
+bool encode_xz_plane_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t px)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    const uint32_t bx = (nx + 3u) & ~3u;
+    if (!fn || nx == 0 || bx > 256 || nz == 0 || nz > 256 || ny == 0 || (px & 3u) || px < nx ||
+        (reinterpret_cast<uintptr_t>(block) & 15u))
+        return false;
+    const cuuint64_t row = static_cast<cuuint64_t>(px) * 4u;
+    const cuuint64_t dims[3] = {nx, ny, nz};
+    const cuuint64_t strides[2] = {row, row * ny};
+    const cuuint32_t box[3] = {bx, 1u, nz};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    const CUresult r = fn(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, block, dims, strides,
                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;

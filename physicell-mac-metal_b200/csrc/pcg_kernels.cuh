@@ -82,7 +82,7 @@ enum : uint32_t { TILE_FACE = 1u, TILE_ROWS = 4u, TILE_TENSOR = 8u, TILE_AXIS_Z 
 constexpr uint32_t kTensorMaxN = 256;
 // Tensor-map slots per rule: x rules use slot 0, y / z rules one per
 // column-tile width (32, 16, 8).
-constexpr uint32_t kMapsPerRule = 3;
+constexpr uint32_t kMapsPerRule = 4;
 
 // x tiles moved with a 2-D tensor map land in shared memory as 32 rows of
 // row_smem_pitch(nx) floats: nx rounded up to 4 with an odd number of
@@ -129,31 +129,43 @@ enum : uint8_t { STEP_DIFFUSE = 1u, STEP_MECH = 2u };
 // Pipelined TMA sweeps: 'warps' warps per CTA, each with 'stages' shared
 // memory stages of 'stage_floats' floats, the last 'tab_floats' of which
 // hold the tile's coefficient table; 'grid' persistent CTAs.
-// One x-y plane (z slab k of one instance-substrate) for the fused x + y
-// sweep kernel: the plane tensor map (box row_smem_pitch(nx) x ny, slot 1
-// of the x rule), its first row k * ny, and both rules.
+// One plane for the plane sweep kernel, of width nx (columns) and height ny
+// (rows).  x-y jobs (z slab k of one instance-substrate): the plane tensor
+// map (box row_smem_pitch(nx) x ny, slot 1 of the x rule), first row
+// row0 = k * ny, x and y rules: every row, then every column is solved.
+// z jobs (kPlaneZ: the x-z plane y = row0): the 3-D map of slot 3 of the z
+// rule (box round4(nx) x 1 x nz), ny = nz, the z rule in the y fields:
+// every column (a z line) is solved.
 struct PlaneJob {
     uint32_t map;
     uint32_t row0;
     uint32_t nx, ny;
     uint32_t tab_x, tab_y;   // table offsets (floats)
     float fold_x, T_x, fold_y, T_y;
-    uint32_t inst;           // instance | kPlaneDirX | kPlaneDirY | kPlaneFaces
+    uint32_t inst;           // instance | kPlaneDirX | kPlaneDirY | kPlaneFaces | kPlaneZ | kPlaneSlabFace
     uint32_t _pad[5];
 };
 static_assert(sizeof(PlaneJob) == 64, "PlaneJob is 64 bytes");
 constexpr uint32_t kPlaneDirX = 1u << 31, kPlaneDirY = 1u << 30, kPlaneFaces = 1u << 29;
-constexpr uint32_t kPlaneInstMask = (1u << 29) - 1u;
+constexpr uint32_t kPlaneZ = 1u << 28;          // an x-z plane of z lines
+constexpr uint32_t kPlaneSlabFace = 1u << 27;   // z job: the plane is a y face of the block
+constexpr uint32_t kPlaneInstMask = (1u << 27) - 1u;
 constexpr uint32_t kPlaneThreads = 128;
-// Shared floats of a plane's data (rows rounded up to a whole chunk of 4,
-// which the column solve may touch; 128-byte multiple) and with both tables.
-__host__ __device__ constexpr uint32_t plane_data_floats(uint32_t nx, uint32_t ny)
+// Row pitch of a plane in shared memory: x-y planes row_smem_pitch(nx) (the
+// rows are solved with 16-byte accesses), z planes nx rounded up to 4.
+__host__ __device__ constexpr uint32_t plane_pitch(uint32_t nx, bool z)
 {
-    return (row_smem_pitch(nx) * ((ny + 3u) & ~3u) + 31u) / 32u * 32u;
+    return z ? ((nx + 3u) & ~3u) : row_smem_pitch(nx);
 }
-__host__ __device__ constexpr uint32_t plane_floats(uint32_t nx, uint32_t ny)
+// Shared floats of a plane's data (rows rounded up to a whole chunk of 4,
+// which the column solve may touch; 128-byte multiple) and with its tables.
+__host__ __device__ constexpr uint32_t plane_data_floats(uint32_t nx, uint32_t ny, bool z = false)
 {
-    return plane_data_floats(nx, ny) + tab_floats(nx) + tab_floats(ny);
+    return (plane_pitch(nx, z) * ((ny + 3u) & ~3u) + 31u) / 32u * 32u;
+}
+__host__ __device__ constexpr uint32_t plane_floats(uint32_t nx, uint32_t ny, bool z = false)
+{
+    return plane_data_floats(nx, ny, z) + (z ? 0u : tab_floats(nx)) + tab_floats(ny);
 }
 
 struct TmaCfg { int warps; int stages; int stage_floats; int grid; int tab_floats; };
@@ -176,6 +188,7 @@ cudaError_t launch_sweep_planes(cudaStream_t st, const PlaneJob* jobs, uint32_t 
 cudaError_t sweep_planes_prepare();
 size_t sweep_planes_smem(uint32_t floats);
 bool encode_plane_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint64_t rows, uint32_t px);
+bool encode_xz_plane_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t px);
 cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,
                              const float* tab, const void* tmaps, int apply_faces,
                              const uint8_t* mask, unsigned* status, TmaCfg cfg);

@@ -374,9 +374,11 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
         PCG_CU(ctx, cudaMemcpyAsync(rules.p, h_rules_.data(), h_rules_.size() * sizeof(LineRule), cudaMemcpyHostToDevice, ctx->stream));
     if (!h_tab_.empty())
         PCG_CU(ctx, cudaMemcpyAsync(tab.p, h_tab_.data(), h_tab_.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    // tensor maps, three 128-byte slots per rule (kMapsPerRule): x rules use
-    // slot 0 (2-D row map); y / z rules one 3-D column map per tile width
-    // (32, 16, 8 columns).  tensor_ok_ bit w: the slot-w map exists.
+    // tensor maps, four 128-byte slots per rule (kMapsPerRule): x rules use
+    // slot 0 (2-D row map) and slot 1 (x-y plane map); y / z rules one 3-D
+    // column map per tile width in slots 0-2 (32, 16, 8 columns), z rules
+    // the x-z plane map in slot 3.  tensor_ok_ bit w: the slot-w column map
+    // exists.
     tensor_ok_.assign(h_rules_.size(), 0);
     {
         std::vector<unsigned char> maps(std::max<size_t>(h_rules_.size(), 1) * kMapsPerRule * 128, 0);
@@ -418,6 +420,23 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
             }
             plane_inst_[i] = ok ? 1 : 0;
         }
+        // x-z plane maps (slot 3 of each z rule) for the z sweep
+        zplane_inst_.assign(inst.size(), 0);
+        for (size_t i = 0; use_planes && i < inst.size(); ++i) {
+            const DiffInstance& d = inst[i];
+            const uint32_t nx = d.g.nx, nz = d.g.nz;
+            if (d.ndim() < 3 || d.g.n_substrates == 0 || ((nx + 3u) & ~3u) > 256 || nz > 256 ||
+                sweep_planes_smem(plane_floats(nx, nz, true)) > kPlaneMaxSmem)
+                continue;
+            bool ok = true;
+            for (uint32_t s = 0; s < d.g.n_substrates && ok; ++s) {
+                const uint32_t rule = rule_of(i, s, 2);
+                unsigned char* m = maps.data() + static_cast<size_t>(rule) * kMapsPerRule * 128;
+                ok = encode_xz_plane_map(m + 3 * 128, dens.as<float>() + d.dens_off + s * d.pitch, nx, d.g.ny, nz,
+                                         d.px);
+            }
+            zplane_inst_[i] = ok ? 1 : 0;
+        }
         PCG_CU(ctx, tmaps.alloc(maps.size()));
         PCG_CU(ctx, cudaMemcpyAsync(tmaps.p, maps.data(), maps.size(), cudaMemcpyHostToDevice, ctx->stream));
     }
@@ -431,58 +450,19 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
     return build_planes();
 }
 
-// Plane jobs (one per z slab of each substrate of each plane instance),
-// grouped by shared-memory size so small planes are not charged the
-// largest plane's footprint, and the x / y tiles of the other instances.
-int Diffusion::build_planes()
+// Plane jobs grouped by shared-memory size, so small planes are not charged
+// the largest plane's footprint; largest planes first.
+static int plane_lists(pcg_ctx* ctx, std::vector<PlaneJob>* jobs, const uint32_t* fl, const uint64_t* un,
+                       int classes, std::vector<PlaneList>& out)
 {
-    planes.clear();
-    for (auto& r : rest) r.clear();
-    bool any = false;
-    for (uint8_t v : plane_inst_) any = any || v;
-    if (!any) return PCG_OK;
-    constexpr int kClasses = 3;
-    const size_t bounds[kClasses] = {28 * 1024, 56 * 1024, kPlaneMaxSmem};
-    std::vector<PlaneJob> jobs[kClasses];
-    uint32_t fl[kClasses] = {0, 0, 0};
-    uint64_t un[kClasses] = {0, 0, 0};
-    for (size_t i = 0; i < inst.size(); ++i) {
-        if (!plane_inst_[i]) continue;
-        const DiffInstance& d = inst[i];
-        const uint32_t nx = d.g.nx, ny = d.g.ny, pf = plane_floats(nx, ny);
-        int c = 0;
-        while (c + 1 < kClasses && sweep_planes_smem(pf) > bounds[c]) ++c;
-        for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
-            const uint32_t rx_i = rule_of(i, s, 0);
-            const LineRule& rx = h_rules_[rx_i];
-            const LineRule& ry = h_rules_[rule_of(i, s, 1)];
-            for (uint32_t k = 0; k < d.g.nz; ++k) {
-                PlaneJob j{};
-                j.map = rx_i * kMapsPerRule + 1;
-                j.row0 = k * ny;
-                j.nx = nx;
-                j.ny = ny;
-                j.tab_x = rx.tab;
-                j.tab_y = ry.tab;
-                j.fold_x = rx.fold;
-                j.T_x = rx.T;
-                j.fold_y = ry.fold;
-                j.T_y = ry.T;
-                j.inst = static_cast<uint32_t>(i) | (rx.dir ? kPlaneDirX : 0u) | (ry.dir ? kPlaneDirY : 0u) |
-                         ((d.ndim() == 2 && ry.dir) ? kPlaneFaces : 0u);
-                jobs[c].push_back(j);
-            }
-        }
-        fl[c] = std::max(fl[c], pf);
-        un[c] += d.nvox() * d.g.n_substrates;
-    }
     int nl = 0;
-    for (int c = 0; c < kClasses; ++c) nl += jobs[c].empty() ? 0 : 1;
-    planes.resize(nl);
+    for (int c = 0; c < classes; ++c) nl += jobs[c].empty() ? 0 : 1;
+    out.clear();
+    out.resize(nl);
     int q = 0;
-    for (int c = kClasses - 1; c >= 0; --c) {   // largest planes first
+    for (int c = classes - 1; c >= 0; --c) {
         if (jobs[c].empty()) continue;
-        PlaneList& pl = planes[q++];
+        PlaneList& pl = out[q++];
         pl.n = static_cast<uint32_t>(jobs[c].size());
         pl.floats = fl[c];
         pl.units = un[c];
@@ -490,11 +470,89 @@ int Diffusion::build_planes()
         PCG_CU(ctx, cudaMemcpyAsync(pl.jobs.p, jobs[c].data(), jobs[c].size() * sizeof(PlaneJob),
                                     cudaMemcpyHostToDevice, ctx->stream));
     }
-    for (int a = 0; a < 2; ++a) {
-        PCG_TRY(build_axis(a, &plane_inst_, rest[a]));
+    return PCG_OK;
+}
+
+// x-y plane jobs (one per z slab of each substrate of each plane instance),
+// x-z plane jobs (one per y of each substrate of each z-plane instance), and
+// the tiles of the instances without planes.
+int Diffusion::build_planes()
+{
+    planes.clear();
+    zplanes.clear();
+    for (auto& r : rest) r.clear();
+    constexpr int kClasses = 3;
+    const size_t bounds[kClasses] = {28 * 1024, 56 * 1024, kPlaneMaxSmem};
+    auto cls = [&](uint32_t pf) {
+        int c = 0;
+        while (c + 1 < kClasses && sweep_planes_smem(pf) > bounds[c]) ++c;
+        return c;
+    };
+    std::vector<PlaneJob> jobs[kClasses], zjobs[kClasses];
+    uint32_t fl[kClasses] = {0, 0, 0}, zfl[kClasses] = {0, 0, 0};
+    uint64_t un[kClasses] = {0, 0, 0}, zun[kClasses] = {0, 0, 0};
+    for (size_t i = 0; i < inst.size(); ++i) {
+        const DiffInstance& d = inst[i];
+        const uint32_t nx = d.g.nx, ny = d.g.ny, nz = d.g.nz;
+        if (plane_inst_[i]) {
+            const uint32_t pf = plane_floats(nx, ny);
+            const int c = cls(pf);
+            for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
+                const uint32_t rx_i = rule_of(i, s, 0);
+                const LineRule& rx = h_rules_[rx_i];
+                const LineRule& ry = h_rules_[rule_of(i, s, 1)];
+                for (uint32_t k = 0; k < nz; ++k) {
+                    PlaneJob j{};
+                    j.map = rx_i * kMapsPerRule + 1;
+                    j.row0 = k * ny;
+                    j.nx = nx;
+                    j.ny = ny;
+                    j.tab_x = rx.tab;
+                    j.tab_y = ry.tab;
+                    j.fold_x = rx.fold;
+                    j.T_x = rx.T;
+                    j.fold_y = ry.fold;
+                    j.T_y = ry.T;
+                    j.inst = static_cast<uint32_t>(i) | (rx.dir ? kPlaneDirX : 0u) | (ry.dir ? kPlaneDirY : 0u) |
+                             ((d.ndim() == 2 && ry.dir) ? kPlaneFaces : 0u);
+                    jobs[c].push_back(j);
+                }
+            }
+            fl[c] = std::max(fl[c], pf);
+            un[c] += d.nvox() * d.g.n_substrates;
+        }
+        if (zplane_inst_[i]) {
+            const uint32_t pf = plane_floats(nx, nz, true);
+            const int c = cls(pf);
+            for (uint32_t s = 0; s < d.g.n_substrates; ++s) {
+                const uint32_t rz_i = rule_of(i, s, 2);
+                const LineRule& rz = h_rules_[rz_i];
+                for (uint32_t y = 0; y < ny; ++y) {
+                    PlaneJob j{};
+                    j.map = rz_i * kMapsPerRule + 3;
+                    j.row0 = y;
+                    j.nx = nx;
+                    j.ny = nz;
+                    j.tab_y = rz.tab;
+                    j.fold_y = rz.fold;
+                    j.T_y = rz.T;
+                    j.inst = static_cast<uint32_t>(i) | kPlaneZ | (rz.dir ? (kPlaneDirY | kPlaneFaces) : 0u) |
+                             ((y == 0 || y + 1 == ny) ? kPlaneSlabFace : 0u);
+                    zjobs[c].push_back(j);
+                }
+            }
+            zfl[c] = std::max(zfl[c], pf);
+            zun[c] += d.nvox() * d.g.n_substrates;
+        }
+    }
+    PCG_TRY(plane_lists(ctx, jobs, fl, un, kClasses, planes));
+    PCG_TRY(plane_lists(ctx, zjobs, zfl, zun, kClasses, zplanes));
+    for (int a = 0; a < 3; ++a) {
+        if (!planes_for(a)) continue;
+        PCG_TRY(build_axis(a, a < 2 ? &plane_inst_ : &zplane_inst_, rest[a]));
         for (auto& l : rest[a]) PCG_TRY(config_list(l, 0));
     }
-    PCG_CU(ctx, sweep_planes_prepare());
+    if (!planes.empty() || !zplanes.empty()) PCG_CU(ctx, sweep_planes_prepare());
     return PCG_OK;
 }
 
@@ -682,7 +740,7 @@ int Diffusion::pin(int kind, int param)
     for (int a = 0; a < 3; ++a)
         for (auto& l : lists[a])
             if (l.kind == kind && l.n) PCG_TRY(config_list(l, param));
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < 3; ++a)
         for (auto& l : rest[a])
             if (l.kind == kind && l.n) PCG_TRY(config_list(l, param));
     return PCG_OK;
@@ -709,16 +767,22 @@ int Diffusion::launch_list(const SweepList& l, bool fuse, const uint8_t* mask)
     return PCG_OK;
 }
 
+int Diffusion::launch_planes(const std::vector<PlaneList>& pls, bool fuse, const uint8_t* mask)
+{
+    for (const auto& pl : pls) {
+        cudaError_t e = launch_sweep_planes(ctx->stream, pl.jobs.as<PlaneJob>(), pl.n, tab.as<float>(), tmaps.p,
+                                            pl.floats, fuse ? 1 : 0, mask, ctx->status);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "plane sweep launch");
+        ctx->launches++;
+    }
+    return PCG_OK;
+}
+
 int Diffusion::sweep(int axis, bool fuse, const uint8_t* mask)
 {
-    if (!planes.empty() && axis < 2) {
-        if (axis == 0)
-            for (const auto& pl : planes) {
-                cudaError_t e = launch_sweep_planes(ctx->stream, pl.jobs.as<PlaneJob>(), pl.n, tab.as<float>(),
-                                                    tmaps.p, pl.floats, fuse ? 1 : 0, mask, ctx->status);
-                if (e != cudaSuccess) return cuda_fail(ctx, e, "plane sweep launch");
-                ctx->launches++;
-            }
+    if (planes_for(axis)) {
+        if (axis == 0) PCG_TRY(launch_planes(planes, fuse, mask));
+        if (axis == 2) PCG_TRY(launch_planes(zplanes, fuse, mask));
         for (const auto& l : rest[axis]) PCG_TRY(launch_list(l, fuse, mask));
         return PCG_OK;
     }
@@ -730,9 +794,11 @@ uint64_t Diffusion::sweep_units_per_step() const
 {
     uint64_t u = 0;
     for (int a = 0; a < 3; ++a) {
-        if (!planes.empty() && a < 2) {
+        if (planes_for(a)) {
             if (a == 0)
                 for (const auto& pl : planes) u += pl.units;
+            if (a == 2)
+                for (const auto& pl : zplanes) u += pl.units;
             for (const auto& l : rest[a]) u += l.units;
         } else {
             for (const auto& l : lists[a]) u += l.units;
@@ -751,8 +817,9 @@ int Diffusion::launches_per_step(bool) const
 {
     int k = 0;
     for (int a = 0; a < 3; ++a) {
-        if (!planes.empty() && a < 2) {
+        if (planes_for(a)) {
             if (a == 0) k += static_cast<int>(planes.size());
+            if (a == 2) k += static_cast<int>(zplanes.size());
             for (const auto& l : rest[a]) k += l.n > 0 ? 1 : 0;
         } else {
             for (const auto& l : lists[a]) k += l.n > 0 ? 1 : 0;
@@ -848,9 +915,10 @@ uint64_t Diffusion::device_bytes() const
     uint64_t b = dens.bytes + rules.bytes + tab.bytes + faces.bytes;
     for (int a = 0; a < 3; ++a)
         for (const auto& l : lists[a]) b += l.tiles.bytes;
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < 3; ++a)
         for (const auto& l : rest[a]) b += l.tiles.bytes;
     for (const auto& pl : planes) b += pl.jobs.bytes;
+    for (const auto& pl : zplanes) b += pl.jobs.bytes;
     return b;
 }
 
@@ -859,8 +927,9 @@ std::string Diffusion::describe() const
     std::ostringstream o;
     const char* ax = "xyz";
     for (const auto& pl : planes) o << "xy:planes(jobs=" << pl.n << ",smem=" << sweep_planes_smem(pl.floats) << ") ";
+    for (const auto& pl : zplanes) o << "z:xz-planes(jobs=" << pl.n << ",smem=" << sweep_planes_smem(pl.floats) << ") ";
     for (int a = 0; a < 3; ++a)
-        for (const auto& l : (!planes.empty() && a < 2) ? rest[a] : lists[a]) {
+        for (const auto& l : planes_for(a) ? rest[a] : lists[a]) {
             if (l.n == 0) continue;
             o << ax[a] << ":";
             if (l.kind != 2)
@@ -903,7 +972,7 @@ int Diffusion::tune()
     int rc = PCG_OK;
     for (int a = 0; a < 3 && rc == PCG_OK; ++a) {
         // the lists a sub-step launches
-        std::vector<SweepList>& la = (!planes.empty() && a < 2) ? rest[a] : lists[a];
+        std::vector<SweepList>& la = planes_for(a) ? rest[a] : lists[a];
         if (la.empty()) continue;
         SweepList& l = la[0];
         if (l.n == 0) continue;

@@ -173,7 +173,10 @@ public:
     // as one plane pass (planes); rest[0] / rest[1] hold the x / y tiles of
     // the others.  sweep(0) then launches planes + rest[0], sweep(1) rest[1].
     std::vector<PlaneList> planes;
-    std::vector<SweepList> rest[2];
+    // 3-D instances whose x-z planes fit run their z sweep as one pass per
+    // x-z plane (zplanes); rest[2] holds the z tiles of the others.
+    std::vector<PlaneList> zplanes;
+    std::vector<SweepList> rest[3];
     bool use_planes = true;            // set before build()
     std::string shapes;
 
@@ -201,6 +204,9 @@ private:
     int build_axis(int axis, const std::vector<uint8_t>* skip, std::vector<SweepList>& ls);
     int build_planes();
     std::vector<uint8_t> plane_inst_;    // instance's x + y sweeps run as planes
+    std::vector<uint8_t> zplane_inst_;   // instance's z sweep runs as x-z planes
+    int launch_planes(const std::vector<PlaneList>& pls, bool fuse_faces, const uint8_t* mask);
+    bool planes_for(int axis) const { return axis < 2 ? !planes.empty() : !zplanes.empty(); }
     int default_configs(int axis);
     int config_list(SweepList& l, int param);
     int launch_list(const SweepList& l, bool fuse_faces, const uint8_t* mask);

@@ -139,15 +139,15 @@ def test_whole_batch_transfers_pipelined(ctx, pcg):
 
 def test_sweep_units_count_the_passes(ctx, pcg):
     """pcg_batch_sweep_units: with planes a 3-D instance's sub-step moves
-    each voxel-substrate twice (x + y pass, z pass) and a 2-D one once;
-    without planes three and two times."""
+    each voxel-substrate twice (x + y plane pass, z plane pass) and a 2-D
+    one once, all in plane launches; without planes three and two times."""
     insts = small_mix(pcg, seed=11)
     per_pass = {True: 0, False: 0}          # 3-D?, voxel-substrates
     for inst in insts:
         g = inst.grid
         per_pass[g.nz > 1] += g.nx * g.ny * g.nz * g.n_substrates
-    for planes, want in ((True, (per_pass[True] + per_pass[False], 2 * per_pass[True] + per_pass[False])),
-                         (False, (0, 3 * per_pass[True] + 2 * per_pass[False]))):
+    with_planes = 2 * per_pass[True] + per_pass[False]
+    for planes, want in ((True, (with_planes, with_planes)), (False, (0, 3 * per_pass[True] + 2 * per_pass[False]))):
         b = pcg.Batch(ctx, insts, autotune=False, planes=planes)
         assert b.sweep_units() == want
         b.close()
