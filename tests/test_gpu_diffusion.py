@@ -48,6 +48,8 @@ CASES = [
     ("3d_w16_groups", 44, 13, 9, [O2, (4e3, 0.3, True, 2.0)]),  # 12-column remainder: 16-wide, 2-slab tiles
     ("3d_x70", 70, 9, 12, [O2, (4e3, 0.3, True, 2.0)]),         # z: 32-wide tiles + a 6-column remainder
     ("3d_x130", 130, 6, 8, [(2e4, 0.1, True, 5.0)]),            # x rows past 128, z remainder of 2 columns
+    ("3d_plane_150", 150, 150, 5, [O2]),                          # x-y planes of ~93 KB: 2 CTAs per SM
+    ("3d_rows_200", 40, 200, 3, [O2, (3e3, 0.2, False, 0.0)]),   # 200 rows: two per plane thread
 ]
 
 
