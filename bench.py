@@ -27,7 +27,7 @@ ranks by predicted bytes (greedy packing, computed identically on every
 rank) and each rank runs its shard as one batch, with no collective on the
 data path: weak scaling.
 --impl reference times the CPU port alone (the reference's shaders exist
-only for Apple Metal).
+only for Apple Metal, which this machine does not have).
 """
 import argparse
 import importlib.util

@@ -1,7 +1,7 @@
 /*
- * pcg_port.c — multi-threaded FP32 CPU port of the hot path (TEST AND
- * BASELINE INFRASTRUCTURE; only the cpu_baseline leg and the reference arm
- * of bench.py time it, and tests check it against the oracle).
+ * pcg_port.c — multi-threaded FP32 CPU port of the hot path (test and CPU
+ * reference-timing infrastructure; only the cpu_baseline leg and the
+ * reference arm of bench.py time it, and tests check it against the oracle).
  *
  * The arithmetic is the reference's FP32 shader math:
  *   sweeps       shaders/diffusion_2d.metal:28-292 (extended to z, 3-D rule
