@@ -142,6 +142,13 @@ pcg_status pcg_destroy(pcg_ctx* ctx)
         }
     for (cudaEvent_t e : ctx->copy_ev)
         if (e) cudaEventDestroy(e);
+    for (cudaStream_t f : ctx->fork_st)
+        if (f) {
+            cudaStreamSynchronize(f);
+            cudaStreamDestroy(f);
+        }
+    for (cudaEvent_t e : ctx->fork_ev)
+        if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->status) cudaFree(ctx->status);
     delete ctx;

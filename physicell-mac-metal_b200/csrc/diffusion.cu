@@ -1017,7 +1017,20 @@ size_t sweep_planes_smem(uint32_t floats) { return 128 + static_cast<size_t>(flo
 
 cudaError_t sweep_planes_prepare()
 {
-    return allow_max_smem(reinterpret_cast<const void*>(k_sweep_planes));
+    const void* fn = reinterpret_cast<const void*>(k_sweep_planes);
+    cudaError_t e = allow_max_smem(fn);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    return e;
+}
+
+int sweep_planes_ctas(uint32_t floats)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_planes, kPlaneThreads, sweep_planes_smem(floats)) !=
+        cudaSuccess)
+        return 0;
+    return n;
 }
 
 cudaError_t launch_sweep_planes(cudaStream_t st, const PlaneJob* jobs, uint32_t njobs, const float* tab,

@@ -183,10 +183,14 @@ int sweep_tma_occupancy(bool rows, int warps, int nstages, int stage_floats);   
 cudaError_t launch_sweep_planes(cudaStream_t st, const PlaneJob* jobs, uint32_t njobs, const float* tab,
                                 const void* tmaps, uint32_t floats, int apply_faces, const uint8_t* mask,
                                 unsigned* status);
-// Lets the plane kernel use the opt-in shared memory (current device; once
-// per device, outside stream capture).
+// Lets the plane kernel use the opt-in shared memory, with the largest
+// shared-memory carveout, so launches of every plane size share one SM
+// configuration (current device; once per device, outside stream capture).
 cudaError_t sweep_planes_prepare();
 size_t sweep_planes_smem(uint32_t floats);
+// Plane CTAs an SM holds at once for planes of 'floats' (0 = does not fit);
+// sweep_planes_prepare() first.
+int sweep_planes_ctas(uint32_t floats);
 bool encode_plane_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint64_t rows, uint32_t px);
 bool encode_xz_plane_map(void* map128, float* block, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t px);
 cudaError_t launch_sweep_tma(cudaStream_t st, bool rows, float* dens, const SweepTile* tiles, uint32_t ntiles,

@@ -481,16 +481,18 @@ int Diffusion::build_planes()
     planes.clear();
     zplanes.clear();
     for (auto& r : rest) r.clear();
-    constexpr int kClasses = 3;
-    const size_t bounds[kClasses] = {28 * 1024, 56 * 1024, kPlaneMaxSmem};
-    auto cls = [&](uint32_t pf) {
-        int c = 0;
-        while (c + 1 < kClasses && sweep_planes_smem(pf) > bounds[c]) ++c;
-        return c;
-    };
+    bool any = false;
+    for (size_t i = 0; i < inst.size(); ++i) any = any || plane_inst_[i] || zplane_inst_[i];
+    if (any) PCG_CU(ctx, sweep_planes_prepare());   // before the occupancy queries
+    // Classes by the plane CTAs an SM holds for the plane's shared memory
+    // (class kMaxCtas - k for k CTAs), so each plane runs at the occupancy
+    // its own size allows; a class launches with its largest plane's size,
+    // which by construction allows the same k.
+    constexpr int kMaxCtas = 32, kClasses = kMaxCtas;
+    auto cls = [&](uint32_t pf) { return kMaxCtas - std::min(std::max(sweep_planes_ctas(pf), 1), kMaxCtas); };
     std::vector<PlaneJob> jobs[kClasses], zjobs[kClasses];
-    uint32_t fl[kClasses] = {0, 0, 0}, zfl[kClasses] = {0, 0, 0};
-    uint64_t un[kClasses] = {0, 0, 0}, zun[kClasses] = {0, 0, 0};
+    uint32_t fl[kClasses] = {}, zfl[kClasses] = {};
+    uint64_t un[kClasses] = {}, zun[kClasses] = {};
     for (size_t i = 0; i < inst.size(); ++i) {
         const DiffInstance& d = inst[i];
         const uint32_t nx = d.g.nx, ny = d.g.ny, nz = d.g.nz;
@@ -552,8 +554,7 @@ int Diffusion::build_planes()
         PCG_TRY(build_axis(a, a < 2 ? &plane_inst_ : &zplane_inst_, rest[a]));
         for (auto& l : rest[a]) PCG_TRY(config_list(l, 0));
     }
-    if (!planes.empty() || !zplanes.empty()) PCG_CU(ctx, sweep_planes_prepare());
-    return PCG_OK;
+    return prepare_forks();
 }
 
 // Copy a line rule into a tile descriptor.
@@ -767,13 +768,47 @@ int Diffusion::launch_list(const SweepList& l, bool fuse, const uint8_t* mask)
     return PCG_OK;
 }
 
+// Side streams and their events (made on first use, outside capture).
+static int ensure_forks(pcg_ctx* ctx, int n)
+{
+    for (int q = 0; q < n; ++q)
+        if (!ctx->fork_st[q]) PCG_CU(ctx, cudaStreamCreateWithFlags(&ctx->fork_st[q], cudaStreamNonBlocking));
+    for (int q = 0; q <= n; ++q)
+        if (!ctx->fork_ev[q]) PCG_CU(ctx, cudaEventCreateWithFlags(&ctx->fork_ev[q], cudaEventDisableTiming));
+    return PCG_OK;
+}
+
+int Diffusion::prepare_forks()
+{
+    const size_t n = std::max(planes.size(), zplanes.size());
+    return n > 1 ? ensure_forks(ctx, std::min<int>(static_cast<int>(n) - 1, pcg_ctx::kForks)) : PCG_OK;
+}
+
+// The plane lists of a pass hold disjoint planes: the first list runs on the
+// context stream, the others on side streams forked from it, and the context
+// stream waits for all of them.  One list's last CTAs then overlap the next
+// list's first, where launches in sequence would drain the GPU between them.
 int Diffusion::launch_planes(const std::vector<PlaneList>& pls, bool fuse, const uint8_t* mask)
 {
-    for (const auto& pl : pls) {
-        cudaError_t e = launch_sweep_planes(ctx->stream, pl.jobs.as<PlaneJob>(), pl.n, tab.as<float>(), tmaps.p,
-                                            pl.floats, fuse ? 1 : 0, mask, ctx->status);
+    const int side = std::min<int>(static_cast<int>(pls.size()) - 1, pcg_ctx::kForks);
+    if (side > 0) {
+        for (int q = 0; q <= side; ++q)
+            if (!ctx->fork_ev[q] || (q < side && !ctx->fork_st[q]))
+                return fail(ctx, PCG_ERR_INVALID, "plane side streams were not made");
+        PCG_CU(ctx, cudaEventRecord(ctx->fork_ev[0], ctx->stream));
+        for (int q = 0; q < side; ++q) PCG_CU(ctx, cudaStreamWaitEvent(ctx->fork_st[q], ctx->fork_ev[0], 0));
+    }
+    for (size_t k = 0; k < pls.size(); ++k) {
+        const PlaneList& pl = pls[k];
+        const cudaStream_t st = k == 0 ? ctx->stream : ctx->fork_st[(k - 1) % side];
+        cudaError_t e = launch_sweep_planes(st, pl.jobs.as<PlaneJob>(), pl.n, tab.as<float>(), tmaps.p, pl.floats,
+                                            fuse ? 1 : 0, mask, ctx->status);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "plane sweep launch");
         ctx->launches++;
+    }
+    for (int q = 0; q < side; ++q) {
+        PCG_CU(ctx, cudaEventRecord(ctx->fork_ev[1 + q], ctx->fork_st[q]));
+        PCG_CU(ctx, cudaStreamWaitEvent(ctx->stream, ctx->fork_ev[1 + q], 0));
     }
     return PCG_OK;
 }

@@ -25,6 +25,13 @@ struct pcg_ctx {
     // copies run there, beside the kernels on 'stream'
     cudaStream_t h2d = nullptr, d2h = nullptr;
     cudaEvent_t copy_ev[2] = {};
+    // side streams for the independent launches of one phase (made on first
+    // use): they fork from 'stream' at an event and 'stream' waits for each
+    // of them before the phase's next launch, so captured graphs hold them
+    // as parallel branches
+    static constexpr int kForks = 8;
+    cudaStream_t fork_st[kForks] = {};
+    cudaEvent_t fork_ev[kForks + 1] = {};   // [0] fork, [1 + q] join of side stream q
 };
 
 namespace pcg {
@@ -140,7 +147,8 @@ struct DiffInstance {
     int ndim() const { return g.nz > 1 ? 3 : 2; }
 };
 
-// Fused x + y plane jobs launched together (one shared-memory size).
+// Plane jobs launched together: the planes whose shared memory allows the
+// same number of CTAs per SM, launched with the largest one's size.
 struct PlaneList {
     DevBuf jobs;
     uint32_t n = 0;
@@ -206,6 +214,7 @@ private:
     std::vector<uint8_t> plane_inst_;    // instance's x + y sweeps run as planes
     std::vector<uint8_t> zplane_inst_;   // instance's z sweep runs as x-z planes
     int launch_planes(const std::vector<PlaneList>& pls, bool fuse_faces, const uint8_t* mask);
+    int prepare_forks();   // the side streams launch_planes forks to
     bool planes_for(int axis) const { return axis < 2 ? !planes.empty() : !zplanes.empty(); }
     int default_configs(int axis);
     int config_list(SweepList& l, int param);
