@@ -92,6 +92,11 @@ int pcg_abi_version(void);
 pcg_status pcg_create(int device, pcg_ctx** out);
 /* Use an existing CUDA stream (cudaStream_t passed as void*). */
 pcg_status pcg_create_on_stream(int device, void* stream, pcg_ctx** out);
+/* Drops the caller's reference.  Every object made on the context (me,
+ * cells, mech, motility, batch, server, snapshot) holds one too, so the
+ * context, its streams and its device status word are freed when the last
+ * of them is destroyed: objects may be destroyed in any order.  The context
+ * must not be used through this handle afterwards. */
 pcg_status pcg_destroy(pcg_ctx* ctx);
 /* MetalContext::waitForCompletion (metal_context.mm:448-461); also reports
  * PCG_ERR_DEVICE when a kernel stopped early since the last sync. */

@@ -335,14 +335,18 @@ pcg_status pcg_batch_create(pcg_ctx* ctx, const pcg_instance_desc* inst, uint32_
         delete b;
         return rc;
     }
+    ctx_retain(ctx);
     *out = b;
     return PCG_OK;
 }
 
 pcg_status pcg_batch_destroy(pcg_batch* b)
 {
-    if (b) cudaStreamSynchronize(b->b.ctx->stream);
+    if (!b) return PCG_OK;
+    pcg_ctx* ctx = b->b.ctx;
+    cudaStreamSynchronize(ctx->stream);
     delete b;
+    ctx_release(ctx);
     return PCG_OK;
 }
 

@@ -70,7 +70,42 @@ int check_mech(pcg_ctx* ctx, const pcg_mechanics_params* p)
     return PCG_OK;
 }
 
+// Frees the context once nothing refers to it any more.
+void ctx_free(pcg_ctx* ctx)
+{
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (cudaStream_t c : {ctx->h2d, ctx->d2h})
+        if (c) {
+            cudaStreamSynchronize(c);
+            cudaStreamDestroy(c);
+        }
+    for (cudaEvent_t e : ctx->copy_ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t f : ctx->fork_st)
+        if (f) {
+            cudaStreamSynchronize(f);
+            cudaStreamDestroy(f);
+        }
+    for (cudaEvent_t e : ctx->fork_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->status) cudaFree(ctx->status);
+    delete ctx;
+}
+
 }  // namespace
+
+namespace pcg {
+
+void ctx_retain(pcg_ctx* ctx) { ctx->refs.fetch_add(1, std::memory_order_relaxed); }
+
+void ctx_release(pcg_ctx* ctx)
+{
+    if (ctx->refs.fetch_sub(1, std::memory_order_acq_rel) == 1) ctx_free(ctx);
+}
+
+}  // namespace pcg
 
 extern "C" {
 
@@ -132,26 +167,7 @@ pcg_status pcg_create_on_stream(int device, void* stream, pcg_ctx** out) { retur
 
 pcg_status pcg_destroy(pcg_ctx* ctx)
 {
-    if (!ctx) return PCG_OK;
-    cudaSetDevice(ctx->device);
-    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (cudaStream_t c : {ctx->h2d, ctx->d2h})
-        if (c) {
-            cudaStreamSynchronize(c);
-            cudaStreamDestroy(c);
-        }
-    for (cudaEvent_t e : ctx->copy_ev)
-        if (e) cudaEventDestroy(e);
-    for (cudaStream_t f : ctx->fork_st)
-        if (f) {
-            cudaStreamSynchronize(f);
-            cudaStreamDestroy(f);
-        }
-    for (cudaEvent_t e : ctx->fork_ev)
-        if (e) cudaEventDestroy(e);
-    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
-    if (ctx->status) cudaFree(ctx->status);
-    delete ctx;
+    if (ctx) pcg::ctx_release(ctx);
     return PCG_OK;
 }
 
@@ -226,13 +242,17 @@ pcg_status pcg_me_create(pcg_ctx* ctx, const pcg_grid_params* grid, const pcg_su
         delete me;
         return rc;
     }
+    ctx_retain(ctx);
     *out = me;
     return PCG_OK;
 }
 
 pcg_status pcg_me_destroy(pcg_me* me)
 {
+    if (!me) return PCG_OK;
+    pcg_ctx* ctx = me->ctx;
     delete me;
+    ctx_release(ctx);
     return PCG_OK;
 }
 
@@ -350,13 +370,17 @@ pcg_status pcg_cells_create(pcg_ctx* ctx, uint32_t max_cells, uint32_t S, pcg_ce
     }
     c->c.has_active = false;
     c->c.h_inst[0].S = S;
+    ctx_retain(ctx);
     *out = c;
     return PCG_OK;
 }
 
 pcg_status pcg_cells_destroy(pcg_cells* c)
 {
+    if (!c) return PCG_OK;
+    pcg_ctx* ctx = c->ctx;
     delete c;
+    ctx_release(ctx);
     return PCG_OK;
 }
 
@@ -451,13 +475,17 @@ pcg_status pcg_mech_create(pcg_ctx* ctx, const pcg_mechanics_params* p, float x_
         delete m;
         return rc;
     }
+    ctx_retain(ctx);
     *out = m;
     return PCG_OK;
 }
 
 pcg_status pcg_mech_destroy(pcg_mech* m)
 {
+    if (!m) return PCG_OK;
+    pcg_ctx* ctx = m->ctx;
     delete m;
+    ctx_release(ctx);
     return PCG_OK;
 }
 

@@ -222,6 +222,7 @@ pcg_status pcg_motility_create(pcg_ctx* ctx, uint32_t max_cells, uint32_t n_subs
         delete m;
         return cuda_fail(ctx, e, "motility allocation");
     }
+    ctx_retain(ctx);
     *out = m;
     return PCG_OK;
 }
@@ -229,7 +230,9 @@ pcg_status pcg_motility_create(pcg_ctx* ctx, uint32_t max_cells, uint32_t n_subs
 pcg_status pcg_motility_destroy(pcg_motility* m)
 {
     if (!m) return PCG_ERR_INVALID;
+    pcg_ctx* ctx = m->ctx;
     delete m;
+    ctx_release(ctx);
     return PCG_OK;
 }
 

@@ -3,6 +3,7 @@
 // and the server, launch-shape selection and the autotuner.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <memory>
@@ -32,11 +33,17 @@ struct pcg_ctx {
     static constexpr int kForks = 8;
     cudaStream_t fork_st[kForks] = {};
     cudaEvent_t fork_ev[kForks + 1] = {};   // [0] fork, [1 + q] join of side stream q
+    // the owner's reference (dropped by pcg_destroy) plus one per live object
+    // made on this context: the context, its streams and its status word are
+    // freed with the last reference, so objects may be destroyed after it
+    std::atomic<int> refs{1};
 };
 
 namespace pcg {
 
 int fail(pcg_ctx* ctx, int code, const std::string& msg);
+void ctx_retain(pcg_ctx* ctx);    // an object made on ctx holds it
+void ctx_release(pcg_ctx* ctx);   // ... and lets it go after its own teardown
 int cuda_fail(pcg_ctx* ctx, cudaError_t e, const char* what);
 
 #define PCG_CU(ctx, call)                                                   \

@@ -131,6 +131,7 @@ pcg_status pcg_serve_create(pcg_ctx* ctx, const pcg_serve_options* opt, pcg_serv
     if (opt) s->opt = *opt;
     if (s->opt.budget_bytes == 0) s->opt.budget_bytes = 150ull * 1000 * 1000 * 1000;
     if (s->opt.steps_per_tick == 0) s->opt.steps_per_tick = 100;
+    ctx_retain(ctx);
     *out = s;
     return PCG_OK;
 }
@@ -138,8 +139,10 @@ pcg_status pcg_serve_create(pcg_ctx* ctx, const pcg_serve_options* opt, pcg_serv
 pcg_status pcg_serve_destroy(pcg_server* s)
 {
     if (!s) return PCG_OK;
-    cudaStreamSynchronize(s->ctx->stream);
+    pcg_ctx* ctx = s->ctx;
+    cudaStreamSynchronize(ctx->stream);
     delete s;
+    ctx_release(ctx);
     return PCG_OK;
 }
 

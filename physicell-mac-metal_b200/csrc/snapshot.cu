@@ -273,6 +273,7 @@ pcg_status pcg_snapshot_create(pcg_ctx* ctx, pcg_snapshot** out)
         delete s;
         return cuda_fail(ctx, e, "snapshot stream");
     }
+    ctx_retain(ctx);
     *out = s;
     return PCG_OK;
 }
@@ -297,7 +298,9 @@ pcg_status pcg_snapshot_destroy(pcg_snapshot* s)
     cudaEventDestroy(s->queued);
     cudaEventDestroy(s->built);
     cudaStreamDestroy(s->st);
+    pcg_ctx* ctx = s->ctx;
     delete s;
+    ctx_release(ctx);
     return rc;
 }
 
