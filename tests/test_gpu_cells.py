@@ -85,6 +85,31 @@ def test_bins_sort_start_and_neighbours_exact(ctx, pcg, po, two_d, n, dense):
     assert np.all(np.abs(p - pr) <= 1e-5 * np.maximum(np.abs(pr), 1.0))
 
 
+@pytest.mark.parametrize("n", [200_000, 1_500_000], ids=["200k", "1.5M"])
+def test_sort_and_start_many_tiles(ctx, pcg, po, n):
+    """The stable radix sort over hundreds of 2048-key tiles per pass (a 3 mm
+    domain: 100^3 mechanics voxels, 20-bit keys, three passes): bins,
+    cell-start table and permutation bit-exact against the oracle."""
+    rng = np.random.default_rng(77 + n % 1000)
+    dom = (0.0, 3000.0, 0.0, 3000.0, 0.0, 3000.0)
+    soa = make_cells(rng, n, n, (1500.0, 1500.0, 1500.0), 1400.0, False)
+    mp = pcg.mech_params_for_domain(*dom, False, 0.1)
+    om = po.mech_params(*dom, False, 0.1)
+    origin = (dom[0], dom[2], dom[4])
+    assert po.mech_nvox(om) >= 1 << 17   # more than two 8-bit digits of key
+    cells = pcg.Cells(ctx, n, 1)
+    cells.upload(soa, n, n)
+    mech = pcg.CellMechanics(ctx, mp, origin, n)
+    mech.computeForces(cells)
+    got = cells.download(n)
+    start, order = mech.syncHashPointers(n)
+    key = po.mech_bin(soa.copy(), n, n, om, origin)
+    oorder, ostart = po.mech_sort(key, om)
+    assert np.array_equal(got[27 * n:28 * n].view(np.uint32), key)
+    assert np.array_equal(start, ostart)
+    assert np.array_equal(order, oorder)
+
+
 def test_integrate_bit_exact_on_same_velocity(ctx, pcg, po):
     n = 2000
     soa, mp, om, origin = setup_mech(pcg, po, False, n, 3)
