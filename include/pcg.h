@@ -168,7 +168,33 @@ pcg_status pcg_cells_download_fields(pcg_cells* cells, uint32_t first, uint32_t 
 pcg_status pcg_cells_set_secretion(pcg_cells* cells, const double* secretion, const double* uptake,
                                    const double* saturation, const double* net_export,
                                    const uint8_t* active);
+/* Read-back of the rates and active flags pcg_cells_set_secretion set (and
+ * removals and appends moved): n_cells * S doubles each, n_cells flags (any
+ * may be NULL). */
+pcg_status pcg_cells_download_secretion(pcg_cells* cells, double* secretion, double* uptake, double* saturation,
+                                        double* net_export, uint8_t* active);
 pcg_status pcg_cells_count(pcg_cells* cells, uint32_t* n_cells);
+/* Dead-cell compaction on the device, without a re-upload: CellData::
+ * removeCell (src/cell_data.cpp:408-498, the last cell moved into the
+ * freed place) for each of 'indices' in descending order, indices at or
+ * past the current count skipped -- phase 3 of updatePhenotypes
+ * (src/cell_phenotype.cpp:837-844).  Every moved cell takes its 28 SoA
+ * fields, its per-substrate rates and its active flag along; the count
+ * drops by the number removed.  One launch (pcg_removal_plan's moves). */
+pcg_status pcg_cells_remove(pcg_cells* cells, const uint32_t* indices, uint32_t count);
+/* The same removal as a list of moves, on the host only (no device work),
+ * for the CPU-only per-cell arrays a host keeps: dest[k] receives the cell
+ * that started at src[k], every other place below *n_final keeps its cell.
+ * dest and src hold at least 'count' entries. */
+pcg_status pcg_removal_plan(uint32_t n_cells, const uint32_t* indices, uint32_t count, uint32_t* dest,
+                            uint32_t* src, uint32_t* n_moves, uint32_t* n_final);
+/* Appends 'count' cells after the current ones, as CellData::addCell
+ * (src/cell_data.cpp:398-406) places new and daughter cells: their 28
+ * fields from a host SoA of field stride soa_max_cells, their per-substrate
+ * rates [cell * S + s] (NULL = zeros) and active flags (NULL = active). */
+pcg_status pcg_cells_append(pcg_cells* cells, const float* soa, uint32_t count, uint32_t soa_max_cells,
+                            const double* secretion, const double* uptake, const double* saturation,
+                            const double* net_export, const uint8_t* active);
 pcg_status pcg_cells_device_soa(pcg_cells* cells, float** dptr, uint32_t* max_cells);
 
 /* ------------------------------------------------------------------------

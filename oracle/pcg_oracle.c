@@ -455,6 +455,43 @@ void or_voxel_refresh(float* soa, uint32_t max_cells, uint32_t n_cells, const or
 }
 
 /* ------------------------------------------------------------------ */
+/* Dead-cell compaction (cell_phenotype.cpp:837-844, cell_data.cpp:408-498) */
+/* ------------------------------------------------------------------ */
+
+static int cmp_desc_u32(const void* a, const void* b)
+{
+    const uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
+    return x < y ? 1 : (x > y ? -1 : 0);
+}
+
+uint32_t or_cells_remove(float* soa, uint32_t max_cells, uint32_t n_cells, uint32_t S, double* sec, double* upt,
+                         double* sat, double* ne, uint8_t* active, const uint32_t* indices, uint32_t count)
+{
+    uint32_t* r = (uint32_t*)malloc((count ? count : 1) * sizeof(uint32_t));
+    if (!r) return n_cells;
+    if (count) memcpy(r, indices, count * sizeof(uint32_t));
+    qsort(r, count, sizeof(uint32_t), cmp_desc_u32);
+    uint32_t* u = (uint32_t*)soa;
+    double* rates[4] = {sec, upt, sat, ne};
+    uint32_t num = n_cells;
+    for (uint32_t q = 0; q < count; q++) {
+        const uint32_t idx = r[q];
+        if (idx >= num) continue;
+        const uint32_t last = num - 1;
+        if (idx != last) {
+            for (int f = 0; f < OR_NUM_FIELDS; f++) u[(size_t)f * max_cells + idx] = u[(size_t)f * max_cells + last];
+            for (int a = 0; a < 4; a++)
+                if (rates[a])
+                    for (uint32_t s = 0; s < S; s++) rates[a][(size_t)idx * S + s] = rates[a][(size_t)last * S + s];
+            if (active) active[idx] = active[last];
+        }
+        num--;
+    }
+    free(r);
+    return num;
+}
+
+/* ------------------------------------------------------------------ */
 /* Whole step (main.mm:341-391)                                         */
 /* ------------------------------------------------------------------ */
 

@@ -151,6 +151,15 @@ void or_mech_integrate(float* soa, uint32_t max_cells, uint32_t n_cells, const o
  * voxel_index = Microenvironment::voxelIndex(x, y, z) (microenvironment.mm:261-269). */
 void or_voxel_refresh(float* soa, uint32_t max_cells, uint32_t n_cells, const or_grid* g);
 
+/* Dead-cell compaction: phase 3 of updatePhenotypes (cell_phenotype.cpp:
+ * 837-844) -- indices sorted descending, those at or past the current count
+ * skipped -- over CellData::removeCell (cell_data.cpp:408-498), which moves
+ * the last cell into the freed place.  Moves the 28 SoA fields (as bits),
+ * the four per-substrate rate arrays [cell * S + s] and active[] (any of
+ * those may be NULL); returns the new count. */
+uint32_t or_cells_remove(float* soa, uint32_t max_cells, uint32_t n_cells, uint32_t S, double* sec, double* upt,
+                         double* sat, double* ne, uint8_t* active, const uint32_t* indices, uint32_t count);
+
 /* ---- whole step (main.mm:341-391 ordering, hot path only) ------------ */
 
 typedef struct {

@@ -222,6 +222,19 @@ def voxel_refresh(soa, max_cells, n, grid):
     oracle().or_voxel_refresh(_p(soa, _F32), _U32(max_cells), _U32(n), C.byref(grid))
 
 
+def _opt(a, t):
+    return None if a is None else _p(a, t)
+
+
+def cells_remove(soa, max_cells, n, S, sec, upt, sat, ne, active, indices):
+    """or_cells_remove, in place; returns the new count."""
+    lib = oracle()
+    lib.or_cells_remove.restype = C.c_uint32
+    idx = np.ascontiguousarray(indices, np.uint32)
+    return lib.or_cells_remove(_p(soa, _F32), _U32(max_cells), _U32(n), _U32(S), _opt(sec, _F64), _opt(upt, _F64),
+                               _opt(sat, _F64), _opt(ne, _F64), _opt(active, _U8), _p(idx, _U32), _U32(idx.size))
+
+
 def nbr_hash(j):
     return oracle().or_nbr_hash(_U32(j))
 
@@ -321,6 +334,16 @@ def ref_forces(soa, max_cells, n, m, origin, threads=1):
     ref().ref_compute_forces(_p(soa, _F32), _U32(max_cells), _U32(n), C.byref(m), C.byref(mg),
                              _p(counts, _U32), _p(cells, _U32), C.c_int(threads))
     return counts, cells
+
+
+def ref_cells_remove(soa, max_cells, n, S, sec, upt, sat, ne, indices):
+    """The reference's CellData::removeCell in phase-3 order, in place;
+    returns the new count (rate arrays of max_cells * S)."""
+    lib = ref()
+    lib.ref_remove_cells.restype = C.c_uint32
+    idx = np.ascontiguousarray(indices, np.uint32)
+    return lib.ref_remove_cells(_p(soa, _F32), _U32(max_cells), _U32(n), _U32(S), _p(sec, _F64), _p(upt, _F64),
+                                _p(sat, _F64), _p(ne, _F64), _p(idx, _U32), _U32(idx.size))
 
 
 def ref_integrate(soa, max_cells, n, m, origin, dt):

@@ -15,9 +15,11 @@
  *   ThomasCoeffs set-up   src/microenvironment.mm:171-177
  *   applyDirichletBC      src/microenvironment.mm:212-237
  */
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <vector>
 #include <atomic>
 
@@ -218,6 +220,44 @@ void ref_write_matlab(const float* soa, uint32_t max_cells, uint32_t n_cells, ui
     std::memcpy(cells.saturation_density, sat, nS * sizeof(double));
     std::memcpy(cells.net_export_rate, ne, nS * sizeof(double));
     writeMatlabSnapshots(cells, density, *g, frame, folder);
+}
+
+/* Phase 3 of updatePhenotypes (cell_phenotype.cpp:837-844, restated: the
+ * dead-cell indices sorted descending, those at or past num_cells skipped)
+ * over the reference's own CellData::removeCell (cell_data.cpp:408-498), on
+ * a CellData holding the 28-field SoA block and the four per-substrate rate
+ * arrays (its CPU-only phenotype arrays absent, which removeCell skips).
+ * soa and the rate arrays (max_cells * S each) are updated in place;
+ * returns the new count. */
+uint32_t ref_remove_cells(float* soa, uint32_t max_cells, uint32_t n_cells, uint32_t n_substrates,
+                          double* sec, double* upt, double* sat, double* ne,
+                          const uint32_t* indices, uint32_t count)
+{
+    CellData cells(max_cells ? max_cells : 1);
+    std::vector<float> block(cells.gpuBufferSize() / sizeof(float), 0.0f);
+    std::memcpy(block.data(), soa, (size_t)NUM_CELL_FIELDS * max_cells * sizeof(float));
+    cells.setGPUBufferBase(block.data());
+    cells.num_cells = n_cells;
+    const size_t nS = (size_t)max_cells * n_substrates;
+    if (n_substrates) {
+        cells.allocateSubstrateBuffers(n_substrates);
+        std::memcpy(cells.secretion_rate, sec, nS * sizeof(double));
+        std::memcpy(cells.uptake_rate, upt, nS * sizeof(double));
+        std::memcpy(cells.saturation_density, sat, nS * sizeof(double));
+        std::memcpy(cells.net_export_rate, ne, nS * sizeof(double));
+    }
+    std::vector<uint32_t> to_remove(indices, indices + count);
+    std::sort(to_remove.begin(), to_remove.end(), std::greater<uint32_t>());
+    for (uint32_t idx : to_remove)
+        if (idx < cells.num_cells) cells.removeCell(idx);
+    std::memcpy(soa, block.data(), (size_t)NUM_CELL_FIELDS * max_cells * sizeof(float));
+    if (n_substrates) {
+        std::memcpy(sec, cells.secretion_rate, nS * sizeof(double));
+        std::memcpy(upt, cells.uptake_rate, nS * sizeof(double));
+        std::memcpy(sat, cells.saturation_density, nS * sizeof(double));
+        std::memcpy(ne, cells.net_export_rate, nS * sizeof(double));
+    }
+    return cells.num_cells;
 }
 
 }  // extern "C"

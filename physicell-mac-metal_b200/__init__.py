@@ -130,6 +130,10 @@ _SIGS = [
     ("pcg_cells_download_fields", C.c_int, [_P, C.c_uint32, C.c_uint32, _F32P, C.c_uint32]),
     ("pcg_cells_set_secretion", C.c_int, [_P, _F64P, _F64P, _F64P, _F64P, _U8P]),
     ("pcg_cells_count", C.c_int, [_P, _U32P]),
+    ("pcg_cells_remove", C.c_int, [_P, _U32P, C.c_uint32]),
+    ("pcg_removal_plan", C.c_int, [C.c_uint32, _U32P, C.c_uint32, _U32P, _U32P, _U32P, _U32P]),
+    ("pcg_cells_append", C.c_int, [_P, _F32P, C.c_uint32, C.c_uint32, _F64P, _F64P, _F64P, _F64P, _U8P]),
+    ("pcg_cells_download_secretion", C.c_int, [_P, _F64P, _F64P, _F64P, _F64P, _U8P]),
     ("pcg_cells_device_soa", C.c_int, [_P, C.POINTER(_F32P), _U32P]),
     ("pcg_mech_create", C.c_int, [_P, C.POINTER(MechanicsParams), C.c_float, C.c_float, C.c_float,
                                   C.c_uint32, C.POINTER(_P)]),
@@ -200,6 +204,19 @@ def lib():
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def removal_plan(n_cells, indices):
+    """Host-only moves of a dead-cell compaction: (dest, src, n_final), the
+    cell that started at src[k] ends at dest[k]."""
+    idx = np.ascontiguousarray(indices, np.uint32)
+    dest = np.zeros(max(idx.size, 1), np.uint32)
+    src = np.zeros(max(idx.size, 1), np.uint32)
+    nm, nf = C.c_uint32(), C.c_uint32()
+    st = lib().pcg_removal_plan(n_cells, _u32(idx), idx.size, _u32(dest), _u32(src), C.byref(nm), C.byref(nf))
+    if st != PCG_OK:
+        raise PcgError(st, "pcg_removal_plan")
+    return dest[:nm.value], src[:nm.value], nf.value
 
 
 def exported_symbols():
@@ -416,6 +433,37 @@ class Cells:
         act = None if active is None else np.ascontiguousarray(active, np.uint8)
         self._keep = (arrs, act)
         self.ctx.check(lib().pcg_cells_set_secretion(self.h, *[_f64(a) for a in arrs], _u8(act)))
+
+    def download_secretion(self):
+        """(secretion, uptake, saturation, net_export, active) of the current cells."""
+        k = self.n * self.S
+        arrs = [np.zeros(max(k, 1), np.float64) for _ in range(4)]
+        act = np.zeros(max(self.n, 1), np.uint8)
+        self.ctx.check(lib().pcg_cells_download_secretion(self.h, *[_f64(a) for a in arrs], _u8(act)))
+        return tuple(a[:k] for a in arrs) + (act[:self.n],)
+
+    def count(self):
+        n = C.c_uint32()
+        self.ctx.check(lib().pcg_cells_count(self.h, C.byref(n)))
+        self.n = n.value
+        return self.n
+
+    def remove(self, indices):
+        """Dead-cell compaction (CellData::removeCell for each index in
+        descending order, cell_phenotype.cpp:837-844) on the device; returns
+        the new count."""
+        idx = np.ascontiguousarray(indices, np.uint32)
+        self.ctx.check(lib().pcg_cells_remove(self.h, _u32(idx), idx.size))
+        return self.count()
+
+    def append(self, soa, count, soa_max, sec=None, upt=None, sat=None, ne=None, active=None):
+        """New cells after the current ones (CellData::addCell); returns the new count."""
+        soa = np.ascontiguousarray(soa, np.float32)
+        assert soa.size >= NUM_FIELDS * soa_max
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (sec, upt, sat, ne)]
+        act = None if active is None else np.ascontiguousarray(active, np.uint8)
+        self.ctx.check(lib().pcg_cells_append(self.h, _f32(soa), count, soa_max, *[_f64(a) for a in arrs], _u8(act)))
+        return self.count()
 
     def close(self):
         if getattr(self, "h", None):

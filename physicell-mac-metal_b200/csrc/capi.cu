@@ -438,6 +438,83 @@ pcg_status pcg_cells_set_secretion(pcg_cells* c, const double* sec, const double
     return PCG_OK;
 }
 
+pcg_status pcg_cells_download_secretion(pcg_cells* c, double* sec, double* upt, double* sat, double* ne,
+                                        uint8_t* active)
+{
+    if (!c) return PCG_ERR_INVALID;
+    const size_t cap = c->c.rates.bytes / (4 * sizeof(double));
+    const size_t count = static_cast<size_t>(c->c.n) * c->S;
+    double* dst[4] = {sec, upt, sat, ne};
+    for (int q = 0; q < 4; ++q)
+        if (dst[q] && count)
+            PCG_CU(c->ctx, cudaMemcpyAsync(dst[q], c->c.rates.as<double>() + q * cap, count * sizeof(double),
+                                           cudaMemcpyDeviceToHost, c->ctx->stream));
+    if (active && c->c.n)
+        PCG_CU(c->ctx, cudaMemcpyAsync(active, c->c.active.p, c->c.n, cudaMemcpyDeviceToHost, c->ctx->stream));
+    PCG_CU(c->ctx, cudaStreamSynchronize(c->ctx->stream));
+    return PCG_OK;
+}
+
+pcg_status pcg_removal_plan(uint32_t n_cells, const uint32_t* indices, uint32_t count, uint32_t* dest, uint32_t* src,
+                            uint32_t* n_moves, uint32_t* n_final)
+{
+    if ((!indices && count) || !n_moves || !n_final || ((!dest || !src) && count)) return PCG_ERR_INVALID;
+    std::vector<uint2> moves;
+    *n_final = removal_plan(n_cells, indices, count, &moves);
+    *n_moves = static_cast<uint32_t>(moves.size());
+    for (size_t k = 0; k < moves.size(); ++k) {
+        dest[k] = moves[k].x;
+        src[k] = moves[k].y;
+    }
+    return PCG_OK;
+}
+
+pcg_status pcg_cells_remove(pcg_cells* c, const uint32_t* indices, uint32_t count)
+{
+    if (!c || (!indices && count)) return PCG_ERR_INVALID;
+    AllocStream pool_scope(c->ctx->stream);
+    std::vector<uint2> moves;
+    const uint32_t n = removal_plan(c->c.n, indices, count, &moves);
+    if (!moves.empty()) {
+        DevBuf dm;
+        PCG_CU(c->ctx, dm.alloc(moves.size() * sizeof(uint2)));
+        PCG_CU(c->ctx, cudaMemcpyAsync(dm.p, moves.data(), moves.size() * sizeof(uint2), cudaMemcpyHostToDevice,
+                                       c->ctx->stream));
+        const uint64_t rate_cap = c->c.rates.bytes / (4 * sizeof(double));
+        PCG_CU(c->ctx, launch_cells_move(c->ctx->stream, c->c.soa.as<float>(), c->c.max_cells, dm.as<uint2>(),
+                                         static_cast<uint32_t>(moves.size()), c->c.rates.as<double>(), rate_cap, c->S,
+                                         c->c.active.as<uint8_t>()));
+        c->ctx->launches++;
+        PCG_CU(c->ctx, cudaStreamSynchronize(c->ctx->stream));   // the move list is released on return
+    }
+    if (n != c->c.n) {
+        c->c.n = n;
+        c->c.h_inst[0].n_cells = n;
+        c->c.inst_dirty = true;
+        c->c.coef_dirty = c->c.order_dirty = true;
+    }
+    return PCG_OK;
+}
+
+pcg_status pcg_cells_append(pcg_cells* c, const float* soa, uint32_t count, uint32_t soa_max, const double* sec,
+                            const double* upt, const double* sat, const double* ne, const uint8_t* active)
+{
+    if (!c || (!soa && count)) return PCG_ERR_INVALID;
+    if (count == 0) return PCG_OK;
+    if (soa_max < count) return bad(c->ctx, "soa_max_cells < count");
+    if (static_cast<uint64_t>(c->c.n) + count > c->c.max_cells) return bad(c->ctx, "appending past max_cells");
+    const uint32_t n0 = c->c.n;
+    PCG_TRY(c->c.upload_soa(n0, count, soa, soa_max, 0, NUM_FIELDS));
+    PCG_TRY(c->c.set_rates(n0 * c->S, count * c->S, sec, upt, sat, ne));
+    PCG_TRY(c->c.set_active(n0, count, active));
+    c->c.n = n0 + count;
+    c->c.h_inst[0].n_cells = c->c.n;
+    c->c.inst_dirty = true;
+    c->c.coef_dirty = c->c.order_dirty = true;
+    PCG_CU(c->ctx, cudaStreamSynchronize(c->ctx->stream));
+    return PCG_OK;
+}
+
 pcg_status pcg_cells_count(pcg_cells* c, uint32_t* n)
 {
     if (!c || !n) return PCG_ERR_INVALID;

@@ -184,6 +184,34 @@ __global__ void __launch_bounds__(256, 6) k_secrete(float* __restrict__ dens, co
     }
 }
 
+// ------------------------------------------------------------------ removal
+
+// The copies of a batch of CellData::removeCell calls (cell_data.cpp:408-
+// 498): move m puts the cell at place src into place dst.  Every source lies
+// at or past the new cell count and every destination before it, so no copy
+// reads a place that another copy writes.  One thread per (move, item): the
+// 28 SoA fields (copied as bits), the four per-substrate rate arrays, the
+// active flag.
+__global__ void k_cells_move(uint32_t* __restrict__ soa, uint32_t stride, const uint2* __restrict__ moves,
+                             uint32_t n_moves, double* __restrict__ rates, uint64_t rate_cap, uint32_t S,
+                             uint8_t* __restrict__ active)
+{
+    const uint32_t items = NUM_FIELDS + 4u * S + 1u;
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<uint64_t>(n_moves) * items) return;
+    const uint32_t m = static_cast<uint32_t>(t / items), it = static_cast<uint32_t>(t % items);
+    const uint32_t dst = moves[m].x, src = moves[m].y;
+    if (it < static_cast<uint32_t>(NUM_FIELDS)) {
+        soa[static_cast<size_t>(it) * stride + dst] = soa[static_cast<size_t>(it) * stride + src];
+    } else if (it < NUM_FIELDS + 4u * S) {
+        const uint32_t q = (it - NUM_FIELDS) / S, s = (it - NUM_FIELDS) % S;
+        double* r = rates + q * rate_cap;
+        r[static_cast<size_t>(dst) * S + s] = r[static_cast<size_t>(src) * S + s];
+    } else {
+        active[dst] = active[src];
+    }
+}
+
 // ------------------------------------------------------------------ mechanics
 
 __global__ void k_mech_bin(float* __restrict__ soa, uint32_t stride, uint32_t n, const uint32_t* __restrict__ cell_inst,
@@ -448,6 +476,16 @@ cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, 
     if (max_runs == 0 || max_s == 0) return cudaSuccess;
     k_secrete<<<blocks_for(max_runs, 256), 256, 0, st>>>(dens, skeys, run_start, run_inst, n_runs, insts, sbeg, cs,
                                                           cap, flags, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cells_move(cudaStream_t st, float* soa, uint32_t stride, const uint2* moves, uint32_t n_moves,
+                              double* rates, uint64_t rate_cap, uint32_t S, uint8_t* active)
+{
+    const uint64_t work = static_cast<uint64_t>(n_moves) * (NUM_FIELDS + 4u * S + 1u);
+    if (work == 0) return cudaSuccess;
+    k_cells_move<<<blocks_for(work, 256), 256, 0, st>>>(reinterpret_cast<uint32_t*>(soa), stride, moves, n_moves, rates,
+                                                       rate_cap, S, active);
     return cudaGetLastError();
 }
 

@@ -254,6 +254,10 @@ cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4
                                const uint32_t* sorder, const uint32_t* start, uint32_t n,
                                const uint32_t* cell_inst, const CellInst* insts, float* soa, uint32_t stride,
                                uint32_t* diag_cnt, uint32_t* diag_hash, const uint8_t* mask, int block);
+// Copies of a removal plan: (dst, src) pairs, each cell's 28 SoA fields,
+// 4 x S rates (arrays of rate_cap doubles, [cell * S + s]) and active flag.
+cudaError_t launch_cells_move(cudaStream_t st, float* soa, uint32_t stride, const uint2* moves, uint32_t n_moves,
+                              double* rates, uint64_t rate_cap, uint32_t S, uint8_t* active);
 // dt_override >= 0 replaces every instance's dt_mech.
 cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
                                   const uint32_t* cell_inst, const CellInst* insts, float dt_override,

@@ -8,6 +8,7 @@
 #include <fstream>
 #include <mutex>
 #include <sstream>
+#include <unordered_map>
 
 namespace pcg {
 
@@ -196,6 +197,30 @@ void HostBuf::release()
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
+}
+
+uint32_t removal_plan(uint32_t n_cells, const uint32_t* indices, uint32_t count, std::vector<uint2>* moves)
+{
+    std::vector<uint32_t> r(indices, indices + count);
+    std::sort(r.begin(), r.end(), std::greater<uint32_t>());
+    std::unordered_map<uint32_t, uint32_t> at;   // place -> starting place of the cell there (absent: its own)
+    auto cell_at = [&](uint32_t p) {
+        const auto it = at.find(p);
+        return it == at.end() ? p : it->second;
+    };
+    uint32_t num = n_cells;
+    for (const uint32_t idx : r) {
+        if (idx >= num) continue;
+        const uint32_t last = num - 1;
+        if (idx != last) at[idx] = cell_at(last);
+        at.erase(last);
+        --num;
+    }
+    moves->clear();
+    for (const auto& kv : at)
+        if (kv.first < num && kv.second != kv.first) moves->push_back(make_uint2(kv.first, kv.second));
+    std::sort(moves->begin(), moves->end(), [](const uint2& a, const uint2& b) { return a.x < b.x; });
+    return num;
 }
 
 int key_bits_for(uint64_t n_keys)

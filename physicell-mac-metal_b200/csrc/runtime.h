@@ -300,4 +300,12 @@ void fill_diff_inst(CellInst& ci, const DiffInstance& d);
 
 int key_bits_for(uint64_t n_keys);
 
+// The moves of CellData::removeCell (cell_data.cpp:408-498: the last cell
+// takes the freed place) called for each of 'indices' in descending order,
+// skipping indices at or past the current count, as phase 3 of
+// updatePhenotypes does (cell_phenotype.cpp:837-844).  Each move (x, y):
+// the cell that started at place y ends at place x; every other place below
+// the returned count keeps its cell.  Moves are sorted by destination.
+uint32_t removal_plan(uint32_t n_cells, const uint32_t* indices, uint32_t count, std::vector<uint2>* moves);
+
 }  // namespace pcg

@@ -178,10 +178,27 @@ def gen_matlab():
                             cells_mat=cells_mat, env_mat=env_mat)
 
 
+def gen_removal():
+    """Dead-cell compaction: the reference's removeCell in phase-3 order on a
+    28-field SoA with two substrates; indices with repeats and some past the
+    count, as the phenotype loop can produce."""
+    rng = np.random.default_rng(31)
+    mc, n, S = 96, 80, 2
+    soa0 = rng.standard_normal(28 * mc).astype(np.float32)
+    soa0[23 * mc:28 * mc] = rng.integers(0, 1 << 20, 5 * mc).astype(np.uint32).view(np.float32)
+    rates0 = [rng.uniform(0, 10, mc * S) for _ in range(4)]
+    indices = np.concatenate([rng.choice(n, 17, replace=False), [79, 3, 3, 85, 0]]).astype(np.uint32)
+    soa, rates = soa0.copy(), [r.copy() for r in rates0]
+    n_final = po.ref_cells_remove(soa, mc, n, S, *rates, indices)
+    np.savez_compressed(os.path.join(OUT, "removal.npz"), max_cells=mc, n=n, S=S, soa0=soa0, sec0=rates0[0],
+                        upt0=rates0[1], sat0=rates0[2], ne0=rates0[3], indices=indices, n_final=n_final, soa=soa,
+                        sec=rates[0], upt=rates[1], sat=rates[2], ne=rates[3])
+
+
 if __name__ == "__main__":
     if not po.ref_available():
         sys.exit("oracle/_ref/libpcg_ref.so not built (make -C oracle with the reference tree present)")
-    which = sys.argv[1:] or ["diffusion", "secretion", "mechanics", "motility", "matlab"]
+    which = sys.argv[1:] or ["diffusion", "secretion", "mechanics", "motility", "matlab", "removal"]
     for w in which:
         globals()["gen_" + w]()
     print("golden vectors written to", OUT)

@@ -231,6 +231,94 @@ def test_secretion_matches_reference_golden(ctx, pcg):
     assert np.array_equal(me.densityBuffer().view(np.uint32), z["density1"].view(np.uint32))
 
 
+def test_remove_matches_reference_fixture(ctx, pcg, po):
+    """Dead-cell compaction on the device against the reference's own
+    removeCell run in phase-3 order (fixture), the active flags against the
+    oracle."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "removal.npz"))
+    mc, n, S = int(d["max_cells"]), int(d["n"]), int(d["S"])
+    act0 = (np.arange(mc) % 3 != 0).astype(np.uint8)
+    cells = pcg.Cells(ctx, mc, S)
+    cells.upload(d["soa0"], n, mc)
+    cells.set_secretion(*[d[k + "0"][:n * S] for k in ("sec", "upt", "sat", "ne")], active=act0[:n])
+    nf = cells.remove(d["indices"])
+    assert nf == int(d["n_final"])
+    got = cells.download(mc).reshape(28, mc)[:, :nf]
+    assert np.array_equal(got.view(np.uint32), d["soa"].reshape(28, mc)[:, :nf].view(np.uint32))
+    rates = cells.download_secretion()
+    for got_r, k in zip(rates[:4], ("sec", "upt", "sat", "ne")):
+        assert np.array_equal(got_r, d[k][:nf * S])
+    want_act = act0.copy()
+    po.cells_remove(d["soa0"].copy(), mc, n, S, None, None, None, None, want_act, d["indices"])
+    assert np.array_equal(rates[4], want_act[:nf])
+
+
+def test_append_and_remove_then_secretion(ctx, pcg, po):
+    """Division and death without re-uploads: cells appended after the
+    current ones, secretion, dead cells compacted out (repeats and indices
+    past the count included), secretion again; every state bit-exact to the
+    oracle, so the secretion order and constants follow the changed
+    population."""
+    nx, ny, nz, S, n_all, n0 = 30, 20, 10, 3, 5000, 4000
+    g, og, subs, osubs, soa, vox, rates, active, d0 = secretion_case(pcg, po, nx, ny, nz, S, n_all, 99)
+    me = pcg.Microenvironment(ctx, g, subs)
+    me.setDensityAll(d0)
+    cells = pcg.Cells(ctx, n_all, S)
+    cells.upload(soa, n0, n_all)
+    cells.set_secretion(*[r[:n0 * S] for r in rates], active=active[:n0])
+    tail = np.ascontiguousarray(soa.reshape(28, n_all)[:, n0:])
+    assert cells.append(tail, n_all - n0, n_all - n0, *[r[n0 * S:] for r in rates], active=active[n0:]) == n_all
+    me.applySecretion(cells, 0.01)
+    ref = d0.copy()
+    po.secretion(ref, og, vox, soa[11 * n_all:12 * n_all], *rates, active, 0.01)
+    assert np.array_equal(me.densityBuffer().view(np.uint32), ref.view(np.uint32))
+
+    rng = np.random.default_rng(7)
+    idx = rng.integers(0, n_all + 50, 700).astype(np.uint32)
+    h_soa, h_rates, h_act = soa.copy(), [r.copy() for r in rates], active.copy()
+    nf = po.cells_remove(h_soa, n_all, n_all, S, *h_rates, h_act, idx)
+    assert cells.remove(idx) == nf
+    got = cells.download(n_all).reshape(28, n_all)[:, :nf]
+    assert np.array_equal(got.view(np.uint32), h_soa.reshape(28, n_all)[:, :nf].view(np.uint32))
+    back = cells.download_secretion()
+    for got_r, want in zip(back[:4], h_rates):
+        assert np.array_equal(got_r, want[:nf * S])
+    assert np.array_equal(back[4], h_act[:nf])
+
+    me.applySecretion(cells, 0.01)
+    h_vox = h_soa[26 * n_all:26 * n_all + nf].view(np.uint32)
+    po.secretion(ref, og, h_vox, h_soa[11 * n_all:11 * n_all + nf], *[r[:nf * S] for r in h_rates], h_act[:nf],
+                 0.01)
+    assert np.array_equal(me.densityBuffer().view(np.uint32), ref.view(np.uint32))
+
+
+def test_remove_then_mechanics_exact(ctx, pcg, po):
+    """Bins, cell-start table, permutation and neighbour sets after a
+    compaction, against the oracle on the compacted population."""
+    n = 3000
+    soa, mp, om, origin = setup_mech(pcg, po, False, n, 123, dense=True)
+    cells = pcg.Cells(ctx, n, 1)
+    cells.upload(soa, n, n)
+    idx = np.random.default_rng(8).choice(n, 400, replace=False).astype(np.uint32)
+    h = soa.copy()
+    nf = po.cells_remove(h, n, n, 0, None, None, None, None, None, idx)
+    assert cells.remove(idx) == nf
+    mech = pcg.CellMechanics(ctx, mp, origin, n)
+    mech.set_diagnostics(True)
+    mech.computeForces(cells)
+    got = cells.download(n)
+    start, order = mech.syncHashPointers(nf)
+    cnt, hsh = mech.neighbor_stats(nf)
+    key = po.mech_bin(h, n, nf, om, origin)
+    oorder, ostart = po.mech_sort(key, om)
+    ocnt, ohsh, _ = po.mech_forces(h, n, nf, om, key, oorder, ostart)
+    assert np.array_equal(got[27 * n:27 * n + nf].view(np.uint32), key)
+    assert np.array_equal(start, ostart)
+    assert np.array_equal(order, oorder)
+    assert np.array_equal(cnt, ocnt) and np.array_equal(hsh, ohsh)
+
+
 def test_main_loop_steps_match_oracle(ctx, pcg, po):
     """Sweeps -> Dirichlet -> secretion -> mechanics every 10th sub-step
     (src/main.mm:341-391) through the plain API, against or_run."""
