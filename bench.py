@@ -244,6 +244,24 @@ def cpu_baseline(instances, budget_s):
             "prepared": prepared}
 
 
+def one_thread_baseline(prepared, cores):
+    """The same port on one host thread, one mechanics period of one
+    (the smallest sampled) instance; the all-thread count is restored
+    afterwards."""
+    import pyoracle as po
+    po.port_threads(1)
+    try:
+        t0 = time.perf_counter()
+        cpu_period([prepared])
+        secs = time.perf_counter() - t0
+    finally:
+        po.port_threads(cores)
+    vox, cells = prepared[10], prepared[5]
+    return {"value": vox * SUB_STEPS / secs, "unit": "voxel-steps/s", "cores": 1,
+            "sample": f"one instance ({vox} voxels, {cells} cells), one mechanics period",
+            "cell_steps_per_s": cells / secs}
+
+
 def run_reference_arm(args, rank, world):
     """--impl reference: the CPU path only, rank 0 only."""
     if rank != 0:
@@ -471,7 +489,8 @@ def main():
                "kind": "port",
                "sample": f"first {cb['instances']} of {len(insts)} instances ({cb['voxels']} voxels, "
                          f"{cb['cells']} cells), one mechanics period each",
-               "cell_steps_per_s": cb["cells"] / cb["seconds"]}
+               "cell_steps_per_s": cb["cells"] / cb["seconds"],
+               "one_thread": one_thread_baseline(min(cb["prepared"], key=lambda q: q[10]), cb["cores"])}
 
     serving = None
     if args.serve_horizon > 0 and rank == 0 and world == 1:
