@@ -32,6 +32,7 @@ uint64_t instance_bytes(const pcg_instance_desc& d)
     b += n * (NUM_FIELDS * 4 + 4 + 1);                     // SoA, instance id, active
     b += n * S * (4 * 8 + 3 * 8);                          // rates, secretion constants
     b += n * 4 * 6 * 2;                                    // two sort workspaces
+    b += n * (8 + 4);                                      // per-run density element and rate slot
     b += n * (16 + 16 + 8);                                // sorted SoA, diagnostics
     b += (V + 1) * 4 * 2;                                  // counts, start
     b += (n / 2048 + 1) * 256 * 4 * 2 + 4096;              // sort / scan scratch

@@ -69,17 +69,27 @@ __global__ void k_sec_heads(const uint32_t* __restrict__ skeys, const uint32_t* 
 
 // rid = exclusive scan of heads: run r starts at run_start[r] and ends at
 // run_start[r + 1]; run_start[n_runs] is the first invalid position (or n).
+// Each run also gets the density element of its voxel (substrate 0, padded
+// rows) and the rate slot of its first cell, so the secretion pass finds
+// both without reading the key or the instance's first sorted place.
 __global__ void k_sec_runs(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder, uint32_t n,
                            const uint32_t* __restrict__ cell_inst, uint32_t invalid_key, const uint32_t* __restrict__ rid,
-                           uint32_t* __restrict__ run_start, uint32_t* __restrict__ run_inst)
+                           const CellInst* __restrict__ insts, const uint32_t* __restrict__ sbeg,
+                           uint32_t* __restrict__ run_start, uint32_t* __restrict__ run_inst,
+                           uint64_t* __restrict__ run_dens, uint32_t* __restrict__ run_slot)
 {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p > n) return;
     const bool valid = p < n && skeys[p] < invalid_key;
     if (valid && (p == 0 || skeys[p - 1] != skeys[p])) {
         const uint32_t r = rid[p];
+        const uint32_t ii = cell_inst[sorder[p]];
+        const CellInst& in = insts[ii];
+        const uint32_t v = skeys[p] - in.vox_base;
         run_start[r] = p;
-        run_inst[r] = cell_inst[sorder[p]];
+        run_inst[r] = ii;
+        run_dens[r] = in.dens_off + static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
+        run_slot[r] = in.rate_off + (p - sbeg[ii]) * in.S;
     }
     if (!valid && (p == 0 || skeys[p - 1] < invalid_key)) run_start[rid[p]] = p;
 }
@@ -147,23 +157,24 @@ __device__ __forceinline__ float secrete_cell(float rho32, const double* __restr
 // each cell.  The run's metadata is read once; with one or two substrates
 // both are held in registers and advanced together.  Constants: three
 // arrays of cap (c0, c1, c2), entry (cell in sorted order, substrate).
-__global__ void __launch_bounds__(256, 6) k_secrete(float* __restrict__ dens, const uint32_t* __restrict__ skeys,
-                          const uint32_t* __restrict__ run_start, const uint32_t* __restrict__ run_inst,
-                          const uint32_t* __restrict__ n_runs, const CellInst* __restrict__ insts,
-                          const uint32_t* __restrict__ sbeg, const double* __restrict__ cs, uint64_t cap,
+__global__ void __launch_bounds__(256, 6) k_secrete(float* __restrict__ dens, const uint32_t* __restrict__ run_start,
+                          const uint32_t* __restrict__ run_inst, const uint64_t* __restrict__ run_dens,
+                          const uint32_t* __restrict__ run_slot, const uint32_t* __restrict__ n_runs,
+                          const CellInst* __restrict__ insts, const double* __restrict__ cs, uint64_t cap,
                           const uint32_t* __restrict__ flags, const uint8_t* __restrict__ mask)
 {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= *n_runs) return;
+    // everything a run needs first comes from per-run arrays: the voxel's
+    // density element and the first cell's rate slot were placed when the
+    // order was built, so the density and the constants are one load away
     const uint32_t ii = run_inst[r];
+    const uint32_t p0 = run_start[r], p1 = run_start[r + 1];
+    float* d = dens + run_dens[r];
+    const uint64_t base = run_slot[r];
     if (mask && !(mask[ii] & STEP_DIFFUSE)) return;
     const CellInst& in = insts[ii];
     const uint32_t S = in.S;
-    const uint32_t p0 = run_start[r], p1 = run_start[r + 1];
-    const uint32_t v = skeys[p0] - in.vox_base;
-    // dense voxel index -> padded-row device offset
-    float* d = dens + in.dens_off + static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
-    const uint64_t base = in.rate_off + static_cast<uint64_t>(p0 - sbeg[ii]) * S;
     const uint32_t f = flags[ii];
     if (S <= 2) {
         float r0 = d[0], r1 = S > 1 ? d[in.sub_pitch] : 0.f;
@@ -443,15 +454,16 @@ cudaError_t launch_sec_keys(cudaStream_t st, const float* soa, uint32_t stride, 
 
 cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
                             const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* heads_rid, uint32_t* sbeg,
-                            uint32_t* run_start, uint32_t* run_inst, void* scan_scratch)
+                            const CellInst* insts, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
+                            uint32_t* run_slot, void* scan_scratch)
 {
     k_sec_heads<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, sorder, n, cell_inst, invalid_key, heads_rid, sbeg);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = scan_exclusive(st, heads_rid, heads_rid, static_cast<uint64_t>(n) + 1, scan_scratch);
     if (e != cudaSuccess) return e;
-    k_sec_runs<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, sorder, n, cell_inst, invalid_key, heads_rid, run_start,
-                                                         run_inst);
+    k_sec_runs<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, sorder, n, cell_inst, invalid_key, heads_rid, insts,
+                                                         sbeg, run_start, run_inst, run_dens, run_slot);
     return cudaGetLastError();
 }
 
@@ -468,14 +480,14 @@ cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t strid
     return cudaGetLastError();
 }
 
-cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* skeys, const uint32_t* run_start,
-                           const uint32_t* run_inst, const uint32_t* n_runs, uint32_t max_runs, uint32_t max_s,
-                           const CellInst* insts, const uint32_t* sbeg, const double* cs, uint32_t cap,
+cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_start, const uint32_t* run_inst,
+                           const uint64_t* run_dens, const uint32_t* run_slot, const uint32_t* n_runs,
+                           uint32_t max_runs, uint32_t max_s, const CellInst* insts, const double* cs, uint32_t cap,
                            const uint32_t* flags, const uint8_t* mask)
 {
     if (max_runs == 0 || max_s == 0) return cudaSuccess;
-    k_secrete<<<blocks_for(max_runs, 256), 256, 0, st>>>(dens, skeys, run_start, run_inst, n_runs, insts, sbeg, cs,
-                                                          cap, flags, mask);
+    k_secrete<<<blocks_for(max_runs, 256), 256, 0, st>>>(dens, run_start, run_inst, run_dens, run_slot, n_runs,
+                                                          insts, cs, cap, flags, mask);
     return cudaGetLastError();
 }
 

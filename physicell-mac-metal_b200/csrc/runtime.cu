@@ -1126,8 +1126,9 @@ int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_
     PCG_CU(ctx, coef_flags.alloc(h_inst.size() * sizeof(uint32_t)));
     PCG_CU(ctx, cudaMemsetAsync(coef_flags.p, 0xFF, coef_flags.bytes, ctx->stream));   // all terms until prepared
     PCG_CU(ctx, active.alloc(max_cells));
-    for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp})
+    for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp, &run_slot})
         PCG_CU(ctx, b->alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint32_t)));
+    PCG_CU(ctx, run_dens.alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint64_t)));
     PCG_CU(ctx, sort_scr.alloc(radix_sort_scratch_bytes(max_cells, 32)));
     PCG_CU(ctx, sbeg.alloc(h_inst.size() * sizeof(uint32_t)));
     PCG_CU(ctx, cudaMemsetAsync(sbeg.p, 0, sbeg.bytes, ctx->stream));
@@ -1225,8 +1226,8 @@ int Cells::build_order(uint64_t total_vox)
                          sorder.as<uint32_t>(), ktmp.as<uint32_t>(), vtmp.as<uint32_t>(), n, key_bits, sort_scr.p);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion sort");
     e = launch_sec_runs(ctx->stream, skeys.as<uint32_t>(), sorder.as<uint32_t>(), n, cell_inst.as<uint32_t>(),
-                        invalid_key, ktmp.as<uint32_t>(), sbeg.as<uint32_t>(), vals.as<uint32_t>(), vtmp.as<uint32_t>(),
-                        run_scr.p);
+                        invalid_key, ktmp.as<uint32_t>(), sbeg.as<uint32_t>(), inst.as<CellInst>(), vals.as<uint32_t>(),
+                        vtmp.as<uint32_t>(), run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), run_scr.p);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion runs");
     ctx->launches += 1 + radix_sort_launches(n, key_bits) + 2 + scan_launches(static_cast<uint64_t>(n) + 1);
     order_dirty = false;
@@ -1262,9 +1263,9 @@ int Cells::secrete(Diffusion& d, const uint8_t* mask)
 {
     uint32_t max_s = 0;
     for (const CellInst& ci : h_inst) max_s = std::max(max_s, ci.S);
-    cudaError_t e = launch_secrete(ctx->stream, d.dens.as<float>(), skeys.as<uint32_t>(), vals.as<uint32_t>(),
-                                   vtmp.as<uint32_t>(), ktmp.as<uint32_t>() + n, n, max_s, inst.as<CellInst>(),
-                                   sbeg.as<uint32_t>(), coef.as<double>(),
+    cudaError_t e = launch_secrete(ctx->stream, d.dens.as<float>(), vals.as<uint32_t>(), vtmp.as<uint32_t>(),
+                                   run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), ktmp.as<uint32_t>() + n, n, max_s,
+                                   inst.as<CellInst>(), coef.as<double>(),
                                    static_cast<uint32_t>(rates.bytes / (4 * sizeof(double))),
                                    coef_flags.as<uint32_t>(), mask);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion launch");
@@ -1276,7 +1277,8 @@ uint64_t Cells::device_bytes() const
 {
     return inst.bytes + soa.bytes + cell_inst.bytes + rates.bytes + coef.bytes + coef_flags.bytes + active.bytes +
            keys.bytes + vals.bytes +
-           skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + sbeg.bytes + run_scr.bytes;
+           skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + sbeg.bytes + run_scr.bytes +
+           run_dens.bytes + run_slot.bytes;
 }
 
 // ------------------------------------------------------------------ mechanics

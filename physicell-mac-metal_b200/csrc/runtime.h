@@ -252,6 +252,7 @@ public:
     // in sorted order (c0, c1, c2 arrays) and coef_flags which of c0 / c1
     // each instance has
     DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr, sbeg, run_scr;
+    DevBuf run_dens, run_slot;   // per run: density element of its voxel, rate slot of its first cell
     uint32_t invalid_key = 0;
     int key_bits = 0;
 
