@@ -141,15 +141,20 @@ __global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, ui
 // One cell's processSecretion on one substrate (cell_phenotype.cpp:526-564):
 // rho += c0; rho = (rho + c1) / c2; clamp at 0; FP32 store.  A term the
 // instance never has (flags) is exactly +0 and is added as the constant.
+__device__ __forceinline__ float secrete_terms(float rho32, double c0, double c1, double c2)
+{
+    double rho = static_cast<double>(rho32);
+    rho = __dadd_rn(rho, c0);
+    rho = __dadd_rn(rho, c1);
+    rho = __ddiv_rn(rho, c2);
+    if (rho < 0.0) rho = 0.0;
+    return __double2float_rn(rho);
+}
+
 __device__ __forceinline__ float secrete_cell(float rho32, const double* __restrict__ cs, uint64_t o, uint64_t cap,
                                               uint32_t f)
 {
-    double rho = static_cast<double>(rho32);
-    rho = __dadd_rn(rho, (f & 1u) ? cs[o] : 0.0);
-    rho = __dadd_rn(rho, (f & 2u) ? cs[cap + o] : 0.0);
-    rho = __ddiv_rn(rho, cs[2 * cap + o]);
-    if (rho < 0.0) rho = 0.0;
-    return __double2float_rn(rho);
+    return secrete_terms(rho32, (f & 1u) ? cs[o] : 0.0, (f & 2u) ? cs[cap + o] : 0.0, cs[2 * cap + o]);
 }
 
 // One thread per run: applies the run's cells to its voxel in ascending
@@ -177,8 +182,20 @@ __global__ void __launch_bounds__(256, 6) k_secrete(float* __restrict__ dens, co
     const uint32_t S = in.S;
     const uint32_t f = flags[ii];
     if (S <= 2) {
-        float r0 = d[0], r1 = S > 1 ? d[in.sub_pitch] : 0.f;
-        for (uint32_t q = p0; q < p1; ++q) {
+        // the first cell's terms and the voxel's densities in one batch of
+        // independent loads (a loop would order the terms after the density)
+        const bool two = S > 1;
+        const double a0 = (f & 1u) ? cs[base] : 0.0, b0 = (f & 2u) ? cs[cap + base] : 0.0, c0 = cs[2 * cap + base];
+        double a1 = 0.0, b1 = 0.0, c1 = 1.0;
+        if (two) {
+            a1 = (f & 1u) ? cs[base + 1] : 0.0;
+            b1 = (f & 2u) ? cs[cap + base + 1] : 0.0;
+            c1 = cs[2 * cap + base + 1];
+        }
+        float r0 = d[0], r1 = two ? d[in.sub_pitch] : 0.f;
+        r0 = secrete_terms(r0, a0, b0, c0);
+        if (two) r1 = secrete_terms(r1, a1, b1, c1);
+        for (uint32_t q = p0 + 1; q < p1; ++q) {
             const uint64_t o = base + static_cast<uint64_t>(q - p0) * S;
             r0 = secrete_cell(r0, cs, o, cap, f);
             if (S > 1) r1 = secrete_cell(r1, cs, o + 1, cap, f);
