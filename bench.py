@@ -421,7 +421,9 @@ def main():
     secs_max = dist_max(dist, local, secs)
     total_vox = dist_sum(dist, local, float(voxels))
     total_cells = dist_sum(dist, local, float(cells))
+    total_vox_sub = dist_sum(dist, local, float(voxel_subs))
     value = total_vox * SUB_STEPS * args.steps / secs_max
+    vox_sub_rate = total_vox_sub * SUB_STEPS * args.steps / secs_max
     cell_rate = total_cells * args.steps / secs_max
 
     # end to end through the C ABI with pinned host buffers
@@ -508,7 +510,7 @@ def main():
                        "voxels_per_gpu": voxels, "voxel_substrates_per_gpu": voxel_subs, "cells_per_gpu": cells,
                        "l2": f"inputs larger than L2 ({voxel_subs * 4 / 1e6:.0f} MB density per GPU)",
                        "launch_shapes": batch.describe()},
-            "cell_steps_per_s": cell_rate,
+            "cell_steps_per_s": cell_rate, "voxel_substrate_steps_per_s": vox_sub_rate,
             "plain_voxel_steps_per_s": plain_rate,
             "batched_over_plain": (value / world / plain_rate) if plain_rate else None,
             "e2e": {"value": e2e_value, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d,
