@@ -350,3 +350,23 @@ def test_main_loop_steps_match_oracle(ctx, pcg, po):
     assert rel_err(me.densityBuffer(), dens) <= 1e-5
     got = cells.download(n)
     assert np.abs(got[:3 * n].astype(np.float64) - soa[:3 * n]).max() <= 1e-4
+
+
+def test_remove_and_append_edge_cases(ctx, pcg):
+    """Removing nothing, removing every cell, appending to an empty store,
+    and an append past max_cells refused without changing the store."""
+    n, S = 50, 2
+    soa = np.arange(28 * n, dtype=np.float32)
+    cells = pcg.Cells(ctx, n, S)
+    cells.upload(soa, n, n)
+    assert cells.remove([]) == n
+    assert np.array_equal(cells.download(n).view(np.uint32), soa.view(np.uint32))
+    assert cells.remove(np.arange(n + 5)) == 0
+    assert cells.append(soa, 10, n) == 10
+    got = cells.download(n).reshape(28, n)[:, :10]
+    assert np.array_equal(got.view(np.uint32), soa.reshape(28, n)[:, :10].view(np.uint32))
+    rates = cells.download_secretion()
+    assert all(np.all(r == 0.0) for r in rates[:4]) and np.all(rates[4] == 1)
+    with pytest.raises(pcg.PcgError):
+        cells.append(soa, 41, n)
+    assert cells.count() == 10

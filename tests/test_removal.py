@@ -79,3 +79,19 @@ def test_removal_plan_reproduces_oracle(pcg, po, with_repeats):
         a = active.copy()
         a[dest] = a[src]
         assert np.array_equal(a[:nf], want_act[:nf])
+
+
+def test_removal_plan_edge_cases(pcg):
+    """Nothing to remove, an empty store, everything removed, indices all
+    past the count."""
+    assert pcg.removal_plan(0, [])[2] == 0
+    d, s, nf = pcg.removal_plan(5, [])
+    assert nf == 5 and len(d) == 0 and len(s) == 0
+    d, s, nf = pcg.removal_plan(0, [0, 3])
+    assert nf == 0 and len(d) == 0
+    d, s, nf = pcg.removal_plan(4, [3, 1, 0, 2])
+    assert nf == 0 and len(d) == 0
+    d, s, nf = pcg.removal_plan(4, [4, 9, 100])
+    assert nf == 4 and len(d) == 0
+    d, s, nf = pcg.removal_plan(4, [0])
+    assert nf == 3 and d.tolist() == [0] and s.tolist() == [3]
