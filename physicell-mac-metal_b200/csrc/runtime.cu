@@ -60,10 +60,11 @@ public:
         cudaError_t e = cudaGetDevice(&dev);
         if (e != cudaSuccess) return e;
         *device = dev;
+        const size_t b = round_up(want);
         {
             std::lock_guard<std::mutex> lk(mu_);
-            const size_t limit = want + want / 8 + (1u << 20);
-            for (auto it = free_.lower_bound(want); it != free_.end() && it->first <= limit; ++it) {
+            const auto range = free_.equal_range(b);
+            for (auto it = range.first; it != range.second; ++it) {
                 if (it->second.device != dev) continue;
                 const cudaError_t q = cudaEventQuery(it->second.ev);
                 if (q == cudaErrorNotReady) continue;
@@ -75,7 +76,6 @@ public:
                 return cudaSuccess;
             }
         }
-        const size_t b = round_up(want);
         e = cudaMalloc(out, b);
         if (e == cudaErrorMemoryAllocation) {
             cudaGetLastError();
@@ -127,10 +127,16 @@ public:
     }
 
 private:
+    // Block sizes: 512-byte steps below 4 KiB, above it four classes per
+    // power of two (2^e x {1, 1.25, 1.5, 1.75}, at most 25% over), so a
+    // rebuild whose buffers differ a little in size from the last one's
+    // finds the freed blocks again instead of allocating anew.
     static size_t round_up(size_t b)
     {
-        const size_t g = b >= (1u << 20) ? (1u << 20) : 512;
-        return (b + g - 1) / g * g;
+        if (b < 4096) return (b + 511) / 512 * 512;
+        const int e = 63 - __builtin_clzll(static_cast<unsigned long long>(b));
+        const size_t step = static_cast<size_t>(1) << (e - 2);
+        return (b + step - 1) / step * step;
     }
     std::mutex mu_;
     std::multimap<size_t, PoolBlock> free_;
