@@ -96,9 +96,18 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
             PCG_TRY(d.fill(i, descs[i].initial_values));
         }
     }
-    // cells
-    PCG_TRY(c_.create(ctx, static_cast<uint32_t>(std::max<uint64_t>(cells_total, 1)),
-                      static_cast<uint32_t>(std::max<uint64_t>(rates_total, 1)), n));
+    // cells.  A server rebuilds its batch whenever requests come and go:
+    // its cell arrays get power-of-two capacities, so consecutive rebuilds
+    // ask the device pool for the same sizes and find the freed blocks.
+    auto capacity = [&](uint64_t v) {
+        v = std::max<uint64_t>(v, 1);
+        if (!masked) return v;
+        uint64_t c = 1;
+        while (c < v) c <<= 1;
+        return std::min<uint64_t>(c, 0xFFFFFFF0ull);
+    };
+    const uint32_t cell_cap = static_cast<uint32_t>(capacity(cells_total));
+    PCG_TRY(c_.create(ctx, cell_cap, static_cast<uint32_t>(capacity(rates_total)), n));
     c_.n = static_cast<uint32_t>(cells_total);
     c_.n_rate = static_cast<uint32_t>(rates_total);
     PCG_TRY(c_.set_cell_instances(ncell));
@@ -151,7 +160,7 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
     }
     c_.inst_dirty = true;
     PCG_TRY(c_.sync_inst());
-    PCG_TRY(m_.create(ctx, moff, std::max<uint32_t>(coff, 1)));
+    PCG_TRY(m_.create(ctx, moff, cell_cap));
     PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
     if (c_.n) PCG_TRY(c_.prepare_secretion(dt_diff, d.total_vox));
     if (tune) {
