@@ -196,6 +196,15 @@ pcg_status pcg_cells_append(pcg_cells* cells, const float* soa, uint32_t count, 
                             const double* secretion, const double* uptake, const double* saturation,
                             const double* net_export, const uint8_t* active);
 pcg_status pcg_cells_device_soa(pcg_cells* cells, float** dptr, uint32_t* max_cells);
+/* FP64 master positions.  The reference keeps positions as FP32 SoA fields
+ * (integrate.metal:58-69 updates them in place); here the AB2 update runs on
+ * an FP64 master copy per cell and stores its rounding into those fields.
+ * The update starts from the master while the master rounds to the field's
+ * FP32 value; a position the host writes through the SoA (an upload of a
+ * different value, an append) replaces it.  Downloads cells [0, n_cells)
+ * (n_cells = the current count) as three arrays of n_cells doubles (x, y, z),
+ * each the value the next update starts from. */
+pcg_status pcg_cells_download_positions64(pcg_cells* cells, double* xyz, uint32_t n_cells);
 
 /* ------------------------------------------------------------------------
  * Mechanics — replaces CellMechanics (src/cell_mechanics.h:15-87).
@@ -301,10 +310,13 @@ pcg_status pcg_snapshot_frame(pcg_snapshot* snap, const pcg_me* me, const pcg_ce
  * must avoid allocation calls because they can synchronise the device).
  * - Sorts n pairs by the low key_bits (1..32) bits of the keys, equal keys
  *   keeping their input order; enqueued on ctx's stream (pcg_sync waits).
+ *   ctx's device is made current for the call and the caller's restored.
  * - n <= PCG_SORT_STATIC_MAX_PAIRS, else PCG_ERR_INVALID with a message;
  *   outputs must not overlap the inputs or each other.
- * - The first call on each device looks up the scratch array's address
- *   (device set-up); make it, e.g. with n = 0, before the calls that
+ * - The first call on each device does the device set-up: it looks up the
+ *   scratch array's address and loads the sort's kernels (which lazy
+ *   module loading would otherwise load, and possibly allocate for, at
+ *   their first launch).  Make it, e.g. with n = 0, before the calls that
  *   matter.  The scratch needs no initial contents.
  * - One scratch array per device: calls on the same device must not
  *   overlap in time (issue them on one stream, or order them with events);
@@ -312,6 +324,16 @@ pcg_status pcg_snapshot_frame(pcg_snapshot* snap, const pcg_me* me, const pcg_ce
 #define PCG_SORT_STATIC_MAX_PAIRS (1u << 18)
 pcg_status pcg_sort_pairs_static(pcg_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in,
                                  uint32_t* keys_out, uint32_t* vals_out, uint32_t n, int key_bits);
+
+/* No reference counterpart (the reference aborts on a failed allocation,
+ * metal_context.mm:52-60).  Test and diagnostics aids, process-wide:
+ * the number of device allocations the library has made with cudaMalloc
+ * and of pooled blocks it has handed out again; and a host-side fault
+ * injector that makes the nth library device allocation from now fail as
+ * out of memory (PCG_ERR_OOM from the call that needed it) without
+ * touching the device (nth = 0 turns it off). */
+void pcg_debug_alloc_stats(uint64_t* device_mallocs, uint64_t* pool_reuses);
+void pcg_debug_fail_alloc(uint64_t nth);
 
 /* ------------------------------------------------------------------------
  * Batch — many independent simulations of uneven grid and cell counts
@@ -359,6 +381,8 @@ pcg_status pcg_batch_step(pcg_batch* batch, int n_diffusion_steps);
 pcg_status pcg_batch_download_density(pcg_batch* batch, uint32_t instance, float* host, size_t n_floats);
 pcg_status pcg_batch_download_cells(pcg_batch* batch, uint32_t instance, float* soa, uint32_t soa_max_cells);
 pcg_status pcg_batch_upload_cells(pcg_batch* batch, uint32_t instance, const float* soa, uint32_t soa_max_cells);
+/* pcg_cells_download_positions64 for one instance (n_cells = its count). */
+pcg_status pcg_batch_download_positions64(pcg_batch* batch, uint32_t instance, double* xyz, uint32_t n_cells);
 /* Whole-batch asynchronous transfers (the end-to-end path; host buffers
  * should come from pcg_host_alloc).  Cells: one SoA of all instances' cells
  * in instance order, field stride = total cells (28 * total floats).
@@ -391,6 +415,18 @@ pcg_status pcg_batch_step_launches(pcg_batch* batch, uint64_t* diffusion_step, u
 pcg_status pcg_batch_phase_times(pcg_batch* batch, float* ms, uint64_t* n_sweep_launches, int reset);
 /* Switch phase profiling on or off after creation. */
 pcg_status pcg_batch_set_profile(pcg_batch* batch, int on);
+/* Neighbour-set diagnostics of the batch's force pass, as
+ * pcg_mech_set_diagnostics gives them for one simulation (the mechanics
+ * step's graph is captured again; results are unchanged). */
+pcg_status pcg_batch_set_diagnostics(pcg_batch* batch, int on);
+/* CellMechanics::syncHashPointers (cell_mechanics.mm:122-133) for one
+ * instance of the batch, as of its last mechanics step: its cell-start
+ * table (V + 1 entries for its V mechanics voxels, counted from its first
+ * sorted place), its sorted cells (n_cells, instance-local indices) and,
+ * with diagnostics on, each cell's neighbour count and hash (n_cells, by
+ * instance-local cell index).  Any pointer may be NULL. */
+pcg_status pcg_batch_mech_bins(pcg_batch* batch, uint32_t instance, uint32_t* start, uint32_t* sorted_cells,
+                               uint32_t* nbr_count, uint32_t* nbr_hash);
 /* Describe the chosen launch shapes as a short string. */
 const char* pcg_batch_describe(pcg_batch* batch);
 

@@ -415,13 +415,20 @@ void or_mech_forces(float* soa, uint32_t max_cells, uint32_t n_cells, const or_m
 void or_mech_integrate(float* soa, uint32_t max_cells, uint32_t n_cells, const or_mech* m,
                        float x_min, float y_min, float z_min, float dt)
 {
+    or_mech_integrate_master(soa, max_cells, n_cells, m, x_min, y_min, z_min, dt, NULL);
+}
+
+void or_mech_integrate_master(float* soa, uint32_t max_cells, uint32_t n_cells, const or_mech* m,
+                              float x_min, float y_min, float z_min, float dt, double* pos64)
+{
     float* p[3] = { soa + (size_t)OR_F_POS_X * max_cells, soa + (size_t)OR_F_POS_Y * max_cells,
                     soa + (size_t)OR_F_POS_Z * max_cells };
     float* v[3] = { soa + (size_t)OR_F_VEL_X * max_cells, soa + (size_t)OR_F_VEL_Y * max_cells,
                     soa + (size_t)OR_F_VEL_Z * max_cells };
     float* pv[3] = { soa + (size_t)OR_F_PREV_VX * max_cells, soa + (size_t)OR_F_PREV_VY * max_cells,
                      soa + (size_t)OR_F_PREV_VZ * max_cells };
-    /* clamp box: mechanics-grid GridParams (cell_mechanics.mm:147-156, integrate.metal:279-285) */
+    /* clamp box: the mechanics grid's GridParams (cell_mechanics.mm:57-70)
+     * as integrate.metal:58-69 clamps to it */
     const float lo[3] = { x_min, y_min, z_min };
     const uint32_t nn[3] = { m->mech_grid_nx, m->mech_grid_ny, m->mech_grid_nz };
     float hi[3];
@@ -431,9 +438,15 @@ void or_mech_integrate(float* soa, uint32_t max_cells, uint32_t n_cells, const o
         for (int a = 0; a < 3; a++) {
             double vv = (double)v[a][t], pp = (double)pv[a][t];
             double inc = 1.5 * vv - 0.5 * pp;
-            double x = (double)p[a][t] + ddt * inc;
+            double x0 = (double)p[a][t];
+            if (pos64) {
+                const double mst = pos64[(size_t)a * max_cells + t];
+                if ((float)mst == p[a][t]) x0 = mst;
+            }
+            double x = x0 + ddt * inc;
             if (x < (double)lo[a]) x = lo[a];
             if (x > (double)hi[a]) x = hi[a];
+            if (pos64) pos64[(size_t)a * max_cells + t] = x;
             p[a][t] = (float)x;
             pv[a][t] = v[a][t];
         }
@@ -687,8 +700,8 @@ void or_run_motile(const or_sim* sim, float* density, float* soa, uint32_t max_c
                     or_motility_update(soa, max_cells, n_cells, density, g, mot, dt_mech, seed, *mot_step, layout);
                     ++*mot_step;
                 }
-                or_mech_integrate(soa, max_cells, n_cells, m, g->x_min, g->y_min, g->z_min,
-                                  (float)dt_mech);
+                or_mech_integrate_master(soa, max_cells, n_cells, m, g->x_min, g->y_min, g->z_min,
+                                         (float)dt_mech, sim->pos64);
                 if (sim->refresh_voxels) or_voxel_refresh(soa, max_cells, n_cells, g);
             }
             *mech_accum = 0.0;

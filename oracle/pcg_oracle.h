@@ -147,6 +147,15 @@ uint32_t or_nbr_hash(uint32_t j);
 void or_mech_integrate(float* soa, uint32_t max_cells, uint32_t n_cells, const or_mech* m,
                        float x_min, float y_min, float z_min, float dt);
 
+/* The same update on FP64 master positions pos64 (three arrays of
+ * max_cells: x, y, z), the FP32 SoA positions being their rounding.  A
+ * master is the starting point when it rounds to the SoA's FP32 value;
+ * otherwise (the FP32 position was written by someone else, or the master
+ * was never set) the FP32 value is.  The result is stored in both.
+ * pos64 = NULL is or_mech_integrate. */
+void or_mech_integrate_master(float* soa, uint32_t max_cells, uint32_t n_cells, const or_mech* m,
+                              float x_min, float y_min, float z_min, float dt, double* pos64);
+
 /* Voxel refresh from positions (3-D aware form of cell_phenotype.cpp:781-789):
  * voxel_index = Microenvironment::voxelIndex(x, y, z) (microenvironment.mm:261-269). */
 void or_voxel_refresh(float* soa, uint32_t max_cells, uint32_t n_cells, const or_grid* g);
@@ -168,6 +177,7 @@ typedef struct {
     or_mech mech;                 /* mechanics grid */
     float dt_mechanics;
     int refresh_voxels;           /* recompute voxel_index after integrate */
+    double* pos64;                /* FP64 master positions (or_mech_integrate_master), or NULL */
 } or_sim;
 
 /* ---------------------------------------------------------------- motility

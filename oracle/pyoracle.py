@@ -57,7 +57,7 @@ class Mech(C.Structure):
 
 class Sim(C.Structure):
     _fields_ = [("grid", Grid), ("subs", C.POINTER(Substrate)), ("mech", Mech),
-                ("dt_mechanics", C.c_float), ("refresh_voxels", C.c_int)]
+                ("dt_mechanics", C.c_float), ("refresh_voxels", C.c_int), ("pos64", C.POINTER(C.c_double))]
 
 
 def make_grid(nx, ny, nz, S, dx=20.0, dt=0.01, x_min=0.0, y_min=0.0, z_min=0.0, dy=None, dz=None):
@@ -213,9 +213,16 @@ def mech_forces(soa, max_cells, n, m, key, order, start):
     return cnt[:n], hsh[:n], scale[:n]
 
 
-def mech_integrate(soa, max_cells, n, m, origin, dt):
-    oracle().or_mech_integrate(_p(soa, _F32), _U32(max_cells), _U32(n), C.byref(m), _F32(origin[0]),
-                               _F32(origin[1]), _F32(origin[2]), _F32(dt))
+def mech_integrate(soa, max_cells, n, m, origin, dt, pos64=None):
+    """AB2 in place; with pos64 (3 * max_cells doubles) on FP64 master
+    positions (or_mech_integrate_master)."""
+    if pos64 is None:
+        oracle().or_mech_integrate(_p(soa, _F32), _U32(max_cells), _U32(n), C.byref(m), _F32(origin[0]),
+                                   _F32(origin[1]), _F32(origin[2]), _F32(dt))
+        return
+    assert pos64.dtype == np.float64 and pos64.size >= 3 * max_cells
+    oracle().or_mech_integrate_master(_p(soa, _F32), _U32(max_cells), _U32(n), C.byref(m), _F32(origin[0]),
+                                      _F32(origin[1]), _F32(origin[2]), _F32(dt), _p(pos64, _F64))
 
 
 def voxel_refresh(soa, max_cells, n, grid):
@@ -235,16 +242,26 @@ def cells_remove(soa, max_cells, n, S, sec, upt, sat, ne, active, indices):
                                _opt(sat, _F64), _opt(ne, _F64), _opt(active, _U8), _p(idx, _U32), _U32(idx.size))
 
 
+def master_positions(soa, max_cells):
+    """FP64 master positions equal to the SoA's FP32 positions."""
+    return np.ascontiguousarray(soa[:3 * max_cells], np.float64).copy()
+
+
 def nbr_hash(j):
     return oracle().or_nbr_hash(_U32(j))
 
 
 def run(grid, subs, mech, dt_mech, density, soa, max_cells, n, sec, upt, sat, ne, active, steps,
-        accum=0.0, refresh=False, motility=None, seed=0, mot_step=0, layout=0):
+        accum=0.0, refresh=False, motility=None, seed=0, mot_step=0, layout=0, pos64=None):
     """The main loop (or_run).  With a motility state (motility_state), the
     motility phase runs between forces and integrate and the state is
-    updated in place; returns (accumulator, next motility step) then."""
-    sim = Sim(grid, C.cast(subs, C.POINTER(Substrate)), mech, dt_mech, 1 if refresh else 0)
+    updated in place; returns (accumulator, next motility step) then.
+    pos64 (3 * max_cells doubles, updated in place): FP64 master positions
+    for the AB2 update (master_positions() gives the starting masters)."""
+    if pos64 is not None:
+        assert pos64.dtype == np.float64 and pos64.size >= 3 * max_cells and pos64.flags.c_contiguous
+    sim = Sim(grid, C.cast(subs, C.POINTER(Substrate)), mech, dt_mech, 1 if refresh else 0,
+              None if pos64 is None else _p(pos64, _F64))
     acc = C.c_double(accum)
     sec, upt, sat, ne = (np.ascontiguousarray(a, np.float64) for a in (sec, upt, sat, ne))
     act = None if active is None else np.ascontiguousarray(active, np.uint8)

@@ -135,6 +135,7 @@ _SIGS = [
     ("pcg_cells_append", C.c_int, [_P, _F32P, C.c_uint32, C.c_uint32, _F64P, _F64P, _F64P, _F64P, _U8P]),
     ("pcg_cells_download_secretion", C.c_int, [_P, _F64P, _F64P, _F64P, _F64P, _U8P]),
     ("pcg_cells_device_soa", C.c_int, [_P, C.POINTER(_F32P), _U32P]),
+    ("pcg_cells_download_positions64", C.c_int, [_P, _F64P, C.c_uint32]),
     ("pcg_mech_create", C.c_int, [_P, C.POINTER(MechanicsParams), C.c_float, C.c_float, C.c_float,
                                   C.c_uint32, C.POINTER(_P)]),
     ("pcg_mech_destroy", C.c_int, [_P]),
@@ -167,6 +168,7 @@ _SIGS = [
     ("pcg_batch_download_density", C.c_int, [_P, C.c_uint32, _F32P, C.c_size_t]),
     ("pcg_batch_download_cells", C.c_int, [_P, C.c_uint32, _F32P, C.c_uint32]),
     ("pcg_batch_upload_cells", C.c_int, [_P, C.c_uint32, _F32P, C.c_uint32]),
+    ("pcg_batch_download_positions64", C.c_int, [_P, C.c_uint32, _F64P, C.c_uint32]),
     ("pcg_batch_upload_all_cells", C.c_int, [_P, _F32P, C.c_uint64]),
     ("pcg_batch_download_all_cells", C.c_int, [_P, _F32P, C.c_uint64]),
     ("pcg_batch_download_all_density", C.c_int, [_P, _F32P, C.c_uint64]),
@@ -178,6 +180,8 @@ _SIGS = [
     ("pcg_batch_step_launches", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_batch_phase_times", C.c_int, [_P, _F32P, C.POINTER(C.c_uint64), C.c_int]),
     ("pcg_batch_set_profile", C.c_int, [_P, C.c_int]),
+    ("pcg_batch_set_diagnostics", C.c_int, [_P, C.c_int]),
+    ("pcg_batch_mech_bins", C.c_int, [_P, C.c_uint32, _U32P, _U32P, _U32P, _U32P]),
     ("pcg_batch_describe", C.c_char_p, [_P]),
     ("pcg_serve_create", C.c_int, [_P, C.POINTER(ServeOptions), C.POINTER(_P)]),
     ("pcg_serve_destroy", C.c_int, [_P]),
@@ -188,6 +192,8 @@ _SIGS = [
     ("pcg_serve_request_times", C.c_int, [_P, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("pcg_serve_totals", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_instance_bytes", C.c_uint64, [C.POINTER(InstanceDesc)]),
+    ("pcg_debug_alloc_stats", None, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("pcg_debug_fail_alloc", None, [C.c_uint64]),
 ]
 
 
@@ -423,6 +429,13 @@ class Cells:
         out = np.zeros(NUM_FIELDS * soa_max, np.float32)
         self.ctx.check(lib().pcg_cells_download(self.h, _f32(out), soa_max))
         return out
+
+    def positions64(self):
+        """FP64 master positions of the current cells: (3, n) array."""
+        n = self.count()
+        out = np.zeros(3 * max(n, 1), np.float64)
+        self.ctx.check(lib().pcg_cells_download_positions64(self.h, _f64(out), n))
+        return out[:3 * n].reshape(3, n)
 
     def upload_fields(self, first, count, soa, soa_max):
         soa = np.ascontiguousarray(soa, np.float32)
@@ -697,6 +710,13 @@ class Batch:
         soa = np.ascontiguousarray(soa, np.float32)
         self.ctx.check(lib().pcg_batch_upload_cells(self.h, i, _f32(soa), soa_max))
 
+    def positions64(self, i):
+        """Instance i's FP64 master positions: (3, n) array (x, y, z)."""
+        n = self.instances[i].n_cells
+        out = np.zeros(3 * max(n, 1), np.float64)
+        self.ctx.check(lib().pcg_batch_download_positions64(self.h, i, _f64(out), n))
+        return out[:3 * n].reshape(3, n)
+
     def totals(self):
         v, vs, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
         self.ctx.check(lib().pcg_batch_totals(self.h, C.byref(v), C.byref(vs), C.byref(c)))
@@ -741,6 +761,24 @@ class Batch:
 
     def describe(self):
         return (lib().pcg_batch_describe(self.h) or b"").decode()
+
+    def set_diagnostics(self, on=True):
+        self.ctx.check(lib().pcg_batch_set_diagnostics(self.h, 1 if on else 0))
+
+    def mech_bins(self, i, stats=False):
+        """Instance i after its last mechanics step: (start[V+1],
+        sorted_cells[n]) and, with stats (diagnostics on), the neighbour
+        counts and hashes by cell."""
+        inst = self.instances[i]
+        m, n = inst.mech, inst.n_cells
+        start = np.zeros(m.mech_grid_nx * m.mech_grid_ny * m.mech_grid_nz + 1, np.uint32)
+        order = np.zeros(max(n, 1), np.uint32)
+        cnt = np.zeros(max(n, 1), np.uint32) if stats else None
+        hsh = np.zeros(max(n, 1), np.uint32) if stats else None
+        self.ctx.check(lib().pcg_batch_mech_bins(self.h, i, _u32(start), _u32(order), _u32(cnt), _u32(hsh)))
+        if stats:
+            return start, order[:n], cnt[:n], hsh[:n]
+        return start, order[:n]
 
     def close(self):
         if getattr(self, "h", None):

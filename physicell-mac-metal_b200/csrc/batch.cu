@@ -145,6 +145,11 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
                                             cudaMemcpyDeviceToDevice, ctx->stream));
             PCG_CU(ctx, cudaMemcpyAsync(c_.active.as<uint8_t>() + coff, sb.c_.active.as<uint8_t>() + so.cell_off,
                                         ds.n_cells, cudaMemcpyDeviceToDevice, ctx->stream));
+            PCG_CU(ctx, cudaMemcpy2DAsync(c_.pos64.as<double>() + coff, static_cast<size_t>(c_.max_cells) * sizeof(double),
+                                          sb.c_.pos64.as<double>() + so.cell_off,
+                                          static_cast<size_t>(sb.c_.max_cells) * sizeof(double),
+                                          static_cast<size_t>(ds.n_cells) * sizeof(double), 3,
+                                          cudaMemcpyDeviceToDevice, ctx->stream));
             if (sb.c_.has_active) c_.has_active = true;
             c_.coef_dirty = c_.order_dirty = true;
         } else if (ds.n_cells) {
@@ -314,6 +319,19 @@ int Batch::step_masked(const uint8_t* mask_host, bool any_mech)
     return PCG_OK;
 }
 
+int Batch::set_diagnostics(bool on)
+{
+    if (m_.diag == on) return PCG_OK;
+    m_.diag = on;
+    if (!use_graphs) return PCG_OK;
+    PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    if (g_mech) {
+        cudaGraphExecDestroy(g_mech);
+        g_mech = nullptr;
+    }
+    return capture(true, &g_mech, &launches_mech);
+}
+
 std::string Batch::describe() const
 {
     std::ostringstream o;
@@ -378,6 +396,14 @@ pcg_status pcg_batch_download_cells(pcg_batch* b, uint32_t i, float* soa, uint32
     PCG_TRY(b->b.c_.download_soa(ci.cell_off, ci.n_cells, soa, soa_max, 0, NUM_FIELDS));
     PCG_CU(b->b.ctx, cudaStreamSynchronize(b->b.ctx->stream));
     return PCG_OK;
+}
+
+pcg_status pcg_batch_download_positions64(pcg_batch* b, uint32_t i, double* xyz, uint32_t n_cells)
+{
+    if (!b || i >= b->b.ncell.size() || (!xyz && n_cells)) return PCG_ERR_INVALID;
+    const CellInst& ci = b->b.c_.h_inst[i];
+    if (n_cells != ci.n_cells) return fail(b->b.ctx, PCG_ERR_INVALID, "n_cells must equal the instance's cell count");
+    return b->b.c_.download_positions(ci.cell_off, n_cells, xyz);
 }
 
 pcg_status pcg_batch_upload_cells(pcg_batch* b, uint32_t i, const float* soa, uint32_t soa_max)
@@ -542,6 +568,43 @@ pcg_status pcg_batch_phase_times(pcg_batch* b, float* ms, uint64_t* n_sweep_step
         for (int q = 0; q < PCG_N_PHASES; ++q) b->b.phase_ms[q] = 0.0;
         b->b.sweep_steps = 0;
     }
+    return PCG_OK;
+}
+
+pcg_status pcg_batch_set_diagnostics(pcg_batch* b, int on)
+{
+    if (!b) return PCG_ERR_INVALID;
+    return b->b.set_diagnostics(on != 0);
+}
+
+pcg_status pcg_batch_mech_bins(pcg_batch* b, uint32_t i, uint32_t* start, uint32_t* sorted_cells,
+                               uint32_t* nbr_count, uint32_t* nbr_hash)
+{
+    if (!b || i >= b->b.ncell.size()) return PCG_ERR_INVALID;
+    Batch& B = b->b;
+    pcg_ctx* ctx = B.ctx;
+    if ((nbr_count || nbr_hash) && !B.m_.diag) return fail(ctx, PCG_ERR_INVALID, "diagnostics are off");
+    const CellInst& ci = B.c_.h_inst[i];
+    const size_t V = static_cast<size_t>(ci.mnx) * ci.mny * ci.mnz;
+    PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    std::vector<uint32_t> st(V + 1);
+    PCG_CU(ctx, cudaMemcpy(st.data(), B.m_.start.as<uint32_t>() + ci.mvox_base, (V + 1) * sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost));
+    const uint32_t first = st[0];
+    if (st[V] - first != ci.n_cells) return fail(ctx, PCG_ERR_INVALID, "no mechanics step has binned this instance");
+    if (start)
+        for (size_t v = 0; v <= V; ++v) start[v] = st[v] - first;
+    if (sorted_cells && ci.n_cells) {
+        PCG_CU(ctx, cudaMemcpy(sorted_cells, B.m_.sorder.as<uint32_t>() + first, ci.n_cells * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost));
+        for (uint32_t q = 0; q < ci.n_cells; ++q) sorted_cells[q] -= ci.cell_off;
+    }
+    if (nbr_count && ci.n_cells)
+        PCG_CU(ctx, cudaMemcpy(nbr_count, B.m_.dcnt.as<uint32_t>() + ci.cell_off, ci.n_cells * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost));
+    if (nbr_hash && ci.n_cells)
+        PCG_CU(ctx, cudaMemcpy(nbr_hash, B.m_.dhash.as<uint32_t>() + ci.cell_off, ci.n_cells * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost));
     return PCG_OK;
 }
 

@@ -63,6 +63,9 @@ public:
     int run_step(bool mech, bool timed, const uint8_t* mask);
     uint64_t count_launches(bool mech) const;
     std::string describe() const;
+    // Neighbour-set diagnostics of the force pass (the mechanics graph is
+    // captured again with them).
+    int set_diagnostics(bool on);
 
 private:
     int capture(bool mech, cudaGraphExec_t* out, uint64_t* launches);

@@ -483,7 +483,7 @@ pcg_status pcg_cells_remove(pcg_cells* c, const uint32_t* indices, uint32_t coun
         const uint64_t rate_cap = c->c.rates.bytes / (4 * sizeof(double));
         PCG_CU(c->ctx, launch_cells_move(c->ctx->stream, c->c.soa.as<float>(), c->c.max_cells, dm.as<uint2>(),
                                          static_cast<uint32_t>(moves.size()), c->c.rates.as<double>(), rate_cap, c->S,
-                                         c->c.active.as<uint8_t>()));
+                                         c->c.active.as<uint8_t>(), c->c.pos64.as<double>()));
         c->ctx->launches++;
         PCG_CU(c->ctx, cudaStreamSynchronize(c->ctx->stream));   // the move list is released on return
     }
@@ -505,6 +505,7 @@ pcg_status pcg_cells_append(pcg_cells* c, const float* soa, uint32_t count, uint
     if (static_cast<uint64_t>(c->c.n) + count > c->c.max_cells) return bad(c->ctx, "appending past max_cells");
     const uint32_t n0 = c->c.n;
     PCG_TRY(c->c.upload_soa(n0, count, soa, soa_max, 0, NUM_FIELDS));
+    PCG_TRY(c->c.clear_masters(n0, count));   // places past the count may hold removed cells' masters
     PCG_TRY(c->c.set_rates(n0 * c->S, count * c->S, sec, upt, sat, ne));
     PCG_TRY(c->c.set_active(n0, count, active));
     c->c.n = n0 + count;
@@ -513,6 +514,13 @@ pcg_status pcg_cells_append(pcg_cells* c, const float* soa, uint32_t count, uint
     c->c.coef_dirty = c->c.order_dirty = true;
     PCG_CU(c->ctx, cudaStreamSynchronize(c->ctx->stream));
     return PCG_OK;
+}
+
+pcg_status pcg_cells_download_positions64(pcg_cells* c, double* xyz, uint32_t n_cells)
+{
+    if (!c || (!xyz && n_cells)) return PCG_ERR_INVALID;
+    if (n_cells != c->c.n) return bad(c->ctx, "n_cells must equal the current cell count");
+    return c->c.download_positions(0, n_cells, xyz);
 }
 
 pcg_status pcg_cells_count(pcg_cells* c, uint32_t* n)
@@ -624,5 +632,12 @@ pcg_status pcg_mech_neighbor_stats(pcg_mech* m, uint32_t* count, uint32_t* hash)
     if (hash && n) PCG_CU(ctx, cudaMemcpy(hash, m->m.dhash.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     return PCG_OK;
 }
+
+void pcg_debug_alloc_stats(uint64_t* device_mallocs, uint64_t* pool_reuses)
+{
+    alloc_stats(device_mallocs, pool_reuses);
+}
+
+void pcg_debug_fail_alloc(uint64_t nth) { fail_alloc_after(nth); }
 
 }  // extern "C"

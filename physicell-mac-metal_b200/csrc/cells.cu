@@ -219,12 +219,12 @@ __global__ void __launch_bounds__(256, 6) k_secrete(float* __restrict__ dens, co
 // at or past the new cell count and every destination before it, so no copy
 // reads a place that another copy writes.  One thread per (move, item): the
 // 28 SoA fields (copied as bits), the four per-substrate rate arrays, the
-// active flag.
+// active flag and the three FP64 master positions.
 __global__ void k_cells_move(uint32_t* __restrict__ soa, uint32_t stride, const uint2* __restrict__ moves,
                              uint32_t n_moves, double* __restrict__ rates, uint64_t rate_cap, uint32_t S,
-                             uint8_t* __restrict__ active)
+                             uint8_t* __restrict__ active, double* __restrict__ pos64)
 {
-    const uint32_t items = NUM_FIELDS + 4u * S + 1u;
+    const uint32_t items = NUM_FIELDS + 4u * S + 1u + 3u;
     const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= static_cast<uint64_t>(n_moves) * items) return;
     const uint32_t m = static_cast<uint32_t>(t / items), it = static_cast<uint32_t>(t % items);
@@ -235,8 +235,11 @@ __global__ void k_cells_move(uint32_t* __restrict__ soa, uint32_t stride, const 
         const uint32_t q = (it - NUM_FIELDS) / S, s = (it - NUM_FIELDS) % S;
         double* r = rates + q * rate_cap;
         r[static_cast<size_t>(dst) * S + s] = r[static_cast<size_t>(src) * S + s];
-    } else {
+    } else if (it == NUM_FIELDS + 4u * S) {
         active[dst] = active[src];
+    } else if (pos64) {
+        const size_t a = it - (NUM_FIELDS + 4u * S + 1u);
+        pos64[a * stride + dst] = pos64[a * stride + src];
     }
 }
 
@@ -417,10 +420,13 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
     }
 }
 
-// AB2 in FP64 with explicit rounding, stored FP32: the FP64 value of
-// p + dt (1.5 v - 0.5 v_prev) rounded once (integrate.metal:273-285 keeps
-// FP32 storage; the oracle forms the same FP64 expression).
-__global__ void k_mech_integrate(float* __restrict__ soa, uint32_t stride, uint32_t n,
+// AB2 in FP64 with explicit rounding (integrate.metal:58-69 forms
+// p + dt (1.5 v - 0.5 v_prev) and clamps it to the box of the mechanics
+// grid): the FP64 value is clamped, kept as the cell's master position and
+// rounded once into the FP32 SoA.  The update starts from the master while
+// it rounds to the SoA's FP32 value, else (no master yet, or the FP32
+// position was written since) from the FP32 value.
+__global__ void k_mech_integrate(float* __restrict__ soa, double* __restrict__ pos64, uint32_t stride, uint32_t n,
                                  const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
                                  float dt_override, const uint8_t* __restrict__ mask)
 {
@@ -438,10 +444,17 @@ __global__ void k_mech_integrate(float* __restrict__ soa, uint32_t stride, uint3
         float* p = soa + static_cast<size_t>(F_POS_X + a) * stride + g;
         const float v = soa[static_cast<size_t>(F_VEL_X + a) * stride + g];
         float* pv = soa + static_cast<size_t>(F_PREV_VX + a) * stride + g;
+        const float p32 = *p;
+        double x0 = static_cast<double>(p32);
+        if (pos64) {
+            const double m = pos64[static_cast<size_t>(a) * stride + g];
+            if (__double2float_rn(m) == p32) x0 = m;
+        }
         const double inc = __dsub_rn(__dmul_rn(1.5, static_cast<double>(v)), __dmul_rn(0.5, static_cast<double>(*pv)));
-        double x = __dadd_rn(static_cast<double>(*p), __dmul_rn(dt, inc));
+        double x = __dadd_rn(x0, __dmul_rn(dt, inc));
         if (x < static_cast<double>(lo[a])) x = lo[a];
         if (x > static_cast<double>(hi[a])) x = hi[a];
+        if (pos64) pos64[static_cast<size_t>(a) * stride + g] = x;
         pos[a] = __double2float_rn(x);
         *p = pos[a];
         *pv = v;
@@ -509,12 +522,12 @@ cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_sta
 }
 
 cudaError_t launch_cells_move(cudaStream_t st, float* soa, uint32_t stride, const uint2* moves, uint32_t n_moves,
-                              double* rates, uint64_t rate_cap, uint32_t S, uint8_t* active)
+                              double* rates, uint64_t rate_cap, uint32_t S, uint8_t* active, double* pos64)
 {
-    const uint64_t work = static_cast<uint64_t>(n_moves) * (NUM_FIELDS + 4u * S + 1u);
+    const uint64_t work = static_cast<uint64_t>(n_moves) * (NUM_FIELDS + 4u * S + 1u + 3u);
     if (work == 0) return cudaSuccess;
     k_cells_move<<<blocks_for(work, 256), 256, 0, st>>>(reinterpret_cast<uint32_t*>(soa), stride, moves, n_moves, rates,
-                                                       rate_cap, S, active);
+                                                       rate_cap, S, active, pos64);
     return cudaGetLastError();
 }
 
@@ -550,11 +563,12 @@ cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4
     return cudaGetLastError();
 }
 
-cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, uint32_t stride, uint32_t n, const uint32_t* cell_inst,
-                                  const CellInst* insts, float dt_override, const uint8_t* mask)
+cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, double* pos64, uint32_t stride, uint32_t n,
+                                  const uint32_t* cell_inst, const CellInst* insts, float dt_override,
+                                  const uint8_t* mask)
 {
     if (n == 0) return cudaSuccess;
-    k_mech_integrate<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, dt_override, mask);
+    k_mech_integrate<<<blocks_for(n, 256), 256, 0, st>>>(soa, pos64, stride, n, cell_inst, insts, dt_override, mask);
     return cudaGetLastError();
 }
 

@@ -34,8 +34,31 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 unsigned char* g_addr[kMaxDevices] = {};
 
-// Device address of g_sort_scratch on ctx's device, looked up once per
-// device with that device current.
+// Makes ctx's device current for the life of the guard and puts the
+// caller's device back afterwards.
+class DeviceGuard {
+public:
+    cudaError_t enter(int device)
+    {
+        cudaError_t e = cudaGetDevice(&prev_);
+        if (e != cudaSuccess) return e;
+        if (prev_ == device) return cudaSuccess;
+        e = cudaSetDevice(device);
+        if (e == cudaSuccess) switched_ = true;
+        return e;
+    }
+    ~DeviceGuard()
+    {
+        if (switched_) cudaSetDevice(prev_);
+    }
+private:
+    int prev_ = -1;
+    bool switched_ = false;
+};
+
+// Device address of g_sort_scratch on ctx's device (the current device),
+// looked up once per device; the same set-up loads the sort's kernels, so
+// that no later call loads a module (which can allocate device memory).
 int scratch_for(pcg_ctx* ctx, unsigned char** out)
 {
     if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, PCG_ERR_INVALID, "device index out of range");
@@ -43,16 +66,9 @@ int scratch_for(pcg_ctx* ctx, unsigned char** out)
     if (!g_addr[ctx->device]) {
         if (radix_sort_scratch_bytes(kStaticMaxPairs, 32) > kHistBytes)
             return fail(ctx, PCG_ERR_INVALID, "static sort scratch reservation is smaller than the sort needs");
-        int prev = -1;
-        PCG_CU(ctx, cudaGetDevice(&prev));
-        if (prev != ctx->device) PCG_CU(ctx, cudaSetDevice(ctx->device));
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
-        if (prev != ctx->device) {
-            const cudaError_t e2 = cudaSetDevice(prev);
-            if (e == cudaSuccess && e2 != cudaSuccess) return cuda_fail(ctx, e2, "cudaSetDevice (restore)");
-        }
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(g_sort_scratch)");
+        PCG_CU(ctx, cudaGetSymbolAddress(&p, g_sort_scratch));
+        PCG_CU(ctx, sort_kernels_load());
         g_addr[ctx->device] = static_cast<unsigned char*>(p);
     }
     *out = g_addr[ctx->device];
@@ -79,6 +95,8 @@ extern "C" pcg_status pcg_sort_pairs_static(pcg_ctx* ctx, const uint32_t* keys_i
     if (n > kStaticMaxPairs)
         return fail(ctx, PCG_ERR_INVALID, "pcg_sort_pairs_static: n = " + std::to_string(n) + " exceeds the static limit of " +
                                               std::to_string(kStaticMaxPairs) + " pairs");
+    DeviceGuard guard;   // the context's device stays current for the whole call
+    PCG_CU(ctx, guard.enter(ctx->device));
     unsigned char* scr = nullptr;
     PCG_TRY(scratch_for(ctx, &scr));
     if (n == 0) return PCG_OK;

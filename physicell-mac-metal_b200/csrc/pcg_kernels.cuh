@@ -257,11 +257,13 @@ cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4
                                const uint32_t* cell_inst, const CellInst* insts, float* soa, uint32_t stride,
                                uint32_t* diag_cnt, uint32_t* diag_hash, const uint8_t* mask, int block);
 // Copies of a removal plan: (dst, src) pairs, each cell's 28 SoA fields,
-// 4 x S rates (arrays of rate_cap doubles, [cell * S + s]) and active flag.
+// 4 x S rates (arrays of rate_cap doubles, [cell * S + s]), active flag and
+// three FP64 master positions (arrays of stride doubles; pos64 may be null).
 cudaError_t launch_cells_move(cudaStream_t st, float* soa, uint32_t stride, const uint2* moves, uint32_t n_moves,
-                              double* rates, uint64_t rate_cap, uint32_t S, uint8_t* active);
-// dt_override >= 0 replaces every instance's dt_mech.
-cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
+                              double* rates, uint64_t rate_cap, uint32_t S, uint8_t* active, double* pos64);
+// dt_override >= 0 replaces every instance's dt_mech.  pos64: FP64 master
+// positions (three arrays of stride doubles) or null for FP32 positions.
+cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, double* pos64, uint32_t stride, uint32_t n,
                                   const uint32_t* cell_inst, const CellInst* insts, float dt_override,
                                   const uint8_t* mask);
 // Threads per cell in the force pass: one, summing in the reference's
@@ -276,6 +278,10 @@ int radix_sort_launches(uint32_t n, int bits);
 cudaError_t radix_sort_pairs(cudaStream_t st, const uint32_t* k_in, const uint32_t* v_in,
                              uint32_t* k_out, uint32_t* v_out, uint32_t* k_tmp, uint32_t* v_tmp,
                              uint32_t n, int bits, void* scratch);
+
+// Loads the radix sort's and the scan's kernels on the current device now
+// rather than at their first launch.
+cudaError_t sort_kernels_load();
 
 // Exclusive prefix sum of n uint32 values (in may equal out).
 size_t scan_scratch_bytes(uint64_t n);

@@ -31,15 +31,30 @@ int cuda_fail(pcg_ctx* ctx, cudaError_t e, const char* what)
 // that was allocated under an AllocStream goes back to the pool with an
 // event recorded on that stream; it is handed out again only once the event
 // has completed, so no kernel still using it can see it reused, and nothing
-// synchronises the device (cudaFree would).  Blocks are reused best-fit
-// within 1/8 (+ 1 MiB) of the request.  On an allocation failure the idle
-// blocks are returned to the driver and the allocation is retried.  The
-// pool lives until process exit (never destroyed, so no CUDA call runs
-// during static destruction).
+// synchronises the device (cudaFree would).  Requests are rounded up to a
+// size class (512-byte steps below 4 KiB, above it four classes per power of
+// two) and a free block of exactly that class is reused.  On an allocation
+// failure the idle blocks are returned to the driver and the allocation is
+// retried.  The pool lives until process exit (never destroyed, so no CUDA
+// call runs during static destruction).
 
 namespace {
 
 thread_local cudaStream_t tl_alloc_stream = nullptr;
+
+// Library-wide allocation counters and the host-side failure injector
+// (pcg_debug_alloc_stats / pcg_debug_fail_alloc).
+std::atomic<uint64_t> g_mallocs{0}, g_reuses{0}, g_fail_in{0};
+
+// True when the injector says this allocation is to fail.
+bool injected_failure()
+{
+    uint64_t v = g_fail_in.load();
+    while (v > 0) {
+        if (g_fail_in.compare_exchange_weak(v, v - 1)) return v == 1;
+    }
+    return false;
+}
 
 struct PoolBlock {
     void* p;
@@ -73,6 +88,7 @@ public:
                 *got = it->first;
                 cudaEventDestroy(it->second.ev);
                 free_.erase(it);
+                g_reuses++;
                 return cudaSuccess;
             }
         }
@@ -86,6 +102,7 @@ public:
             *out = nullptr;
             return e;
         }
+        g_mallocs++;
         *got = b;
         return cudaSuccess;
     }
@@ -151,6 +168,7 @@ cudaError_t DevBuf::alloc(size_t b)
 {
     release();
     if (b == 0) return cudaSuccess;
+    if (injected_failure()) return cudaErrorMemoryAllocation;
     if (tl_alloc_stream) {
         size_t got = 0;
         const cudaError_t e = DevicePool::get().take(b, &p, &got, &dev_);
@@ -168,11 +186,20 @@ cudaError_t DevBuf::alloc(size_t b)
         p = nullptr;
         return e;
     }
+    g_mallocs++;
     bytes = b;
     cap_ = 0;
     stream_ = nullptr;
     return cudaSuccess;
 }
+
+void alloc_stats(uint64_t* mallocs, uint64_t* reuses)
+{
+    if (mallocs) *mallocs = g_mallocs.load();
+    if (reuses) *reuses = g_reuses.load();
+}
+
+void fail_alloc_after(uint64_t nth) { g_fail_in.store(nth); }
 
 void DevBuf::release()
 {
@@ -1132,6 +1159,8 @@ int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_
     PCG_CU(ctx, coef_flags.alloc(h_inst.size() * sizeof(uint32_t)));
     PCG_CU(ctx, cudaMemsetAsync(coef_flags.p, 0xFF, coef_flags.bytes, ctx->stream));   // all terms until prepared
     PCG_CU(ctx, active.alloc(max_cells));
+    PCG_CU(ctx, pos64.alloc(3ull * max_cells * sizeof(double)));
+    PCG_CU(ctx, cudaMemsetAsync(pos64.p, 0xFF, pos64.bytes, ctx->stream));   // no masters yet
     for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp, &run_slot})
         PCG_CU(ctx, b->alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint32_t)));
     PCG_CU(ctx, run_dens.alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint64_t)));
@@ -1219,6 +1248,29 @@ int Cells::set_cell_instances(const std::vector<uint32_t>& counts)
     return PCG_OK;
 }
 
+int Cells::clear_masters(uint32_t off, uint32_t count)
+{
+    if (count == 0) return PCG_OK;
+    for (int a = 0; a < 3; ++a)
+        PCG_CU(ctx, cudaMemsetAsync(pos64.as<double>() + static_cast<size_t>(a) * max_cells + off, 0xFF,
+                                    static_cast<size_t>(count) * sizeof(double), ctx->stream));
+    return PCG_OK;
+}
+
+int Cells::download_positions(uint32_t off, uint32_t count, double* xyz)
+{
+    if (count == 0) return PCG_OK;
+    std::vector<float> p32(3ull * count);
+    PCG_CU(ctx, cudaMemcpy2DAsync(xyz, static_cast<size_t>(count) * sizeof(double), pos64.as<double>() + off,
+                                  static_cast<size_t>(max_cells) * sizeof(double),
+                                  static_cast<size_t>(count) * sizeof(double), 3, cudaMemcpyDeviceToHost, ctx->stream));
+    PCG_TRY(download_soa(off, count, p32.data(), count, F_POS_X, 3));
+    PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    for (size_t q = 0; q < 3ull * count; ++q)
+        if (static_cast<float>(xyz[q]) != p32[q]) xyz[q] = p32[q];
+    return PCG_OK;
+}
+
 int Cells::build_order(uint64_t total_vox)
 {
     PCG_TRY(sync_inst());
@@ -1281,7 +1333,7 @@ int Cells::secrete(Diffusion& d, const uint8_t* mask)
 
 uint64_t Cells::device_bytes() const
 {
-    return inst.bytes + soa.bytes + cell_inst.bytes + rates.bytes + coef.bytes + coef_flags.bytes + active.bytes +
+    return inst.bytes + soa.bytes + pos64.bytes + cell_inst.bytes + rates.bytes + coef.bytes + coef_flags.bytes + active.bytes +
            keys.bytes + vals.bytes +
            skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + sbeg.bytes + run_scr.bytes +
            run_dens.bytes + run_slot.bytes;
@@ -1360,8 +1412,8 @@ int Mechanics::integrate(Cells& c, float dt_override, const uint8_t* mask)
 {
     if (c.n == 0) return PCG_OK;
     PCG_TRY(c.sync_inst());
-    cudaError_t e = launch_mech_integrate(ctx->stream, c.soa.as<float>(), c.max_cells, c.n, c.cell_inst.as<uint32_t>(),
-                                          c.inst.as<CellInst>(), dt_override, mask);
+    cudaError_t e = launch_mech_integrate(ctx->stream, c.soa.as<float>(), c.pos64.as<double>(), c.max_cells, c.n,
+                                          c.cell_inst.as<uint32_t>(), c.inst.as<CellInst>(), dt_override, mask);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "integrate launch");
     ctx->launches++;
     bool refresh = false;

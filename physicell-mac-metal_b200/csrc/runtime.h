@@ -111,6 +111,13 @@ private:
     int dev_ = 0;                      // device of the pool block
 };
 
+// Device allocations the library has made with cudaMalloc, and pool blocks
+// it has handed out again, since the process started.
+void alloc_stats(uint64_t* mallocs, uint64_t* reuses);
+// Failure injection on the host: the nth DevBuf allocation from now fails
+// with cudaErrorMemoryAllocation without touching the device (0 = off).
+void fail_alloc_after(uint64_t nth);
+
 // Page-locked host allocation (staging for end-to-end copies).
 struct HostBuf {
     void* p = nullptr;
@@ -243,6 +250,12 @@ public:
     uint32_t n_rate = 0;          // sum over instances of n_cells * S
     std::vector<CellInst> h_inst;
     DevBuf inst, soa, cell_inst, rates, coef, coef_flags, active;
+    // FP64 master positions, three arrays of max_cells (x, y, z); the SoA's
+    // FP32 positions are their rounding.  The AB2 update starts from a
+    // master only while it rounds to the SoA's value, so a position written
+    // through the SoA (uploads, host edits) replaces the master.  All-ones
+    // (NaN) = no master.
+    DevBuf pos64;
     bool has_active = false;
     bool inst_dirty = true, coef_dirty = true, order_dirty = true;
     double coef_dt = -1.0;
@@ -266,6 +279,12 @@ public:
                   const double* ne);
     int set_active(uint32_t cell_off, uint32_t count, const uint8_t* act);
     int set_cell_instances(const std::vector<uint32_t>& per_instance_counts);
+    // Drop the masters of cells [off, off + count) (their FP32 positions count).
+    int clear_masters(uint32_t off, uint32_t count);
+    // Positions of cells [off, off + count) as the AB2 update would start
+    // from them (the master where it rounds to the FP32 value, else the FP32
+    // value): three host arrays of count doubles at xyz.
+    int download_positions(uint32_t off, uint32_t count, double* xyz);
     // Recompute secretion constants / ordering when stale.
     int prepare_secretion(double dt, uint64_t total_vox);
     int build_order(uint64_t total_vox);   // order, runs and (once a dt is known) the constants

@@ -183,6 +183,20 @@ __global__ void __launch_bounds__(kThreads) k_scan_add(uint32_t* __restrict__ ou
 
 static uint64_t tiles_of(uint64_t n) { return (n + kTile - 1) / kTile; }
 
+cudaError_t sort_kernels_load()
+{
+    // querying a kernel's attributes loads its module on the current device
+    // (lazy loading defers that to the first launch otherwise)
+    cudaFuncAttributes a;
+    const void* ks[] = {reinterpret_cast<const void*>(&k_radix_hist), reinterpret_cast<const void*>(&k_radix_scatter),
+                        reinterpret_cast<const void*>(&k_scan_tiles), reinterpret_cast<const void*>(&k_scan_add)};
+    for (const void* k : ks) {
+        const cudaError_t e = cudaFuncGetAttributes(&a, k);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 size_t scan_scratch_bytes(uint64_t n)
 {
     size_t bytes = 0;

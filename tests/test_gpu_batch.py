@@ -174,7 +174,9 @@ def test_batch_instance_matches_oracle(ctx, pcg, po):
                      m.mechanics_voxel_size, m.mech_grid_nx, m.mech_grid_ny, m.mech_grid_nz)
         dens = np.repeat(inst.initial_values, g.nx * g.ny * g.nz).astype(np.float32)
         soa = inst.soa.copy()
-        po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, steps, refresh=bool(inst.flags & 1))
+        pm = po.master_positions(soa, n)
+        po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, steps, refresh=bool(inst.flags & 1),
+               pos64=pm)
         b = np.asarray(dens, np.float64)
         err = np.abs(res[i][0] - b) / np.maximum(np.abs(b), 1e-6 * np.abs(b).max())
         assert err.max() <= 1e-5, (i, err.max())

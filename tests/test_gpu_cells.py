@@ -136,18 +136,23 @@ def test_trajectory_within_1e4_um(ctx, pcg, po, two_d):
     cells.upload(soa, n, n)
     mech = pcg.CellMechanics(ctx, mp, origin, n)
     ref = soa.copy()
+    pm = po.master_positions(ref, n)
     for _ in range(50):
         mech.computeForces(cells)
         mech.integratePositions(cells, 0.1)
         key = po.mech_bin(ref, n, n, om, origin)
         oorder, ostart = po.mech_sort(key, om)
         po.mech_forces(ref, n, n, om, key, oorder, ostart)
-        po.mech_integrate(ref, n, n, om, origin, 0.1)
+        po.mech_integrate(ref, n, n, om, origin, 0.1, pos64=pm)
     got = cells.download(n)
-    dpos = np.abs(got[:3 * n].astype(np.float64) - ref[:3 * n]).max()
-    moved = np.abs(ref[:3 * n].astype(np.float64) - soa[:3 * n]).max()
+    dev64 = cells.positions64()
+    dpos = np.abs(dev64.ravel() - pm).max()
+    moved = np.abs(pm - soa[:3 * n]).max()
     assert moved > 1.0          # the cells did move
-    assert dpos <= 1e-4, dpos
+    assert dpos <= 1e-4, dpos   # FP64 master positions against the oracle's
+    # the SoA holds the masters' rounding
+    assert np.array_equal(got[:3 * n], dev64.ravel().astype(np.float32))
+    assert np.abs(got[:3 * n].astype(np.float64) - ref[:3 * n]).max() <= 1e-4
 
 
 def test_empty_and_single_cell(ctx, pcg):
@@ -346,9 +351,11 @@ def test_main_loop_steps_match_oracle(ctx, pcg, po):
             acc = 0.0
     dens = np.full(2500, 38.0, np.float32)
     soa = inst.soa.copy()
-    po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, steps)
+    pm = po.master_positions(soa, n)
+    po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, steps, pos64=pm)
     assert rel_err(me.densityBuffer(), dens) <= 1e-5
     got = cells.download(n)
+    assert np.abs(cells.positions64().ravel() - pm).max() <= 1e-4
     assert np.abs(got[:3 * n].astype(np.float64) - soa[:3 * n]).max() <= 1e-4
 
 

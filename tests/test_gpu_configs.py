@@ -18,13 +18,13 @@ def rel_err(a, b):
     return float((np.abs(np.asarray(a, np.float64) - b) / np.maximum(np.abs(b), 1e-6 * scale)).max())
 
 
-def positions_close(got, ref):
-    """Positions within 1e-4 um or two FP32 ulps of their magnitude (the
-    force terms are a few ulp off the reference's forms; positions past
-    1024 um have an ulp of 1.2e-4 um)."""
-    ref = np.asarray(ref, np.float32)
-    tol = np.maximum(1e-4, 2.0 * np.spacing(np.abs(ref)).astype(np.float64))
-    return bool(np.all(np.abs(np.asarray(got, np.float64) - ref.astype(np.float64)) <= tol))
+def positions_close(got64, ref64, got32):
+    """FP64 master positions within 1e-4 um of the oracle's, and the SoA's
+    FP32 positions their rounding."""
+    err = float(np.abs(np.asarray(got64, np.float64).ravel() - ref64).max())
+    assert err <= 1e-4, err
+    assert np.array_equal(np.asarray(got32, np.float32), np.asarray(got64, np.float64).ravel().astype(np.float32))
+    return True
 
 
 def oracle_inputs(po, inst):
@@ -43,8 +43,8 @@ def oracle_inputs(po, inst):
 def test_plain_3d_full_size_matches_oracle(ctx, pcg, po):
     """150^3 x 4 substrates, 200k cells: one mechanics period (10 sub-steps of
     sweeps, Dirichlet reset and secretion, then forces and AB2) through the
-    single-simulation API; density within 1e-5 of the FP64 oracle, positions
-    within 1e-4 um or two FP32 ulps."""
+    single-simulation API; density within 1e-5 of the FP64 oracle, FP64
+    master positions within 1e-4 um."""
     from pcg import workloads
     inst = workloads.plain_3d()
     g, n = inst.grid, inst.n_cells
@@ -64,10 +64,11 @@ def test_plain_3d_full_size_matches_oracle(ctx, pcg, po):
             acc = 0.0
     og, osubs, om, dens = oracle_inputs(po, inst)
     soa = inst.soa.copy()
-    po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, steps, refresh=bool(inst.flags & 1))
+    pm = po.master_positions(soa, n)
+    po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, steps, refresh=bool(inst.flags & 1), pos64=pm)
     assert rel_err(me.densityBuffer(), dens) <= 1e-5
     got = cells.download(n)
-    assert positions_close(got[:3 * n], soa[:3 * n])
+    assert positions_close(cells.positions64(), pm, got[:3 * n])
 
 
 def test_batched_2d_full_set(ctx, pcg, po):
@@ -82,7 +83,7 @@ def test_batched_2d_full_set(ctx, pcg, po):
     b.step(steps)
     ctx.sync()
     picked = list(range(0, 256, 16))
-    together = {i: (b.density(i), b.cells(i)) for i in picked}
+    together = {i: (b.density(i), b.cells(i), b.positions64(i)) for i in picked}
     b.close()
     for i in picked:
         a = pcg.Batch(ctx, [insts[i]])
@@ -97,6 +98,8 @@ def test_batched_2d_full_set(ctx, pcg, po):
         og, osubs, om, dens = oracle_inputs(po, inst)
         n = inst.n_cells
         soa = inst.soa.copy()
-        po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, steps, refresh=bool(inst.flags & 1))
+        pm = po.master_positions(soa, n)
+        po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, steps, refresh=bool(inst.flags & 1),
+               pos64=pm)
         assert rel_err(together[i][0], dens) <= 1e-5, f"density {i}"
-        assert positions_close(together[i][1][:3 * n], soa[:3 * n]), f"cells {i}"
+        assert positions_close(together[i][2], pm, together[i][1][:3 * n]), f"cells {i}"

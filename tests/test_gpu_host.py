@@ -34,7 +34,8 @@ def test_main_loop_twin_matches_oracle(tmp_path, pcg, po):
     om = po.mech_params(-500, 500, -500, 500, -10, 10, True, 0.1)
     rd = np.full(2500, 38.0, np.float32)
     rs = inst.soa.copy()
-    po.run(og, po.make_subs([(1e5, 0.1, True, 38.0)]), om, 0.1, rd, rs, n, n, *inst.rates, None, steps)
+    po.run(og, po.make_subs([(1e5, 0.1, True, 38.0)]), om, 0.1, rd, rs, n, n, *inst.rates, None, steps,
+           pos64=po.master_positions(rs, n))
     assert np.abs(dens - rd).max() / np.abs(rd).max() <= 1e-5
     assert np.abs(block[:3 * n].astype(np.float64) - rs[:3 * n]).max() <= 1e-4
     assert np.array_equal(block[27 * n:28 * n].view(np.uint32), rs[27 * n:28 * n].view(np.uint32))
@@ -99,7 +100,8 @@ def test_main_loop_twin_with_motility_and_mat_frames(tmp_path, pcg, po, n_sens):
     rd = np.full(2500, 38.0, np.float32)
     rs = soa.copy()
     _, next_step = po.run(og, po.make_subs([(1e5, 0.1, True, 38.0)]), om, 0.1, rd, rs, n, n, *inst.rates, None,
-                          steps, motility=st, seed=seed, mot_step=0, layout=po.MOT_REF)
+                          steps, motility=st, seed=seed, mot_step=0, layout=po.MOT_REF,
+                          pos64=po.master_positions(rs, n))
     assert next_step == 4                                       # mechanics every 10 diffusion steps
     assert np.abs(dens - rd).max() / np.abs(rd).max() <= 1e-5
     assert np.abs(block[:3 * n].astype(np.float64) - rs[:3 * n]).max() <= 1e-3

@@ -5,7 +5,15 @@ mechanics-voxel keys with their indices as values gives the cell order of
 the existing entry point, bit for bit, on two consecutive calls.
 
 Named to be collected last, so it also runs after every other GPU test has
-used (and freed) device memory in the same process."""
+used (and freed) device memory in the same process.  One case runs in a
+fresh process, where no mechanics step has loaded the sort's kernels: after
+the set-up call, a sort makes no library allocation and leaves the device's
+free memory unchanged."""
+import os
+import subprocess
+import sys
+import textwrap
+
 import numpy as np
 import pytest
 
@@ -61,6 +69,55 @@ def test_static_sort_matches_mechanics_binning(ctx, pcg, n):
             assert np.array_equal(ks, keys[order])
             ko.fill_(-1)
             vo.fill_(-1)
+
+
+FRESH = textwrap.dedent("""
+    import ctypes as C, importlib.util, os, sys
+    import numpy as np
+    import torch
+    pkg = sys.argv[1]
+    spec = importlib.util.spec_from_file_location("pcg", os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    pcg = importlib.util.module_from_spec(spec); sys.modules["pcg"] = pcg; spec.loader.exec_module(pcg)
+    L = pcg.lib()
+    ctx = pcg.Context(0)
+    ctx.check(L.pcg_sort_pairs_static(ctx.h, None, None, None, None, 0, 32))    # set-up call
+    n = 60000
+    rng = np.random.default_rng(5)
+    keys = rng.integers(0, 1 << 20, n).astype(np.uint32)
+    kd = torch.from_numpy(keys.view(np.int32)).cuda()
+    vd = torch.arange(n, dtype=torch.int32, device="cuda")
+    ko, vo = torch.empty_like(kd), torch.empty_like(vd)
+    torch.cuda.synchronize()
+    m0, r0 = C.c_uint64(), C.c_uint64()
+    L.pcg_debug_alloc_stats(C.byref(m0), C.byref(r0))
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        ctx.check(L.pcg_sort_pairs_static(ctx.h, kd.data_ptr(), vd.data_ptr(), ko.data_ptr(), vo.data_ptr(), n, 20))
+        ctx.sync()
+    free1 = torch.cuda.mem_get_info()[0]
+    m1, r1 = C.c_uint64(), C.c_uint64()
+    L.pcg_debug_alloc_stats(C.byref(m1), C.byref(r1))
+    order = np.argsort(keys, kind="stable").astype(np.uint32)
+    assert np.array_equal(vo.cpu().numpy().view(np.uint32), order)
+    assert np.array_equal(ko.cpu().numpy().view(np.uint32), keys[order])
+    assert (m1.value, r1.value) == (m0.value, r0.value), ((m0.value, r0.value), (m1.value, r1.value))
+    assert free1 == free0, (free0, free1)
+    ctx.close()
+    print("fresh ok")
+""")
+
+
+def test_fresh_process_sort_allocates_nothing(pcg, tmp_path):
+    """In a process where nothing but the set-up call has run, two sorts make
+    no library allocation and the device's free memory does not change."""
+    pytest.importorskip("torch")
+    script = tmp_path / "fresh_sort.py"
+    script.write_text(FRESH)
+    pkg = os.path.dirname(pcg.__file__)
+    res = subprocess.run([sys.executable, str(script), pkg], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "fresh ok" in res.stdout
 
 
 def test_static_sort_rejects_oversize_and_overlap(ctx, pcg):
