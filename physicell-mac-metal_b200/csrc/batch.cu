@@ -30,6 +30,7 @@ uint64_t instance_bytes(const pcg_instance_desc& d)
     uint64_t b = pitch * S * 4;                            // density
     b += (nv / 32 + 3) * 32 * S;                           // tile lists (~32 B per 32 lines per axis)
     b += n * (NUM_FIELDS * 4 + 4 + 1);                     // SoA, instance id, active
+    b += n * 3 * 8;                                        // FP64 master positions
     b += n * S * (4 * 8 + 3 * 8);                          // rates, secretion constants
     b += n * 4 * 6 * 2;                                    // two sort workspaces
     b += n * (8 + 4);                                      // per-run density element and rate slot
@@ -214,7 +215,10 @@ uint64_t Batch::count_launches(bool mech) const
     if (c_.n) k += 1;
     if (mech && c_.n) {
         k += m_.launches_forces(c_.n) - 1 + 1;   // bin..forces (memset excluded) + integrate
-        if (any_refresh) k += 1 + radix_sort_launches(c_.n, key_bits_for(d.total_vox + 1));
+        // the secretion order after the voxel refresh: keys, sort, heads, scan, runs, constants
+        if (any_refresh)
+            k += 1 + radix_sort_launches(c_.n, key_bits_for(d.total_vox + 1)) + 2 +
+                 scan_launches(static_cast<uint64_t>(c_.n) + 1) + 1;
     }
     return k;
 }
@@ -335,7 +339,8 @@ int Batch::set_diagnostics(bool on)
 std::string Batch::describe() const
 {
     std::ostringstream o;
-    o << d.describe() << "forces(lanes=" << kForceLanes << ",block=" << m_.block << ") graphs=" << (use_graphs ? 1 : 0)
+    o << d.describe() << "forces(block=" << m_.fshape.block << ",queue=" << m_.fshape.queue
+      << ") graphs=" << (use_graphs ? 1 : 0)
       << " launches/step=" << launches_diff << "/" << launches_mech;
     return o.str();
 }

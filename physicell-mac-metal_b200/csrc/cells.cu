@@ -245,9 +245,18 @@ __global__ void k_cells_move(uint32_t* __restrict__ soa, uint32_t stride, const 
 
 // ------------------------------------------------------------------ mechanics
 
+// Binning is a counting sort over the mechanics voxels of the whole batch.
+// k_mech_bin finds each cell's voxel (FP32 divide, truncation and clamp,
+// as mechanics.metal:54-76) and counts it; the atomic's return value is the
+// cell's arrival slot in its voxel.  The exclusive scan of the counts is the
+// cell-start table.  k_mech_place drops each cell at start + slot, which
+// groups the voxel's cells in arrival order, and k_mech_order puts every
+// voxel's cells in ascending index (a cell's place is the voxel's start
+// plus the number of its cells with a lower index) -- the stable order --
+// and writes the sorted keys, the order and the sorted SoA there.
 __global__ void k_mech_bin(float* __restrict__ soa, uint32_t stride, uint32_t n, const uint32_t* __restrict__ cell_inst,
                            const CellInst* __restrict__ insts, uint32_t* __restrict__ keys,
-                           uint32_t* __restrict__ vals, uint32_t* __restrict__ counts,
+                           uint32_t* __restrict__ slots, uint32_t* __restrict__ counts,
                            const uint8_t* __restrict__ mask)
 {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -267,24 +276,29 @@ __global__ void k_mech_bin(float* __restrict__ soa, uint32_t stride, uint32_t n,
     if (mask == nullptr || (mask[ii] & STEP_MECH)) soa[static_cast<size_t>(F_MECH_VOXEL) * stride + g] = __uint_as_float(local);
     const uint32_t key = in.mvox_base + local;
     keys[g] = key;
-    vals[g] = g;
-    atomicAdd(&counts[key], 1u);
+    slots[g] = atomicAdd(&counts[key], 1u);
 }
 
-// Sorted SoA: rank[g] = place of cell g in the sorted order, then each cell
-// reads its own fields (coalesced) and writes them to its place.
-__global__ void k_mech_rank(const uint32_t* __restrict__ sorder, uint32_t n, uint32_t* __restrict__ rank)
+__global__ void k_mech_place(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ slots,
+                             const uint32_t* __restrict__ start, uint32_t n, uint32_t* __restrict__ placed)
 {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < n) rank[sorder[p]] = p;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < n) placed[start[keys[g]] + slots[g]] = g;
 }
 
-__global__ void k_mech_sorted_soa(const float* __restrict__ soa, uint32_t stride, const uint32_t* __restrict__ rank,
-                                  uint32_t n, float4* __restrict__ spos, float4* __restrict__ sprm)
+__global__ void k_mech_order(const float* __restrict__ soa, uint32_t stride, const uint32_t* __restrict__ keys,
+                             const uint32_t* __restrict__ start, const uint32_t* __restrict__ placed, uint32_t n,
+                             uint32_t* __restrict__ skeys, uint32_t* __restrict__ sorder, float4* __restrict__ spos,
+                             float4* __restrict__ sprm)
 {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
-    const uint32_t p = rank[g];
+    const uint32_t key = keys[g];
+    const uint32_t s0 = start[key], s1 = start[key + 1];
+    uint32_t p = s0;
+    for (uint32_t q = s0; q < s1; ++q) p += placed[q] < g ? 1u : 0u;
+    skeys[p] = key;
+    sorder[p] = g;
     spos[p] = make_float4(soa[static_cast<size_t>(F_POS_X) * stride + g], soa[static_cast<size_t>(F_POS_Y) * stride + g],
                           soa[static_cast<size_t>(F_POS_Z) * stride + g], soa[static_cast<size_t>(F_RADIUS) * stride + g]);
     // square roots of the (non-negative) strengths: the pair factors
@@ -305,10 +319,6 @@ __device__ __forceinline__ uint32_t nbr_hash(uint32_t j)
     return x;
 }
 
-// G lanes per cell (cells in sorted order); each neighbour row (dk, dj) is
-// one contiguous range of the sorted order covering di = -1..1, which the G
-// lanes stride through; partial sums are combined with a fixed xor-shuffle
-// tree, so the result does not depend on scheduling.
 // Distance from c to the mechanics-voxel slab [lo, lo + vs) along one axis,
 // slabs at the grid edge reaching to infinity (clamped cells), minus a
 // 0.01 um margin that covers FP32 rounding of positions and bounds.
@@ -319,6 +329,30 @@ __device__ __forceinline__ float slab_gap(float c, float lo, float vs, int idx, 
     return fmaxf(fmaxf(l - c, c - h) - 0.01f, 0.0f);
 }
 
+// One pair's force terms (mechanics.metal:167-208) added to the running
+// sums: d = p_i - p_j with dsq = |d|^2 (the test's exact FP32 value), Ri /
+// Rj the radii, mp = (sqrt rep_i, sqrt adh_i, relmax_i), op the same for j.
+// Reciprocal / rsqrt forms and per-cell square roots of the strengths (a
+// few ulp per term against the reference's sqrt and divides).
+__device__ __forceinline__ void pair_force(float ddx, float ddy, float ddz, float dsq, float Ri, float Rj,
+                                           const float4& mp, const float4& op, float& fx, float& fy, float& fz,
+                                           float& P)
+{
+    constexpr float kInvPressureScale = 1.0f / 0.027288820670331f;
+    const float inv = rsqrtf(dsq);
+    const float dist = dsq * inv;
+    const float R = Ri + Rj;
+    const float ov = fmaxf(1.0f - __fdividef(dist, R), 0.0f);         // repulsion overlap
+    const float t = fmaxf(1.0f - __fdividef(dist, mp.z * R), 0.0f);    // adhesion reach
+    const float ov2 = ov * ov;
+    const float F = ov2 * (mp.x * op.x) - t * t * (mp.y * op.y);
+    P += ov2 * kInvPressureScale;
+    const float Fi = F * inv;
+    fx += Fi * ddx;
+    fy += Fi * ddy;
+    fz += Fi * ddz;
+}
+
 // One thread per cell (sorted order p): candidates are visited in the
 // reference's order (dk, dj, di, then the voxel's cells in ascending index;
 // mechanics.metal:125-208) and summed sequentially.  The nine voxel rows'
@@ -326,9 +360,18 @@ __device__ __forceinline__ float slab_gap(float c, float lo, float vs, int idx, 
 // of a row) that lie entirely beyond the interaction distance are skipped,
 // and the next candidate's position is loaded while the current one is
 // tested.  The neighbour test is the reference's FP32 one without
-// contraction (mechanics.metal:159-165), so neighbour sets are exact; the
-// force terms (mechanics.metal:167-208) use reciprocal / rsqrt forms and
-// per-cell square roots of the strengths (a few ulp per term).
+// contraction (mechanics.metal:159-165), so neighbour sets are exact.
+//
+// QCAP == 0: the force terms are computed in the walk, where a lane meets
+// its neighbour.  QCAP > 0: the walk only tests; each lane keeps the
+// candidates that pass, in order, in its own QCAP slots of shared memory
+// (slot k of thread t at queue[k * blockDim + t]), and the force terms of
+// the queued neighbours are computed when a lane's queue is full (every
+// lane walking with it then empties its own) and at the end.  Every lane
+// adds its terms in candidate order either way, so both forms give the same
+// bits; the queued form runs the force terms for the neighbours only,
+// where the direct form runs them whenever any lane of the warp has one.
+template <int QCAP, bool DIAG>
 __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ spos, const float4* __restrict__ sprm,
                                                      const uint32_t* __restrict__ skeys,
                                                      const uint32_t* __restrict__ sorder,
@@ -339,7 +382,7 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
                                                      uint32_t* __restrict__ diag_hash,
                                                      const uint8_t* __restrict__ mask)
 {
-    constexpr float kInvPressureScale = 1.0f / 0.027288820670331f;
+    extern __shared__ uint32_t queue[];
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const uint32_t g = sorder[p];
@@ -378,6 +421,20 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
     }
     float fx = 0.f, fy = 0.f, fz = 0.f, P = 0.f;
     uint32_t cnt = 0, hsh = 0;
+    uint32_t* myq = queue + threadIdx.x;
+    const uint32_t qstride = blockDim.x;
+    uint32_t nq = 0;
+    // force terms of the queued neighbours, in the order they were queued
+    auto flush = [&]() {
+        for (uint32_t k = 0; k < nq; ++k) {
+            const uint32_t q = myq[k * qstride];
+            const float4 cur = spos[q];
+            const float ddx = __fsub_rn(me.x, cur.x), ddy = __fsub_rn(me.y, cur.y), ddz = __fsub_rn(me.z, cur.z);
+            const float dsq = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
+            pair_force(ddx, ddy, ddz, dsq, me.w, cur.w, mp, sprm[q], fx, fy, fz, P);
+        }
+        nq = 0;
+    };
 #pragma unroll
     for (int r = 0; r < 9; ++r) {
         uint32_t q = rq0[r];
@@ -390,31 +447,25 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
             // the cell itself (q == p, distance 0) fails it like any coincident cell
             const float ddx = __fsub_rn(me.x, cur.x), ddy = __fsub_rn(me.y, cur.y), ddz = __fsub_rn(me.z, cur.z);
             const float dsq = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
-            if (dsq >= maxd2 || dsq < 1e-12f) continue;
-            if (diag_cnt) {
+            const bool nb = !(dsq >= maxd2 || dsq < 1e-12f);
+            if (DIAG && nb) {
                 ++cnt;
                 hsh += nbr_hash(sorder[q] - in.cell_off);
             }
-            const float inv = rsqrtf(dsq);
-            const float dist = dsq * inv;
-            const float R = me.w + cur.w;
-            const float4 op = sprm[q];
-            const float ov = fmaxf(1.0f - __fdividef(dist, R), 0.0f);         // repulsion overlap
-            const float t = fmaxf(1.0f - __fdividef(dist, mp.z * R), 0.0f);    // adhesion reach
-            const float ov2 = ov * ov;
-            const float F = ov2 * (mp.x * op.x) - t * t * (mp.y * op.y);
-            P += ov2 * kInvPressureScale;
-            const float Fi = F * inv;
-            fx += Fi * ddx;
-            fy += Fi * ddy;
-            fz += Fi * ddz;
+            if (QCAP == 0) {
+                if (nb) pair_force(ddx, ddy, ddz, dsq, me.w, cur.w, mp, sprm[q], fx, fy, fz, P);
+            } else {
+                if (nb) myq[nq++ * qstride] = q;
+                if (__any_sync(__activemask(), nq == QCAP)) flush();
+            }
         }
     }
+    if (QCAP > 0) flush();
     soa[static_cast<size_t>(F_VEL_X) * stride + g] = fx;
     soa[static_cast<size_t>(F_VEL_Y) * stride + g] = fy;
     soa[static_cast<size_t>(F_VEL_Z) * stride + g] = fz;
     soa[static_cast<size_t>(F_PRESSURE) * stride + g] = P;
-    if (diag_cnt) {
+    if (DIAG) {
         diag_cnt[g] = cnt;
         diag_hash[g] = hsh;
     }
@@ -532,35 +583,71 @@ cudaError_t launch_cells_move(cudaStream_t st, float* soa, uint32_t stride, cons
 }
 
 cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n, const uint32_t* cell_inst,
-                            const CellInst* insts, uint32_t* keys, uint32_t* vals, uint32_t* counts,
+                            const CellInst* insts, uint32_t* keys, uint32_t* slots, uint32_t* counts,
                             const uint8_t* mask)
 {
     if (n == 0) return cudaSuccess;
-    k_mech_bin<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, keys, vals, counts, mask);
+    k_mech_bin<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, keys, slots, counts, mask);
     return cudaGetLastError();
 }
 
-cudaError_t launch_mech_sorted_soa(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* sorder,
-                                   uint32_t n, uint32_t* rank, float4* spos, float4* sprm)
+cudaError_t launch_mech_order(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* keys,
+                              const uint32_t* slots, const uint32_t* start, uint32_t n, uint32_t* placed,
+                              uint32_t* skeys, uint32_t* sorder, float4* spos, float4* sprm)
 {
     if (n == 0) return cudaSuccess;
-    k_mech_rank<<<blocks_for(n, 256), 256, 0, st>>>(sorder, n, rank);
+    k_mech_place<<<blocks_for(n, 256), 256, 0, st>>>(keys, slots, start, n, placed);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_mech_sorted_soa<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, rank, n, spos, sprm);
+    k_mech_order<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, keys, start, placed, n, skeys, sorder, spos, sprm);
     return cudaGetLastError();
+}
+
+template <int QCAP, bool DIAG>
+static cudaError_t forces_variant(cudaStream_t st, unsigned grid, int block, const float4* spos, const float4* sprm,
+                                  const uint32_t* skeys, const uint32_t* sorder, const uint32_t* start, uint32_t n,
+                                  const uint32_t* cell_inst, const CellInst* insts, float* soa, uint32_t stride,
+                                  uint32_t* diag_cnt, uint32_t* diag_hash, const uint8_t* mask)
+{
+    const size_t smem = static_cast<size_t>(QCAP) * block * sizeof(uint32_t);   // at most 64 KiB
+    k_mech_forces<QCAP, DIAG><<<grid, block, smem, st>>>(spos, sprm, skeys, sorder, start, n, cell_inst, insts, soa,
+                                                         stride, diag_cnt, diag_hash, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t mech_forces_prepare()
+{
+    const void* ks[] = {reinterpret_cast<const void*>(&k_mech_forces<64, false>),
+                        reinterpret_cast<const void*>(&k_mech_forces<64, true>)};
+    for (const void* k : ks) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* skeys,
                                const uint32_t* sorder, const uint32_t* start, uint32_t n, const uint32_t* cell_inst,
                                const CellInst* insts, float* soa, uint32_t stride, uint32_t* diag_cnt,
-                               uint32_t* diag_hash, const uint8_t* mask, int block)
+                               uint32_t* diag_hash, const uint8_t* mask, ForceShape shape)
 {
     if (n == 0) return cudaSuccess;
-    const unsigned grid = blocks_for(static_cast<uint64_t>(n) * kForceLanes, block);
-    k_mech_forces<<<grid, block, 0, st>>>(spos, sprm, skeys, sorder, start, n, cell_inst, insts, soa, stride, diag_cnt,
-                                          diag_hash, mask);
-    return cudaGetLastError();
+    if (shape.block < 32 || shape.block > 256 || shape.block % 32 != 0) return cudaErrorInvalidValue;
+    const unsigned grid = blocks_for(n, shape.block);
+    const bool dg = diag_cnt != nullptr;
+#define PCG_FORCES(Q)                                                                                                \
+    return dg ? forces_variant<Q, true>(st, grid, shape.block, spos, sprm, skeys, sorder, start, n, cell_inst,      \
+                                        insts, soa, stride, diag_cnt, diag_hash, mask)                               \
+              : forces_variant<Q, false>(st, grid, shape.block, spos, sprm, skeys, sorder, start, n, cell_inst,     \
+                                         insts, soa, stride, diag_cnt, diag_hash, mask)
+    switch (shape.queue) {
+    case 0: PCG_FORCES(0);
+    case 16: PCG_FORCES(16);
+    case 32: PCG_FORCES(32);
+    case 64: PCG_FORCES(64);
+    default: return cudaErrorInvalidValue;
+    }
+#undef PCG_FORCES
 }
 
 cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, double* pos64, uint32_t stride, uint32_t n,

@@ -245,17 +245,32 @@ cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_sta
                            uint32_t max_runs, uint32_t max_s, const CellInst* insts, const double* cs, uint32_t cap,
                            const uint32_t* flags, const uint8_t* mask);
 
-// Mechanics.
+// Mechanics binning as a counting sort: launch_mech_bin writes each cell's
+// global mechanics-voxel key, counts it (counts: V + 1 zeroed words) and
+// records its arrival slot; after the exclusive scan of the counts into
+// start, launch_mech_order (two launches; placed: n scratch words) writes
+// the stable order (skeys, sorder: cells by voxel, ascending index within
+// a voxel) and the sorted positions / radii and strengths.
 cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
                             const uint32_t* cell_inst, const CellInst* insts,
-                            uint32_t* keys, uint32_t* vals, uint32_t* counts, const uint8_t* mask);
-// Positions / radii and strengths in sorted order (rank: n scratch words).
-cudaError_t launch_mech_sorted_soa(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* sorder,
-                                   uint32_t n, uint32_t* rank, float4* spos, float4* sprm);
+                            uint32_t* keys, uint32_t* slots, uint32_t* counts, const uint8_t* mask);
+cudaError_t launch_mech_order(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* keys,
+                              const uint32_t* slots, const uint32_t* start, uint32_t n, uint32_t* placed,
+                              uint32_t* skeys, uint32_t* sorder, float4* spos, float4* sprm);
+// Launch shape of the force pass: threads per block (a multiple of 32, at
+// most 256) and the neighbour queue per thread (0 = force terms in the walk;
+// 16, 32 or 64 slots of shared memory).  Every shape gives the same bits.
+struct ForceShape {
+    int block = 256;
+    int queue = 32;
+};
+// Lets the 64-slot queue variants use 64 KiB of shared memory (current
+// device; once per device, outside stream capture).
+cudaError_t mech_forces_prepare();
 cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* skeys,
                                const uint32_t* sorder, const uint32_t* start, uint32_t n,
                                const uint32_t* cell_inst, const CellInst* insts, float* soa, uint32_t stride,
-                               uint32_t* diag_cnt, uint32_t* diag_hash, const uint8_t* mask, int block);
+                               uint32_t* diag_cnt, uint32_t* diag_hash, const uint8_t* mask, ForceShape shape);
 // Copies of a removal plan: (dst, src) pairs, each cell's 28 SoA fields,
 // 4 x S rates (arrays of rate_cap doubles, [cell * S + s]), active flag and
 // three FP64 master positions (arrays of stride doubles; pos64 may be null).
@@ -266,10 +281,6 @@ cudaError_t launch_cells_move(cudaStream_t st, float* soa, uint32_t stride, cons
 cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, double* pos64, uint32_t stride, uint32_t n,
                                   const uint32_t* cell_inst, const CellInst* insts, float dt_override,
                                   const uint8_t* mask);
-// Threads per cell in the force pass: one, summing in the reference's
-// candidate order, so a cell's result never depends on what else is in the
-// batch.
-constexpr int kForceLanes = 1;
 
 // Radix sort of (key, value) pairs, stable, 'bits' significant key bits.
 // Scratch from radix_sort_scratch_bytes().  Result lands in (k_out, v_out).

@@ -1346,10 +1346,9 @@ int Mechanics::create(pcg_ctx* c, uint32_t tmv, uint32_t maxc)
     ctx = c;
     total_mvox = tmv;
     cap = std::max<uint32_t>(maxc, 1);
-    key_bits = key_bits_for(std::max<uint64_t>(tmv, 1));
-    for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp, &dcnt, &dhash})
+    PCG_CU(ctx, mech_forces_prepare());
+    for (DevBuf* b : {&keys, &slots, &placed, &skeys, &sorder, &dcnt, &dhash})
         PCG_CU(ctx, b->alloc(static_cast<size_t>(cap) * sizeof(uint32_t)));
-    PCG_CU(ctx, sort_scr.alloc(radix_sort_scratch_bytes(cap, key_bits)));
     PCG_CU(ctx, counts.alloc((static_cast<size_t>(tmv) + 1) * sizeof(uint32_t)));
     PCG_CU(ctx, start.alloc((static_cast<size_t>(tmv) + 1) * sizeof(uint32_t)));
     PCG_CU(ctx, cudaMemsetAsync(start.p, 0, start.bytes, ctx->stream));
@@ -1362,11 +1361,11 @@ int Mechanics::create(pcg_ctx* c, uint32_t tmv, uint32_t maxc)
 
 int Mechanics::launches_forces(uint32_t n) const
 {
-    return 1 /*memset*/ + 1 /*bin*/ + radix_sort_launches(n, key_bits) + scan_launches(total_mvox + 1ull) +
-           2 /*rank, sorted SoA*/ + 1 /*forces*/;
+    (void)n;
+    return 1 /*memset*/ + 1 /*bin*/ + scan_launches(total_mvox + 1ull) + 2 /*place, order*/ + 1 /*forces*/;
 }
 
-// computeForces: bin -> stable radix sort -> cell-start table -> sorted SoA -> forces
+// computeForces: bin -> counting sort (start table, stable order, sorted SoA) -> forces
 int Mechanics::forces(Cells& c, const uint8_t* mask)
 {
     PCG_TRY(binsort(c, mask));
@@ -1381,16 +1380,15 @@ int Mechanics::binsort(Cells& c, const uint8_t* mask)
     cudaStream_t st = ctx->stream;
     PCG_CU(ctx, cudaMemsetAsync(counts.p, 0, counts.bytes, st));
     cudaError_t e = launch_mech_bin(st, c.soa.as<float>(), c.max_cells, c.n, c.cell_inst.as<uint32_t>(),
-                                    c.inst.as<CellInst>(), keys.as<uint32_t>(), vals.as<uint32_t>(), counts.as<uint32_t>(), mask);
+                                    c.inst.as<CellInst>(), keys.as<uint32_t>(), slots.as<uint32_t>(),
+                                    counts.as<uint32_t>(), mask);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "bin launch");
-    e = radix_sort_pairs(st, keys.as<uint32_t>(), vals.as<uint32_t>(), skeys.as<uint32_t>(), sorder.as<uint32_t>(),
-                         ktmp.as<uint32_t>(), vtmp.as<uint32_t>(), c.n, key_bits, sort_scr.p);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "radix sort");
     e = scan_exclusive(st, counts.as<uint32_t>(), start.as<uint32_t>(), static_cast<uint64_t>(total_mvox) + 1, scan_scr.p);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "start-table scan");
-    e = launch_mech_sorted_soa(st, c.soa.as<float>(), c.max_cells, sorder.as<uint32_t>(), c.n, ktmp.as<uint32_t>(),
-                               spos.as<float4>(), sprm.as<float4>());
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "sorted SoA launch");
+    e = launch_mech_order(st, c.soa.as<float>(), c.max_cells, keys.as<uint32_t>(), slots.as<uint32_t>(),
+                          start.as<uint32_t>(), c.n, placed.as<uint32_t>(), skeys.as<uint32_t>(),
+                          sorder.as<uint32_t>(), spos.as<float4>(), sprm.as<float4>());
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "bin order launch");
     ctx->launches += launches_forces(c.n) - 2;   // the memset is not a kernel; forces counted below
     return PCG_OK;
 }
@@ -1402,7 +1400,7 @@ int Mechanics::force_pass(Cells& c, const uint8_t* mask)
     cudaError_t e = launch_mech_forces(st, spos.as<float4>(), sprm.as<float4>(), skeys.as<uint32_t>(), sorder.as<uint32_t>(),
                            start.as<uint32_t>(), c.n, c.cell_inst.as<uint32_t>(), c.inst.as<CellInst>(), c.soa.as<float>(),
                            c.max_cells, diag ? dcnt.as<uint32_t>() : nullptr, diag ? dhash.as<uint32_t>() : nullptr,
-                           mask, block);
+                           mask, fshape);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "forces launch");
     ctx->launches++;
     return PCG_OK;
@@ -1424,7 +1422,7 @@ int Mechanics::integrate(Cells& c, float dt_override, const uint8_t* mask)
 
 uint64_t Mechanics::device_bytes() const
 {
-    return keys.bytes + vals.bytes + skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + counts.bytes +
+    return keys.bytes + slots.bytes + placed.bytes + skeys.bytes + sorder.bytes + counts.bytes +
            start.bytes + scan_scr.bytes + spos.bytes + sprm.bytes + dcnt.bytes + dhash.bytes;
 }
 

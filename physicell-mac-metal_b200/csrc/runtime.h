@@ -300,14 +300,17 @@ public:
     pcg_ctx* ctx = nullptr;
     uint32_t total_mvox = 0;
     uint32_t cap = 0;
-    int key_bits = 0;
-    int block = 256;
+    ForceShape fshape;   // launch shape of the force pass
     bool diag = false;
-    DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr, counts, start, scan_scr, spos, sprm, dcnt, dhash;
+    // binning: keys / slots (voxel key and arrival slot per cell), counts
+    // (per voxel, + 1), start (the cell-start table), placed (cells in
+    // arrival order per voxel), skeys / sorder (the stable order), spos /
+    // sprm (sorted SoA)
+    DevBuf keys, slots, placed, skeys, sorder, counts, start, scan_scr, spos, sprm, dcnt, dhash;
 
     int create(pcg_ctx* c, uint32_t total_mvox, uint32_t max_cells);
     int forces(Cells& c, const uint8_t* mask);       // binsort + force_pass
-    int binsort(Cells& c, const uint8_t* mask);      // bin, stable radix sort, cell-start table, sorted SoA
+    int binsort(Cells& c, const uint8_t* mask);      // bin, counting sort, cell-start table, sorted SoA
     int force_pass(Cells& c, const uint8_t* mask);
     int integrate(Cells& c, float dt_override, const uint8_t* mask);
     int launches_forces(uint32_t n) const;
