@@ -362,13 +362,19 @@ typedef struct {
 
 typedef struct {
     int use_graphs;        /* capture each step into a CUDA graph (default 1) */
-    int autotune;          /* pick tile shapes / block sizes by measurement (default 1) */
+    int autotune;          /* pick sweep shapes, the force pass shape and the cell kernels'
+                              block sizes by measurement on the batch's data (default 1) */
     const char* tune_cache;/* JSON cache path for autotuned choices, or NULL */
     int profile_phases;    /* record CUDA events around phases (default 0) */
     int pin_x;             /* launch shape of the x sweeps instead of the tuned one: */
     int pin_cols;          /* warps * 16 + stages (y and z sweeps: pin_cols); 0 = tuned */
     int disable_planes;    /* 1: x and y sweeps as separate tile passes even where an x-y plane
                               fits shared memory (same results; 0 = one pass per plane) */
+    int pin_forces;        /* force pass shape instead of the tuned one: threads per block
+                              (32..256, a multiple of 32) * 1000 + neighbour queue slots per
+                              thread (0, 16, 32 or 64); 0 = tuned.  Same results for every shape */
+    int pin_cell_threads;  /* threads per block (32..256, a multiple of 32) of the secretion,
+                              binning and AB2 kernels instead of the tuned ones; 0 = tuned */
 } pcg_batch_options;
 
 pcg_status pcg_batch_create(pcg_ctx* ctx, const pcg_instance_desc* instances, uint32_t n_instances,

@@ -89,7 +89,7 @@ class InstanceDesc(C.Structure):
 class BatchOptions(C.Structure):
     _fields_ = [("use_graphs", C.c_int), ("autotune", C.c_int), ("tune_cache", C.c_char_p),
                 ("profile_phases", C.c_int), ("pin_x", C.c_int), ("pin_cols", C.c_int),
-                ("disable_planes", C.c_int)]
+                ("disable_planes", C.c_int), ("pin_forces", C.c_int), ("pin_cell_threads", C.c_int)]
 
 
 class ServeOptions(C.Structure):
@@ -676,16 +676,19 @@ class Batch:
     """pcg_batch: many simulations advanced in one graph launch per step."""
 
     def __init__(self, ctx, instances, use_graphs=True, autotune=True, tune_cache=None, profile=False,
-                 pin_x=0, pin_cols=0, planes=True):
+                 pin_x=0, pin_cols=0, planes=True, pin_forces=0, pin_cell_threads=0):
         """pin_x / pin_cols: launch shape warps * 16 + stages of the x /
         column sweeps instead of the tuned one (0 = tuned).  planes=False:
-        x and y sweeps as separate passes even where a plane fits."""
+        x and y sweeps as separate passes even where a plane fits.
+        pin_forces: force pass threads * 1000 + queue slots; pin_cell_threads:
+        threads per block of the secretion, binning and AB2 kernels (0 =
+        tuned)."""
         self.ctx = ctx
         self.instances = list(instances)
         arr = (InstanceDesc * len(self.instances))(*[i.desc() for i in self.instances])
         opt = BatchOptions(1 if use_graphs else 0, 1 if autotune else 0,
                            tune_cache.encode() if tune_cache else None, 1 if profile else 0, pin_x, pin_cols,
-                           0 if planes else 1)
+                           0 if planes else 1, pin_forces, pin_cell_threads)
         h = _P()
         ctx.check(lib().pcg_batch_create(ctx.h, arr, len(self.instances), C.byref(opt), C.byref(h)))
         self.h = h

@@ -172,12 +172,13 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
     if (tune) {
         if (!tune_cache.empty()) Tuner::get().load(tune_cache);
         PCG_TRY(d.tune());
-        if (!tune_cache.empty()) Tuner::get().save(tune_cache);
     }
     if (opt) {
         PCG_TRY(d.pin(0, opt->pin_x));
         PCG_TRY(d.pin(1, opt->pin_cols));
     }
+    PCG_TRY(tune_cells(opt, tune));
+    if (tune && !tune_cache.empty()) Tuner::get().save(tune_cache);
     for (int q = 0; q < 8; ++q) PCG_CU(ctx, cudaEventCreate(&ev[q]));
     if (masked) {
         PCG_CU(ctx, mask_d.alloc(n));
@@ -207,6 +208,117 @@ Batch::~Batch()
     if (g_mech) cudaGraphExecDestroy(g_mech);
     for (int q = 0; q < 8; ++q)
         if (ev[q]) cudaEventDestroy(ev[q]);
+}
+
+namespace {
+
+int log2_bucket(uint64_t v)
+{
+    int b = 0;
+    while ((1ull << (b + 1)) <= v) ++b;
+    return b;
+}
+
+bool valid_threads(int t, int hi) { return t >= 32 && t <= hi && t % 32 == 0; }
+
+}  // namespace
+
+int Batch::tune_cells(const pcg_batch_options* opt, bool tune)
+{
+    const int pin_f = opt ? opt->pin_forces : 0, pin_t = opt ? opt->pin_cell_threads : 0;
+    if (pin_f) {
+        const int t = pin_f / 1000, q = pin_f % 1000;
+        if (!valid_threads(t, 256) || (q != 0 && q != 16 && q != 32 && q != 64))
+            return fail(ctx, PCG_ERR_INVALID, "pin_forces must be threads (32..256, multiple of 32) * 1000 + queue (0, 16, 32, 64)");
+        m_.fshape.block = t;
+        m_.fshape.queue = q;
+    }
+    if (pin_t) {
+        if (!valid_threads(pin_t, 256)) return fail(ctx, PCG_ERR_INVALID, "pin_cell_threads must be 32..256, a multiple of 32");
+        c_.sec_block = m_.bin_block = m_.int_block = pin_t;
+    }
+    if (!tune || c_.n == 0 || (pin_f && pin_t)) return PCG_OK;
+    const std::string sfx = ":c" + std::to_string(log2_bucket(c_.n)) + ":v" + std::to_string(log2_bucket(m_.total_mvox)) +
+                            ":r" + std::to_string(log2_bucket(c_.n_rate));
+    const std::string kf = "forces" + sfx, ks = "secrete" + sfx, kb = "bin" + sfx, ki = "integrate" + sfx;
+    int vf = 0, vs = 0, vb = 0, vi = 0;
+    Tuner& T = Tuner::get();
+    const bool cached = T.lookup(kf, &vf) && T.lookup(ks, &vs) && T.lookup(kb, &vb) && T.lookup(ki, &vi);
+    if (!cached) {
+        // everything the timed launches write: the cell SoA, the master
+        // positions and the density (secretion)
+        DevBuf b_soa, b_pos, b_dens;
+        if (b_soa.alloc(c_.soa.bytes) != cudaSuccess || b_pos.alloc(c_.pos64.bytes) != cudaSuccess ||
+            b_dens.alloc(d.dens.bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return PCG_OK;   // not enough memory to tune safely: keep the defaults
+        }
+        cudaStream_t st = ctx->stream;
+        PCG_CU(ctx, cudaMemcpyAsync(b_soa.p, c_.soa.p, c_.soa.bytes, cudaMemcpyDeviceToDevice, st));
+        PCG_CU(ctx, cudaMemcpyAsync(b_pos.p, c_.pos64.p, c_.pos64.bytes, cudaMemcpyDeviceToDevice, st));
+        PCG_CU(ctx, cudaMemcpyAsync(b_dens.p, d.dens.p, d.dens.bytes, cudaMemcpyDeviceToDevice, st));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        PCG_CU(ctx, cudaEventCreate(&e0));
+        PCG_CU(ctx, cudaEventCreate(&e1));
+        const uint64_t launches0 = ctx->launches;
+        const bool order_dirty = c_.order_dirty;   // the timed AB2 launches may flag it (voxel refresh)
+        // best of the candidates by the time of 3 launches after a warm one
+        auto pick = [&](const std::vector<int>& cands, auto set, auto run, int* best) -> int {
+            float best_ms = 1e30f;
+            for (int c : cands) {
+                set(c);
+                PCG_TRY(run());
+                PCG_CU(ctx, cudaEventRecord(e0, st));
+                for (int r = 0; r < 3; ++r) PCG_TRY(run());
+                PCG_CU(ctx, cudaEventRecord(e1, st));
+                PCG_CU(ctx, cudaEventSynchronize(e1));
+                float ms = 0;
+                PCG_CU(ctx, cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    *best = c;
+                }
+            }
+            set(*best);
+            return PCG_OK;
+        };
+        int rc = pick({128, 256, 512, 1024}, [&](int b) { m_.bin_block = b; },
+                      [&]() { return m_.binsort(c_, nullptr); }, &vb);
+        std::vector<int> fc;
+        for (int t : {64, 128, 256})
+            for (int q : {0, 16, 32, 64}) fc.push_back(t * 1000 + q);
+        if (rc == PCG_OK)
+            rc = pick(fc, [&](int v) { m_.fshape.block = v / 1000; m_.fshape.queue = v % 1000; },
+                      [&]() { return m_.force_pass(c_, nullptr); }, &vf);
+        if (rc == PCG_OK)
+            rc = pick({64, 128, 256}, [&](int b) { c_.sec_block = b; }, [&]() { return c_.secrete(d, nullptr); }, &vs);
+        if (rc == PCG_OK)
+            rc = pick({128, 256, 512, 1024}, [&](int b) { m_.int_block = b; },
+                      [&]() { return m_.integrate(c_, -1.0f, nullptr); }, &vi);
+        ctx->launches = launches0;   // tuning launches are not the caller's work
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        PCG_CU(ctx, cudaMemcpyAsync(c_.soa.p, b_soa.p, c_.soa.bytes, cudaMemcpyDeviceToDevice, st));
+        PCG_CU(ctx, cudaMemcpyAsync(c_.pos64.p, b_pos.p, c_.pos64.bytes, cudaMemcpyDeviceToDevice, st));
+        PCG_CU(ctx, cudaMemcpyAsync(d.dens.p, b_dens.p, d.dens.bytes, cudaMemcpyDeviceToDevice, st));
+        PCG_CU(ctx, cudaStreamSynchronize(st));
+        if (rc != PCG_OK) return rc;
+        c_.order_dirty = order_dirty;   // the SoA is back as it was: so is the secretion order
+        T.store(kf, vf);
+        T.store(ks, vs);
+        T.store(kb, vb);
+        T.store(ki, vi);
+    }
+    if (!pin_f) {
+        m_.fshape.block = vf / 1000;
+        m_.fshape.queue = vf % 1000;
+    }
+    if (!pin_t) {
+        c_.sec_block = vs;
+        m_.bin_block = vb;
+        m_.int_block = vi;
+    }
+    return PCG_OK;
 }
 
 uint64_t Batch::count_launches(bool mech) const
@@ -340,7 +452,8 @@ std::string Batch::describe() const
 {
     std::ostringstream o;
     o << d.describe() << "forces(block=" << m_.fshape.block << ",queue=" << m_.fshape.queue
-      << ") graphs=" << (use_graphs ? 1 : 0)
+      << ") secrete(block=" << c_.sec_block << ") bin(block=" << m_.bin_block << ") integrate(block="
+      << m_.int_block << ") graphs=" << (use_graphs ? 1 : 0)
       << " launches/step=" << launches_diff << "/" << launches_mech;
     return o.str();
 }

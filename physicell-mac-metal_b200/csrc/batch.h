@@ -69,6 +69,10 @@ public:
 
 private:
     int capture(bool mech, cudaGraphExec_t* out, uint64_t* launches);
+    // Launch shapes of the cell kernels: pinned by the options, else cached
+    // by shape bucket or measured on the batch's own data (the state the
+    // timed launches write is saved first and put back).
+    int tune_cells(const pcg_batch_options* opt, bool tune);
 };
 
 }  // namespace pcg

@@ -564,10 +564,11 @@ cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t strid
 cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_start, const uint32_t* run_inst,
                            const uint64_t* run_dens, const uint32_t* run_slot, const uint32_t* n_runs,
                            uint32_t max_runs, uint32_t max_s, const CellInst* insts, const double* cs, uint32_t cap,
-                           const uint32_t* flags, const uint8_t* mask)
+                           const uint32_t* flags, const uint8_t* mask, int block)
 {
     if (max_runs == 0 || max_s == 0) return cudaSuccess;
-    k_secrete<<<blocks_for(max_runs, 256), 256, 0, st>>>(dens, run_start, run_inst, run_dens, run_slot, n_runs,
+    if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
+    k_secrete<<<blocks_for(max_runs, block), block, 0, st>>>(dens, run_start, run_inst, run_dens, run_slot, n_runs,
                                                           insts, cs, cap, flags, mask);
     return cudaGetLastError();
 }
@@ -584,22 +585,24 @@ cudaError_t launch_cells_move(cudaStream_t st, float* soa, uint32_t stride, cons
 
 cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n, const uint32_t* cell_inst,
                             const CellInst* insts, uint32_t* keys, uint32_t* slots, uint32_t* counts,
-                            const uint8_t* mask)
+                            const uint8_t* mask, int block)
 {
     if (n == 0) return cudaSuccess;
-    k_mech_bin<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, keys, slots, counts, mask);
+    if (block < 32 || block > 1024 || block % 32) return cudaErrorInvalidValue;
+    k_mech_bin<<<blocks_for(n, block), block, 0, st>>>(soa, stride, n, cell_inst, insts, keys, slots, counts, mask);
     return cudaGetLastError();
 }
 
 cudaError_t launch_mech_order(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* keys,
                               const uint32_t* slots, const uint32_t* start, uint32_t n, uint32_t* placed,
-                              uint32_t* skeys, uint32_t* sorder, float4* spos, float4* sprm)
+                              uint32_t* skeys, uint32_t* sorder, float4* spos, float4* sprm, int block)
 {
     if (n == 0) return cudaSuccess;
-    k_mech_place<<<blocks_for(n, 256), 256, 0, st>>>(keys, slots, start, n, placed);
+    if (block < 32 || block > 1024 || block % 32) return cudaErrorInvalidValue;
+    k_mech_place<<<blocks_for(n, block), block, 0, st>>>(keys, slots, start, n, placed);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_mech_order<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, keys, start, placed, n, skeys, sorder, spos, sprm);
+    k_mech_order<<<blocks_for(n, block), block, 0, st>>>(soa, stride, keys, start, placed, n, skeys, sorder, spos, sprm);
     return cudaGetLastError();
 }
 
@@ -652,10 +655,12 @@ cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4
 
 cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, double* pos64, uint32_t stride, uint32_t n,
                                   const uint32_t* cell_inst, const CellInst* insts, float dt_override,
-                                  const uint8_t* mask)
+                                  const uint8_t* mask, int block)
 {
     if (n == 0) return cudaSuccess;
-    k_mech_integrate<<<blocks_for(n, 256), 256, 0, st>>>(soa, pos64, stride, n, cell_inst, insts, dt_override, mask);
+    if (block < 32 || block > 1024 || block % 32) return cudaErrorInvalidValue;
+    k_mech_integrate<<<blocks_for(n, block), block, 0, st>>>(soa, pos64, stride, n, cell_inst, insts, dt_override,
+                                                             mask);
     return cudaGetLastError();
 }
 

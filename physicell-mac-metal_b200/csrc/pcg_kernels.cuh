@@ -243,7 +243,7 @@ cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t strid
 cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_start, const uint32_t* run_inst,
                            const uint64_t* run_dens, const uint32_t* run_slot, const uint32_t* n_runs,
                            uint32_t max_runs, uint32_t max_s, const CellInst* insts, const double* cs, uint32_t cap,
-                           const uint32_t* flags, const uint8_t* mask);
+                           const uint32_t* flags, const uint8_t* mask, int block = 256);
 
 // Mechanics binning as a counting sort: launch_mech_bin writes each cell's
 // global mechanics-voxel key, counts it (counts: V + 1 zeroed words) and
@@ -253,10 +253,10 @@ cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_sta
 // a voxel) and the sorted positions / radii and strengths.
 cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
                             const uint32_t* cell_inst, const CellInst* insts,
-                            uint32_t* keys, uint32_t* slots, uint32_t* counts, const uint8_t* mask);
+                            uint32_t* keys, uint32_t* slots, uint32_t* counts, const uint8_t* mask, int block = 256);
 cudaError_t launch_mech_order(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* keys,
                               const uint32_t* slots, const uint32_t* start, uint32_t n, uint32_t* placed,
-                              uint32_t* skeys, uint32_t* sorder, float4* spos, float4* sprm);
+                              uint32_t* skeys, uint32_t* sorder, float4* spos, float4* sprm, int block = 256);
 // Launch shape of the force pass: threads per block (a multiple of 32, at
 // most 256) and the neighbour queue per thread (0 = force terms in the walk;
 // 16, 32 or 64 slots of shared memory).  Every shape gives the same bits.
@@ -280,7 +280,7 @@ cudaError_t launch_cells_move(cudaStream_t st, float* soa, uint32_t stride, cons
 // positions (three arrays of stride doubles) or null for FP32 positions.
 cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, double* pos64, uint32_t stride, uint32_t n,
                                   const uint32_t* cell_inst, const CellInst* insts, float dt_override,
-                                  const uint8_t* mask);
+                                  const uint8_t* mask, int block = 256);
 
 // Radix sort of (key, value) pairs, stable, 'bits' significant key bits.
 // Scratch from radix_sort_scratch_bytes().  Result lands in (k_out, v_out).

@@ -1325,7 +1325,7 @@ int Cells::secrete(Diffusion& d, const uint8_t* mask)
                                    run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), ktmp.as<uint32_t>() + n, n, max_s,
                                    inst.as<CellInst>(), coef.as<double>(),
                                    static_cast<uint32_t>(rates.bytes / (4 * sizeof(double))),
-                                   coef_flags.as<uint32_t>(), mask);
+                                   coef_flags.as<uint32_t>(), mask, sec_block);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion launch");
     if (n && max_s) ctx->launches++;
     return PCG_OK;
@@ -1381,13 +1381,13 @@ int Mechanics::binsort(Cells& c, const uint8_t* mask)
     PCG_CU(ctx, cudaMemsetAsync(counts.p, 0, counts.bytes, st));
     cudaError_t e = launch_mech_bin(st, c.soa.as<float>(), c.max_cells, c.n, c.cell_inst.as<uint32_t>(),
                                     c.inst.as<CellInst>(), keys.as<uint32_t>(), slots.as<uint32_t>(),
-                                    counts.as<uint32_t>(), mask);
+                                    counts.as<uint32_t>(), mask, bin_block);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "bin launch");
     e = scan_exclusive(st, counts.as<uint32_t>(), start.as<uint32_t>(), static_cast<uint64_t>(total_mvox) + 1, scan_scr.p);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "start-table scan");
     e = launch_mech_order(st, c.soa.as<float>(), c.max_cells, keys.as<uint32_t>(), slots.as<uint32_t>(),
                           start.as<uint32_t>(), c.n, placed.as<uint32_t>(), skeys.as<uint32_t>(),
-                          sorder.as<uint32_t>(), spos.as<float4>(), sprm.as<float4>());
+                          sorder.as<uint32_t>(), spos.as<float4>(), sprm.as<float4>(), bin_block);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "bin order launch");
     ctx->launches += launches_forces(c.n) - 2;   // the memset is not a kernel; forces counted below
     return PCG_OK;
@@ -1411,7 +1411,8 @@ int Mechanics::integrate(Cells& c, float dt_override, const uint8_t* mask)
     if (c.n == 0) return PCG_OK;
     PCG_TRY(c.sync_inst());
     cudaError_t e = launch_mech_integrate(ctx->stream, c.soa.as<float>(), c.pos64.as<double>(), c.max_cells, c.n,
-                                          c.cell_inst.as<uint32_t>(), c.inst.as<CellInst>(), dt_override, mask);
+                                          c.cell_inst.as<uint32_t>(), c.inst.as<CellInst>(), dt_override, mask,
+                                          int_block);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "integrate launch");
     ctx->launches++;
     bool refresh = false;

@@ -256,6 +256,7 @@ public:
     // through the SoA (uploads, host edits) replaces the master.  All-ones
     // (NaN) = no master.
     DevBuf pos64;
+    int sec_block = 256;   // threads per block of the secretion kernel
     bool has_active = false;
     bool inst_dirty = true, coef_dirty = true, order_dirty = true;
     double coef_dt = -1.0;
@@ -300,7 +301,9 @@ public:
     pcg_ctx* ctx = nullptr;
     uint32_t total_mvox = 0;
     uint32_t cap = 0;
-    ForceShape fshape;   // launch shape of the force pass
+    ForceShape fshape;     // launch shape of the force pass
+    int bin_block = 256;   // threads per block of the binning kernels
+    int int_block = 256;   // threads per block of the AB2 kernel
     bool diag = false;
     // binning: keys / slots (voxel key and arrival slot per cell), counts
     // (per voxel, + 1), start (the cell-start table), placed (cells in

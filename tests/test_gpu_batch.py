@@ -153,6 +153,43 @@ def test_sweep_units_count_the_passes(ctx, pcg):
         b.close()
 
 
+@pytest.mark.parametrize("forces,threads", [(256000, 256), (64016, 64), (128032, 128), (256064, 96),
+                                            (96000, 160), (32064, 32)])
+def test_pinned_cell_kernel_shapes_match_tuned(ctx, pcg, forces, threads, tmp_path):
+    """Force pass shapes (threads per block, neighbour queue slots) and the
+    block sizes of the secretion, binning and AB2 kernels change no bit:
+    every pinned shape gives what the autotuned batch gives, over 23
+    sub-steps with two mechanics steps."""
+    insts = small_mix(pcg, seed=11)
+    tuned = run_batch(pcg, ctx, insts, 23, tune_cache=str(tmp_path / "tune.json"))
+    pinned = run_batch(pcg, ctx, insts, 23, autotune=False, pin_forces=forces, pin_cell_threads=threads)
+    for (d0, c0), (d1, c1) in zip(tuned, pinned):
+        assert np.array_equal(d0.view(np.uint32), d1.view(np.uint32))
+        assert np.array_equal(c0.view(np.uint32), c1.view(np.uint32))
+
+
+def test_tuned_shapes_reported_and_cached(ctx, pcg, tmp_path):
+    """The autotuner records its choices for the cell kernels in the tune
+    cache and the batch reports them."""
+    import json
+    cache = tmp_path / "tune.json"
+    b = pcg.Batch(ctx, small_mix(pcg, seed=12), tune_cache=str(cache))
+    desc = b.describe()
+    b.close()
+    for k in ("forces(block=", "secrete(block=", "bin(block=", "integrate(block="):
+        assert k in desc
+    keys = json.loads(cache.read_text()).keys()
+    for k in ("forces:", "secrete:", "bin:", "integrate:"):
+        assert any(x.startswith(k) for x in keys), (k, list(keys))
+
+
+@pytest.mark.parametrize("kw", [{"pin_forces": 256000 + 8}, {"pin_forces": 300032}, {"pin_cell_threads": 48},
+                                {"pin_cell_threads": 512}])
+def test_bad_pinned_cell_shape_is_refused(ctx, pcg, kw):
+    with pytest.raises(pcg.PcgError):
+        pcg.Batch(ctx, small_mix(pcg, seed=9)[:1], autotune=False, **kw)
+
+
 def test_bad_pinned_shape_is_refused(ctx, pcg):
     with pytest.raises(pcg.PcgError):
         pcg.Batch(ctx, small_mix(pcg, seed=9)[:1], autotune=False, pin_x=17 * 16 + 2)
