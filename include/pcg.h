@@ -10,7 +10,7 @@
  * Calls on one pcg_ctx are serialised on that context's CUDA stream and must
  * come from one host thread at a time; separate contexts may be used from
  * separate threads.  Floating-point layouts match the reference exactly:
- *   density   float32 [s][k][j][i]        (src/microenvironment.mm:133-145)
+ *   density   float32 [s][k][j][i]        (src/microenvironment.mm:48-60)
  *   cell SoA  float32 [field * max_cells + cell], 28 fields, fields 23..27
  *             hold uint32 bits            (src/cell_data.cpp:101-180,
  *                                          shaders/types.h:74-102)
@@ -123,16 +123,16 @@ pcg_status pcg_host_free(void* p);
 pcg_status pcg_me_create(pcg_ctx* ctx, const pcg_grid_params* grid,
                          const pcg_substrate_params* substrates, pcg_me** out);
 pcg_status pcg_me_destroy(pcg_me* me);
-/* Microenvironment::initialize density fill (microenvironment.mm:139-145). */
+/* Microenvironment::initialize density fill (microenvironment.mm:54-60). */
 pcg_status pcg_me_fill(pcg_me* me, const float* value_per_substrate);
-/* Bulk setDensity / densityBuffer() read-back (microenvironment.mm:239-247);
+/* Bulk setDensity / densityBuffer() read-back (microenvironment.mm:154-162);
  * n_floats must equal nx*ny*nz*S. */
 pcg_status pcg_me_upload(pcg_me* me, const float* host, size_t n_floats);
 pcg_status pcg_me_download(pcg_me* me, float* host, size_t n_floats);
-/* Microenvironment::simulateDiffusionDecay (microenvironment.mm:191-200):
+/* Microenvironment::simulateDiffusionDecay (microenvironment.mm:106-115):
  * the x, y (, z) sweeps only, n_steps times. */
 pcg_status pcg_me_diffuse(pcg_me* me, int n_steps);
-/* Microenvironment::applyDirichletBC (microenvironment.mm:212-237). */
+/* Microenvironment::applyDirichletBC (microenvironment.mm:127-152). */
 pcg_status pcg_me_apply_dirichlet(pcg_me* me);
 /* processSecretion (src/cell_phenotype.cpp:526-564) for every active cell
  * of 'cells', applied per voxel in ascending cell index. */
@@ -141,7 +141,7 @@ pcg_status pcg_me_secrete(pcg_me* me, pcg_cells* cells, double dt);
  * sweeps -> Dirichlet reset (fused into the last sweep) -> secretion (when
  * cells is not NULL), dt = grid->dt. */
 pcg_status pcg_me_step(pcg_me* me, pcg_cells* cells, int n_steps);
-/* Microenvironment::computeGradients + read-back (microenvironment.mm:282-342):
+/* Microenvironment::computeGradients + read-back (microenvironment.mm:197-257):
  * three arrays of nx*ny*nz*S floats (any may be NULL). */
 pcg_status pcg_me_gradients(pcg_me* me, float* gx, float* gy, float* gz, size_t n_floats);
 /* Device pointer of the density block.  On the device, rows of x are
@@ -178,7 +178,7 @@ pcg_status pcg_cells_count(pcg_cells* cells, uint32_t* n_cells);
  * removeCell (src/cell_data.cpp:408-498, the last cell moved into the
  * freed place) for each of 'indices' in descending order, indices at or
  * past the current count skipped -- phase 3 of updatePhenotypes
- * (src/cell_phenotype.cpp:837-844).  Every moved cell takes its 28 SoA
+ * (src/cell_phenotype.cpp:838-844).  Every moved cell takes its 28 SoA
  * fields, its per-substrate rates and its active flag along; the count
  * drops by the number removed.  One launch (pcg_removal_plan's moves). */
 pcg_status pcg_cells_remove(pcg_cells* cells, const uint32_t* indices, uint32_t count);
@@ -212,20 +212,20 @@ pcg_status pcg_cells_download_positions64(pcg_cells* cells, double* xyz, uint32_
  * cell-start table replaces the 64-slot hash: voxelCellCount(v) =
  * start[v+1] - start[v], voxelCells(v) = sorted + start[v].
  * ---------------------------------------------------------------------- */
-/* CellMechanics::initialize (cell_mechanics.mm:112-171): the mechanics
+/* CellMechanics::initialize (cell_mechanics.mm:23-82): the mechanics
  * grid of params->mech_grid_* voxels of params->mechanics_voxel_size with
  * origin (x_min, y_min, z_min). */
 pcg_status pcg_mech_create(pcg_ctx* ctx, const pcg_mechanics_params* params,
                            float x_min, float y_min, float z_min, uint32_t max_cells, pcg_mech** out);
 pcg_status pcg_mech_destroy(pcg_mech* mech);
-/* CellMechanics::computeForces (cell_mechanics.mm:188-200): bin, sort,
+/* CellMechanics::computeForces (cell_mechanics.mm:99-111): bin, sort,
  * cell-start table, forces -> velocity and simple pressure. */
 pcg_status pcg_mech_forces(pcg_mech* mech, pcg_cells* cells);
-/* CellMechanics::integratePositions (cell_mechanics.mm:202-209). */
+/* CellMechanics::integratePositions (cell_mechanics.mm:113-120). */
 pcg_status pcg_mech_integrate(pcg_mech* mech, pcg_cells* cells, float dt);
-/* CellMechanics::update (cell_mechanics.mm:173-186): forces + integrate. */
+/* CellMechanics::update (cell_mechanics.mm:84-97): forces + integrate. */
 pcg_status pcg_mech_update(pcg_mech* mech, pcg_cells* cells, float dt);
-/* CellMechanics::syncHashPointers (cell_mechanics.mm:211-222): copy the
+/* CellMechanics::syncHashPointers (cell_mechanics.mm:122-133): copy the
  * cell-start table (V + 1 entries) and the sorted cell indices (n_cells)
  * to the host; either pointer may be NULL. */
 pcg_status pcg_mech_bins(pcg_mech* mech, uint32_t* start, uint32_t* sorted_cells);
@@ -254,7 +254,7 @@ uint32_t pcg_neighbor_hash(uint32_t cell);
  * ---------------------------------------------------------------------- */
 enum { PCG_MOT_REFERENCE = 0, PCG_MOT_SUBSTRATE_MAJOR = 1 };
 
-/* MotilityData::allocate / allocateSubstrate (motility.cpp:91-113);
+/* MotilityData::allocate / allocateSubstrate (motility.cpp:90-116);
  * n_substrates = 0: the single-substrate chemotaxis rule only. */
 pcg_status pcg_motility_create(pcg_ctx* ctx, uint32_t max_cells, uint32_t n_substrates, pcg_motility** out);
 pcg_status pcg_motility_destroy(pcg_motility* mot);
@@ -334,6 +334,14 @@ pcg_status pcg_sort_pairs_static(pcg_ctx* ctx, const uint32_t* keys_in, const ui
  * touching the device (nth = 0 turns it off). */
 void pcg_debug_alloc_stats(uint64_t* device_mallocs, uint64_t* pool_reuses);
 void pcg_debug_fail_alloc(uint64_t nth);
+/* No reference counterpart (a failed Metal command buffer is logged and
+ * the loop goes on, metal_context.mm:448-461).  Test aid for the bounded
+ * device waits: with on != 0, the first wait of every plane-sweep CTA
+ * launched on ctx reports that its bound ran out at once.  The CTA records
+ * it in the context's status word, waits (with the normal bound) for the
+ * copies it issued and exits without storing its plane, so pcg_sync
+ * returns PCG_ERR_DEVICE; with on = 0 the context works as before. */
+pcg_status pcg_debug_give_up_waits(pcg_ctx* ctx, int on);
 
 /* ------------------------------------------------------------------------
  * Batch — many independent simulations of uneven grid and cell counts
@@ -355,7 +363,7 @@ typedef struct {
     const double* saturation;
     const double* net_export;
     const uint8_t* active;                   /* NULL = all active */
-    pcg_mechanics_params mech;               /* mechanics grid (cell_mechanics.mm:115-130) */
+    pcg_mechanics_params mech;               /* mechanics grid (cell_mechanics.mm:26-41) */
     float dt_mechanics;
     uint32_t flags;
 } pcg_instance_desc;
@@ -448,9 +456,18 @@ typedef struct {
     uint32_t steps_per_tick;   /* diffusion sub-steps per tick (default 100) */
 } pcg_serve_options;
 
-enum { PCG_REQ_QUEUED = 0, PCG_REQ_RUNNING = 1, PCG_REQ_DONE = 2 };
+enum { PCG_REQ_QUEUED = 0, PCG_REQ_RUNNING = 1, PCG_REQ_DONE = 2, PCG_REQ_CANCELLED = 3 };
 
 pcg_status pcg_serve_create(pcg_ctx* ctx, const pcg_serve_options* options, pcg_server** out);
+/* One server over several contexts, normally one per GPU (a device may
+ * also appear more than once).  Each request runs on one context, chosen
+ * when it is admitted: the one with the most unused budget among those
+ * where it fits.  budget_bytes and max_active apply to each context.
+ * Every context's sub-steps of a tick are issued before any is waited for,
+ * so the GPUs work at the same time.  The contexts are used from the
+ * calling thread only; each is made current while its work is issued. */
+pcg_status pcg_serve_create_multi(pcg_ctx* const* ctxs, uint32_t n_ctx, const pcg_serve_options* options,
+                                  pcg_server** out);
 pcg_status pcg_serve_destroy(pcg_server* srv);
 /* Queue a request (the host data is copied); *id receives its id. */
 pcg_status pcg_serve_submit(pcg_server* srv, const pcg_instance_desc* inst, uint32_t n_diffusion_steps,
@@ -459,6 +476,14 @@ pcg_status pcg_serve_submit(pcg_server* srv, const pcg_instance_desc* inst, uint
  * finished ones.  *n_running / *n_queued / *n_finished_now may be NULL. */
 pcg_status pcg_serve_tick(pcg_server* srv, uint32_t* n_running, uint32_t* n_queued, uint32_t* n_finished_now);
 pcg_status pcg_serve_state(pcg_server* srv, uint64_t id, int* state);
+/* Cancels a request: a queued one leaves the queue now, a running one
+ * leaves its batch (and frees its budget) at the next tick; its state
+ * becomes PCG_REQ_CANCELLED and fetch / request_times refuse it.  A finished
+ * request cannot be cancelled (PCG_ERR_INVALID). */
+pcg_status pcg_serve_cancel(pcg_server* srv, uint64_t id);
+/* Index (into the contexts the server was made with) of the context a
+ * request was admitted to, -1 while it is queued. */
+pcg_status pcg_serve_placement(pcg_server* srv, uint64_t id, int* ctx_index);
 /* Results of a finished request; either pointer may be NULL. */
 pcg_status pcg_serve_fetch(pcg_server* srv, uint64_t id, float* density, size_t n_floats,
                            float* soa, uint32_t soa_max_cells);

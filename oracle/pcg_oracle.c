@@ -129,7 +129,7 @@ void or_sweep_axis(float* density, const or_grid* g, const or_substrate* subs, i
     for (uint32_t s = 0; s < g->n_substrates; s++) {
         const or_substrate* sp = &subs[s];
         const int dir = sp->dirichlet_enabled != 0;
-        /* coefficient D*dt/h^2 (microenvironment.mm:175, diffusion_2d.metal:181-184) */
+        /* coefficient D*dt/h^2 (microenvironment.mm:90, diffusion_2d.metal:181-184) */
         const double c64 = (double)sp->diffusion_coefficient * (double)g->dt / ((double)h * (double)h);
         const double hd64 = (double)sp->decay_rate * (double)g->dt / (double)d;
         const float D = sp->diffusion_coefficient, dt = g->dt;
@@ -175,7 +175,7 @@ void or_apply_dirichlet(float* density, const or_grid* g, const or_substrate* su
                 for (size_t v = 0; v < nx * ny; v++) slab[v] = T;
                 continue;
             }
-            /* microenvironment.mm:225-235 */
+            /* microenvironment.mm:140-150 */
             for (size_t i = 0; i < nx; i++) { slab[i] = T; slab[(ny - 1) * nx + i] = T; }
             for (size_t j = 0; j < ny; j++) { slab[j * nx] = T; slab[j * nx + nx - 1] = T; }
         }
@@ -256,7 +256,7 @@ void or_secretion(float* density, const or_grid* g, uint32_t n_cells,
 void or_mech_params(float x_min, float x_max, float y_min, float y_max,
                     float z_min, float z_max, int use_2d, float dt_mech, or_mech* m)
 {
-    /* cell_mechanics.mm:115-130 */
+    /* cell_mechanics.mm:26-41 */
     const float vs = 30.0f;
     float Lx = x_max - x_min, Ly = y_max - y_min, Lz = z_max - z_min;
     uint32_t nx = (uint32_t)(Lx / vs), ny = (uint32_t)(Ly / vs), nz = (uint32_t)(Lz / vs);
@@ -468,7 +468,7 @@ void or_voxel_refresh(float* soa, uint32_t max_cells, uint32_t n_cells, const or
 }
 
 /* ------------------------------------------------------------------ */
-/* Dead-cell compaction (cell_phenotype.cpp:837-844, cell_data.cpp:408-498) */
+/* Dead-cell compaction (cell_phenotype.cpp:838-844, cell_data.cpp:408-498) */
 /* ------------------------------------------------------------------ */
 
 static int cmp_desc_u32(const void* a, const void* b)

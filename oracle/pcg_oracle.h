@@ -7,12 +7,12 @@
  *
  * It restates, in plain C, the arithmetic of the reference's hot path:
  *   - LOD Thomas sweeps          shaders/diffusion_2d.metal:28-157 (x), :165-292 (y)
- *   - Dirichlet edge reset       src/microenvironment.mm:212-237 (applyDirichletBC)
+ *   - Dirichlet edge reset       src/microenvironment.mm:127-152 (applyDirichletBC)
  *   - secretion / uptake         src/cell_phenotype.cpp:526-564 (processSecretion)
  *   - spatial-hash binning       shaders/mechanics.metal:41-85 (build_spatial_hash)
  *   - neighbour forces           shaders/mechanics.metal:91-216 (compute_forces)
  *   - AB2 position update        shaders/integrate.metal:31-80 (integrate_positions)
- *   - mechanics grid set-up      src/cell_mechanics.mm:112-171 (CellMechanics::initialize)
+ *   - mechanics grid set-up      src/cell_mechanics.mm:23-82 (CellMechanics::initialize)
  *   - sub-step ordering          src/main.mm:341-391
  *
  * Precision modes for the diffusion sweeps:
@@ -95,7 +95,7 @@ void or_sweep_axis(float* density, const or_grid* g, const or_substrate* subs, i
  * resets all six faces. */
 void or_apply_dirichlet(float* density, const or_grid* g, const or_substrate* subs);
 
-/* Gradients (Microenvironment::computeGradients, microenvironment.mm:282-342),
+/* Gradients (Microenvironment::computeGradients, microenvironment.mm:197-257),
  * computed in double from FP32 density, stored FP32. */
 void or_gradients(const float* density, const or_grid* g, float* gx, float* gy, float* gz);
 
@@ -143,7 +143,7 @@ void or_mech_forces(float* soa, uint32_t max_cells, uint32_t n_cells, const or_m
 uint32_t or_nbr_hash(uint32_t j);
 
 /* AB2 update (integrate.metal:31-80) in double, stored FP32; clamp box is
- * the mechanics grid [min, min + n * voxel] (cell_mechanics.mm:146-159). */
+ * the mechanics grid [min, min + n * voxel] (cell_mechanics.mm:57-70). */
 void or_mech_integrate(float* soa, uint32_t max_cells, uint32_t n_cells, const or_mech* m,
                        float x_min, float y_min, float z_min, float dt);
 
@@ -157,7 +157,7 @@ void or_mech_integrate_master(float* soa, uint32_t max_cells, uint32_t n_cells, 
                               float x_min, float y_min, float z_min, float dt, double* pos64);
 
 /* Voxel refresh from positions (3-D aware form of cell_phenotype.cpp:781-789):
- * voxel_index = Microenvironment::voxelIndex(x, y, z) (microenvironment.mm:261-269). */
+ * voxel_index = Microenvironment::voxelIndex(x, y, z) (microenvironment.mm:176-184). */
 void or_voxel_refresh(float* soa, uint32_t max_cells, uint32_t n_cells, const or_grid* g);
 
 /* Dead-cell compaction: phase 3 of updatePhenotypes (cell_phenotype.cpp:

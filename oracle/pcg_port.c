@@ -8,7 +8,7 @@
  *                as in pcg_oracle.h), with the per-line Thomas constants
  *                (c' and 1/denominator, identical for every line of one
  *                substrate and axis) hoisted out of the line loop;
- *   Dirichlet    src/microenvironment.mm:212-237 (six faces in 3-D);
+ *   Dirichlet    src/microenvironment.mm:127-152 (six faces in 3-D);
  *   secretion    src/cell_phenotype.cpp:526-564 (FP64 per cell, ascending);
  *   mechanics    shaders/mechanics.metal:41-216, shaders/integrate.metal:31-80.
  * Lines are parallel over OpenMP threads; the y and z sweeps walk a whole

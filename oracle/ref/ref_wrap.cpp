@@ -12,8 +12,8 @@
  *   src/output_writer.cpp + src/matlab_writer.cpp (writeMatlabSnapshots)
  * The host-side steps that live in Objective-C++ files and cannot be
  * compiled here are restated below with their citations:
- *   ThomasCoeffs set-up   src/microenvironment.mm:171-177
- *   applyDirichletBC      src/microenvironment.mm:212-237
+ *   ThomasCoeffs set-up   src/microenvironment.mm:86-92
+ *   applyDirichletBC      src/microenvironment.mm:127-152
  */
 #include <algorithm>
 #include <cstdint>
@@ -53,7 +53,7 @@ int ref_sizeof_substrate(void) { return (int)sizeof(SubstrateParams); }
 int ref_sizeof_mech(void) { return (int)sizeof(MechanicsParams); }
 int ref_max_cells_per_voxel(void) { return MAX_CELLS_PER_VOXEL; }
 
-/* microenvironment.mm:171-177 */
+/* microenvironment.mm:86-92 */
 void ref_thomas_coeffs(const GridParams* g, const SubstrateParams* sp, ThomasCoeffs* tc)
 {
     for (uint32_t s = 0; s < g->n_substrates; s++) {
@@ -66,7 +66,7 @@ void ref_thomas_coeffs(const GridParams* g, const SubstrateParams* sp, ThomasCoe
     }
 }
 
-/* Microenvironment::simulateDiffusionDecay: x then y (microenvironment.mm:191-200). */
+/* Microenvironment::simulateDiffusionDecay: x then y (microenvironment.mm:106-115). */
 void ref_simulate_diffusion_decay(float* density, const GridParams* g, const SubstrateParams* sp, int threads)
 {
     std::vector<ThomasCoeffs> tc(g->n_substrates ? g->n_substrates : 1);
@@ -97,7 +97,7 @@ void ref_sweep_y(float* density, const GridParams* g, const SubstrateParams* sp)
     for (uint32_t t = 0; t < g->nx; t++) diffusion_sweep_y(density, *g, sp, tc.data(), t);
 }
 
-/* microenvironment.mm:212-237 */
+/* microenvironment.mm:127-152 */
 void ref_apply_dirichlet(float* density, const GridParams* g, const SubstrateParams* sp)
 {
     const uint32_t nx = g->nx, ny = g->ny, total = nx * ny * g->nz;
@@ -222,7 +222,7 @@ void ref_write_matlab(const float* soa, uint32_t max_cells, uint32_t n_cells, ui
     writeMatlabSnapshots(cells, density, *g, frame, folder);
 }
 
-/* Phase 3 of updatePhenotypes (cell_phenotype.cpp:837-844, restated: the
+/* Phase 3 of updatePhenotypes (cell_phenotype.cpp:838-844, restated: the
  * dead-cell indices sorted descending, those at or past num_cells skipped)
  * over the reference's own CellData::removeCell (cell_data.cpp:408-498), on
  * a CellData holding the 28-field SoA block and the four per-substrate rate

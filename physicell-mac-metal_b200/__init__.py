@@ -35,7 +35,7 @@ NUM_FIELDS = 28
 
 PCG_OK = 0
 INST_REFRESH_VOXELS = 1
-REQ_QUEUED, REQ_RUNNING, REQ_DONE = 0, 1, 2
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_CANCELLED = 0, 1, 2, 3
 N_PHASES = 7
 PHASES = ("x_sweep", "y_sweep", "z_sweep", "secretion", "bin_sort", "forces", "integrate")
 
@@ -185,6 +185,9 @@ _SIGS = [
     ("pcg_batch_describe", C.c_char_p, [_P]),
     ("pcg_serve_create", C.c_int, [_P, C.POINTER(ServeOptions), C.POINTER(_P)]),
     ("pcg_serve_destroy", C.c_int, [_P]),
+    ("pcg_serve_create_multi", C.c_int, [C.POINTER(_P), C.c_uint32, C.POINTER(ServeOptions), C.POINTER(_P)]),
+    ("pcg_serve_cancel", C.c_int, [_P, C.c_uint64]),
+    ("pcg_serve_placement", C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int)]),
     ("pcg_serve_submit", C.c_int, [_P, C.POINTER(InstanceDesc), C.c_uint32, C.POINTER(C.c_uint64)]),
     ("pcg_serve_tick", C.c_int, [_P, _U32P, _U32P, _U32P]),
     ("pcg_serve_state", C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int)]),
@@ -194,6 +197,7 @@ _SIGS = [
     ("pcg_instance_bytes", C.c_uint64, [C.POINTER(InstanceDesc)]),
     ("pcg_debug_alloc_stats", None, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_debug_fail_alloc", None, [C.c_uint64]),
+    ("pcg_debug_give_up_waits", C.c_int, [_P, C.c_int]),
 ]
 
 
@@ -264,7 +268,7 @@ def make_substrates(params):
 
 
 def mech_params_for_domain(x_min, x_max, y_min, y_max, z_min, z_max, use_2d, dt_mech=0.1, voxel=30.0):
-    """CellMechanics::initialize grid rule (src/cell_mechanics.mm:115-130):
+    """CellMechanics::initialize grid rule (src/cell_mechanics.mm:26-41):
     30 um voxels, truncation, at least 1, nz = 1 in 2-D (FP32 arithmetic)."""
     f = np.float32
     vs = f(voxel)
@@ -463,7 +467,7 @@ class Cells:
 
     def remove(self, indices):
         """Dead-cell compaction (CellData::removeCell for each index in
-        descending order, cell_phenotype.cpp:837-844) on the device; returns
+        descending order, cell_phenotype.cpp:838-844) on the device; returns
         the new count."""
         idx = np.ascontiguousarray(indices, np.uint32)
         self.ctx.check(lib().pcg_cells_remove(self.h, _u32(idx), idx.size))
@@ -796,15 +800,29 @@ class Batch:
 
 
 class Server:
-    """pcg_server: continuous batching of simulation requests."""
+    """pcg_server: continuous batching of simulation requests.  ctx may be
+    one Context or a list of them (one per GPU, pcg_serve_create_multi);
+    budget_bytes and max_active then apply to each."""
 
     def __init__(self, ctx, budget_bytes=150e9, max_active=0, steps_per_tick=100):
-        self.ctx = ctx
+        ctxs = list(ctx) if isinstance(ctx, (list, tuple)) else [ctx]
+        self.ctx = ctxs[0]
+        self.ctxs = ctxs
         opt = ServeOptions(int(budget_bytes), max_active, steps_per_tick)
         h = _P()
-        ctx.check(lib().pcg_serve_create(ctx.h, C.byref(opt), C.byref(h)))
+        arr = (_P * len(ctxs))(*[c.h for c in ctxs])
+        self.ctx.check(lib().pcg_serve_create_multi(arr, len(ctxs), C.byref(opt), C.byref(h)))
         self.h = h
         self.requests = {}
+
+    def cancel(self, rid):
+        self.ctx.check(lib().pcg_serve_cancel(self.h, rid))
+
+    def placement(self, rid):
+        """Index of the context request rid runs on (-1 while queued)."""
+        k = C.c_int()
+        self.ctx.check(lib().pcg_serve_placement(self.h, rid, C.byref(k)))
+        return k.value
 
     def submit(self, inst, n_steps):
         d = inst.desc()

@@ -149,8 +149,9 @@ static pcg_status create_ctx(int device, void* stream, pcg_ctx** out)
         }
         c->own_stream = true;
     }
-    if (cudaMalloc(&c->status, sizeof(unsigned)) != cudaSuccess ||
-        cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream) != cudaSuccess ||
+    // [0] the status word, [1] test switches (PCG_DEV_TEST_*)
+    if (cudaMalloc(&c->status, 2 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMemsetAsync(c->status, 0, 2 * sizeof(unsigned), c->stream) != cudaSuccess ||
         cudaStreamSynchronize(c->stream) != cudaSuccess) {
         g_create_err = "status word allocation failed";
         if (c->own_stream) cudaStreamDestroy(c->stream);
@@ -639,5 +640,14 @@ void pcg_debug_alloc_stats(uint64_t* device_mallocs, uint64_t* pool_reuses)
 }
 
 void pcg_debug_fail_alloc(uint64_t nth) { fail_alloc_after(nth); }
+
+pcg_status pcg_debug_give_up_waits(pcg_ctx* ctx, int on)
+{
+    if (!ctx) return PCG_ERR_INVALID;
+    const unsigned v = on ? PCG_DEV_TEST_GIVE_UP : 0u;
+    PCG_CU(ctx, cudaMemcpyAsync(ctx->status + 1, &v, sizeof v, cudaMemcpyHostToDevice, ctx->stream));
+    PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    return PCG_OK;
+}
 
 }  // extern "C"

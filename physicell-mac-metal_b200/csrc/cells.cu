@@ -7,8 +7,8 @@
 //   binning    shaders/mechanics.metal:54-76 (FP32 divide + truncation);
 //   forces     shaders/mechanics.metal:91-216;
 //   integrate  shaders/integrate.metal:31-80, clamp box = mechanics grid
-//              (src/cell_mechanics.mm:147-159);
-//   voxel refresh  Microenvironment::voxelIndex (microenvironment.mm:261-269).
+//              (src/cell_mechanics.mm:57-70);
+//   voxel refresh  Microenvironment::voxelIndex (microenvironment.mm:176-184).
 // The reference's GPU hash and CPU secretion loop are racy; here every
 // result is deterministic: cells are sorted by (voxel, cell index) with a
 // stable radix sort and each voxel's cells are processed in that order.

@@ -2,7 +2,7 @@
 //
 // Reference semantics: shaders/diffusion_2d.metal:28-157 (x sweep) and
 // :165-292 (y sweep), one tridiagonal solve per line over the interior
-// nodes 1..n-2 with the decay on the diagonal; src/microenvironment.mm:212-237
+// nodes 1..n-2 with the decay on the diagonal; src/microenvironment.mm:127-152
 // (applyDirichletBC); :282-342 (computeGradients).  The z sweep applies the
 // same per-line rule along k.
 //
@@ -718,7 +718,13 @@ __global__ void __launch_bounds__(kPlaneThreads) k_sweep_planes(const PlaneJob* 
         }
         bulk_load(ty, tab + jb.tab_y, tby, bar);
     }
-    const bool got = mbar_wait(bar, 0, status);
+    bool got;
+    if (status[1] & PCG_DEV_TEST_GIVE_UP) {   // test switch: this wait's bound ran out
+        if (threadIdx.x == 0) atomicOr(status, PCG_DEV_TIMEOUT);
+        got = false;
+    } else {
+        got = mbar_wait(bar, 0, status);
+    }
     if (!__syncthreads_and(got)) {
         // a wait ran out: one more bounded wait for the copies before the
         // CTA releases its shared memory
@@ -813,7 +819,7 @@ __global__ void k_dirichlet(float* __restrict__ dens, const FaceJob* __restrict_
     float* base = dens + jb.base;
     const uint32_t nx = jb.nx, ny = jb.ny, nz = jb.nz;
     const size_t px = jb.px, slab = px * ny;
-    // edges of every slab (microenvironment.mm:225-235)
+    // edges of every slab (microenvironment.mm:140-150)
     const uint32_t per = 2u * nx + 2u * ny;
     const size_t total = static_cast<size_t>(nz) * per;
     for (size_t e = threadIdx.x; e < total; e += blockDim.x) {

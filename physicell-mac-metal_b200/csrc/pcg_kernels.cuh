@@ -93,6 +93,10 @@ constexpr uint32_t kRowTensorMaxN = 252;
 
 // Device status word bits (a kernel that cannot finish records why and returns).
 enum : unsigned { PCG_DEV_TIMEOUT = 1u, PCG_DEV_ALIGN = 2u };
+// Test switches, in the word after the status word: PCG_DEV_TEST_GIVE_UP
+// makes the first wait of every plane CTA report that its bound ran out at
+// once (the wait for the CTA's own copies before it exits keeps its bound).
+enum : unsigned { PCG_DEV_TEST_GIVE_UP = 1u };
 
 // ---------------------------------------------------------------- cells
 
@@ -111,7 +115,7 @@ struct CellInst {
     uint32_t cell_off;     // global index of the instance's first cell
     uint32_t n_cells;
     uint32_t rate_off;     // index of (cell 0, substrate 0) in the rate arrays
-    // mechanics grid (cell_mechanics.mm:115-159): origin, voxel, clamp box
+    // mechanics grid (cell_mechanics.mm:26-70): origin, voxel, clamp box
     uint32_t mnx, mny, mnz, mvox_base;
     float vs, maxd, mx_min, my_min;
     float mz_min, box_hi_x, box_hi_y, box_hi_z;
@@ -215,7 +219,7 @@ cudaError_t launch_sweep_global(cudaStream_t st, float* dens, const SweepTile* t
 struct FaceJob { uint64_t base; uint32_t nx, ny, nz, px; float T; uint32_t _pad; };
 cudaError_t launch_dirichlet(cudaStream_t st, float* dens, const FaceJob* jobs, uint32_t njobs);
 
-// Central / one-sided gradients (microenvironment.mm:282-342).
+// Central / one-sided gradients (microenvironment.mm:197-257).
 struct GradJob { uint64_t base; uint64_t out_base; uint32_t nx, ny, nz, px; float inv_dx, inv_dy, inv_dz, _pad; };
 cudaError_t launch_gradients(cudaStream_t st, const float* dens, float* gx, float* gy, float* gz,
                              const GradJob* jobs, uint32_t njobs, uint64_t max_voxels);

@@ -374,7 +374,7 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
                 const uint32_t n = axis_n(g, a);
                 const double h = axis_h(g, a);
                 // D dt / h^2 and the split decay, in FP64 from the FP32 parameters
-                // (microenvironment.mm:171-177; decay lambda dt / d per sweep)
+                // (microenvironment.mm:86-92; decay lambda dt / d per sweep)
                 const double cc = static_cast<double>(sp.diffusion_coefficient) * static_cast<double>(g.dt) / (h * h);
                 const double hd = static_cast<double>(sp.decay_rate) * static_cast<double>(g.dt) / nd;
                 const bool dir = sp.dirichlet_enabled != 0;
@@ -1133,7 +1133,7 @@ void fill_mech_inst(CellInst& ci, const pcg_mechanics_params& m, float x_min, fl
     ci.mx_min = x_min;
     ci.my_min = y_min;
     ci.mz_min = z_min;
-    // integrate.metal:279-281 with the mechanics GridParams (cell_mechanics.mm:147-156), FP32
+    // integrate.metal:63-65 with the mechanics GridParams (cell_mechanics.mm:57-67), FP32
     ci.box_hi_x = x_min + static_cast<float>(m.mech_grid_nx) * m.mechanics_voxel_size;
     ci.box_hi_y = y_min + static_cast<float>(m.mech_grid_ny) * m.mechanics_voxel_size;
     ci.box_hi_z = z_min + static_cast<float>(m.mech_grid_nz) * m.mechanics_voxel_size;

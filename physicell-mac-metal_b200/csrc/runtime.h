@@ -320,7 +320,7 @@ public:
     uint64_t device_bytes() const;
 };
 
-// Mechanics grid of the reference (cell_mechanics.mm:115-130).
+// Mechanics grid of the reference (cell_mechanics.mm:26-41).
 void fill_mech_inst(CellInst& ci, const pcg_mechanics_params& m, float x_min, float y_min, float z_min);
 void fill_diff_inst(CellInst& ci, const DiffInstance& d);
 
@@ -329,7 +329,7 @@ int key_bits_for(uint64_t n_keys);
 // The moves of CellData::removeCell (cell_data.cpp:408-498: the last cell
 // takes the freed place) called for each of 'indices' in descending order,
 // skipping indices at or past the current count, as phase 3 of
-// updatePhenotypes does (cell_phenotype.cpp:837-844).  Each move (x, y):
+// updatePhenotypes does (cell_phenotype.cpp:838-844).  Each move (x, y):
 // the cell that started at place y ends at place x; every other place below
 // the returned count keeps its cell.  Moves are sorted by destination.
 uint32_t removal_plan(uint32_t n_cells, const uint32_t* indices, uint32_t count, std::vector<uint2>* moves);

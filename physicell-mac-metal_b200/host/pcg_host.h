@@ -95,9 +95,9 @@ public:
     template <class Config>
     void initialize(const Config& config, Context* ctx);
 
-    // x, y (, z) sweeps on the device (microenvironment.mm:191-200)
+    // x, y (, z) sweeps on the device (microenvironment.mm:106-115)
     void simulateDiffusionDecay();
-    // microenvironment.mm:212-237
+    // microenvironment.mm:127-152
     void applyDirichletBC();
     // One main-loop diffusion sub-step on the device: sweeps, Dirichlet reset
     // and secretion of every active cell (main.mm:341-363).
@@ -109,12 +109,12 @@ public:
 
     float getDensity(uint32_t voxel_index, uint32_t substrate_index) const;
     void setDensity(uint32_t voxel_index, uint32_t substrate_index, float value);
-    // microenvironment.mm:249-259 (single voxel, CPU formula, on the mirror)
+    // microenvironment.mm:164-174 (single voxel, CPU formula, on the mirror)
     void applySecretion(uint32_t voxel_index, uint32_t substrate_index, float secretion_rate, float uptake_rate,
                         float saturation_density, float dt);
 
     uint32_t numVoxels() const { return grid_.nx * grid_.ny * grid_.nz; }
-    uint32_t voxelIndex(float x, float y, float z) const;   // microenvironment.mm:261-269
+    uint32_t voxelIndex(float x, float y, float z) const;   // microenvironment.mm:176-184
     pcg_grid_params getGridParams() const { return grid_; }
     Context* context() const { return ctx_; }
 
@@ -151,13 +151,13 @@ public:
     template <class Config>
     void initialize(const Config& config, Context* ctx, uint32_t max_cells = 200000);
 
-    // clear/build/forces + integrate (cell_mechanics.mm:173-186)
+    // clear/build/forces + integrate (cell_mechanics.mm:84-97)
     template <class Cells>
     void update(Cells& cells, float dt);
-    // bin + sort + cell-start table + forces (cell_mechanics.mm:188-200)
+    // bin + sort + cell-start table + forces (cell_mechanics.mm:99-111)
     template <class Cells>
     void computeForces(Cells& cells, float dt);
-    // AB2 + clamp (cell_mechanics.mm:202-209)
+    // AB2 + clamp (cell_mechanics.mm:113-120)
     template <class Cells>
     void integratePositions(Cells& cells, float dt);
 
@@ -166,7 +166,7 @@ public:
     uint32_t voxelIndexFromPosition(float px, float py, float pz) const;   // cell_mechanics.h:40-50
     uint32_t voxelCellCount(uint32_t v) const;                             // cell_mechanics.h:53-56
     const uint32_t* voxelCells(uint32_t v) const;                          // cell_mechanics.h:59-62
-    void syncHashPointers();                                               // cell_mechanics.mm:211-222
+    void syncHashPointers();                                               // cell_mechanics.mm:122-133
 
     pcg_cells* device_cells() const { return cells_; }
 private:
@@ -206,7 +206,7 @@ struct MotilityData {
     MotilityData(const MotilityData&) = delete;
     MotilityData& operator=(const MotilityData&) = delete;
 
-    void allocate(uint32_t max_cells);               // motility.cpp:91-107
+    void allocate(uint32_t max_cells);               // motility.cpp:90-107
     void allocateSubstrate(uint32_t n_substrates);   // motility.cpp:109-116
     void free_all();                                 // motility.cpp:118-131
     void setDefaults(uint32_t index);                // motility.cpp:133-152

@@ -17,7 +17,7 @@ template <class Config>
 void Microenvironment::initialize(const Config& config, Context* ctx)
 {
     ctx_ = ctx;
-    // microenvironment.mm:117-130: truncating voxel counts, nz = 1 in 2-D
+    // microenvironment.mm:33-35: truncating voxel counts, nz = 1 in 2-D
     grid_ = pcg_grid_params{};
     grid_.nx = static_cast<uint32_t>((config.x_max - config.x_min) / config.grid.dx);
     grid_.ny = static_cast<uint32_t>((config.y_max - config.y_min) / config.grid.dy);
@@ -85,7 +85,7 @@ template <class Config>
 void CellMechanics::initialize(const Config& config, Context* ctx, uint32_t max_cells)
 {
     ctx_ = ctx;
-    // cell_mechanics.mm:115-130
+    // cell_mechanics.mm:26-41
     const float vs = 30.0f;
     params_ = pcg_mechanics_params{};
     params_.dt = config.dt_mechanics;

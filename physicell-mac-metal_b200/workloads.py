@@ -34,7 +34,7 @@ DT_MECH = 0.1
 
 
 def voxel_index(x, y, z, grid):
-    """Microenvironment::voxelIndex (src/microenvironment.mm:261-269), FP32."""
+    """Microenvironment::voxelIndex (src/microenvironment.mm:176-184), FP32."""
     f = np.float32
 
     def axis(p, lo, h, n):
