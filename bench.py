@@ -245,21 +245,26 @@ def cpu_baseline(instances, budget_s):
 
 
 def one_thread_baseline(prepared, cores):
-    """The same port on one host thread, one mechanics period of one
-    (the smallest sampled) instance; the all-thread count is restored
-    afterwards."""
+    """The same port on one sample, one host thread against all of them:
+    one mechanics period of one (the smallest sampled) instance each way;
+    the all-thread count is restored afterwards."""
     import pyoracle as po
-    po.port_threads(1)
-    try:
-        t0 = time.perf_counter()
-        cpu_period([prepared])
-        secs = time.perf_counter() - t0
-    finally:
-        po.port_threads(cores)
     vox, cells = prepared[10], prepared[5]
-    return {"value": vox * SUB_STEPS / secs, "unit": "voxel-steps/s", "cores": 1,
-            "sample": f"one instance ({vox} voxels, {cells} cells), one mechanics period",
-            "cell_steps_per_s": cells / secs}
+    out = {}
+    for n_thr in (1, cores):
+        po.port_threads(n_thr)
+        try:
+            t0 = time.perf_counter()
+            cpu_period([prepared])
+            secs = time.perf_counter() - t0
+        finally:
+            po.port_threads(cores)
+        out[n_thr] = secs
+    sample = f"one instance ({vox} voxels, {cells} cells), one mechanics period"
+    return {"value": vox * SUB_STEPS / out[1], "unit": "voxel-steps/s", "cores": 1, "sample": sample,
+            "cell_steps_per_s": cells / out[1],
+            "all_threads_same_sample": {"value": vox * SUB_STEPS / out[cores], "cores": cores,
+                                        "cell_steps_per_s": cells / out[cores]}}
 
 
 def run_reference_arm(args, rank, world):
@@ -380,6 +385,8 @@ def main():
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-refresh", action="store_true",
+                    help="skip the leg with voxel indices refreshed after every mechanics step")
     ap.add_argument("--tune-cache", default=None, help="JSON file of autotuned launch shapes (read and updated)")
     ap.add_argument("--pin-x", type=int, default=0,
                     help="x-sweep launch shape warps*16 + stages instead of the tuned one")
@@ -462,6 +469,7 @@ def main():
     # is a plane pass (x + y planes, x-z planes; 8 bytes per voxel-substrate
     # each covers), else all the sweep launches together
     plane_units, all_units = batch.sweep_units()
+    launch_shapes = batch.describe()
     sweep_ms = (ph["x_sweep"] + ph["y_sweep"] + ph["z_sweep"]) / max(nst, 1)
     if plane_units and plane_units == all_units:
         kname = "k_sweep_planes (x+y plane pass and z plane pass)"
@@ -478,6 +486,24 @@ def main():
     traffic = None
     if tr and tr.get("plane_bytes_per_voxel_substrate") and plane_units:
         traffic = tr["plane_bytes_per_voxel_substrate"] * plane_units
+
+    # the same workload with voxel indices refreshed after every mechanics
+    # step (the secretion order is rebuilt inside the mechanics graph)
+    refresh = None
+    if not args.no_refresh:
+        batch.close()
+        rinsts = workloads.batched_3d(n_instances=args.instances * world, seed=1237, only=shard,
+                                      flags=pcg.INST_REFRESH_VOXELS)
+        rb = pcg.Batch(ctx, rinsts, tune_cache=args.tune_cache)
+        for _ in range(2):
+            rb.step(SUB_STEPS)
+        barrier(dist)
+        rk = max(3, args.steps // 2)
+        rsecs = dist_max(dist, local, time_steps(ctx, lambda: rb.step(SUB_STEPS), rk))
+        refresh = {"value": total_vox * SUB_STEPS * rk / rsecs, "unit": "voxel-steps/s",
+                   "cell_steps_per_s": total_cells * rk / rsecs, "ms_per_step": 1000 * rsecs / rk, "steps": rk}
+        rb.close()
+        batch = None
 
     plain_rate = None
     if not args.no_plain and rank == 0:
@@ -509,7 +535,7 @@ def main():
                                    f"step = 10 diffusion sub-steps + 1 mechanics step",
                        "voxels_per_gpu": voxels, "voxel_substrates_per_gpu": voxel_subs, "cells_per_gpu": cells,
                        "l2": f"inputs larger than L2 ({voxel_subs * 4 / 1e6:.0f} MB density per GPU)",
-                       "launch_shapes": batch.describe()},
+                       "launch_shapes": launch_shapes},
             "cell_steps_per_s": cell_rate, "voxel_substrate_steps_per_s": vox_sub_rate,
             "plain_voxel_steps_per_s": plain_rate,
             "batched_over_plain": (value / world / plain_rate) if plain_rate else None,
@@ -521,6 +547,7 @@ def main():
                          "sweeps": {"achieved": sweeps_gbs, "frac": sweeps_gbs / peak,
                                     "algorithmic_bytes_per_substep": 8 * all_units, "ms_per_substep": sweep_ms},
                          "phase_ms_per_substep": {k: v / max(nst, 1) for k, v in ph.items()}},
+            "refresh_voxels": refresh,
             "cpu_baseline": cpu,
             "serving": serving,
             "gpu_launches": launches,
@@ -529,7 +556,8 @@ def main():
         print(json.dumps(line), flush=True)
     for a in (soa_h, soa_out, dens_out):
         a.free()
-    batch.close()
+    if batch is not None:
+        batch.close()
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()

@@ -249,11 +249,13 @@ __global__ void k_cells_move(uint32_t* __restrict__ soa, uint32_t stride, const 
 // k_mech_bin finds each cell's voxel (FP32 divide, truncation and clamp,
 // as mechanics.metal:54-76) and counts it; the atomic's return value is the
 // cell's arrival slot in its voxel.  The exclusive scan of the counts is the
-// cell-start table.  k_mech_place drops each cell at start + slot, which
-// groups the voxel's cells in arrival order, and k_mech_order puts every
-// voxel's cells in ascending index (a cell's place is the voxel's start
-// plus the number of its cells with a lower index) -- the stable order --
-// and writes the sorted keys, the order and the sorted SoA there.
+// cell-start table.  k_mech_place drops each cell, with its x position, at
+// start + slot, which groups the voxel's cells in arrival order, and
+// k_mech_order ranks every cell in its voxel twice: by index (the stable
+// order of the cell-start table, sorder: syncHashPointers' voxelCells) and
+// by x position, index breaking ties (the force pass's order, forder, with
+// the sorted positions and strengths).  Bins grow with x, so the cells of a
+// run of voxels along x are in x order as a whole in the force order.
 __global__ void k_mech_bin(float* __restrict__ soa, uint32_t stride, uint32_t n, const uint32_t* __restrict__ cell_inst,
                            const CellInst* __restrict__ insts, uint32_t* __restrict__ keys,
                            uint32_t* __restrict__ slots, uint32_t* __restrict__ counts,
@@ -279,33 +281,50 @@ __global__ void k_mech_bin(float* __restrict__ soa, uint32_t stride, uint32_t n,
     slots[g] = atomicAdd(&counts[key], 1u);
 }
 
-__global__ void k_mech_place(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ slots,
-                             const uint32_t* __restrict__ start, uint32_t n, uint32_t* __restrict__ placed)
+// Order-preserving map of FP32 bit patterns to uint32 (negative values
+// reversed below the positive ones), so that every pattern has a place.
+__device__ __forceinline__ uint32_t x_order_key(float x)
+{
+    const uint32_t b = __float_as_uint(x);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__global__ void k_mech_place(const float* __restrict__ soa, uint32_t stride, const uint32_t* __restrict__ keys,
+                             const uint32_t* __restrict__ slots, const uint32_t* __restrict__ start, uint32_t n,
+                             uint2* __restrict__ placed)
 {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g < n) placed[start[keys[g]] + slots[g]] = g;
+    if (g >= n) return;
+    const float x = soa[static_cast<size_t>(F_POS_X) * stride + g];
+    placed[start[keys[g]] + slots[g]] = make_uint2(x_order_key(x), g);
 }
 
 __global__ void k_mech_order(const float* __restrict__ soa, uint32_t stride, const uint32_t* __restrict__ keys,
-                             const uint32_t* __restrict__ start, const uint32_t* __restrict__ placed, uint32_t n,
-                             uint32_t* __restrict__ skeys, uint32_t* __restrict__ sorder, float4* __restrict__ spos,
+                             const uint32_t* __restrict__ start, const uint2* __restrict__ placed, uint32_t n,
+                             uint32_t* __restrict__ sorder, uint32_t* __restrict__ forder, float4* __restrict__ spos,
                              float4* __restrict__ sprm)
 {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
     const uint32_t key = keys[g];
     const uint32_t s0 = start[key], s1 = start[key + 1];
-    uint32_t p = s0;
-    for (uint32_t q = s0; q < s1; ++q) p += placed[q] < g ? 1u : 0u;
-    skeys[p] = key;
-    sorder[p] = g;
-    spos[p] = make_float4(soa[static_cast<size_t>(F_POS_X) * stride + g], soa[static_cast<size_t>(F_POS_Y) * stride + g],
-                          soa[static_cast<size_t>(F_POS_Z) * stride + g], soa[static_cast<size_t>(F_RADIUS) * stride + g]);
+    const float x = soa[static_cast<size_t>(F_POS_X) * stride + g];
+    const uint32_t xk = x_order_key(x);
+    uint32_t pi = s0, px = s0;
+    for (uint32_t q = s0; q < s1; ++q) {
+        const uint2 o = placed[q];
+        pi += o.y < g ? 1u : 0u;
+        px += (o.x < xk || (o.x == xk && o.y < g)) ? 1u : 0u;
+    }
+    sorder[pi] = g;
+    forder[px] = g;
+    spos[px] = make_float4(x, soa[static_cast<size_t>(F_POS_Y) * stride + g], soa[static_cast<size_t>(F_POS_Z) * stride + g],
+                           soa[static_cast<size_t>(F_RADIUS) * stride + g]);
     // square roots of the (non-negative) strengths: the pair factors
     // sqrt(rep_i rep_j), sqrt(adh_i adh_j) become one product each
-    sprm[p] = make_float4(sqrtf(soa[static_cast<size_t>(F_REPULSION) * stride + g]),
-                          sqrtf(soa[static_cast<size_t>(F_ADHESION) * stride + g]),
-                          soa[static_cast<size_t>(F_REL_MAX_ADH) * stride + g], 0.0f);
+    sprm[px] = make_float4(sqrtf(soa[static_cast<size_t>(F_REPULSION) * stride + g]),
+                           sqrtf(soa[static_cast<size_t>(F_ADHESION) * stride + g]),
+                           soa[static_cast<size_t>(F_REL_MAX_ADH) * stride + g], 0.0f);
 }
 
 __device__ __forceinline__ uint32_t nbr_hash(uint32_t j)
@@ -353,14 +372,19 @@ __device__ __forceinline__ void pair_force(float ddx, float ddy, float ddz, floa
     fz += Fi * ddz;
 }
 
-// One thread per cell (sorted order p): candidates are visited in the
-// reference's order (dk, dj, di, then the voxel's cells in ascending index;
-// mechanics.metal:125-208) and summed sequentially.  The nine voxel rows'
-// ranges in the cell-start table are loaded up front; rows (and side voxels
-// of a row) that lie entirely beyond the interaction distance are skipped,
-// and the next candidate's position is loaded while the current one is
-// tested.  The neighbour test is the reference's FP32 one without
-// contraction (mechanics.metal:159-165), so neighbour sets are exact.
+// One thread per cell, cells in the force order p (by mechanics voxel,
+// then x; forder[p] = cell).  Candidates are the cells of the 3 x 3 (x 3)
+// voxels around the cell's own (mechanics.metal:125-208), visited row by
+// row (dk, then dj), each row of three voxels along x being one run of the
+// force order sorted by x.  A row whose slab lies beyond the interaction
+// distance in y / z is skipped; in the others only the candidates whose x
+// lies within sqrt(d^2 - g^2) (+ 0.05 um) of the cell's are tested, g the
+// row's y / z gap: the walk skips the lower end of the row and stops at the
+// first candidate past the upper bound.  Every candidate that can pass is
+// tested, with the reference's FP32 test without contraction
+// (mechanics.metal:159-165), so neighbour sets are exact (for finite
+// positions).  The next candidate's position is loaded while the current
+// one is tested; the force terms follow pair_force.
 //
 // QCAP == 0: the force terms are computed in the walk, where a lane meets
 // its neighbour.  QCAP > 0: the walk only tests; each lane keeps the
@@ -373,8 +397,7 @@ __device__ __forceinline__ void pair_force(float ddx, float ddy, float ddz, floa
 // where the direct form runs them whenever any lane of the warp has one.
 template <int QCAP, bool DIAG>
 __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ spos, const float4* __restrict__ sprm,
-                                                     const uint32_t* __restrict__ skeys,
-                                                     const uint32_t* __restrict__ sorder,
+                                                     const uint32_t* __restrict__ forder,
                                                      const uint32_t* __restrict__ start, uint32_t n,
                                                      const uint32_t* __restrict__ cell_inst,
                                                      const CellInst* __restrict__ insts, float* __restrict__ soa,
@@ -385,39 +408,39 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
     extern __shared__ uint32_t queue[];
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    const uint32_t g = sorder[p];
+    const uint32_t g = forder[p];
     const uint32_t ii = cell_inst[g];
     if (mask && !(mask[ii] & STEP_MECH)) return;
     const CellInst& in = insts[ii];
     const float4 me = spos[p];
     const float4 mp = sprm[p];
-    const uint32_t local = skeys[p] - in.mvox_base;
     const int mnx = static_cast<int>(in.mnx), mny = static_cast<int>(in.mny), mnz = static_cast<int>(in.mnz);
-    const int ci = static_cast<int>(local % in.mnx);
-    const int cj = static_cast<int>((local / in.mnx) % in.mny);
-    const int ck = static_cast<int>(local / (in.mnx * in.mny));
+    // the cell's voxel, from its position exactly as k_mech_bin binned it
+    const int ci = clampi(bin_of(me.x, in.mx_min, in.vs), 0, mnx - 1);
+    const int cj = clampi(bin_of(me.y, in.my_min, in.vs), 0, mny - 1);
+    const int ck = clampi(bin_of(me.z, in.mz_min, in.vs), 0, mnz - 1);
     const float vs = in.vs;
     const float maxd2 = __fmul_rn(in.maxd, in.maxd);
     const int ilo = ci > 0 ? ci - 1 : 0, ihi = ci + 1 < mnx ? ci + 1 : mnx - 1;
-    const float gxl = ci > 0 ? slab_gap(me.x, in.mx_min + (ci - 1) * vs, vs, ci - 1, mnx) : 0.f;
-    const float gxr = ci + 1 < mnx ? slab_gap(me.x, in.mx_min + (ci + 1) * vs, vs, ci + 1, mnx) : 0.f;
-    // row ranges [q0, q1) of the cell-start table, dk-major then dj
+    // row ranges [q0, q1) of the cell-start table, dk-major then dj, and
+    // each row's half-width of the x window (negative: row skipped)
     uint32_t rq0[9], rq1[9];
+    float rw[9];
 #pragma unroll
     for (int r = 0; r < 9; ++r) {
         const int dk = r / 3 - 1, dj = r % 3 - 1;
         const int nk = ck + dk, nj = cj + dj;
         rq0[r] = rq1[r] = 0;
+        rw[r] = -1.0f;
         if ((mnz == 1 && dk != 0) || nk < 0 || nk >= mnz || nj < 0 || nj >= mny) continue;
         const float gz = mnz > 1 ? slab_gap(me.z, in.mz_min + nk * vs, vs, nk, mnz) : 0.f;
         const float gy = slab_gap(me.y, in.my_min + nj * vs, vs, nj, mny);
         const float gyz = gy * gy + gz * gz;
         if (gyz >= maxd2) continue;   // the whole row is out of reach
-        const int i0 = (ilo < ci && gxl * gxl + gyz < maxd2) ? ilo : ci;
-        const int i1 = (ihi > ci && gxr * gxr + gyz < maxd2) ? ihi : ci;
         const uint32_t row = in.mvox_base + static_cast<uint32_t>(nk * mny + nj) * static_cast<uint32_t>(mnx);
-        rq0[r] = start[row + i0];
-        rq1[r] = start[row + i1 + 1];
+        rq0[r] = start[row + ilo];
+        rq1[r] = start[row + ihi + 1];
+        rw[r] = __fsqrt_rn(maxd2 - gyz) + 0.05f;
     }
     float fx = 0.f, fy = 0.f, fz = 0.f, P = 0.f;
     uint32_t cnt = 0, hsh = 0;
@@ -435,14 +458,18 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
         }
         nq = 0;
     };
+    const float* sx = reinterpret_cast<const float*>(spos);   // x of position q at sx[4 q]
 #pragma unroll
     for (int r = 0; r < 9; ++r) {
         uint32_t q = rq0[r];
         const uint32_t q1 = rq1[r];
+        const float xlo = me.x - rw[r], xhi = me.x + rw[r];
+        while (q < q1 && sx[4 * q] <= xlo) ++q;   // below the window
         float4 o = spos[q];   // q <= n: in bounds even for an empty row
         for (; q < q1; ++q) {
             const float4 cur = o;
             o = spos[q + 1];   // next candidate in flight (spos has one spare element)
+            if (cur.x >= xhi) break;   // this and every later candidate of the row lie past the window
             // neighbour test exactly as mechanics.metal:159-165 (no contraction);
             // the cell itself (q == p, distance 0) fails it like any coincident cell
             const float ddx = __fsub_rn(me.x, cur.x), ddy = __fsub_rn(me.y, cur.y), ddz = __fsub_rn(me.z, cur.z);
@@ -450,7 +477,7 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
             const bool nb = !(dsq >= maxd2 || dsq < 1e-12f);
             if (DIAG && nb) {
                 ++cnt;
-                hsh += nbr_hash(sorder[q] - in.cell_off);
+                hsh += nbr_hash(forder[q] - in.cell_off);
             }
             if (QCAP == 0) {
                 if (nb) pair_force(ddx, ddy, ddz, dsq, me.w, cur.w, mp, sprm[q], fx, fy, fz, P);
@@ -594,27 +621,28 @@ cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32
 }
 
 cudaError_t launch_mech_order(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* keys,
-                              const uint32_t* slots, const uint32_t* start, uint32_t n, uint32_t* placed,
-                              uint32_t* skeys, uint32_t* sorder, float4* spos, float4* sprm, int block)
+                              const uint32_t* slots, const uint32_t* start, uint32_t n, uint2* placed,
+                              uint32_t* sorder, uint32_t* forder, float4* spos, float4* sprm, int block)
 {
     if (n == 0) return cudaSuccess;
     if (block < 32 || block > 1024 || block % 32) return cudaErrorInvalidValue;
-    k_mech_place<<<blocks_for(n, block), block, 0, st>>>(keys, slots, start, n, placed);
+    k_mech_place<<<blocks_for(n, block), block, 0, st>>>(soa, stride, keys, slots, start, n, placed);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_mech_order<<<blocks_for(n, block), block, 0, st>>>(soa, stride, keys, start, placed, n, skeys, sorder, spos, sprm);
+    k_mech_order<<<blocks_for(n, block), block, 0, st>>>(soa, stride, keys, start, placed, n, sorder, forder, spos,
+                                                         sprm);
     return cudaGetLastError();
 }
 
 template <int QCAP, bool DIAG>
 static cudaError_t forces_variant(cudaStream_t st, unsigned grid, int block, const float4* spos, const float4* sprm,
-                                  const uint32_t* skeys, const uint32_t* sorder, const uint32_t* start, uint32_t n,
+                                  const uint32_t* forder, const uint32_t* start, uint32_t n,
                                   const uint32_t* cell_inst, const CellInst* insts, float* soa, uint32_t stride,
                                   uint32_t* diag_cnt, uint32_t* diag_hash, const uint8_t* mask)
 {
     const size_t smem = static_cast<size_t>(QCAP) * block * sizeof(uint32_t);   // at most 64 KiB
-    k_mech_forces<QCAP, DIAG><<<grid, block, smem, st>>>(spos, sprm, skeys, sorder, start, n, cell_inst, insts, soa,
-                                                         stride, diag_cnt, diag_hash, mask);
+    k_mech_forces<QCAP, DIAG><<<grid, block, smem, st>>>(spos, sprm, forder, start, n, cell_inst, insts, soa, stride,
+                                                         diag_cnt, diag_hash, mask);
     return cudaGetLastError();
 }
 
@@ -629,8 +657,8 @@ cudaError_t mech_forces_prepare()
     return cudaSuccess;
 }
 
-cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* skeys,
-                               const uint32_t* sorder, const uint32_t* start, uint32_t n, const uint32_t* cell_inst,
+cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* forder,
+                               const uint32_t* start, uint32_t n, const uint32_t* cell_inst,
                                const CellInst* insts, float* soa, uint32_t stride, uint32_t* diag_cnt,
                                uint32_t* diag_hash, const uint8_t* mask, ForceShape shape)
 {
@@ -639,10 +667,10 @@ cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4
     const unsigned grid = blocks_for(n, shape.block);
     const bool dg = diag_cnt != nullptr;
 #define PCG_FORCES(Q)                                                                                                \
-    return dg ? forces_variant<Q, true>(st, grid, shape.block, spos, sprm, skeys, sorder, start, n, cell_inst,      \
-                                        insts, soa, stride, diag_cnt, diag_hash, mask)                               \
-              : forces_variant<Q, false>(st, grid, shape.block, spos, sprm, skeys, sorder, start, n, cell_inst,     \
-                                         insts, soa, stride, diag_cnt, diag_hash, mask)
+    return dg ? forces_variant<Q, true>(st, grid, shape.block, spos, sprm, forder, start, n, cell_inst, insts, soa, \
+                                        stride, diag_cnt, diag_hash, mask)                                           \
+              : forces_variant<Q, false>(st, grid, shape.block, spos, sprm, forder, start, n, cell_inst, insts, soa,\
+                                         stride, diag_cnt, diag_hash, mask)
     switch (shape.queue) {
     case 0: PCG_FORCES(0);
     case 16: PCG_FORCES(16);

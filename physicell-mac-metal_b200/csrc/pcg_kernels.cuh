@@ -252,15 +252,16 @@ cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_sta
 // Mechanics binning as a counting sort: launch_mech_bin writes each cell's
 // global mechanics-voxel key, counts it (counts: V + 1 zeroed words) and
 // records its arrival slot; after the exclusive scan of the counts into
-// start, launch_mech_order (two launches; placed: n scratch words) writes
-// the stable order (skeys, sorder: cells by voxel, ascending index within
-// a voxel) and the sorted positions / radii and strengths.
+// start, launch_mech_order (two launches; placed: n scratch pairs) writes
+// the stable order (sorder: cells by voxel, ascending index within a voxel)
+// and the force order (forder: by voxel, then x, index breaking ties) with
+// the positions / radii and strengths in that order (spos, sprm).
 cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
                             const uint32_t* cell_inst, const CellInst* insts,
                             uint32_t* keys, uint32_t* slots, uint32_t* counts, const uint8_t* mask, int block = 256);
 cudaError_t launch_mech_order(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* keys,
-                              const uint32_t* slots, const uint32_t* start, uint32_t n, uint32_t* placed,
-                              uint32_t* skeys, uint32_t* sorder, float4* spos, float4* sprm, int block = 256);
+                              const uint32_t* slots, const uint32_t* start, uint32_t n, uint2* placed,
+                              uint32_t* sorder, uint32_t* forder, float4* spos, float4* sprm, int block = 256);
 // Launch shape of the force pass: threads per block (a multiple of 32, at
 // most 256) and the neighbour queue per thread (0 = force terms in the walk;
 // 16, 32 or 64 slots of shared memory).  Every shape gives the same bits.
@@ -271,8 +272,8 @@ struct ForceShape {
 // Lets the 64-slot queue variants use 64 KiB of shared memory (current
 // device; once per device, outside stream capture).
 cudaError_t mech_forces_prepare();
-cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* skeys,
-                               const uint32_t* sorder, const uint32_t* start, uint32_t n,
+cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* forder,
+                               const uint32_t* start, uint32_t n,
                                const uint32_t* cell_inst, const CellInst* insts, float* soa, uint32_t stride,
                                uint32_t* diag_cnt, uint32_t* diag_hash, const uint8_t* mask, ForceShape shape);
 // Copies of a removal plan: (dst, src) pairs, each cell's 28 SoA fields,

@@ -306,10 +306,11 @@ public:
     int int_block = 256;   // threads per block of the AB2 kernel
     bool diag = false;
     // binning: keys / slots (voxel key and arrival slot per cell), counts
-    // (per voxel, + 1), start (the cell-start table), placed (cells in
-    // arrival order per voxel), skeys / sorder (the stable order), spos /
-    // sprm (sorted SoA)
-    DevBuf keys, slots, placed, skeys, sorder, counts, start, scan_scr, spos, sprm, dcnt, dhash;
+    // (per voxel, + 1), start (the cell-start table), placed ((x key, cell)
+    // in arrival order per voxel), sorder (the stable order: by voxel, then
+    // index), forder (the force order: by voxel, then x) with spos / sprm
+    // (positions and strengths in the force order)
+    DevBuf keys, slots, placed, sorder, forder, counts, start, scan_scr, spos, sprm, dcnt, dhash;
 
     int create(pcg_ctx* c, uint32_t total_mvox, uint32_t max_cells);
     int forces(Cells& c, const uint8_t* mask);       // binsort + force_pass

@@ -123,11 +123,40 @@ __global__ void __launch_bounds__(kThreads) k_radix_scatter(const uint32_t* __re
 
 // ------------------------------------------------------------------ scan
 
+// Scans over more than one tile reduce, then scan: k_tile_sums writes every
+// tile's total, the totals are scanned (recursively), and k_scan_tiles
+// scans every tile once more, starting from its scanned total -- one read
+// pass and one read / write pass over the values.
+
+// Sum of one 2048-value tile per block.
+__global__ void __launch_bounds__(kThreads) k_tile_sums(const uint32_t* __restrict__ in, uint64_t n,
+                                                        uint32_t* __restrict__ sums)
+{
+    __shared__ uint32_t wsum[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kTile + static_cast<uint64_t>(threadIdx.x) * kItems;
+    uint32_t tot = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const uint64_t i = base + k;
+        tot += i < n ? in[i] : 0u;
+    }
+    tot = __reduce_add_sync(0xffffffffu, tot);
+    if (lane == 0) wsum[warp] = tot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) t += wsum[w];
+        sums[blockIdx.x] = t;
+    }
+}
+
 // Exclusive scan of one 2048-value tile per block (8 consecutive values per
-// thread, warp shuffles across lanes, shared memory across warps); writes
-// the tile total to sums[blockIdx.x] when sums != nullptr.
+// thread, warp shuffles across lanes, shared memory across warps), each
+// tile starting from offs[blockIdx.x] when offs != nullptr.
 __global__ void __launch_bounds__(kThreads) k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                                                         uint64_t n, uint32_t* __restrict__ sums)
+                                                         uint64_t n, const uint32_t* __restrict__ offs)
 {
     __shared__ uint32_t wsum[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -159,25 +188,13 @@ __global__ void __launch_bounds__(kThreads) k_scan_tiles(const uint32_t* __restr
             if (lane >= o) wi += y;
         }
         if (lane < kWarps) wsum[lane] = wi - w;
-        if (lane == kWarps - 1 && sums) sums[blockIdx.x] = wi;
     }
     __syncthreads();
-    const uint32_t pre = wsum[warp] + (incl - tot);
+    const uint32_t pre = wsum[warp] + (incl - tot) + (offs ? offs[blockIdx.x] : 0u);
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
         const uint64_t i = base + k;
         if (i < n) out[i] = v[k] + pre;
-    }
-}
-
-__global__ void __launch_bounds__(kThreads) k_scan_add(uint32_t* __restrict__ out, uint64_t n,
-                                                       const uint32_t* __restrict__ offs)
-{
-    const uint32_t add = offs[blockIdx.x];
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kTile;
-    for (int k = threadIdx.x; k < kTile; k += kThreads) {
-        const uint64_t i = base + k;
-        if (i < n) out[i] += add;
     }
 }
 
@@ -189,7 +206,7 @@ cudaError_t sort_kernels_load()
     // (lazy loading defers that to the first launch otherwise)
     cudaFuncAttributes a;
     const void* ks[] = {reinterpret_cast<const void*>(&k_radix_hist), reinterpret_cast<const void*>(&k_radix_scatter),
-                        reinterpret_cast<const void*>(&k_scan_tiles), reinterpret_cast<const void*>(&k_scan_add)};
+                        reinterpret_cast<const void*>(&k_scan_tiles), reinterpret_cast<const void*>(&k_tile_sums)};
     for (const void* k : ks) {
         const cudaError_t e = cudaFuncGetAttributes(&a, k);
         if (e != cudaSuccess) return e;
@@ -210,13 +227,8 @@ size_t scan_scratch_bytes(uint64_t n)
 
 int scan_launches(uint64_t n)
 {
-    int l = 1;
-    uint64_t m = tiles_of(n);
-    while (m > 1) {
-        l += 2;
-        m = tiles_of(m);
-    }
-    return l;
+    const uint64_t nt = tiles_of(n);
+    return nt <= 1 ? 1 : 2 + scan_launches(nt);
 }
 
 static cudaError_t scan_rec(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n, char* scratch)
@@ -229,12 +241,12 @@ static cudaError_t scan_rec(cudaStream_t st, const uint32_t* in, uint32_t* out, 
     }
     uint32_t* sums = reinterpret_cast<uint32_t*>(scratch);
     char* next = scratch + ((nt * sizeof(uint32_t) + 255) / 256) * 256;
-    k_scan_tiles<<<static_cast<unsigned>(nt), kThreads, 0, st>>>(in, out, n, sums);
+    k_tile_sums<<<static_cast<unsigned>(nt), kThreads, 0, st>>>(in, n, sums);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = scan_rec(st, sums, sums, nt, next);
     if (e != cudaSuccess) return e;
-    k_scan_add<<<static_cast<unsigned>(nt), kThreads, 0, st>>>(out, n, sums);
+    k_scan_tiles<<<static_cast<unsigned>(nt), kThreads, 0, st>>>(in, out, n, sums);
     return cudaGetLastError();
 }
 

@@ -175,9 +175,12 @@ def batched_3d_work(n_instances=64, seed=1237, min_cells=1_000, max_cells=100_00
     return out
 
 
-def batched_3d(n_instances=64, seed=1237, min_cells=1_000, max_cells=100_000, side_range=(40, 120), only=None):
+def batched_3d(n_instances=64, seed=1237, min_cells=1_000, max_cells=100_000, side_range=(40, 120), only=None,
+               flags=0):
     """The batched 3-D configuration; 'only' restricts it to the given
-    instance indices (a shard), each drawn exactly as in the full set."""
+    instance indices (a shard), each drawn exactly as in the full set.
+    flags: instance flags (INST_REFRESH_VOXELS: voxel indices recomputed
+    after every mechanics step, so the secretion order is rebuilt)."""
     out = []
     for i in (range(n_instances) if only is None else only):
         rng, side, drug_D, drug_lam, target, n = _batched_3d_spec(i, seed, min_cells, max_cells, side_range)
@@ -190,7 +193,7 @@ def batched_3d(n_instances=64, seed=1237, min_cells=1_000, max_cells=100_000, si
         adh = float(rng.uniform(0, 1))
         upt = np.stack([np.full(n, 10.0), rng.uniform(0, 2, n)], 1).ravel()
         out.append(instance(grid, subs, pos, radius, rep, adh, 1.25, sec=np.zeros(n * 2), upt=upt,
-                            sat=np.tile([38.0, 0.0], n), two_d=False))
+                            sat=np.tile([38.0, 0.0], n), two_d=False, flags=flags))
     return out
 
 

@@ -197,7 +197,7 @@ def gen_removal():
 
 if __name__ == "__main__":
     if not po.ref_available():
-        sys.exit("oracle/_ref/libpcg_ref.so not built (make -C oracle with the reference tree present)")
+        sys.exit("oracle/_ref/libpcg_ref.so not built (make -C oracle REF=<reference checkout>)")
     which = sys.argv[1:] or ["diffusion", "secretion", "mechanics", "motility", "matlab", "removal"]
     for w in which:
         globals()["gen_" + w]()
