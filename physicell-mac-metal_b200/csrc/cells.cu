@@ -464,7 +464,17 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
         uint32_t q = rq0[r];
         const uint32_t q1 = rq1[r];
         const float xlo = me.x - rw[r], xhi = me.x + rw[r];
-        while (q < q1 && sx[4 * q] <= xlo) ++q;   // below the window
+        // first candidate above the window's lower bound: a binary search
+        // over the row, the same number of steps for every lane
+        for (uint32_t len = q1 - q; len > 0;) {
+            const uint32_t half = len >> 1;
+            if (sx[4 * (q + half)] <= xlo) {
+                q += half + 1;
+                len -= half + 1;
+            } else {
+                len = half;
+            }
+        }
         float4 o = spos[q];   // q <= n: in bounds even for an empty row
         for (; q < q1; ++q) {
             const float4 cur = o;

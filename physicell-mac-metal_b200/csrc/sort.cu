@@ -152,26 +152,13 @@ __global__ void __launch_bounds__(kThreads) k_tile_sums(const uint32_t* __restri
     }
 }
 
-// Exclusive scan of one 2048-value tile per block (8 consecutive values per
-// thread, warp shuffles across lanes, shared memory across warps), each
-// tile starting from offs[blockIdx.x] when offs != nullptr.
-__global__ void __launch_bounds__(kThreads) k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                                                         uint64_t n, const uint32_t* __restrict__ offs)
+// Exclusive scan of 256 per-thread values across the block: returns the
+// sum of the values of the threads before this one; *total gets the sum of
+// all (wsum: kWarps + 1 shared words).
+__device__ __forceinline__ uint32_t block_exclusive(uint32_t x, uint32_t* wsum, uint32_t* total)
 {
-    __shared__ uint32_t wsum[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kTile + static_cast<uint64_t>(threadIdx.x) * kItems;
-    uint32_t v[kItems];
-    uint32_t tot = 0;
-#pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-        const uint64_t i = base + k;
-        v[k] = i < n ? in[i] : 0u;
-        const uint32_t x = v[k];
-        v[k] = tot;
-        tot += x;
-    }
-    uint32_t incl = tot;
+    uint32_t incl = x;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
@@ -180,7 +167,7 @@ __global__ void __launch_bounds__(kThreads) k_scan_tiles(const uint32_t* __restr
     if (lane == 31) wsum[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = lane < kWarps ? wsum[lane] : 0u;
+        const uint32_t w = lane < kWarps ? wsum[lane] : 0u;
         uint32_t wi = w;
 #pragma unroll
         for (int o = 1; o < kWarps; o <<= 1) {
@@ -188,13 +175,56 @@ __global__ void __launch_bounds__(kThreads) k_scan_tiles(const uint32_t* __restr
             if (lane >= o) wi += y;
         }
         if (lane < kWarps) wsum[lane] = wi - w;
+        if (lane == kWarps - 1) wsum[kWarps] = wi;
     }
     __syncthreads();
-    const uint32_t pre = wsum[warp] + (incl - tot) + (offs ? offs[blockIdx.x] : 0u);
+    const uint32_t before = wsum[warp] + (incl - x);
+    *total = wsum[kWarps];
+    __syncthreads();   // wsum is reused by the next call
+    return before;
+}
+
+// Exclusive scan of one 2048-value tile per block, each tile starting from
+// offs[blockIdx.x] when offs != nullptr.  The tile is two halves of 1024
+// values; in each, thread t owns values 4t .. 4t + 3, moved as one 16-byte
+// access when the tile is whole and the arrays 16-byte aligned, so that a
+// warp's loads and stores are contiguous.
+__global__ void __launch_bounds__(kThreads) k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                         uint64_t n, const uint32_t* __restrict__ offs)
+{
+    static_assert(kTile == 2 * 4 * kThreads, "two halves of four values per thread");
+    __shared__ uint32_t wsum[kWarps + 1];
+    const uint64_t tile = static_cast<uint64_t>(blockIdx.x) * kTile;
+    const bool vec = tile + kTile <= n && ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0;
+    uint32_t run = offs ? offs[blockIdx.x] : 0u;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-        const uint64_t i = base + k;
-        if (i < n) out[i] = v[k] + pre;
+    for (int h = 0; h < 2; ++h) {
+        const uint64_t i0 = tile + static_cast<uint64_t>(h) * (kTile / 2) + 4ull * threadIdx.x;
+        uint32_t v[4];
+        if (vec) {
+            const uint4 q = *reinterpret_cast<const uint4*>(in + i0);
+            v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[k] = i0 + k < n ? in[i0 + k] : 0u;
+        }
+        uint32_t tot = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t x = v[k];
+            v[k] = tot;
+            tot += x;
+        }
+        uint32_t half_total = 0;
+        const uint32_t pre = run + block_exclusive(tot, wsum, &half_total);
+        if (vec) {
+            *reinterpret_cast<uint4*>(out + i0) = make_uint4(v[0] + pre, v[1] + pre, v[2] + pre, v[3] + pre);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (i0 + k < n) out[i0 + k] = v[k] + pre;
+        }
+        run += half_total;
     }
 }
 
