@@ -510,24 +510,41 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
 
 // Plane jobs grouped by shared-memory size, so small planes are not charged
 // the largest plane's footprint; largest planes first.
-static int plane_lists(pcg_ctx* ctx, std::vector<PlaneJob>* jobs, const uint32_t* fl, const uint64_t* un,
-                       int classes, std::vector<PlaneList>& out)
+// Plane lists from per-class jobs: runs of 'merge' consecutive non-empty
+// classes (0: all of them) become one list, launched with the largest
+// plane's shared memory.
+static int plane_lists(pcg_ctx* ctx, const std::vector<PlaneJob>* jobs, const uint32_t* fl, const uint64_t* un,
+                       int classes, int merge, std::vector<PlaneList>& out)
 {
-    int nl = 0;
-    for (int c = 0; c < classes; ++c) nl += jobs[c].empty() ? 0 : 1;
+    std::vector<int> used;
+    for (int c = classes - 1; c >= 0; --c)
+        if (!jobs[c].empty()) used.push_back(c);
+    const size_t per = merge <= 0 ? std::max<size_t>(used.size(), 1) : static_cast<size_t>(merge);
     out.clear();
-    out.resize(nl);
-    int q = 0;
-    for (int c = classes - 1; c >= 0; --c) {
-        if (jobs[c].empty()) continue;
-        PlaneList& pl = out[q++];
-        pl.n = static_cast<uint32_t>(jobs[c].size());
-        pl.floats = fl[c];
-        pl.units = un[c];
-        PCG_CU(ctx, pl.jobs.alloc(jobs[c].size() * sizeof(PlaneJob)));
-        PCG_CU(ctx, cudaMemcpyAsync(pl.jobs.p, jobs[c].data(), jobs[c].size() * sizeof(PlaneJob),
-                                    cudaMemcpyHostToDevice, ctx->stream));
+    out.resize((used.size() + per - 1) / per);
+    for (size_t q = 0; q < out.size(); ++q) {
+        PlaneList& pl = out[q];
+        std::vector<PlaneJob> all;
+        for (size_t k = q * per; k < std::min(used.size(), (q + 1) * per); ++k) {
+            const int c = used[k];
+            all.insert(all.end(), jobs[c].begin(), jobs[c].end());
+            pl.floats = std::max(pl.floats, fl[c]);
+            pl.units += un[c];
+        }
+        pl.n = static_cast<uint32_t>(all.size());
+        PCG_CU(ctx, pl.jobs.alloc(all.size() * sizeof(PlaneJob)));
+        PCG_CU(ctx, cudaMemcpyAsync(pl.jobs.p, all.data(), all.size() * sizeof(PlaneJob), cudaMemcpyHostToDevice,
+                                    ctx->stream));
     }
+    if (!out.empty()) PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));   // the host vectors go
+    return PCG_OK;
+}
+
+int Diffusion::regroup_planes(int merge)
+{
+    plane_merge = merge;
+    PCG_TRY(plane_lists(ctx, cls_jobs_[0], cls_floats_[0], cls_units_[0], kPlaneClasses, merge, planes));
+    PCG_TRY(plane_lists(ctx, cls_jobs_[1], cls_floats_[1], cls_units_[1], kPlaneClasses, merge, zplanes));
     return PCG_OK;
 }
 
@@ -546,11 +563,20 @@ int Diffusion::build_planes()
     // (class kMaxCtas - k for k CTAs), so each plane runs at the occupancy
     // its own size allows; a class launches with its largest plane's size,
     // which by construction allows the same k.
-    constexpr int kMaxCtas = 32, kClasses = kMaxCtas;
+    constexpr int kMaxCtas = kPlaneClasses;
     auto cls = [&](uint32_t pf) { return kMaxCtas - std::min(std::max(sweep_planes_ctas(pf), 1), kMaxCtas); };
-    std::vector<PlaneJob> jobs[kClasses], zjobs[kClasses];
-    uint32_t fl[kClasses] = {}, zfl[kClasses] = {};
-    uint64_t un[kClasses] = {}, zun[kClasses] = {};
+    std::vector<PlaneJob>* jobs = cls_jobs_[0];
+    std::vector<PlaneJob>* zjobs = cls_jobs_[1];
+    uint32_t* fl = cls_floats_[0];
+    uint32_t* zfl = cls_floats_[1];
+    uint64_t* un = cls_units_[0];
+    uint64_t* zun = cls_units_[1];
+    for (int c = 0; c < kPlaneClasses; ++c) {
+        jobs[c].clear();
+        zjobs[c].clear();
+        fl[c] = zfl[c] = 0;
+        un[c] = zun[c] = 0;
+    }
     for (size_t i = 0; i < inst.size(); ++i) {
         const DiffInstance& d = inst[i];
         const uint32_t nx = d.g.nx, ny = d.g.ny, nz = d.g.nz;
@@ -605,8 +631,7 @@ int Diffusion::build_planes()
             zun[c] += d.nvox() * d.g.n_substrates;
         }
     }
-    PCG_TRY(plane_lists(ctx, jobs, fl, un, kClasses, planes));
-    PCG_TRY(plane_lists(ctx, zjobs, zfl, zun, kClasses, zplanes));
+    PCG_TRY(regroup_planes(plane_merge));
     for (int a = 0; a < 3; ++a) {
         if (!planes_for(a)) continue;
         PCG_TRY(build_axis(a, a < 2 ? &plane_inst_ : &zplane_inst_, rest[a]));
@@ -1019,6 +1044,7 @@ std::string Diffusion::describe() const
 {
     std::ostringstream o;
     const char* ax = "xyz";
+    if (!planes.empty() || !zplanes.empty()) o << "plane-classes-per-launch=" << (plane_merge == 0 ? std::string("all") : std::to_string(plane_merge)) << " ";
     for (const auto& pl : planes) o << "xy:planes(jobs=" << pl.n << ",smem=" << sweep_planes_smem(pl.floats) << ") ";
     for (const auto& pl : zplanes) o << "z:xz-planes(jobs=" << pl.n << ",smem=" << sweep_planes_smem(pl.floats) << ") ";
     for (int a = 0; a < 3; ++a)
@@ -1093,6 +1119,47 @@ int Diffusion::tune()
             Tuner::get().store(key, best);
         }
         rc = config_list(l, best);
+    }
+    // plane launches: one per occupancy class (parallel graph branches) or
+    // runs of classes merged into fewer, larger launches
+    if (rc == PCG_OK && (!planes.empty() || !zplanes.empty())) {
+        int ncls[2] = {0, 0};
+        uint64_t njobs = 0;
+        for (int p = 0; p < 2; ++p)
+            for (int c = 0; c < kPlaneClasses; ++c) {
+                ncls[p] += cls_jobs_[p][c].empty() ? 0 : 1;
+                njobs += cls_jobs_[p][c].size();
+            }
+        const std::string key = "planes:x" + std::to_string(ncls[0]) + ":z" + std::to_string(ncls[1]) + ":j" +
+                                std::to_string(bucket(njobs));
+        int best = 1;
+        if (!Tuner::get().lookup(key, &best)) {
+            float best_ms = 1e30f;
+            auto passes = [&]() -> int {
+                PCG_TRY(launch_planes(planes, false, nullptr));
+                return launch_planes(zplanes, false, nullptr);
+            };
+            for (int m : {1, 2, 3, 0}) {
+                rc = regroup_planes(m);
+                if (rc != PCG_OK) break;
+                rc = passes();   // warm
+                if (rc != PCG_OK) break;
+                cudaError_t ce = cudaEventRecord(e0, ctx->stream);
+                for (int r = 0; r < 3 && rc == PCG_OK && ce == cudaSuccess; ++r) rc = passes();
+                if (ce == cudaSuccess) ce = cudaEventRecord(e1, ctx->stream);
+                if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+                float ms = 0;
+                if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+                if (ce != cudaSuccess) rc = cuda_fail(ctx, ce, "plane grouping timing");
+                if (rc != PCG_OK) break;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = m;
+                }
+            }
+            if (rc == PCG_OK) Tuner::get().store(key, best);
+        }
+        if (rc == PCG_OK) rc = regroup_planes(best);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

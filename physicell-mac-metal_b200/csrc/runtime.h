@@ -216,6 +216,11 @@ public:
     int download(uint32_t i, float* host, bool async_pinned = false);
     int fill(uint32_t i, const float* values);
     int launches_per_step(bool three_d_only = false) const;
+    // Plane launches: runs of 'merge' consecutive occupancy classes share
+    // one launch (at the largest plane's shared memory); 1 = one launch per
+    // class, 0 = one launch per pass.  Chosen by tune() unless pinned.
+    int plane_merge = 1;
+    int regroup_planes(int merge);
     // Voxel-substrates the sweep launches of one sub-step cover, summed over
     // launches (each moves 8 bytes per unit: one read, one write).
     uint64_t sweep_units_per_step() const;
@@ -225,6 +230,12 @@ public:
 private:
     int build_axis(int axis, const std::vector<uint8_t>* skip, std::vector<SweepList>& ls);
     int build_planes();
+    // plane jobs per occupancy class (class kPlaneClasses - k: k CTAs per
+    // SM), their largest plane and the voxel-substrates they cover
+    static constexpr int kPlaneClasses = 32;
+    std::vector<PlaneJob> cls_jobs_[2][kPlaneClasses];
+    uint32_t cls_floats_[2][kPlaneClasses] = {};
+    uint64_t cls_units_[2][kPlaneClasses] = {};
     std::vector<uint8_t> plane_inst_;    // instance's x + y sweeps run as planes
     std::vector<uint8_t> zplane_inst_;   // instance's z sweep runs as x-z planes
     int launch_planes(const std::vector<PlaneList>& pls, bool fuse_faces, const uint8_t* mask);
