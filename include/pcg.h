@@ -301,8 +301,9 @@ pcg_status pcg_snapshot_cells(pcg_snapshot* snap, const pcg_cells* cells, uint32
 pcg_status pcg_snapshot_frame(pcg_snapshot* snap, const pcg_me* me, const pcg_cells* cells, uint32_t n_cell_types,
                               const char* folder, int frame);
 
-/* No reference counterpart.  The stable (key, value) radix sort that bins
- * cells by mechanics voxel, run on caller-owned DEVICE buffers and making
+/* No reference counterpart.  A stable (key, value) radix sort -- sorting
+ * mechanics-voxel keys with cell indices as values gives the cell order of
+ * the mechanics binning -- run on caller-owned DEVICE buffers and making
  * no device allocation: all scratch lives in one fixed 2.5 MiB array
  * compiled into the library.  For callers that cannot allocate device
  * memory at the point of the call (a server that partitioned the device up

@@ -1,5 +1,6 @@
-// noalloc.cu — pcg_sort_pairs_static: the stable radix sort of the
-// mechanics binning, run on caller-owned device buffers with every piece of
+// noalloc.cu — pcg_sort_pairs_static: a stable radix sort of (key, value)
+// pairs (mechanics-voxel keys with cell indices give the mechanics
+// binning's cell order), run on caller-owned device buffers with every piece of
 // scratch taken from one fixed file-scope device array, so that the call
 // makes no device allocation of any kind (no cudaMalloc / cudaFree, no
 // allocating library).
