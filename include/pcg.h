@@ -48,11 +48,20 @@ typedef struct {
     float x_min, y_min, z_min, _pad0;
 } pcg_grid_params;
 
-/* Same layout as SubstrateParams (shaders/types.h:40-48). */
+/* Same layout as SubstrateParams (shaders/types.h:40-48); the first pad
+ * word of the reference's struct holds an option the reference does not
+ * have (0 there, the reference's behaviour):
+ *   dirichlet_consistent != 0: on Dirichlet lines the first and last
+ *   interior nodes use the interior diagonal 1 + 2c + hd rather than the
+ *   reference's 1 + c + hd (diffusion_2d.metal:47-48, 90-142), keeping the
+ *   c T coupling to the boundary value, so that a uniform field at the
+ *   target stays there.  The reference's rule (both the boundary diagonal
+ *   and the coupling) is the default, for parity. */
 typedef struct {
     float diffusion_coefficient, decay_rate, supply_rate, target_value;
     uint32_t dirichlet_enabled;
-    float _pad[3];
+    uint32_t dirichlet_consistent;
+    float _pad[2];
 } pcg_substrate_params;
 
 /* Same layout as MechanicsParams (shaders/types.h:51-61). */

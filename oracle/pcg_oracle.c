@@ -18,10 +18,12 @@
 /* Line solve in double, following diffusion_2d.metal:55-155 (x sweep; the y
  * sweep :196-290 is the same rule along another axis).  v holds the n values
  * of the line; cp is scratch of n doubles. */
-static void solve_line_f64(double* v, double* cp, int n, double c, double hd, int dir, double T)
+static void solve_line_f64(double* v, double* cp, int n, double c, double hd, int dir, double T, int consistent)
 {
     const double b_int = 1.0 + 2.0 * c + hd;   /* :47 */
-    const double b_bnd = 1.0 + c + hd;         /* :48 */
+    /* :48; the consistent Dirichlet option gives the end interior nodes of a
+     * Dirichlet line the interior diagonal */
+    const double b_bnd = (dir && consistent) ? b_int : 1.0 + c + hd;
     if (dir) { v[0] = T; v[n - 1] = T; }       /* :55-58 */
     if (n <= 2) return;                        /* :60-63 */
     if (n == 3) {                              /* :66-84: b_int, both folds */
@@ -145,7 +147,8 @@ void or_sweep_axis(float* density, const or_grid* g, const or_substrate* subs, i
                     for (size_t m = 0; m < n; m++) line[m * stride] = vf[m];
                 } else {
                     for (size_t m = 0; m < n; m++) vd[m] = (double)line[m * stride];
-                    solve_line_f64(vd, cd, (int)n, c64, hd64, dir, (double)sp->target_value);
+                    solve_line_f64(vd, cd, (int)n, c64, hd64, dir, (double)sp->target_value,
+                                   sp->dirichlet_consistent != 0);
                     for (size_t m = 0; m < n; m++) line[m * stride] = (float)vd[m];
                 }
             }

@@ -55,10 +55,14 @@ typedef struct {
     float x_min, y_min, z_min, _pad0;
 } or_grid;
 
+/* dirichlet_consistent (the library's option, not the reference's): on
+ * Dirichlet lines the end interior nodes take the interior diagonal
+ * 1 + 2c + hd instead of 1 + c + hd (OR_FP64 only). */
 typedef struct {
     float diffusion_coefficient, decay_rate, supply_rate, target_value;
     uint32_t dirichlet_enabled;
-    float _pad[3];
+    uint32_t dirichlet_consistent;
+    float _pad[2];
 } or_substrate;
 
 typedef struct {

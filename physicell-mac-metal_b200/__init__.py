@@ -58,7 +58,8 @@ class SubstrateParams(C.Structure):
     """SubstrateParams (shaders/types.h:40-48)."""
     _fields_ = [("diffusion_coefficient", C.c_float), ("decay_rate", C.c_float),
                 ("supply_rate", C.c_float), ("target_value", C.c_float),
-                ("dirichlet_enabled", C.c_uint32), ("_pad", C.c_float * 3)]
+                ("dirichlet_enabled", C.c_uint32), ("dirichlet_consistent", C.c_uint32),
+                ("_pad", C.c_float * 2)]
 
 
 class MechanicsParams(C.Structure):
@@ -255,10 +256,13 @@ def make_grid(nx, ny, nz, S, dx=20.0, dt=0.01, x_min=0.0, y_min=0.0, z_min=0.0, 
 
 
 def make_substrates(params):
-    """params: iterable of (D, decay, dirichlet_enabled, target)."""
+    """params: iterable of (D, decay, dirichlet_enabled, target[, consistent]);
+    consistent: the consistent Dirichlet option (pcg_substrate_params)."""
     params = list(params)
     arr = (SubstrateParams * max(1, len(params)))()
-    for s, (D, lam, dirichlet, T) in enumerate(params):
+    for s, p in enumerate(params):
+        D, lam, dirichlet, T = p[:4]
+        arr[s].dirichlet_consistent = 1 if len(p) > 4 and p[4] else 0
         arr[s].diffusion_coefficient = D
         arr[s].decay_rate = lam
         arr[s].supply_rate = 0.0

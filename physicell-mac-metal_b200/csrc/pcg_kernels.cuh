@@ -265,9 +265,10 @@ cudaError_t launch_mech_order(cudaStream_t st, const float* soa, uint32_t stride
 // Launch shape of the force pass: threads per block (a multiple of 32, at
 // most 256) and the neighbour queue per thread (0 = force terms in the walk;
 // 16, 32 or 64 slots of shared memory).  Every shape gives the same bits.
+// The default is the shape the tuner chooses on the batched 3-D workload.
 struct ForceShape {
-    int block = 256;
-    int queue = 32;
+    int block = 128;
+    int queue = 0;
 };
 // Lets the 64-slot queue variants use 64 KiB of shared memory (current
 // device; once per device, outside stream capture).

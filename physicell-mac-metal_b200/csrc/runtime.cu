@@ -393,7 +393,11 @@ int Diffusion::build(pcg_ctx* c, std::vector<DiffInstance> instances)
                     tb[(i / 4) * 8 + i % 4] = static_cast<float>(g);
                     tb[(i / 4) * 8 + 4 + i % 4] = static_cast<float>(inv);
                 };
-                const double b_int = 1.0 + 2.0 * cc + hd, b_bnd = 1.0 + cc + hd;
+                // the end interior nodes' diagonal: the reference's 1 + c + hd
+                // (diffusion_2d.metal:48), or with the consistent Dirichlet
+                // option the interior one on Dirichlet lines
+                const double b_int = 1.0 + 2.0 * cc + hd;
+                const double b_bnd = (dir && sp.dirichlet_consistent) ? b_int : 1.0 + cc + hd;
                 if (n == 3) {
                     put(1, 0.0, 1.0 / b_int);
                     r.fold = dir ? static_cast<float>(2.0 * cc * T) : 0.f;

@@ -161,3 +161,34 @@ def test_size_mismatch_is_an_error(ctx, pcg):
     me = pcg.Microenvironment(ctx, g, pcg.make_substrates([O2]))
     with pytest.raises(pcg.PcgError):
         me.setDensityAll(np.zeros(10, np.float32))
+
+
+@pytest.mark.parametrize("shape", [(50, 50, 1), (41, 37, 23), (150, 150, 1)], ids=["2d", "3d", "2d_150"])
+def test_consistent_dirichlet_matches_oracle(ctx, pcg, po, shape):
+    """The consistent Dirichlet option on the device against the oracle's,
+    on a field with structure; and a uniform field at the target stays
+    there (no decay)."""
+    nx, ny, nz = shape
+    rng = np.random.default_rng(nx + ny + nz)
+    params = [(1e5, 0.1, True, 38.0, True), (3e3, 0.3, True, 5.0, True), (2e4, 0.0, False, 0.0, True)]
+    g = pcg.make_grid(nx, ny, nz, 3, dx=20.0, dt=0.01)
+    me = pcg.Microenvironment(ctx, g, pcg.make_substrates(params))
+    d0 = rng.uniform(0, 40, 3 * nx * ny * nz).astype(np.float32)
+    me.setDensityAll(d0)
+    me.step(None, 5)
+    og = po.make_grid(nx, ny, nz, 3, dx=20.0, dt=0.01)
+    osubs = po.make_subs(params)
+    ref = d0.copy()
+    for _ in range(5):
+        po.sweeps(ref, og, osubs)
+        po.dirichlet(ref, og, osubs)
+    assert rel_err(me.densityBuffer(), ref) <= 1e-5
+    flat = [(1e5, 0.0, True, 38.0, True)]
+    g1 = pcg.make_grid(nx, ny, nz, 1, dx=20.0, dt=0.01)
+    m1 = pcg.Microenvironment(ctx, g1, pcg.make_substrates(flat))
+    m1.fill([38.0])
+    m1.step(None, 20)
+    assert np.abs(m1.densityBuffer().astype(np.float64) - 38.0).max() <= 1e-4
+    me.close()
+    m1.close()
+

@@ -221,6 +221,36 @@ def test_dirichlet_quirk_uniform_target_not_stationary(po):
     assert z["density_steps"][-1].max() > 38.5
 
 
+@pytest.mark.parametrize("shape", [(40, 30, 1), (17, 9, 11)], ids=["2d", "3d"])
+def test_consistent_dirichlet_keeps_uniform_target(po, shape):
+    """The library's consistent Dirichlet option (not the reference's rule):
+    with no decay a uniform field at the target stays there, where the
+    reference's rule moves it; away from the boundary lines both agree on a
+    field that only varies inside."""
+    nx, ny, nz = shape
+    g = po.make_grid(nx, ny, nz, 1, dx=20.0, dt=0.01)
+    ref = po.make_subs([(1e5, 0.0, True, 38.0)])
+    cons = po.make_subs([(1e5, 0.0, True, 38.0, True)])
+    a = np.full(nx * ny * nz, 38.0, np.float32)
+    b = a.copy()
+    for _ in range(20):
+        po.sweeps(a, g, cons)
+        po.dirichlet(a, g, cons)
+        po.sweeps(b, g, ref)
+        po.dirichlet(b, g, ref)
+    assert np.abs(a.astype(np.float64) - 38.0).max() <= 1e-4
+    assert b.max() > 38.5
+    # without Dirichlet lines the option changes nothing
+    nd_ref = po.make_subs([(1e5, 0.1, False, 0.0)])
+    nd_cons = po.make_subs([(1e5, 0.1, False, 0.0, True)])
+    rng = np.random.default_rng(3)
+    c = rng.uniform(0, 40, nx * ny * nz).astype(np.float32)
+    d = c.copy()
+    po.sweeps(c, g, nd_ref)
+    po.sweeps(d, g, nd_cons)
+    assert np.array_equal(c, d)
+
+
 def test_gradients_central_and_one_sided(po):
     g = po.make_grid(5, 4, 3, 1, dx=20.0, dt=0.01)
     x = np.arange(5, dtype=np.float32)
