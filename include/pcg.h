@@ -419,6 +419,18 @@ pcg_status pcg_batch_download_positions64(pcg_batch* batch, uint32_t instance, d
 pcg_status pcg_batch_upload_all_cells(pcg_batch* batch, const float* soa, uint64_t n_floats);
 pcg_status pcg_batch_download_all_cells(pcg_batch* batch, float* soa, uint64_t n_floats);
 pcg_status pcg_batch_download_all_density(pcg_batch* batch, float* host, uint64_t n_floats);
+/* pcg_batch_download_all_cells for the fields whose bit is set in
+ * field_mask (bit f = field f), into the same places of the host SoA; the
+ * other fields of the host SoA are left as they are.  A main loop whose host
+ * keeps the fields only it writes (radius, volumes, phenotype, ...) reads
+ * back PCG_STEP_WRITTEN_FIELDS: what the sub-steps and mechanics steps
+ * change. */
+#define PCG_STEP_WRITTEN_FIELDS                                                                   \
+    ((1u << PCG_F_POS_X) | (1u << PCG_F_POS_Y) | (1u << PCG_F_POS_Z) | (1u << PCG_F_VEL_X) |      \
+     (1u << PCG_F_VEL_Y) | (1u << PCG_F_VEL_Z) | (1u << PCG_F_PREV_VX) | (1u << PCG_F_PREV_VY) |  \
+     (1u << PCG_F_PREV_VZ) | (1u << PCG_F_PRESSURE) | (1u << PCG_F_VOXEL_IDX) |                   \
+     (1u << PCG_F_MECH_VOXEL))
+pcg_status pcg_batch_download_cell_fields(pcg_batch* batch, float* soa, uint64_t n_floats, uint32_t field_mask);
 pcg_status pcg_batch_density_layout(pcg_batch* batch, uint32_t instance, uint64_t* offset, uint64_t* row_pitch,
                                     uint64_t* substrate_pitch, uint64_t* arena_floats);
 /* Totals: voxels (sum nx*ny*nz), voxel-substrates, cells. */

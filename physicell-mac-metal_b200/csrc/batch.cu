@@ -627,6 +627,56 @@ pcg_status pcg_batch_download_all_cells(pcg_batch* b, float* soa, uint64_t n_flo
                            NUM_FIELDS);
 }
 
+pcg_status pcg_batch_download_cell_fields(pcg_batch* b, float* soa, uint64_t n_floats, uint32_t field_mask)
+{
+    if (!b || !soa) return PCG_ERR_INVALID;
+    Batch& B = b->b;
+    Cells& c = B.c_;
+    pcg_ctx* ctx = B.ctx;
+    if (n_floats != static_cast<uint64_t>(NUM_FIELDS) * c.n) return fail(ctx, PCG_ERR_INVALID, "size mismatch");
+    if (field_mask >> NUM_FIELDS) return fail(ctx, PCG_ERR_INVALID, "field mask names a field past the 28");
+    if (c.n == 0 || field_mask == 0) return PCG_OK;
+    // runs of consecutive fields: device -> staging (packed) on the context
+    // stream, staging -> each run's place in the host SoA on the copy stream
+    std::vector<std::pair<uint32_t, uint32_t>> runs;
+    for (uint32_t f = 0; f < static_cast<uint32_t>(NUM_FIELDS);) {
+        if (!(field_mask >> f & 1u)) {
+            ++f;
+            continue;
+        }
+        uint32_t e = f;
+        while (e < static_cast<uint32_t>(NUM_FIELDS) && (field_mask >> e & 1u)) ++e;
+        runs.emplace_back(f, e);
+        f = e;
+    }
+    const size_t row = static_cast<size_t>(c.n) * sizeof(float);
+    const size_t nsel = static_cast<size_t>(__builtin_popcount(field_mask));
+    PCG_TRY(ensure_copy_streams(ctx));
+    PCG_TRY(ensure_stage(ctx, B.stage_cells, row * nsel));
+    PCG_TRY(ensure_event(ctx, &B.ev_cells_ready));
+    PCG_TRY(ensure_event(ctx, &B.ev_cells_done));
+    PCG_CU(ctx, cudaStreamWaitEvent(ctx->stream, B.ev_cells_done, 0));
+    size_t at = 0;
+    for (const auto& r : runs) {
+        PCG_CU(ctx, cudaMemcpy2DAsync(static_cast<char*>(B.stage_cells.p) + at * row, row,
+                                      c.soa.as<float>() + static_cast<size_t>(r.first) * c.max_cells,
+                                      static_cast<size_t>(c.max_cells) * sizeof(float), row, r.second - r.first,
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+        at += r.second - r.first;
+    }
+    PCG_CU(ctx, cudaEventRecord(B.ev_cells_ready, ctx->stream));
+    PCG_CU(ctx, cudaStreamWaitEvent(ctx->d2h, B.ev_cells_ready, 0));
+    at = 0;
+    for (const auto& r : runs) {
+        PCG_CU(ctx, cudaMemcpyAsync(soa + static_cast<size_t>(r.first) * c.n,
+                                    static_cast<char*>(B.stage_cells.p) + at * row, (r.second - r.first) * row,
+                                    cudaMemcpyDeviceToHost, ctx->d2h));
+        at += r.second - r.first;
+    }
+    PCG_CU(ctx, cudaEventRecord(B.ev_cells_done, ctx->d2h));
+    return PCG_OK;
+}
+
 pcg_status pcg_batch_download_all_density(pcg_batch* b, float* host, uint64_t n_floats)
 {
     if (!b || !host) return PCG_ERR_INVALID;

@@ -137,6 +137,43 @@ def test_whole_batch_transfers_pipelined(ctx, pcg):
         assert np.array_equal(da.view(np.uint32), db.view(np.uint32)), f"density round {k}"
 
 
+def test_masked_cell_download(ctx, pcg):
+    """pcg_batch_download_cell_fields: the fields in the mask come back as the
+    full download gives them, every other field of the host SoA is left as
+    it was; with the steps' field set, a host that keeps the other fields
+    holds the whole state."""
+    insts = small_mix(pcg, seed=14)
+    n_tot = sum(i.n_cells for i in insts)
+    b = pcg.Batch(ctx, insts)
+    b.step(13)
+    full = pcg.PinnedArray((28 * n_tot,))
+    part = pcg.PinnedArray((28 * n_tot,))
+    b.download_all_cells(full.array)
+    ctx.sync()
+    for mask in (pcg.STEP_WRITTEN_FIELDS, (1 << 27) | 1, 0b101 << 5):
+        part.array[:] = -7.0
+        b.download_cell_fields(part.array, mask)
+        ctx.sync()
+        f = full.array.reshape(28, n_tot)
+        q = part.array.reshape(28, n_tot)
+        for k in range(28):
+            if mask >> k & 1:
+                assert np.array_equal(q[k].view(np.uint32), f[k].view(np.uint32)), k
+            else:
+                assert np.all(q[k] == -7.0), k
+    # the fields the steps do not write are those of the upload
+    start = np.concatenate([i.soa.reshape(28, -1)[:, :i.n_cells] for i in insts], axis=1)
+    f = full.array.reshape(28, n_tot)
+    for k in range(28):
+        if not (pcg.STEP_WRITTEN_FIELDS >> k & 1):
+            assert np.array_equal(f[k].view(np.uint32), start[k].view(np.uint32)), k
+    with pytest.raises(pcg.PcgError):
+        b.download_cell_fields(part.array, 1 << 28)
+    full.free()
+    part.free()
+    b.close()
+
+
 def test_sweep_units_count_the_passes(ctx, pcg):
     """pcg_batch_sweep_units: with planes a 3-D instance's sub-step moves
     each voxel-substrate twice (x + y plane pass, z plane pass) and a 2-D
