@@ -322,9 +322,9 @@ __global__ void k_mech_order(const float* __restrict__ soa, uint32_t stride, con
                            soa[static_cast<size_t>(F_RADIUS) * stride + g]);
     // square roots of the (non-negative) strengths: the pair factors
     // sqrt(rep_i rep_j), sqrt(adh_i adh_j) become one product each
+    const float relmax = soa[static_cast<size_t>(F_REL_MAX_ADH) * stride + g];
     sprm[px] = make_float4(sqrtf(soa[static_cast<size_t>(F_REPULSION) * stride + g]),
-                           sqrtf(soa[static_cast<size_t>(F_ADHESION) * stride + g]),
-                           soa[static_cast<size_t>(F_REL_MAX_ADH) * stride + g], 0.0f);
+                           sqrtf(soa[static_cast<size_t>(F_ADHESION) * stride + g]), relmax, 1.0f / relmax);
 }
 
 __device__ __forceinline__ uint32_t nbr_hash(uint32_t j)
@@ -350,9 +350,10 @@ __device__ __forceinline__ float slab_gap(float c, float lo, float vs, int idx, 
 
 // One pair's force terms (mechanics.metal:167-208) added to the running
 // sums: d = p_i - p_j with dsq = |d|^2 (the test's exact FP32 value), Ri /
-// Rj the radii, mp = (sqrt rep_i, sqrt adh_i, relmax_i), op the same for j.
-// Reciprocal / rsqrt forms and per-cell square roots of the strengths (a
-// few ulp per term against the reference's sqrt and divides).
+// Rj the radii, mp = (sqrt rep_i, sqrt adh_i, relmax_i, 1 / relmax_i), op
+// the strengths of j.  Reciprocal / rsqrt forms and per-cell square roots
+// of the strengths (a few ulp per term against the reference's sqrt and
+// divides); dist / (relmax_i R) is taken as (dist / R) / relmax_i.
 __device__ __forceinline__ void pair_force(float ddx, float ddy, float ddz, float dsq, float Ri, float Rj,
                                            const float4& mp, const float4& op, float& fx, float& fy, float& fz,
                                            float& P)
@@ -360,9 +361,9 @@ __device__ __forceinline__ void pair_force(float ddx, float ddy, float ddz, floa
     constexpr float kInvPressureScale = 1.0f / 0.027288820670331f;
     const float inv = rsqrtf(dsq);
     const float dist = dsq * inv;
-    const float R = Ri + Rj;
-    const float ov = fmaxf(1.0f - __fdividef(dist, R), 0.0f);         // repulsion overlap
-    const float t = fmaxf(1.0f - __fdividef(dist, mp.z * R), 0.0f);    // adhesion reach
+    const float u = __fdividef(dist, Ri + Rj);                         // dist / R
+    const float ov = fmaxf(1.0f - u, 0.0f);                            // repulsion overlap
+    const float t = fmaxf(1.0f - u * mp.w, 0.0f);                      // adhesion reach
     const float ov2 = ov * ov;
     const float F = ov2 * (mp.x * op.x) - t * t * (mp.y * op.y);
     P += ov2 * kInvPressureScale;
