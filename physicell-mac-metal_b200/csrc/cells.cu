@@ -10,8 +10,11 @@
 //              (src/cell_mechanics.mm:57-70);
 //   voxel refresh  Microenvironment::voxelIndex (microenvironment.mm:176-184).
 // The reference's GPU hash and CPU secretion loop are racy; here every
-// result is deterministic: cells are sorted by (voxel, cell index) with a
-// stable radix sort and each voxel's cells are processed in that order.
+// result is deterministic: for secretion, cells are sorted by (diffusion
+// voxel, cell index) with the stable radix sort and each voxel's cells are
+// applied in that order; the mechanics binning is a counting sort whose
+// order within a voxel is fixed by ranks (index, and x for the force
+// pass), so every cell's neighbour walk and sum have a fixed order.
 #include "pcg_kernels.cuh"
 
 namespace pcg {

@@ -1,7 +1,8 @@
 // sort.cu — stable LSD radix sort of (key, value) pairs and a warp-shuffle
-// exclusive scan (sm_100a).  Used to bin cells by mechanics voxel (the
-// cell-start table is the exclusive scan of per-voxel counts) and to order
-// cells by diffusion voxel for secretion.
+// exclusive scan (sm_100a).  The sort orders cells by diffusion voxel for
+// secretion (and backs pcg_sort_pairs_static); the scan turns the per-voxel
+// counts of the mechanics binning into the cell-start table, and serves the
+// sort's digit histograms and the secretion run list.
 //
 // One radix pass over D-bit digits:
 //   k_radix_hist     per-tile digit histogram -> hist[digit * tiles + tile]
