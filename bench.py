@@ -6,8 +6,9 @@ grid side U{40..120} voxels at dx = 20 um, 2 substrates, 1k-100k cells each
 (physicell-mac-metal_b200/workloads.py: batched_3d).  One bench step is one
 mechanics period of the main loop (src/main.mm:341-391): 10 diffusion
 sub-steps (x/y/z Thomas sweeps, Dirichlet reset, secretion) and one
-mechanics step (binning, stable radix sort, cell-start table, forces, AB2),
-over all instances, one CUDA graph launch per sub-step.
+mechanics step (binning, cell-start table, forces, AB2, then every cell's
+voxel index recomputed from its new position and the secretion order
+rebuilt), over all instances, one CUDA graph launch per sub-step.
 
 Reports (one JSON line on rank 0):
   value            aggregate voxel-steps/s of the batched path, inputs resident
@@ -209,18 +210,21 @@ def cpu_prepare(inst):
     vox_idx = soa[26 * n:27 * n].view(np.uint32).copy()
     vol = soa[11 * n:12 * n].copy()
     return (og, osubs, om, dens, soa, n, vox_idx, vol, inst.rates, (g.x_min, g.y_min, g.z_min),
-            g.nx * g.ny * g.nz)
+            g.nx * g.ny * g.nz, bool(inst.flags & 1))
 
 
 def cpu_period(prepared):
     """One mechanics period of the CPU port over the prepared instances."""
     import pyoracle as po
-    for og, osubs, om, dens, soa, n, vox_idx, vol, rates, origin, _ in prepared:
+    for og, osubs, om, dens, soa, n, vox_idx, vol, rates, origin, _, refresh in prepared:
         for _ in range(SUB_STEPS):
             po.port_sweeps(dens, og, osubs)
             po.port_dirichlet(dens, og, osubs)
             po.port_secretion(dens, og, vox_idx, vol, *rates, None, 0.01)
         po.port_mech_step(soa, n, n, om, origin, 0.1)
+        if refresh:   # voxel indices from the new positions, as the device does
+            po.voxel_refresh(soa, n, n, og)
+            vox_idx[:] = soa[26 * n:27 * n].view(np.uint32)
 
 
 def cpu_baseline(instances, budget_s):
@@ -328,6 +332,8 @@ def plain_path(pcg, ctx, insts, periods):
         c = pcg.Cells(ctx, max(inst.n_cells, 1), inst.grid.n_substrates)
         c.upload(inst.soa, inst.n_cells, inst.soa_max)
         c.set_secretion(*inst.rates)
+        if inst.flags & pcg.INST_REFRESH_VOXELS:
+            c.set_voxel_refresh(me)
         g = inst.grid
         m = pcg.CellMechanics(ctx, inst.mech, (g.x_min, g.y_min, g.z_min), max(inst.n_cells, 1))
         objs.append((me, c, m))
@@ -387,7 +393,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-refresh", action="store_true",
-                    help="skip the leg with voxel indices refreshed after every mechanics step")
+                    help="skip the leg with the reference's stale voxel indices (no refresh after mechanics)")
     ap.add_argument("--tune-cache", default=None, help="JSON file of autotuned launch shapes (read and updated)")
     ap.add_argument("--pin-x", type=int, default=0,
                     help="x-sweep launch shape warps*16 + stages instead of the tuned one")
@@ -493,13 +499,12 @@ def main():
     if tr and tr.get("plane_bytes_per_voxel_substrate") and plane_units:
         traffic = tr["plane_bytes_per_voxel_substrate"] * plane_units
 
-    # the same workload with voxel indices refreshed after every mechanics
-    # step (the secretion order is rebuilt inside the mechanics graph)
+    # the same workload with the reference's stale voxel indices (never
+    # refreshed within the run, so the secretion order is never rebuilt)
     refresh = None
     if not args.no_refresh:
         batch.close()
-        rinsts = workloads.batched_3d(n_instances=args.instances * world, seed=1237, only=shard,
-                                      flags=pcg.INST_REFRESH_VOXELS)
+        rinsts = workloads.batched_3d(n_instances=args.instances * world, seed=1237, only=shard, flags=0)
         rb = pcg.Batch(ctx, rinsts, tune_cache=args.tune_cache)
         for _ in range(2):
             rb.step(SUB_STEPS)
@@ -538,7 +543,8 @@ def main():
             "data": "synthetic (seeded)",
             "config": {"workload": f"batched_3d: {args.instances} instances per GPU ({args.instances * world} in all, "
                                    f"sharded by predicted bytes), side U{{40..120}}, S=2, 1k-100k cells; "
-                                   f"step = 10 diffusion sub-steps + 1 mechanics step",
+                                   f"step = 10 diffusion sub-steps + 1 mechanics step, voxel indices "
+                                   f"refreshed after it",
                        "voxels_per_gpu": voxels, "voxel_substrates_per_gpu": voxel_subs, "cells_per_gpu": cells,
                        "l2": f"inputs larger than L2 ({voxel_subs * 4 / 1e6:.0f} MB density per GPU)",
                        "launch_shapes": launch_shapes},
@@ -553,7 +559,7 @@ def main():
                          "sweeps": {"achieved": sweeps_gbs, "frac": sweeps_gbs / peak,
                                     "algorithmic_bytes_per_substep": 8 * all_units, "ms_per_substep": sweep_ms},
                          "phase_ms_per_substep": {k: v / max(nst, 1) for k, v in ph.items()}},
-            "refresh_voxels": refresh,
+            "reference_stale_voxels": refresh,
             "cpu_baseline": cpu,
             "serving": serving,
             "gpu_launches": launches,

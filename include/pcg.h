@@ -183,6 +183,14 @@ pcg_status pcg_cells_set_secretion(pcg_cells* cells, const double* secretion, co
 pcg_status pcg_cells_download_secretion(pcg_cells* cells, double* secretion, double* uptake, double* saturation,
                                         double* net_export, uint8_t* active);
 pcg_status pcg_cells_count(pcg_cells* cells, uint32_t* n_cells);
+/* Voxel index refresh.  The reference recomputes voxel_index only at
+ * phenotype steps, from x and y (cell_phenotype.cpp:781-789).  With on != 0
+ * every pcg_mech_integrate / pcg_mech_update on 'cells' recomputes each
+ * cell's voxel_index from its new position on me's grid
+ * (Microenvironment::voxelIndex, microenvironment.mm:176-184, 3-D aware),
+ * and the next secretion rebuilds its order.  Off (the default) keeps the
+ * indices the host set.  The batch form is PCG_INST_REFRESH_VOXELS. */
+pcg_status pcg_cells_set_voxel_refresh(pcg_cells* cells, const pcg_me* me, int on);
 /* Dead-cell compaction on the device, without a re-upload: CellData::
  * removeCell (src/cell_data.cpp:408-498, the last cell moved into the
  * freed place) for each of 'indices' in descending order, indices at or

@@ -133,6 +133,7 @@ _SIGS = [
     ("pcg_cells_download_fields", C.c_int, [_P, C.c_uint32, C.c_uint32, _F32P, C.c_uint32]),
     ("pcg_cells_set_secretion", C.c_int, [_P, _F64P, _F64P, _F64P, _F64P, _U8P]),
     ("pcg_cells_count", C.c_int, [_P, _U32P]),
+    ("pcg_cells_set_voxel_refresh", C.c_int, [_P, _P, C.c_int]),
     ("pcg_cells_remove", C.c_int, [_P, _U32P, C.c_uint32]),
     ("pcg_removal_plan", C.c_int, [C.c_uint32, _U32P, C.c_uint32, _U32P, _U32P, _U32P, _U32P]),
     ("pcg_cells_append", C.c_int, [_P, _F32P, C.c_uint32, C.c_uint32, _F64P, _F64P, _F64P, _F64P, _U8P]),
@@ -440,6 +441,10 @@ class Cells:
         out = np.zeros(NUM_FIELDS * soa_max, np.float32)
         self.ctx.check(lib().pcg_cells_download(self.h, _f32(out), soa_max))
         return out
+
+    def set_voxel_refresh(self, me, on=True):
+        """Recompute voxel indices on me's grid after every integrate."""
+        self.ctx.check(lib().pcg_cells_set_voxel_refresh(self.h, me.h if me is not None else None, 1 if on else 0))
 
     def positions64(self):
         """FP64 master positions of the current cells: (3, n) array."""

@@ -524,6 +524,18 @@ pcg_status pcg_cells_download_positions64(pcg_cells* c, double* xyz, uint32_t n_
     return c->c.download_positions(0, n_cells, xyz);
 }
 
+pcg_status pcg_cells_set_voxel_refresh(pcg_cells* c, const pcg_me* me, int on)
+{
+    if (!c || (on && !me)) return PCG_ERR_INVALID;
+    if (on) PCG_TRY(bind_me(c, me));
+    const uint32_t f = on ? (c->c.h_inst[0].flags | INST_REFRESH_VOXELS) : (c->c.h_inst[0].flags & ~INST_REFRESH_VOXELS);
+    if (f != c->c.h_inst[0].flags) {
+        c->c.h_inst[0].flags = f;
+        c->c.inst_dirty = true;
+    }
+    return PCG_OK;
+}
+
 pcg_status pcg_cells_count(pcg_cells* c, uint32_t* n)
 {
     if (!c || !n) return PCG_ERR_INVALID;

@@ -27,7 +27,8 @@ with a fixed seed (seed + instance index), so a workload is reproducible.
 import numpy as np
 
 from . import (F_ADHESION, F_POS_X, F_POS_Y, F_POS_Z, F_RADIUS, F_REL_MAX_ADH, F_REPULSION, F_TOTAL_VOL,
-               F_VOXEL_IDX, NUM_FIELDS, Instance, make_grid, make_substrates, mech_params_for_domain)
+               F_VOXEL_IDX, INST_REFRESH_VOXELS, NUM_FIELDS, Instance, make_grid, make_substrates,
+               mech_params_for_domain)
 
 DT_DIFF = 0.01
 DT_MECH = 0.1
@@ -176,11 +177,13 @@ def batched_3d_work(n_instances=64, seed=1237, min_cells=1_000, max_cells=100_00
 
 
 def batched_3d(n_instances=64, seed=1237, min_cells=1_000, max_cells=100_000, side_range=(40, 120), only=None,
-               flags=0):
+               flags=INST_REFRESH_VOXELS):
     """The batched 3-D configuration; 'only' restricts it to the given
     instance indices (a shard), each drawn exactly as in the full set.
-    flags: instance flags (INST_REFRESH_VOXELS: voxel indices recomputed
-    after every mechanics step, so the secretion order is rebuilt)."""
+    flags: instance flags.  By default INST_REFRESH_VOXELS: voxel indices
+    are recomputed from the positions after every mechanics step (so the
+    secretion order is rebuilt), the path's own rule; flags=0 keeps the
+    reference's indices, which it refreshes only at phenotype steps."""
     out = []
     for i in (range(n_instances) if only is None else only):
         rng, side, drug_D, drug_lam, target, n = _batched_3d_spec(i, seed, min_cells, max_cells, side_range)

@@ -2,7 +2,7 @@
 (sides 40-120 voxels, two substrates, 1k-100k cells in central spheres;
 39.9 M voxels and 3.0 M cells) in one batch, one mechanics period (10
 diffusion sub-steps of sweeps, Dirichlet reset and secretion, then one
-mechanics step), as the bench times it.
+mechanics step, voxel indices refreshed after it), as the bench times it.
 
 Against the FP64 oracle, for the largest grid, the densest instance, the
 instance with the most cells, the smallest grid and the instance whose drug
@@ -93,7 +93,7 @@ def test_instance_matches_oracle(batched, po, which):
     dens = np.repeat(inst.initial_values, g.nx * g.ny * g.nz).astype(np.float32)
     soa = inst.soa.copy()
     pm = po.master_positions(soa, n)
-    po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, STEPS, pos64=pm)
+    po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, None, STEPS, refresh=bool(inst.flags & 1), pos64=pm)
     assert rel_err(r["density"], dens) <= 1e-5
     assert float(np.abs(r["pos64"].ravel() - pm).max()) <= 1e-4
     assert np.array_equal(r["cells"][:3 * n], r["pos64"].ravel().astype(np.float32))

@@ -359,6 +359,45 @@ def test_main_loop_steps_match_oracle(ctx, pcg, po):
     assert np.abs(got[:3 * n].astype(np.float64) - soa[:3 * n]).max() <= 1e-4
 
 
+def test_main_loop_with_voxel_refresh_matches_oracle(ctx, pcg, po):
+    """The single-simulation API with voxel indices refreshed after every
+    integrate (pcg_cells_set_voxel_refresh) against or_run with the same
+    rule: density, master positions and voxel indices."""
+    from pcg import workloads
+    inst = workloads.plain_2d(n_cells=800)
+    g, n = inst.grid, inst.n_cells
+    me = pcg.Microenvironment(ctx, g, inst.substrates)
+    me.fill([38.0])
+    cells = pcg.Cells(ctx, n, 1)
+    cells.upload(inst.soa, n, n)
+    cells.set_secretion(*inst.rates)
+    cells.set_voxel_refresh(me)
+    mech = pcg.CellMechanics(ctx, inst.mech, (g.x_min, g.y_min, -10.0), n)
+    acc = 0.0
+    steps = 60
+    for _ in range(steps):
+        me.step(cells, 1)
+        acc += np.float64(np.float32(0.01))
+        if acc >= np.float64(np.float32(0.1)) - 0.5 * np.float64(np.float32(0.01)):
+            mech.computeForces(cells)
+            mech.integratePositions(cells, 0.1)
+            acc = 0.0
+    og = po.make_grid(g.nx, g.ny, g.nz, 1, dx=g.dx, dt=g.dt, x_min=g.x_min, y_min=g.y_min, z_min=g.z_min)
+    om = po.mech_params(-500, 500, -500, 500, -10, 10, True, 0.1)
+    dens = np.full(2500, 38.0, np.float32)
+    soa = inst.soa.copy()
+    pm = po.master_positions(soa, n)
+    po.run(og, po.make_subs([(1e5, 0.1, True, 38.0)]), om, 0.1, dens, soa, n, n, *inst.rates, None, steps,
+           refresh=True, pos64=pm)
+    got = cells.download(n)
+    assert rel_err(me.densityBuffer(), dens) <= 1e-5
+    assert np.abs(cells.positions64().ravel() - pm).max() <= 1e-4
+    moved = np.sum(got[26 * n:27 * n].view(np.uint32) != inst.soa[26 * n:27 * n].view(np.uint32))
+    assert moved > 0                                    # some cells changed voxel
+    assert np.array_equal(got[26 * n:27 * n].view(np.uint32), soa[26 * n:27 * n].view(np.uint32))
+    cells.set_voxel_refresh(None, False)
+
+
 def test_remove_and_append_edge_cases(ctx, pcg):
     """Removing nothing, removing every cell, appending to an empty store,
     and an append past max_cells refused without changing the store."""
