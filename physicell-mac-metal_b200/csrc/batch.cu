@@ -31,7 +31,7 @@ uint64_t instance_bytes(const pcg_instance_desc& d)
     b += (nv / 32 + 3) * 32 * S;                           // tile lists (~32 B per 32 lines per axis)
     b += n * (NUM_FIELDS * 4 + 4 + 1);                     // SoA, instance id, active
     b += n * 3 * 8;                                        // FP64 master positions
-    b += n * S * (4 * 8 + 3 * 8);                          // rates, secretion constants
+    b += n * S * (4 * 8 + 3 * 8 * 2);                      // rates, secretion constants (cell and sorted order)
     b += n * 4 * 6 * 2;                                    // two sort workspaces
     b += n * (8 + 4);                                      // per-run density element and rate slot
     b += n * (16 + 16 + 8);                                // sorted SoA, diagnostics

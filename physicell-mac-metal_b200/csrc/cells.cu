@@ -47,12 +47,28 @@ __global__ void k_sec_keys(const float* __restrict__ soa, uint32_t stride, uint3
     vals[g] = g;
 }
 
+// Instance of a valid secretion key: instances own increasing, disjoint key
+// ranges [vox_base, vox_base + voxels), so it is the last instance whose
+// vox_base is <= key (an instance without voxels shares its vox_base with the
+// next one and is passed over).  The top levels of the search are the same
+// for every thread and stay in L1.
+__device__ __forceinline__ uint32_t inst_of_key(const CellInst* __restrict__ insts, uint32_t n_inst, uint32_t key)
+{
+    uint32_t lo = 0, hi = n_inst;   // first instance with vox_base > key lies in [lo, hi]
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&insts[mid].vox_base) <= key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo - 1;
+}
+
 // Runs of the sorted order.  A run is the cells of one voxel (equal keys);
 // heads[p] = 1 at the first position of each run, sbeg[i] = first sorted
 // position of instance i's cells (valid keys form a prefix of the order and
 // instances occupy increasing key ranges).  heads has n + 1 entries.
-__global__ void k_sec_heads(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder, uint32_t n,
-                            const uint32_t* __restrict__ cell_inst, uint32_t invalid_key, uint32_t* __restrict__ heads,
+__global__ void k_sec_heads(const uint32_t* __restrict__ skeys, uint32_t n, const CellInst* __restrict__ insts,
+                            uint32_t n_inst, uint32_t invalid_key, uint32_t* __restrict__ heads,
                             uint32_t* __restrict__ sbeg)
 {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -63,10 +79,12 @@ __global__ void k_sec_heads(const uint32_t* __restrict__ skeys, const uint32_t* 
     }
     const uint32_t key = skeys[p];
     const bool valid = key < invalid_key;
-    heads[p] = (valid && (p == 0 || skeys[p - 1] != key)) ? 1u : 0u;
-    if (valid) {
-        const uint32_t ii = cell_inst[sorder[p]];
-        if (p == 0 || cell_inst[sorder[p - 1]] != ii) sbeg[ii] = p;
+    const bool head = valid && (p == 0 || skeys[p - 1] != key);
+    heads[p] = head ? 1u : 0u;
+    if (head) {
+        // a new instance starts here if the previous key lies below its range
+        const uint32_t ii = inst_of_key(insts, n_inst, key);
+        if (p == 0 || skeys[p - 1] < insts[ii].vox_base) sbeg[ii] = p;
     }
 }
 
@@ -75,9 +93,9 @@ __global__ void k_sec_heads(const uint32_t* __restrict__ skeys, const uint32_t* 
 // Each run also gets the density element of its voxel (substrate 0, padded
 // rows) and the rate slot of its first cell, so the secretion pass finds
 // both without reading the key or the instance's first sorted place.
-__global__ void k_sec_runs(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder, uint32_t n,
-                           const uint32_t* __restrict__ cell_inst, uint32_t invalid_key, const uint32_t* __restrict__ rid,
-                           const CellInst* __restrict__ insts, const uint32_t* __restrict__ sbeg,
+__global__ void k_sec_runs(const uint32_t* __restrict__ skeys, uint32_t n, uint32_t n_inst, uint32_t invalid_key,
+                           const uint32_t* __restrict__ rid, const CellInst* __restrict__ insts,
+                           const uint32_t* __restrict__ sbeg,
                            uint32_t* __restrict__ run_start, uint32_t* __restrict__ run_inst,
                            uint64_t* __restrict__ run_dens, uint32_t* __restrict__ run_slot)
 {
@@ -86,7 +104,7 @@ __global__ void k_sec_runs(const uint32_t* __restrict__ skeys, const uint32_t* _
     const bool valid = p < n && skeys[p] < invalid_key;
     if (valid && (p == 0 || skeys[p - 1] != skeys[p])) {
         const uint32_t r = rid[p];
-        const uint32_t ii = cell_inst[sorder[p]];
+        const uint32_t ii = inst_of_key(insts, n_inst, skeys[p]);
         const CellInst& in = insts[ii];
         const uint32_t v = skeys[p] - in.vox_base;
         run_start[r] = p;
@@ -97,23 +115,21 @@ __global__ void k_sec_runs(const uint32_t* __restrict__ skeys, const uint32_t* _
     if (!valid && (p == 0 || skeys[p - 1] < invalid_key)) run_start[rid[p]] = p;
 }
 
-// Secretion constants in sorted order: cell sorder[q] of instance i goes to
-// rate slot in.rate_off + (q - sbeg[i]) * S (+ s), as
-// cs[3 * slot + {0,1,2}] = {dt*ne/V_vox, ic*sec*sat, 1 + ic*(sec+upt)} with
+// Secretion constants of every cell, in cell order: for rate slot
+// o = in.rate_off + (g - in.cell_off) * S + s,
+// cc[3 * o + {0,1,2}] = {dt*ne/V_vox, ic*sec*sat, 1 + ic*(sec+upt)} with
 // ic = dt*V_cell/V_vox, exactly as processSecretion forms them
-// (cell_phenotype.cpp:526-564).
-__global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, uint32_t n,
-                              const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder,
-                              const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
-                              const uint32_t* __restrict__ sbeg, uint32_t invalid_key,
-                              const double* __restrict__ rates4, uint32_t n_rate, double dt, double* __restrict__ cs,
-                              uint32_t* __restrict__ flags)
+// (cell_phenotype.cpp:526-564).  They change only with the rates, volumes,
+// voxel size or dt; a new order only permutes them (k_sec_permute).
+__global__ void k_sec_cell_consts(const float* __restrict__ soa, uint32_t stride, uint32_t n,
+                                  const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
+                                  const double* __restrict__ rates4, uint32_t n_rate, double dt,
+                                  double* __restrict__ cc, uint32_t* __restrict__ flags)
 {
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = q < n && skeys[q] < invalid_key;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = g < n;
     const unsigned live_lanes = __ballot_sync(0xFFFFFFFFu, live);   // blocks are whole warps
     if (!live) return;
-    const uint32_t g = sorder[q];
     const uint32_t ii = cell_inst[g];
     const CellInst& in = insts[ii];
     const double V_vox = __dmul_rn(__dmul_rn(static_cast<double>(in.dx), static_cast<double>(in.dy)),
@@ -121,7 +137,6 @@ __global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, ui
     const double V_cell = static_cast<double>(soa[static_cast<size_t>(F_TOTAL_VOL) * stride + g]);
     const double ic = __ddiv_rn(__dmul_rn(dt, V_cell), V_vox);
     const uint32_t src = in.rate_off + (g - in.cell_off) * in.S;
-    const uint32_t dst = in.rate_off + (q - sbeg[ii]) * in.S;
     uint32_t f = 0;
     for (uint32_t s = 0; s < in.S; ++s) {
         const uint32_t o = src + s;
@@ -129,16 +144,44 @@ __global__ void k_sec_prepare(const float* __restrict__ soa, uint32_t stride, ui
                      ne = rates4[3ull * n_rate + o];
         const double c0 = __ddiv_rn(__dmul_rn(dt, ne), V_vox);
         const double c1 = __dmul_rn(__dmul_rn(ic, sec), sat);
-        cs[dst + s] = c0;
-        cs[n_rate + dst + s] = c1;
-        cs[2ull * n_rate + dst + s] = __dadd_rn(1.0, __dmul_rn(ic, __dadd_rn(sec, upt)));
+        cc[3ull * o] = c0;
+        cc[3ull * o + 1] = c1;
+        cc[3ull * o + 2] = __dadd_rn(1.0, __dmul_rn(ic, __dadd_rn(sec, upt)));
         f |= (__double_as_longlong(c0) != 0 ? 1u : 0u) | (__double_as_longlong(c1) != 0 ? 2u : 0u);
     }
     // per instance: does any cell have an export (bit 0) or a secretion
     // (bit 1) term other than +0?  Cells of a warp mostly share the instance.
+    // (A cell outside the sorted order may set a bit: the secretion pass
+    // then reads that instance's stored terms, which give the same bits.)
     const unsigned grp = __match_any_sync(live_lanes, ii);
     f = __reduce_or_sync(grp, f);
     if (f && (threadIdx.x & 31) == static_cast<unsigned>(__ffs(grp) - 1)) atomicOr(&flags[ii], f);
+}
+
+// The constants in sorted order: cell sorder[q] of instance i goes to rate
+// slot in.rate_off + (q - sbeg[i]) * S (+ s) of the three arrays
+// cs[{0,1,2} * n_rate + slot], from its 3 * S contiguous cell-order values.
+__global__ void k_sec_permute(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder, uint32_t n,
+                              const CellInst* __restrict__ insts, uint32_t n_inst,
+                              const uint32_t* __restrict__ sbeg, uint32_t invalid_key,
+                              const double* __restrict__ cc, uint32_t n_rate, double* __restrict__ cs)
+{
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const uint32_t key = skeys[q];
+    if (key >= invalid_key) return;
+    const uint32_t g = sorder[q];
+    const uint32_t ii = inst_of_key(insts, n_inst, key);
+    const CellInst& in = insts[ii];
+    const uint32_t src = in.rate_off + (g - in.cell_off) * in.S;
+    const uint32_t dst = in.rate_off + (q - sbeg[ii]) * in.S;
+    for (uint32_t s = 0; s < in.S; ++s) {
+        const double* c = cc + 3ull * (src + s);
+        const double c0 = c[0], c1 = c[1], c2 = c[2];
+        cs[dst + s] = c0;
+        cs[n_rate + dst + s] = c1;
+        cs[2ull * n_rate + dst + s] = c2;
+    }
 }
 
 // One cell's processSecretion on one substrate (cell_phenotype.cpp:526-564):
@@ -574,31 +617,39 @@ cudaError_t launch_sec_keys(cudaStream_t st, const float* soa, uint32_t stride, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
-                            const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* heads_rid, uint32_t* sbeg,
-                            const CellInst* insts, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
-                            uint32_t* run_slot, void* scan_scratch)
+cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, uint32_t n, const CellInst* insts,
+                            uint32_t n_inst, uint32_t invalid_key, uint32_t* heads_rid, uint32_t* sbeg,
+                            uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens, uint32_t* run_slot,
+                            void* scan_scratch)
 {
-    k_sec_heads<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, sorder, n, cell_inst, invalid_key, heads_rid, sbeg);
+    k_sec_heads<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, n, insts, n_inst, invalid_key, heads_rid, sbeg);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = scan_exclusive(st, heads_rid, heads_rid, static_cast<uint64_t>(n) + 1, scan_scratch);
     if (e != cudaSuccess) return e;
-    k_sec_runs<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, sorder, n, cell_inst, invalid_key, heads_rid, insts,
-                                                         sbeg, run_start, run_inst, run_dens, run_slot);
+    k_sec_runs<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, n, n_inst, invalid_key, heads_rid, insts, sbeg,
+                                                         run_start, run_inst, run_dens, run_slot);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n, const uint32_t* skeys,
-                               const uint32_t* sorder, const uint32_t* cell_inst, const CellInst* insts,
-                               const uint32_t* sbeg, uint32_t invalid_key, const double* rates4, uint32_t n_rate,
-                               double dt, double* cs, uint32_t* flags, uint32_t n_inst)
+cudaError_t launch_sec_cell_consts(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
+                                   const uint32_t* cell_inst, const CellInst* insts, const double* rates4,
+                                   uint32_t n_rate, double dt, double* cc, uint32_t* flags, uint32_t n_inst)
+{
+    cudaError_t e = cudaMemsetAsync(flags, 0, static_cast<size_t>(n_inst) * sizeof(uint32_t), st);
+    if (e != cudaSuccess || n == 0) return e;
+    k_sec_cell_consts<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, rates4, n_rate, dt, cc,
+                                                           flags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sec_permute(cudaStream_t st, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
+                               const CellInst* insts, uint32_t n_inst, const uint32_t* sbeg, uint32_t invalid_key,
+                               const double* cc, uint32_t n_rate, double* cs)
 {
     if (n == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(flags, 0, static_cast<size_t>(n_inst) * sizeof(uint32_t), st);
-    if (e != cudaSuccess) return e;
-    k_sec_prepare<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, skeys, sorder, cell_inst, insts, sbeg,
-                                                       invalid_key, rates4, n_rate, dt, cs, flags);
+    k_sec_permute<<<blocks_for(n, 256), 256, 0, st>>>(skeys, sorder, n, insts, n_inst, sbeg, invalid_key, cc, n_rate,
+                                                       cs);
     return cudaGetLastError();
 }
 

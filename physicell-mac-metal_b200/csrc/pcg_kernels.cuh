@@ -233,17 +233,23 @@ cudaError_t launch_sec_keys(cudaStream_t st, const float* soa, uint32_t stride, 
 // run_start: n + 1 entries; run_inst, run_dens (density element of the
 // run's voxel, substrate 0) and run_slot (rate slot of its first cell): n;
 // sbeg: one per instance; scan_scratch: scan_scratch_bytes(n + 1).
-cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
-                            const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* heads_rid, uint32_t* sbeg,
-                            const CellInst* insts, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
-                            uint32_t* run_slot, void* scan_scratch);
-cudaError_t launch_sec_prepare(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n, const uint32_t* skeys,
-                               const uint32_t* sorder, const uint32_t* cell_inst, const CellInst* insts,
-                               const uint32_t* sbeg, uint32_t invalid_key, const double* rates4, uint32_t n_rate,
-                               double dt, double* cs, uint32_t* flags, uint32_t n_inst);
+// The instance of a key is found from the instances' increasing vox_base.
+cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, uint32_t n, const CellInst* insts,
+                            uint32_t n_inst, uint32_t invalid_key, uint32_t* heads_rid, uint32_t* sbeg,
+                            uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens, uint32_t* run_slot,
+                            void* scan_scratch);
+// Constants in cell order (cc: 3 * n_rate doubles, the three of a rate slot
+// together) and the per-instance flags; then, for an order, their
+// permutation into the sorted arrays cs.
+cudaError_t launch_sec_cell_consts(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
+                                   const uint32_t* cell_inst, const CellInst* insts, const double* rates4,
+                                   uint32_t n_rate, double dt, double* cc, uint32_t* flags, uint32_t n_inst);
+cudaError_t launch_sec_permute(cudaStream_t st, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
+                               const CellInst* insts, uint32_t n_inst, const uint32_t* sbeg, uint32_t invalid_key,
+                               const double* cc, uint32_t n_rate, double* cs);
 // n_runs: device count (heads_rid[n]); max_runs >= it; max_s = largest S.
 // cs: constants c0, c1, c2 as three arrays of cap; flags: per instance, bit 0
-// some c0 not +0, bit 1 some c1 not +0 (written by launch_sec_prepare).
+// some c0 not +0, bit 1 some c1 not +0 (written by launch_sec_cell_consts).
 cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_start, const uint32_t* run_inst,
                            const uint64_t* run_dens, const uint32_t* run_slot, const uint32_t* n_runs,
                            uint32_t max_runs, uint32_t max_s, const CellInst* insts, const double* cs, uint32_t cap,

@@ -1227,6 +1227,7 @@ int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_
     PCG_CU(ctx, rates.alloc(4 * rc * sizeof(double)));
     PCG_CU(ctx, cudaMemsetAsync(rates.p, 0, rates.bytes, ctx->stream));
     PCG_CU(ctx, coef.alloc(3 * rc * sizeof(double)));
+    PCG_CU(ctx, coef_cells.alloc(3 * rc * sizeof(double)));
     PCG_CU(ctx, coef_flags.alloc(h_inst.size() * sizeof(uint32_t)));
     PCG_CU(ctx, cudaMemsetAsync(coef_flags.p, 0xFF, coef_flags.bytes, ctx->stream));   // all terms until prepared
     PCG_CU(ctx, active.alloc(max_cells));
@@ -1354,9 +1355,9 @@ int Cells::build_order(uint64_t total_vox)
     e = radix_sort_pairs(ctx->stream, keys.as<uint32_t>(), vals.as<uint32_t>(), skeys.as<uint32_t>(),
                          sorder.as<uint32_t>(), ktmp.as<uint32_t>(), vtmp.as<uint32_t>(), n, key_bits, sort_scr.p);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion sort");
-    e = launch_sec_runs(ctx->stream, skeys.as<uint32_t>(), sorder.as<uint32_t>(), n, cell_inst.as<uint32_t>(),
-                        invalid_key, ktmp.as<uint32_t>(), sbeg.as<uint32_t>(), inst.as<CellInst>(), vals.as<uint32_t>(),
-                        vtmp.as<uint32_t>(), run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), run_scr.p);
+    e = launch_sec_runs(ctx->stream, skeys.as<uint32_t>(), n, inst.as<CellInst>(), static_cast<uint32_t>(h_inst.size()),
+                        invalid_key, ktmp.as<uint32_t>(), sbeg.as<uint32_t>(), vals.as<uint32_t>(), vtmp.as<uint32_t>(),
+                        run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), run_scr.p);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion runs");
     ctx->launches += 1 + radix_sort_launches(n, key_bits) + 2 + scan_launches(static_cast<uint64_t>(n) + 1);
     order_dirty = false;
@@ -1367,21 +1368,28 @@ int Cells::build_order(uint64_t total_vox)
 int Cells::sorted_constants()
 {
     const uint32_t cap = static_cast<uint32_t>(rates.bytes / (4 * sizeof(double)));
-    cudaError_t e = launch_sec_prepare(ctx->stream, soa.as<float>(), max_cells, n, skeys.as<uint32_t>(),
-                                       sorder.as<uint32_t>(), cell_inst.as<uint32_t>(), inst.as<CellInst>(),
-                                       sbeg.as<uint32_t>(), invalid_key, rates.as<double>(), cap, coef_dt,
-                                       coef.as<double>(), coef_flags.as<uint32_t>(),
-                                       static_cast<uint32_t>(h_inst.size()));
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion prepare");
+    cudaError_t e;
+    if (coef_dirty) {
+        e = launch_sec_cell_consts(ctx->stream, soa.as<float>(), max_cells, n, cell_inst.as<uint32_t>(),
+                                   inst.as<CellInst>(), rates.as<double>(), cap, coef_dt, coef_cells.as<double>(),
+                                   coef_flags.as<uint32_t>(), static_cast<uint32_t>(h_inst.size()));
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion constants");
+        if (n) ctx->launches++;
+        coef_dirty = false;
+    }
+    e = launch_sec_permute(ctx->stream, skeys.as<uint32_t>(), sorder.as<uint32_t>(), n, inst.as<CellInst>(),
+                           static_cast<uint32_t>(h_inst.size()), sbeg.as<uint32_t>(), invalid_key,
+                           coef_cells.as<double>(), cap, coef.as<double>());
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion permute");
     if (n) ctx->launches++;
-    coef_dirty = false;
     return PCG_OK;
 }
 
 int Cells::prepare_secretion(double dt, uint64_t total_vox)
 {
     PCG_TRY(sync_inst());
-    const bool stale = coef_dirty || coef_dt != dt;
+    if (coef_dt != dt) coef_dirty = true;
+    const bool stale = coef_dirty;
     coef_dt = dt;
     if (order_dirty || invalid_key != static_cast<uint32_t>(total_vox)) return build_order(total_vox);
     if (stale) return sorted_constants();
@@ -1404,7 +1412,7 @@ int Cells::secrete(Diffusion& d, const uint8_t* mask)
 
 uint64_t Cells::device_bytes() const
 {
-    return inst.bytes + soa.bytes + pos64.bytes + cell_inst.bytes + rates.bytes + coef.bytes + coef_flags.bytes + active.bytes +
+    return inst.bytes + soa.bytes + pos64.bytes + cell_inst.bytes + rates.bytes + coef.bytes + coef_cells.bytes + coef_flags.bytes + active.bytes +
            keys.bytes + vals.bytes +
            skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + sbeg.bytes + run_scr.bytes +
            run_dens.bytes + run_slot.bytes;

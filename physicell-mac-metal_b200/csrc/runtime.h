@@ -260,7 +260,7 @@ public:
     uint32_t n = 0;
     uint32_t n_rate = 0;          // sum over instances of n_cells * S
     std::vector<CellInst> h_inst;
-    DevBuf inst, soa, cell_inst, rates, coef, coef_flags, active;
+    DevBuf inst, soa, cell_inst, rates, coef, coef_cells, coef_flags, active;
     // FP64 master positions, three arrays of max_cells (x, y, z); the SoA's
     // FP32 positions are their rounding.  The AB2 update starts from a
     // master only while it rounds to the SoA's value, so a position written
@@ -274,8 +274,9 @@ public:
     // secretion ordering: keys/vals sort input, (skeys, sorder) the order;
     // after the sort ktmp holds the run index of every position (+ count),
     // vals the run starts and vtmp the run instances; coef the constants
-    // in sorted order (c0, c1, c2 arrays) and coef_flags which of c0 / c1
-    // each instance has
+    // in sorted order (c0, c1, c2 arrays), coef_cells the same constants in
+    // cell order (the three of a rate slot together; coef_dirty: stale) and
+    // coef_flags which of c0 / c1 each instance has
     DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr, sbeg, run_scr;
     DevBuf run_dens, run_slot;   // per run: density element of its voxel, rate slot of its first cell
     uint32_t invalid_key = 0;
@@ -300,7 +301,7 @@ public:
     // Recompute secretion constants / ordering when stale.
     int prepare_secretion(double dt, uint64_t total_vox);
     int build_order(uint64_t total_vox);   // order, runs and (once a dt is known) the constants
-    int sorted_constants();
+    int sorted_constants();   // cell-order constants when stale, then their permutation
     int secrete(Diffusion& d, const uint8_t* mask);
     uint64_t device_bytes() const;
 };

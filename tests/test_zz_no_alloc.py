@@ -71,6 +71,28 @@ def test_static_sort_matches_mechanics_binning(ctx, pcg, n):
             vo.fill_(-1)
 
 
+@pytest.mark.parametrize("n", [31, 2048, 2049, 100_003, MAX_PAIRS])
+@pytest.mark.parametrize("kind", ["equal", "descending", "random32", "top_digit", "few"])
+def test_static_sort_key_patterns(ctx, pcg, n, kind):
+    """Stable order (numpy's stable argsort) for key patterns that stress the
+    per-digit look-back: one key, descending keys, full 32-bit keys, keys
+    that differ only in the top digit and a handful of distinct keys."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(n + len(kind))
+    keys = {"equal": np.full(n, 0xABCDE, np.uint32),
+            "descending": np.arange(n, 0, -1, dtype=np.uint32) * 977,
+            "random32": rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32),
+            "top_digit": (rng.integers(0, 256, n).astype(np.uint32) << 24) | 0x00123456,
+            "few": rng.choice(np.array([3, 70000, 1 << 31, 5], np.uint32), n)}[kind]
+    kd = torch.from_numpy(keys.view(np.int32)).cuda()
+    vd = torch.arange(n, dtype=torch.int32, device="cuda")
+    ko, vo = torch.empty_like(kd), torch.empty_like(vd)
+    ks, vs = _static_sort(pcg, ctx, torch, kd, vd, ko, vo, n, 32)
+    order = np.argsort(keys, kind="stable").astype(np.uint32)
+    assert np.array_equal(vs, order)
+    assert np.array_equal(ks, keys[order])
+
+
 FRESH = textwrap.dedent("""
     import ctypes as C, importlib.util, os, sys
     import numpy as np
