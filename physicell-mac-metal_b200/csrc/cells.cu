@@ -430,13 +430,15 @@ __device__ __forceinline__ void pair_force(float ddx, float ddy, float ddz, floa
 // first candidate past the upper bound.  Every candidate that can pass is
 // tested, with the reference's FP32 test without contraction
 // (mechanics.metal:159-165), so neighbour sets are exact (for finite
-// positions).  The next candidate's position is loaded while the current
-// one is tested; the force terms follow pair_force.
+// positions).  The force terms follow pair_force.
 //
-// QCAP == 0: the force terms are computed in the walk, where a lane meets
-// its neighbour.  QCAP > 0: the walk only tests; each lane keeps the
+// QCAP == 0: the walk takes two candidates a step, both positions and both
+// strengths loaded before either is tested (four independent loads in
+// flight per lane), and the force terms are computed where a lane meets its
+// neighbour.  QCAP > 0: the walk only tests; each lane keeps the
 // candidates that pass, in order, in its own QCAP slots of shared memory
-// (slot k of thread t at queue[k * blockDim + t]), and the force terms of
+// (slot k of thread t at queue[k * blockDim + t]; the next candidate's
+// position is loaded while the current one is tested), and the force terms of
 // the queued neighbours are computed when a lane's queue is full (every
 // lane walking with it then empties its own) and at the end.  Every lane
 // adds its terms in candidate order either way, so both forms give the same
@@ -522,13 +524,47 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
                 len = half;
             }
         }
+        if (QCAP == 0) {
+            // two candidates a step, positions and strengths of both loaded
+            // before either is tested (q + 1 <= q1 <= n: spos and sprm have
+            // one spare element)
+            while (q < q1) {
+                const float4 c0 = spos[q], c1 = spos[q + 1];
+                const float4 p0 = sprm[q], p1 = sprm[q + 1];
+                bool more = true;
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const float4& cur = k == 0 ? c0 : c1;
+                    // past the row or the window: so is every later candidate of the row
+                    const bool in_win = q + k < q1 && cur.x < xhi;
+                    if (in_win) {
+                        // neighbour test exactly as mechanics.metal:159-165 (no contraction);
+                        // the cell itself (distance 0) fails it like any coincident cell
+                        const float ddx = __fsub_rn(me.x, cur.x), ddy = __fsub_rn(me.y, cur.y),
+                                    ddz = __fsub_rn(me.z, cur.z);
+                        const float dsq =
+                            __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
+                        if (!(dsq >= maxd2 || dsq < 1e-12f)) {
+                            if (DIAG) {
+                                ++cnt;
+                                hsh += nbr_hash(forder[q + k] - in.cell_off);
+                            }
+                            pair_force(ddx, ddy, ddz, dsq, me.w, cur.w, mp, k == 0 ? p0 : p1, fx, fy, fz, P);
+                        }
+                    }
+                    more = in_win;
+                }
+                if (!more) break;
+                q += 2;
+            }
+            continue;
+        }
         float4 o = spos[q];   // q <= n: in bounds even for an empty row
         for (; q < q1; ++q) {
             const float4 cur = o;
             o = spos[q + 1];   // next candidate in flight (spos has one spare element)
             if (cur.x >= xhi) break;   // this and every later candidate of the row lie past the window
-            // neighbour test exactly as mechanics.metal:159-165 (no contraction);
-            // the cell itself (q == p, distance 0) fails it like any coincident cell
+            // neighbour test exactly as mechanics.metal:159-165 (no contraction)
             const float ddx = __fsub_rn(me.x, cur.x), ddy = __fsub_rn(me.y, cur.y), ddz = __fsub_rn(me.z, cur.z);
             const float dsq = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
             const bool nb = !(dsq >= maxd2 || dsq < 1e-12f);
@@ -536,12 +572,8 @@ __global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ 
                 ++cnt;
                 hsh += nbr_hash(forder[q] - in.cell_off);
             }
-            if (QCAP == 0) {
-                if (nb) pair_force(ddx, ddy, ddz, dsq, me.w, cur.w, mp, sprm[q], fx, fy, fz, P);
-            } else {
-                if (nb) myq[nq++ * qstride] = q;
-                if (__any_sync(__activemask(), nq == QCAP)) flush();
-            }
+            if (nb) myq[nq++ * qstride] = q;
+            if (__any_sync(__activemask(), nq == QCAP)) flush();
         }
     }
     if (QCAP > 0) flush();
