@@ -327,10 +327,8 @@ uint64_t Batch::count_launches(bool mech) const
     if (c_.n) k += 1;
     if (mech && c_.n) {
         k += m_.launches_forces(c_.n) - 1 + 1;   // bin..forces (memset excluded) + integrate
-        // the secretion order after the voxel refresh: keys, sort, heads, scan, runs, constants
-        if (any_refresh)
-            k += 1 + radix_sort_launches(c_.n, key_bits_for(d.total_vox + 1)) + 2 +
-                 scan_launches(static_cast<uint64_t>(c_.n) + 1) + 1;
+        // the secretion order after the voxel refresh: sort passes, run list, constants
+        if (any_refresh) k += c_.order_launches();
     }
     return k;
 }

@@ -11,8 +11,8 @@
 //   voxel refresh  Microenvironment::voxelIndex (microenvironment.mm:176-184).
 // The reference's GPU hash and CPU secretion loop are racy; here every
 // result is deterministic: for secretion, cells are sorted by (diffusion
-// voxel, cell index) with the stable radix sort and each voxel's cells are
-// applied in that order; the mechanics binning is a counting sort whose
+// voxel, cell index) (secorder.cu) and each voxel's cells are applied in
+// that order; the mechanics binning is a counting sort whose
 // order within a voxel is fixed by ranks (index, and x for the force
 // pass), so every cell's neighbour walk and sum have a fixed order.
 #include "pcg_kernels.cuh"
@@ -32,92 +32,9 @@ __device__ __forceinline__ int bin_of(float p, float lo, float h)
 
 // ------------------------------------------------------------------ secretion
 
-__global__ void k_sec_keys(const float* __restrict__ soa, uint32_t stride, uint32_t n,
-                           const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
-                           const uint8_t* __restrict__ active, uint32_t invalid_key, uint32_t* __restrict__ keys,
-                           uint32_t* __restrict__ vals)
-{
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    const CellInst& in = insts[cell_inst[g]];
-    const uint32_t v = fbits(soa[static_cast<size_t>(F_VOXEL_IDX) * stride + g]);
-    const uint32_t nv = in.nx * in.ny * in.nz;
-    const bool ok = (active == nullptr || active[g] != 0) && v < nv && in.S > 0;
-    keys[g] = ok ? in.vox_base + v : invalid_key;
-    vals[g] = g;
-}
-
-// Instance of a valid secretion key: instances own increasing, disjoint key
-// ranges [vox_base, vox_base + voxels), so it is the last instance whose
-// vox_base is <= key (an instance without voxels shares its vox_base with the
-// next one and is passed over).  The top levels of the search are the same
-// for every thread and stay in L1.
-__device__ __forceinline__ uint32_t inst_of_key(const CellInst* __restrict__ insts, uint32_t n_inst, uint32_t key)
-{
-    uint32_t lo = 0, hi = n_inst;   // first instance with vox_base > key lies in [lo, hi]
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(&insts[mid].vox_base) <= key) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo - 1;
-}
-
-// Runs of the sorted order.  A run is the cells of one voxel (equal keys);
-// heads[p] = 1 at the first position of each run, sbeg[i] = first sorted
-// position of instance i's cells (valid keys form a prefix of the order and
-// instances occupy increasing key ranges).  heads has n + 1 entries.
-__global__ void k_sec_heads(const uint32_t* __restrict__ skeys, uint32_t n, const CellInst* __restrict__ insts,
-                            uint32_t n_inst, uint32_t invalid_key, uint32_t* __restrict__ heads,
-                            uint32_t* __restrict__ sbeg)
-{
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p > n) return;
-    if (p == n) {
-        heads[n] = 0;
-        return;
-    }
-    const uint32_t key = skeys[p];
-    const bool valid = key < invalid_key;
-    const bool head = valid && (p == 0 || skeys[p - 1] != key);
-    heads[p] = head ? 1u : 0u;
-    if (head) {
-        // a new instance starts here if the previous key lies below its range
-        const uint32_t ii = inst_of_key(insts, n_inst, key);
-        if (p == 0 || skeys[p - 1] < insts[ii].vox_base) sbeg[ii] = p;
-    }
-}
-
-// rid = exclusive scan of heads: run r starts at run_start[r] and ends at
-// run_start[r + 1]; run_start[n_runs] is the first invalid position (or n).
-// Each run also gets the density element of its voxel (substrate 0, padded
-// rows) and the rate slot of its first cell, so the secretion pass finds
-// both without reading the key or the instance's first sorted place.
-__global__ void k_sec_runs(const uint32_t* __restrict__ skeys, uint32_t n, uint32_t n_inst, uint32_t invalid_key,
-                           const uint32_t* __restrict__ rid, const CellInst* __restrict__ insts,
-                           const uint32_t* __restrict__ sbeg,
-                           uint32_t* __restrict__ run_start, uint32_t* __restrict__ run_inst,
-                           uint64_t* __restrict__ run_dens, uint32_t* __restrict__ run_slot)
-{
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p > n) return;
-    const bool valid = p < n && skeys[p] < invalid_key;
-    if (valid && (p == 0 || skeys[p - 1] != skeys[p])) {
-        const uint32_t r = rid[p];
-        const uint32_t ii = inst_of_key(insts, n_inst, skeys[p]);
-        const CellInst& in = insts[ii];
-        const uint32_t v = skeys[p] - in.vox_base;
-        run_start[r] = p;
-        run_inst[r] = ii;
-        run_dens[r] = in.dens_off + static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
-        run_slot[r] = in.rate_off + (p - sbeg[ii]) * in.S;
-    }
-    if (!valid && (p == 0 || skeys[p - 1] < invalid_key)) run_start[rid[p]] = p;
-}
-
 // Secretion constants of every cell, in cell order: for rate slot
-// o = in.rate_off + (g - in.cell_off) * S + s,
-// cc[3 * o + {0,1,2}] = {dt*ne/V_vox, ic*sec*sat, 1 + ic*(sec+upt)} with
+// o = in.rate_off + (g - in.cell_off) * S + s, three arrays of n_rate,
+// cc[{0,1,2} * n_rate + o] = {dt*ne/V_vox, ic*sec*sat, 1 + ic*(sec+upt)} with
 // ic = dt*V_cell/V_vox, exactly as processSecretion forms them
 // (cell_phenotype.cpp:526-564).  They change only with the rates, volumes,
 // voxel size or dt; a new order only permutes them (k_sec_permute).
@@ -144,9 +61,9 @@ __global__ void k_sec_cell_consts(const float* __restrict__ soa, uint32_t stride
                      ne = rates4[3ull * n_rate + o];
         const double c0 = __ddiv_rn(__dmul_rn(dt, ne), V_vox);
         const double c1 = __dmul_rn(__dmul_rn(ic, sec), sat);
-        cc[3ull * o] = c0;
-        cc[3ull * o + 1] = c1;
-        cc[3ull * o + 2] = __dadd_rn(1.0, __dmul_rn(ic, __dadd_rn(sec, upt)));
+        cc[o] = c0;
+        cc[static_cast<uint64_t>(n_rate) + o] = c1;
+        cc[2ull * n_rate + o] = __dadd_rn(1.0, __dmul_rn(ic, __dadd_rn(sec, upt)));
         f |= (__double_as_longlong(c0) != 0 ? 1u : 0u) | (__double_as_longlong(c1) != 0 ? 2u : 0u);
     }
     // per instance: does any cell have an export (bit 0) or a secretion
@@ -158,29 +75,29 @@ __global__ void k_sec_cell_consts(const float* __restrict__ soa, uint32_t stride
     if (f && (threadIdx.x & 31) == static_cast<unsigned>(__ffs(grp) - 1)) atomicOr(&flags[ii], f);
 }
 
-// The constants in sorted order: cell sorder[q] of instance i goes to rate
-// slot in.rate_off + (q - sbeg[i]) * S (+ s) of the three arrays
-// cs[{0,1,2} * n_rate + slot], from its 3 * S contiguous cell-order values.
+// The constants in sorted order: the cell sorder[q] of instance i goes to
+// rate slot in.rate_off + (q - in.cell_off) * S (+ s) of the three arrays
+// cs[{0,1,2} * n_rate + slot] (an instance's secreting cells fill the start
+// of its range).  c0 and c1 are moved only for instances that have a term
+// other than +0 (flags), the only ones the secretion pass reads them for.
 __global__ void k_sec_permute(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder, uint32_t n,
-                              const CellInst* __restrict__ insts, uint32_t n_inst,
-                              const uint32_t* __restrict__ sbeg, uint32_t invalid_key,
+                              const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
+                              uint32_t invalid_key, const uint32_t* __restrict__ flags,
                               const double* __restrict__ cc, uint32_t n_rate, double* __restrict__ cs)
 {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
-    const uint32_t key = skeys[q];
-    if (key >= invalid_key) return;
+    if (skeys[q] >= invalid_key) return;
     const uint32_t g = sorder[q];
-    const uint32_t ii = inst_of_key(insts, n_inst, key);
+    const uint32_t ii = cell_inst[g];
     const CellInst& in = insts[ii];
-    const uint32_t src = in.rate_off + (g - in.cell_off) * in.S;
-    const uint32_t dst = in.rate_off + (q - sbeg[ii]) * in.S;
+    const uint32_t f = flags[ii];
+    const uint64_t src = in.rate_off + (g - in.cell_off) * in.S;
+    const uint64_t dst = in.rate_off + (q - in.cell_off) * in.S;
     for (uint32_t s = 0; s < in.S; ++s) {
-        const double* c = cc + 3ull * (src + s);
-        const double c0 = c[0], c1 = c[1], c2 = c[2];
-        cs[dst + s] = c0;
-        cs[n_rate + dst + s] = c1;
-        cs[2ull * n_rate + dst + s] = c2;
+        if (f & 1u) cs[dst + s] = cc[src + s];
+        if (f & 2u) cs[n_rate + dst + s] = cc[n_rate + src + s];
+        cs[2ull * n_rate + dst + s] = cc[2ull * n_rate + src + s];
     }
 }
 
@@ -220,6 +137,7 @@ __global__ void __launch_bounds__(256, 6) k_secrete(float* __restrict__ dens, co
     // density element and the first cell's rate slot were placed when the
     // order was built, so the density and the constants are one load away
     const uint32_t ii = run_inst[r];
+    if (ii == kNoRunInst) return;   // the instance's non-secreting cells
     const uint32_t p0 = run_start[r], p1 = run_start[r + 1];
     float* d = dens + run_dens[r];
     const uint64_t base = run_slot[r];
@@ -640,30 +558,6 @@ __global__ void k_mech_integrate(float* __restrict__ soa, double* __restrict__ p
 
 static inline unsigned blocks_for(uint64_t n, int b) { return static_cast<unsigned>((n + b - 1) / b); }
 
-cudaError_t launch_sec_keys(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n, const uint32_t* cell_inst,
-                            const CellInst* insts, const uint8_t* active, uint32_t invalid_key, uint32_t* keys,
-                            uint32_t* vals)
-{
-    if (n == 0) return cudaSuccess;
-    k_sec_keys<<<blocks_for(n, 256), 256, 0, st>>>(soa, stride, n, cell_inst, insts, active, invalid_key, keys, vals);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, uint32_t n, const CellInst* insts,
-                            uint32_t n_inst, uint32_t invalid_key, uint32_t* heads_rid, uint32_t* sbeg,
-                            uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens, uint32_t* run_slot,
-                            void* scan_scratch)
-{
-    k_sec_heads<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, n, insts, n_inst, invalid_key, heads_rid, sbeg);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    e = scan_exclusive(st, heads_rid, heads_rid, static_cast<uint64_t>(n) + 1, scan_scratch);
-    if (e != cudaSuccess) return e;
-    k_sec_runs<<<blocks_for(n + 1, 256), 256, 0, st>>>(skeys, n, n_inst, invalid_key, heads_rid, insts, sbeg,
-                                                         run_start, run_inst, run_dens, run_slot);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_sec_cell_consts(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
                                    const uint32_t* cell_inst, const CellInst* insts, const double* rates4,
                                    uint32_t n_rate, double dt, double* cc, uint32_t* flags, uint32_t n_inst)
@@ -676,12 +570,12 @@ cudaError_t launch_sec_cell_consts(cudaStream_t st, const float* soa, uint32_t s
 }
 
 cudaError_t launch_sec_permute(cudaStream_t st, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
-                               const CellInst* insts, uint32_t n_inst, const uint32_t* sbeg, uint32_t invalid_key,
-                               const double* cc, uint32_t n_rate, double* cs)
+                               const uint32_t* cell_inst, const CellInst* insts, uint32_t invalid_key,
+                               const uint32_t* flags, const double* cc, uint32_t n_rate, double* cs)
 {
     if (n == 0) return cudaSuccess;
-    k_sec_permute<<<blocks_for(n, 256), 256, 0, st>>>(skeys, sorder, n, insts, n_inst, sbeg, invalid_key, cc, n_rate,
-                                                       cs);
+    k_sec_permute<<<blocks_for(n, 256), 256, 0, st>>>(skeys, sorder, n, cell_inst, insts, invalid_key, flags, cc,
+                                                       n_rate, cs);
     return cudaGetLastError();
 }
 

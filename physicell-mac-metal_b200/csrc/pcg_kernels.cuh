@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace pcg {
 
@@ -224,30 +225,19 @@ struct GradJob { uint64_t base; uint64_t out_base; uint32_t nx, ny, nz, px; floa
 cudaError_t launch_gradients(cudaStream_t st, const float* dens, float* gx, float* gy, float* gz,
                              const GradJob* jobs, uint32_t njobs, uint64_t max_voxels);
 
-// Secretion: keys, then (after the stable sort by key) the run list of the
-// sorted order, constants in sorted order and the ordered application.
-cudaError_t launch_sec_keys(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
-                            const uint32_t* cell_inst, const CellInst* insts, const uint8_t* active,
-                            uint32_t invalid_key, uint32_t* keys, uint32_t* vals);
-// heads_rid: n + 1 entries (run index of every position; [n] = run count);
-// run_start: n + 1 entries; run_inst, run_dens (density element of the
-// run's voxel, substrate 0) and run_slot (rate slot of its first cell): n;
-// sbeg: one per instance; scan_scratch: scan_scratch_bytes(n + 1).
-// The instance of a key is found from the instances' increasing vox_base.
-cudaError_t launch_sec_runs(cudaStream_t st, const uint32_t* skeys, uint32_t n, const CellInst* insts,
-                            uint32_t n_inst, uint32_t invalid_key, uint32_t* heads_rid, uint32_t* sbeg,
-                            uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens, uint32_t* run_slot,
-                            void* scan_scratch);
-// Constants in cell order (cc: 3 * n_rate doubles, the three of a rate slot
-// together) and the per-instance flags; then, for an order, their
-// permutation into the sorted arrays cs.
+// Secretion: the order and its run list (launch_sec_order, below), the
+// constants in cell order (cc: three arrays of n_rate doubles, c0, c1, c2)
+// with the per-instance flags, their permutation into the order's slots
+// (cs; c0 / c1 only for instances whose flags have them) and the ordered
+// application.
 cudaError_t launch_sec_cell_consts(cudaStream_t st, const float* soa, uint32_t stride, uint32_t n,
                                    const uint32_t* cell_inst, const CellInst* insts, const double* rates4,
                                    uint32_t n_rate, double dt, double* cc, uint32_t* flags, uint32_t n_inst);
 cudaError_t launch_sec_permute(cudaStream_t st, const uint32_t* skeys, const uint32_t* sorder, uint32_t n,
-                               const CellInst* insts, uint32_t n_inst, const uint32_t* sbeg, uint32_t invalid_key,
-                               const double* cc, uint32_t n_rate, double* cs);
-// n_runs: device count (heads_rid[n]); max_runs >= it; max_s = largest S.
+                               const uint32_t* cell_inst, const CellInst* insts, uint32_t invalid_key,
+                               const uint32_t* flags, const double* cc, uint32_t n_rate, double* cs);
+// n_runs: device count (heads_rid[n]); max_runs >= it; max_s = largest S;
+// runs marked kNoRunInst are skipped.
 // cs: constants c0, c1, c2 as three arrays of cap; flags: per instance, bit 0
 // some c0 not +0, bit 1 some c1 not +0 (written by launch_sec_cell_consts).
 cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_start, const uint32_t* run_inst,
@@ -293,6 +283,42 @@ cudaError_t launch_cells_move(cudaStream_t st, float* soa, uint32_t stride, cons
 cudaError_t launch_mech_integrate(cudaStream_t st, float* soa, double* pos64, uint32_t stride, uint32_t n,
                                   const uint32_t* cell_inst, const CellInst* insts, float dt_override,
                                   const uint8_t* mask, int block = 256);
+
+// The secretion order (secorder.cu): every instance's cells sorted by
+// (voxel index in the instance's grid, cell index), non-secreting cells
+// (inactive, voxel index outside the grid, no substrates) after them; each
+// instance keeps its range [cell_off, cell_off + n_cells).  A tile is up to
+// 2048 consecutive cells of one instance: first cell, count, instance, the
+// instance's first tile and its number of tiles.
+struct SegTile {
+    uint32_t first, count, inst, tb, nt;
+    uint32_t _pad[3];
+};
+// run_inst of a run of non-secreting cells
+constexpr uint32_t kNoRunInst = 0xFFFFFFFFu;
+// Passes and digit bits for grids of at most max_local_voxels voxels.
+void so_plan(uint32_t max_local_voxels, int* passes, int* digit_bits);
+// Most tiles a store of max_cells cells over n_inst instances can need.
+uint32_t so_max_tiles(uint32_t max_cells, uint32_t n_inst);
+// The tiles of the instances' cell ranges (host, from the CellInst table),
+// and the first tile of every instance that has cells.
+void so_tiles(const CellInst* inst, uint32_t n_inst, std::vector<SegTile>& out, std::vector<uint32_t>& inst_tile);
+size_t so_scratch_bytes(uint32_t max_tiles);
+int so_launches(uint32_t ntiles, int passes, uint32_t n);
+// Keys, the sort and the run list in one call.  Outputs: skeys (global
+// voxel key vox_base + index, or invalid_key) and sorder (cell) per sorted
+// position; heads_rid (n + 1: the run index of every position, [n] = run
+// count); run_start (n + 1), run_inst, run_dens, run_slot per run.  keys,
+// ktmp and vtmp are n-entry work arrays (heads_rid may be ktmp and run_inst
+// vtmp); scratch: so_scratch_bytes, run_scratch: scan_scratch_bytes(n + 1);
+// inst_tile: the n_inst_tiled entries of so_tiles.
+cudaError_t launch_sec_order(cudaStream_t st, const SegTile* tiles, uint32_t ntiles, const uint32_t* inst_tile,
+                             uint32_t n_inst_tiled, uint32_t n, int passes,
+                             int digit_bits, const float* soa, uint32_t stride, const CellInst* insts,
+                             const uint8_t* active, const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* keys,
+                             uint32_t* ktmp, uint32_t* vtmp, uint32_t* skeys, uint32_t* sorder, void* scratch,
+                             uint32_t* heads_rid, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
+                             uint32_t* run_slot, void* run_scratch);
 
 // Radix sort of (key, value) pairs, stable, 'bits' significant key bits.
 // Scratch from radix_sort_scratch_bytes().  Result lands in (k_out, v_out).

@@ -1236,9 +1236,10 @@ int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_
     for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp, &run_slot})
         PCG_CU(ctx, b->alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint32_t)));
     PCG_CU(ctx, run_dens.alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint64_t)));
-    PCG_CU(ctx, sort_scr.alloc(radix_sort_scratch_bytes(max_cells, 32)));
-    PCG_CU(ctx, sbeg.alloc(h_inst.size() * sizeof(uint32_t)));
-    PCG_CU(ctx, cudaMemsetAsync(sbeg.p, 0, sbeg.bytes, ctx->stream));
+    max_tiles = so_max_tiles(max_cells, static_cast<uint32_t>(h_inst.size()));
+    PCG_CU(ctx, tiles.alloc(static_cast<size_t>(max_tiles) * sizeof(SegTile)));
+    PCG_CU(ctx, inst_tile.alloc(h_inst.size() * sizeof(uint32_t)));
+    PCG_CU(ctx, sort_scr.alloc(so_scratch_bytes(max_tiles)));
     PCG_CU(ctx, run_scr.alloc(scan_scratch_bytes(static_cast<uint64_t>(max_cells) + 1)));
     PCG_CU(ctx, cudaMemsetAsync(ktmp.p, 0, ktmp.bytes, ctx->stream));   // run count 0 until the first order
     inst_dirty = coef_dirty = order_dirty = true;
@@ -1250,6 +1251,21 @@ int Cells::sync_inst()
     if (!inst_dirty) return PCG_OK;
     PCG_CU(ctx, cudaMemcpyAsync(inst.p, h_inst.data(), h_inst.size() * sizeof(CellInst), cudaMemcpyHostToDevice,
                                 ctx->stream));
+    // the secretion order's tiles and digits follow the instances' cell
+    // ranges and grids
+    std::vector<SegTile> ht;
+    std::vector<uint32_t> hit;
+    so_tiles(h_inst.data(), static_cast<uint32_t>(h_inst.size()), ht, hit);
+    if (ht.size() > max_tiles) return fail(ctx, PCG_ERR_INVALID, "cell ranges need more sort tiles than allocated");
+    ntiles = static_cast<uint32_t>(ht.size());
+    n_inst_tiled = static_cast<uint32_t>(hit.size());
+    if (n_inst_tiled) PCG_CU(ctx, cudaMemcpyAsync(inst_tile.p, hit.data(), hit.size() * sizeof(uint32_t),
+                                                  cudaMemcpyHostToDevice, ctx->stream));
+    uint32_t max_vox = 1;
+    for (const CellInst& ci : h_inst) max_vox = std::max(max_vox, ci.nx * ci.ny * ci.nz);
+    so_plan(max_vox, &so_passes, &so_bits);
+    if (ntiles) PCG_CU(ctx, cudaMemcpyAsync(tiles.p, ht.data(), ht.size() * sizeof(SegTile), cudaMemcpyHostToDevice,
+                                            ctx->stream));
     PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
     inst_dirty = false;
     return PCG_OK;
@@ -1347,22 +1363,23 @@ int Cells::build_order(uint64_t total_vox)
 {
     PCG_TRY(sync_inst());
     invalid_key = static_cast<uint32_t>(total_vox);
-    key_bits = key_bits_for(total_vox + 1);
-    cudaError_t e = launch_sec_keys(ctx->stream, soa.as<float>(), max_cells, n, cell_inst.as<uint32_t>(),
-                                    inst.as<CellInst>(), has_active ? active.as<uint8_t>() : nullptr, invalid_key,
-                                    keys.as<uint32_t>(), vals.as<uint32_t>());
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion keys");
-    e = radix_sort_pairs(ctx->stream, keys.as<uint32_t>(), vals.as<uint32_t>(), skeys.as<uint32_t>(),
-                         sorder.as<uint32_t>(), ktmp.as<uint32_t>(), vtmp.as<uint32_t>(), n, key_bits, sort_scr.p);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion sort");
-    e = launch_sec_runs(ctx->stream, skeys.as<uint32_t>(), n, inst.as<CellInst>(), static_cast<uint32_t>(h_inst.size()),
-                        invalid_key, ktmp.as<uint32_t>(), sbeg.as<uint32_t>(), vals.as<uint32_t>(), vtmp.as<uint32_t>(),
-                        run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), run_scr.p);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion runs");
-    ctx->launches += 1 + radix_sort_launches(n, key_bits) + 2 + scan_launches(static_cast<uint64_t>(n) + 1);
+    cudaError_t e = launch_sec_order(ctx->stream, tiles.as<SegTile>(), ntiles, inst_tile.as<uint32_t>(), n_inst_tiled,
+                                     n, so_passes, so_bits, soa.as<float>(),
+                                     max_cells, inst.as<CellInst>(), has_active ? active.as<uint8_t>() : nullptr,
+                                     cell_inst.as<uint32_t>(), invalid_key, keys.as<uint32_t>(), ktmp.as<uint32_t>(),
+                                     vtmp.as<uint32_t>(), skeys.as<uint32_t>(), sorder.as<uint32_t>(), sort_scr.p,
+                                     ktmp.as<uint32_t>(), vals.as<uint32_t>(), vtmp.as<uint32_t>(),
+                                     run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), run_scr.p);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion order");
+    ctx->launches += so_launches(ntiles, so_passes, n);
     order_dirty = false;
     if (coef_dt >= 0.0) PCG_TRY(sorted_constants());   // constants follow the order
     return PCG_OK;
+}
+
+int Cells::order_launches() const
+{
+    return so_launches(ntiles, so_passes, n) + (n ? 1 : 0);
 }
 
 int Cells::sorted_constants()
@@ -1377,9 +1394,9 @@ int Cells::sorted_constants()
         if (n) ctx->launches++;
         coef_dirty = false;
     }
-    e = launch_sec_permute(ctx->stream, skeys.as<uint32_t>(), sorder.as<uint32_t>(), n, inst.as<CellInst>(),
-                           static_cast<uint32_t>(h_inst.size()), sbeg.as<uint32_t>(), invalid_key,
-                           coef_cells.as<double>(), cap, coef.as<double>());
+    e = launch_sec_permute(ctx->stream, skeys.as<uint32_t>(), sorder.as<uint32_t>(), n, cell_inst.as<uint32_t>(),
+                           inst.as<CellInst>(), invalid_key, coef_flags.as<uint32_t>(), coef_cells.as<double>(), cap,
+                           coef.as<double>());
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion permute");
     if (n) ctx->launches++;
     return PCG_OK;
@@ -1414,7 +1431,8 @@ uint64_t Cells::device_bytes() const
 {
     return inst.bytes + soa.bytes + pos64.bytes + cell_inst.bytes + rates.bytes + coef.bytes + coef_cells.bytes + coef_flags.bytes + active.bytes +
            keys.bytes + vals.bytes +
-           skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + sbeg.bytes + run_scr.bytes +
+           skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + tiles.bytes + inst_tile.bytes +
+           run_scr.bytes +
            run_dens.bytes + run_slot.bytes;
 }
 

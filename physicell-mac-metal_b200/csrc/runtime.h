@@ -271,16 +271,21 @@ public:
     bool has_active = false;
     bool inst_dirty = true, coef_dirty = true, order_dirty = true;
     double coef_dt = -1.0;
-    // secretion ordering: keys/vals sort input, (skeys, sorder) the order;
-    // after the sort ktmp holds the run index of every position (+ count),
-    // vals the run starts and vtmp the run instances; coef the constants
-    // in sorted order (c0, c1, c2 arrays), coef_cells the same constants in
-    // cell order (the three of a rate slot together; coef_dirty: stale) and
-    // coef_flags which of c0 / c1 each instance has
-    DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr, sbeg, run_scr;
+    // secretion ordering (launch_sec_order): keys the first pass's keys in
+    // cell order, (skeys, sorder) the order, ktmp / vtmp the passes' work
+    // arrays; after the sort ktmp holds the run index of every position
+    // (+ count), vals the run starts and vtmp the run instances; coef the
+    // constants in sorted order (c0, c1, c2 arrays), coef_cells the same
+    // constants in cell order (coef_dirty: stale) and coef_flags which of
+    // c0 / c1 each instance has.  tiles: the instances' 2048-cell tiles
+    // (rebuilt with the instance table), so_passes x so_bits the digits.
+    DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr, run_scr, tiles, inst_tile;
     DevBuf run_dens, run_slot;   // per run: density element of its voxel, rate slot of its first cell
     uint32_t invalid_key = 0;
-    int key_bits = 0;
+    uint32_t ntiles = 0, max_tiles = 0, n_inst_tiled = 0;
+    int so_passes = 1, so_bits = 0;
+    // kernel launches of one build_order (with the constants' permutation)
+    int order_launches() const;
 
     int create(pcg_ctx* c, uint32_t max_cells, uint32_t rate_capacity, uint32_t n_instances);
     int sync_inst();

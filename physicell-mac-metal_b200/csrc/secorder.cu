@@ -1,0 +1,387 @@
+// secorder.cu — the secretion order (sm_100a): every instance's cells sorted
+// by (diffusion voxel, cell index), rebuilt whenever voxel indices change
+// (after every mechanics step when they are refreshed).
+//
+// processSecretion (cell_phenotype.cpp:526-564) runs cell by cell in the
+// reference; the order of the cells that share a voxel decides the FP32
+// roundings, so the device applies each voxel's cells in ascending index.
+//
+// The order is a stable LSD radix sort of each instance's cells on the
+// cell's voxel index within its own grid (at most 21 bits for a 120^3 grid,
+// so three passes of 7-bit digits), segmented by instance: tiles of 2048
+// cells never straddle two instances, so every instance's cells stay in the
+// instance's own range [cell_off, cell_off + n_cells) and the places of one
+// instance's (digit, tile) runs depend on that instance's counts alone.
+// A cell that takes no part in secretion (inactive, voxel index outside the
+// grid, no substrates) has the extra digit R of every pass, so it ends up
+// after the instance's secreting cells, in index order.
+//
+// One pass:
+//   k_so_hist     per tile: digit counts, one row of R + 1 per tile (the
+//                 first pass also computes the keys from the SoA and stores
+//                 them in cell order)
+//   k_so_offsets  per instance: digit totals over its tiles, their scan from
+//                 cell_off, then each tile's row turned into the first place
+//                 of each of its digit runs (digit-major, tiles in order)
+//   k_so_scatter  per tile: stable ranks (each warp ranks its 256 keys with
+//                 __match_any_sync and its own running digit counts, warps
+//                 combined in order), the tile laid out in shared
+//                 memory in digit order, then written so that consecutive
+//                 threads store consecutive elements of one digit's run; the
+//                 last pass writes global keys (vox_base + index, or the
+//                 invalid key).
+// The run list of the order follows: a run is the cells of one voxel, and
+// each instance's non-secreting cells form one run marked kNoRunInst.
+#include "pcg_kernels.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace pcg {
+
+namespace {
+constexpr int kThreads = 256;
+constexpr int kItems = 8;
+constexpr uint32_t kTile = kThreads * kItems;   // 2048 cells per tile
+constexpr int kWarps = kThreads / 32;
+constexpr uint32_t kInvalid = 0xFFFFFFFFu;      // local key of a non-secreting cell
+constexpr int kMaxDigitBits = 8;
+constexpr uint32_t kMaxBins = (1u << kMaxDigitBits) + 1;   // digits + the non-secreting bin
+}  // namespace
+
+__device__ __forceinline__ uint32_t so_digit(uint32_t key, int shift, uint32_t R)
+{
+    return key == kInvalid ? R : (key >> shift) & (R - 1u);
+}
+
+// Digit counts of one tile; the first pass computes each cell's local key
+// (its voxel index, or kInvalid) from the SoA and stores it in cell order.
+template <bool FIRST>
+__global__ void __launch_bounds__(kThreads) k_so_hist(const SegTile* __restrict__ tiles, const float* __restrict__ soa,
+                                                      uint32_t stride, const CellInst* __restrict__ insts,
+                                                      const uint8_t* __restrict__ active, uint32_t* __restrict__ keys,
+                                                      int shift, uint32_t R, uint32_t* __restrict__ hist)
+{
+    __shared__ uint32_t cnt[kMaxBins];
+    const SegTile tl = tiles[blockIdx.x];
+    for (uint32_t d = threadIdx.x; d <= R; d += kThreads) cnt[d] = 0;
+    __syncthreads();
+    const CellInst& in = insts[tl.inst];
+    const uint32_t nv = in.nx * in.ny * in.nz;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const uint32_t t = k * kThreads + threadIdx.x;
+        if (t >= tl.count) continue;
+        const uint32_t i = tl.first + t;
+        uint32_t key;
+        if (FIRST) {
+            const uint32_t v = __float_as_uint(soa[static_cast<size_t>(F_VOXEL_IDX) * stride + i]);
+            const bool ok = (active == nullptr || active[i] != 0) && v < nv && in.S > 0;
+            key = ok ? v : kInvalid;
+            keys[i] = key;
+        } else {
+            key = keys[i];
+        }
+        atomicAdd(&cnt[so_digit(key, shift, R)], 1u);
+    }
+    __syncthreads();
+    for (uint32_t d = threadIdx.x; d <= R; d += kThreads) hist[static_cast<size_t>(R + 1) * blockIdx.x + d] = cnt[d];
+}
+
+// Exclusive scan of one instance's counts in (digit, tile) order, in place:
+// hist row t (R + 1 counts of tile t) becomes the first place of each of
+// the tile's digit runs.  One block per instance with cells (inst_tile[b]
+// = its first tile); thread j covers digits j, j + 256, ...
+constexpr int kOffThreads = 256;
+__global__ void __launch_bounds__(kOffThreads, 1) k_so_offsets(const SegTile* __restrict__ tiles,
+                                                            const uint32_t* __restrict__ inst_tile,
+                                                            const CellInst* __restrict__ insts, uint32_t R,
+                                                            uint32_t* __restrict__ hist)
+{
+    __shared__ uint32_t wsum[kOffThreads / 32];
+    const SegTile t0 = tiles[inst_tile[blockIdx.x]];
+    const uint32_t nb = R + 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr uint32_t kPer = (kMaxBins + kOffThreads - 1) / kOffThreads;   // digits per thread
+    uint32_t tot[kPer];
+    uint32_t* base = hist + static_cast<size_t>(nb) * t0.tb;
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+        const uint32_t d = threadIdx.x + k * kOffThreads;
+        uint32_t s = 0;
+        if (d < nb)
+            for (uint32_t t = 0; t < t0.nt; ++t) s += base[static_cast<size_t>(t) * nb + d];
+        tot[k] = s;
+    }
+    // digits in order: digit d = threadIdx.x + k * 256, so the scan runs
+    // over k-major blocks of 256 digits
+    uint32_t run = insts[t0.inst].cell_off;
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+        uint32_t incl = tot[k];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t before = 0, all = 0;
+        for (int w = 0; w < kOffThreads / 32; ++w) {
+            const uint32_t x = wsum[w];
+            before += w < warp ? x : 0u;
+            all += x;
+        }
+        __syncthreads();
+        const uint32_t d = threadIdx.x + k * kOffThreads;
+        if (d < nb) {
+            uint32_t at = run + before + incl - tot[k];
+            for (uint32_t t = 0; t < t0.nt; ++t) {
+                uint32_t* h = base + static_cast<size_t>(t) * nb + d;
+                const uint32_t c = *h;
+                *h = at;
+                at += c;
+            }
+        }
+        run += all;
+    }
+}
+
+template <bool FIRST, bool LAST>
+__global__ void __launch_bounds__(kThreads) k_so_scatter(const SegTile* __restrict__ tiles,
+                                                         const uint32_t* __restrict__ kin,
+                                                         const uint32_t* __restrict__ vin,
+                                                         uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                         int shift, uint32_t R, const uint32_t* __restrict__ offs,
+                                                         const CellInst* __restrict__ insts, uint32_t invalid_key)
+{
+    __shared__ uint32_t wcnt[kWarps][kMaxBins];
+    __shared__ uint32_t cnt[kMaxBins];
+    __shared__ uint32_t tbase[kMaxBins];
+    __shared__ uint32_t gbase[kMaxBins];
+    __shared__ uint32_t sk[kTile], sv[kTile];
+    __shared__ uint32_t wsum[kWarps + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const SegTile tl = tiles[blockIdx.x];
+    for (uint32_t d = threadIdx.x; d <= R; d += kThreads) {
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) wcnt[w][d] = 0;
+        gbase[d] = offs[static_cast<size_t>(R + 1) * blockIdx.x + d];
+    }
+    uint32_t kk[kItems], vv[kItems], rk[kItems], dg[kItems];
+#pragma unroll
+    for (int r = 0; r < kItems; ++r) {
+        const uint32_t t = warp * (32 * kItems) + r * 32 + lane;
+        const bool ok = t < tl.count;
+        const uint32_t i = tl.first + t;
+        kk[r] = ok ? kin[i] : 0u;
+        vv[r] = ok ? (FIRST ? i : vin[i]) : 0u;
+        dg[r] = ok ? so_digit(kk[r], shift, R) : R + 1u;   // R + 1 marks an empty lane
+    }
+    __syncthreads();
+    // stable ranks within each warp's 256 keys, against the warp's own counts
+    const uint32_t lt_mask = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < kItems; ++r) {
+        const uint32_t peers = __match_any_sync(0xffffffffu, dg[r]);
+        const bool ok = dg[r] <= R;
+        rk[r] = (ok ? wcnt[warp][dg[r]] : 0u) + __popc(peers & lt_mask);
+        __syncwarp();
+        if (ok && lane == __ffs(peers) - 1) wcnt[warp][dg[r]] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // warps in order: each warp's counts become its first place within the digit
+    for (uint32_t d = threadIdx.x; d <= R; d += kThreads) {
+        uint32_t sum = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = wcnt[w][d];
+            wcnt[w][d] = sum;
+            sum += c;
+        }
+        cnt[d] = sum;
+    }
+    __syncthreads();
+    // exclusive scan of the tile's digit counts: thread t covers a run of
+    // consecutive digits
+    {
+        const uint32_t per = (R + 1u + kThreads - 1u) / kThreads;
+        const uint32_t d0 = threadIdx.x * per;
+        uint32_t sum = 0;
+        for (uint32_t d = d0; d < d0 + per && d <= R; ++d) sum += cnt[d];
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t before = 0;
+        for (int w = 0; w < warp; ++w) before += wsum[w];
+        uint32_t run = before + incl - sum;
+        for (uint32_t d = d0; d < d0 + per && d <= R; ++d) {
+            tbase[d] = run;
+            run += cnt[d];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kItems; ++r) {
+        if (dg[r] <= R) {
+            const uint32_t t = tbase[dg[r]] + wcnt[warp][dg[r]] + rk[r];
+            sk[t] = kk[r];
+            sv[t] = vv[r];
+        }
+    }
+    __syncthreads();
+    uint32_t vox_base = 0;
+    if (LAST) vox_base = insts[tl.inst].vox_base;
+    for (uint32_t t = threadIdx.x; t < tl.count; t += kThreads) {
+        const uint32_t k = sk[t];
+        const uint32_t d = so_digit(k, shift, R);
+        const uint32_t dst = gbase[d] + (t - tbase[d]);
+        kout[dst] = LAST ? (k == kInvalid ? invalid_key : vox_base + k) : k;
+        vout[dst] = sv[t];
+    }
+}
+
+// Runs of the order: a run starts where the key changes (each instance's
+// non-secreting cells, key invalid_key, form one run).  heads has n + 1
+// entries (heads[n] = 0).
+__global__ void k_so_heads(const uint32_t* __restrict__ skeys, uint32_t n, uint32_t* __restrict__ heads)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > n) return;
+    heads[p] = p < n && (p == 0 || skeys[p - 1] != skeys[p]) ? 1u : 0u;
+}
+
+// rid = exclusive scan of heads: run r starts at run_start[r] and ends at
+// run_start[r + 1] (run_start[n_runs] = n).  A run of secreting cells gets
+// its instance, the density element of its voxel (substrate 0, padded
+// rows) and the rate slot of its first cell; a run of non-secreting cells
+// gets kNoRunInst.
+__global__ void k_so_runs(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder, uint32_t n,
+                          uint32_t invalid_key, const uint32_t* __restrict__ rid,
+                          const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
+                          uint32_t* __restrict__ run_start, uint32_t* __restrict__ run_inst,
+                          uint64_t* __restrict__ run_dens, uint32_t* __restrict__ run_slot)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > n) return;
+    if (p == n) {
+        run_start[rid[n]] = n;
+        return;
+    }
+    const uint32_t key = skeys[p];
+    if (p > 0 && skeys[p - 1] == key) return;
+    const uint32_t r = rid[p];
+    run_start[r] = p;
+    if (key >= invalid_key) {
+        run_inst[r] = kNoRunInst;
+        return;
+    }
+    const uint32_t ii = cell_inst[sorder[p]];
+    const CellInst& in = insts[ii];
+    const uint32_t v = key - in.vox_base;
+    run_inst[r] = ii;
+    run_dens[r] = in.dens_off + static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
+    run_slot[r] = in.rate_off + (p - in.cell_off) * in.S;
+}
+
+// ------------------------------------------------------------------ host
+
+void so_plan(uint32_t max_local_voxels, int* passes, int* digit_bits)
+{
+    int bits = 0;
+    while ((1ull << bits) < max_local_voxels) ++bits;
+    const int p = bits == 0 ? 1 : (bits + kMaxDigitBits - 1) / kMaxDigitBits;
+    *passes = p;
+    *digit_bits = (bits + p - 1) / p;
+}
+
+uint32_t so_max_tiles(uint32_t max_cells, uint32_t n_inst) { return max_cells / kTile + n_inst + 1; }
+
+void so_tiles(const CellInst* inst, uint32_t n_inst, std::vector<SegTile>& out, std::vector<uint32_t>& inst_tile)
+{
+    out.clear();
+    inst_tile.clear();
+    for (uint32_t i = 0; i < n_inst; ++i) {
+        const uint32_t nt = (inst[i].n_cells + kTile - 1) / kTile;
+        const uint32_t tb = static_cast<uint32_t>(out.size());
+        if (nt) inst_tile.push_back(tb);
+        for (uint32_t t = 0; t < nt; ++t) {
+            SegTile s{};
+            s.first = inst[i].cell_off + t * kTile;
+            s.count = std::min(kTile, inst[i].n_cells - t * kTile);
+            s.inst = i;
+            s.tb = tb;
+            s.nt = nt;
+            out.push_back(s);
+        }
+    }
+}
+
+size_t so_scratch_bytes(uint32_t max_tiles)
+{
+    return static_cast<size_t>(max_tiles) * kMaxBins * sizeof(uint32_t);
+}
+
+int so_launches(uint32_t ntiles, int passes, uint32_t n)
+{
+    if (n == 0 || ntiles == 0) return 0;
+    return passes * 3 + 2 + scan_launches(static_cast<uint64_t>(n) + 1);
+}
+
+cudaError_t launch_sec_order(cudaStream_t st, const SegTile* tiles, uint32_t ntiles, const uint32_t* inst_tile,
+                             uint32_t n_inst_tiled, uint32_t n, int passes,
+                             int digit_bits, const float* soa, uint32_t stride, const CellInst* insts,
+                             const uint8_t* active, const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* keys,
+                             uint32_t* ktmp, uint32_t* vtmp, uint32_t* skeys, uint32_t* sorder, void* scratch,
+                             uint32_t* heads_rid, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
+                             uint32_t* run_slot, void* run_scratch)
+{
+    if (n == 0 || ntiles == 0) return cudaSuccess;
+    if (digit_bits > kMaxDigitBits || passes < 1) return cudaErrorInvalidValue;
+    const uint32_t R = 1u << digit_bits;
+    uint32_t* hist = static_cast<uint32_t*>(scratch);
+    const uint32_t* ks = keys;
+    const uint32_t* vs = nullptr;
+    cudaError_t e;
+    for (int p = 0; p < passes; ++p) {
+        const bool first = p == 0, last = p == passes - 1;
+        // the last pass writes (skeys, sorder); earlier ones alternate so that it does
+        const bool to_out = ((passes - 1 - p) & 1) == 0;
+        uint32_t* kd = to_out ? skeys : ktmp;
+        uint32_t* vd = to_out ? sorder : vtmp;
+        const int shift = p * digit_bits;
+        if (first)
+            k_so_hist<true><<<ntiles, kThreads, 0, st>>>(tiles, soa, stride, insts, active, keys, shift, R, hist);
+        else
+            k_so_hist<false><<<ntiles, kThreads, 0, st>>>(tiles, soa, stride, insts, active, const_cast<uint32_t*>(ks),
+                                                           shift, R, hist);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        k_so_offsets<<<n_inst_tiled, kOffThreads, 0, st>>>(tiles, inst_tile, insts, R, hist);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+#define PCG_SO_SCATTER(F, L) \
+    k_so_scatter<F, L><<<ntiles, kThreads, 0, st>>>(tiles, ks, vs, kd, vd, shift, R, hist, insts, invalid_key)
+        if (first && last) PCG_SO_SCATTER(true, true);
+        else if (first) PCG_SO_SCATTER(true, false);
+        else if (last) PCG_SO_SCATTER(false, true);
+        else PCG_SO_SCATTER(false, false);
+#undef PCG_SO_SCATTER
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        ks = kd;
+        vs = vd;
+    }
+    k_so_heads<<<(n + 1 + 255) / 256, 256, 0, st>>>(skeys, n, heads_rid);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = scan_exclusive(st, heads_rid, heads_rid, static_cast<uint64_t>(n) + 1, run_scratch)) != cudaSuccess)
+        return e;
+    k_so_runs<<<(n + 1 + 255) / 256, 256, 0, st>>>(skeys, sorder, n, invalid_key, heads_rid, cell_inst, insts,
+                                                    run_start, run_inst, run_dens, run_slot);
+    return cudaGetLastError();
+}
+
+}  // namespace pcg
