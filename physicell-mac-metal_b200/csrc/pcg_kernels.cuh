@@ -305,20 +305,23 @@ uint32_t so_max_tiles(uint32_t max_cells, uint32_t n_inst);
 void so_tiles(const CellInst* inst, uint32_t n_inst, std::vector<SegTile>& out, std::vector<uint32_t>& inst_tile);
 size_t so_scratch_bytes(uint32_t max_tiles);
 int so_launches(uint32_t ntiles, int passes, uint32_t n);
+size_t so_run_scratch_bytes(uint32_t max_cells);
 // Keys, the sort and the run list in one call.  Outputs: skeys (global
 // voxel key vox_base + index, or invalid_key) and sorder (cell) per sorted
-// position; heads_rid (n + 1: the run index of every position, [n] = run
-// count); run_start (n + 1), run_inst, run_dens, run_slot per run.  keys,
-// ktmp and vtmp are n-entry work arrays (heads_rid may be ktmp and run_inst
-// vtmp); scratch: so_scratch_bytes, run_scratch: scan_scratch_bytes(n + 1);
-// inst_tile: the n_inst_tiled entries of so_tiles.
+// position; *n_runs; run_start (n + 1), run_inst, run_dens, run_slot per
+// run.  keys, ktmp and vtmp are n-entry work arrays (run_inst may be vtmp);
+// scratch: so_scratch_bytes, run_scratch: so_run_scratch_bytes; inst_tile:
+// the n_inst_tiled entries of so_tiles.  With cc non-null the last pass
+// also permutes the constants (cc in cell order, three arrays of cap) into
+// the order's slots (cs), as launch_sec_permute does.
 cudaError_t launch_sec_order(cudaStream_t st, const SegTile* tiles, uint32_t ntiles, const uint32_t* inst_tile,
                              uint32_t n_inst_tiled, uint32_t n, int passes,
                              int digit_bits, const float* soa, uint32_t stride, const CellInst* insts,
                              const uint8_t* active, const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* keys,
                              uint32_t* ktmp, uint32_t* vtmp, uint32_t* skeys, uint32_t* sorder, void* scratch,
-                             uint32_t* heads_rid, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
-                             uint32_t* run_slot, void* run_scratch);
+                             uint32_t* n_runs, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
+                             uint32_t* run_slot, void* run_scratch, const double* cc, double* cs, uint32_t cap,
+                             const uint32_t* flags);
 
 // Radix sort of (key, value) pairs, stable, 'bits' significant key bits.
 // Scratch from radix_sort_scratch_bytes().  Result lands in (k_out, v_out).

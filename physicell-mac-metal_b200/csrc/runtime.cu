@@ -1240,7 +1240,7 @@ int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_
     PCG_CU(ctx, tiles.alloc(static_cast<size_t>(max_tiles) * sizeof(SegTile)));
     PCG_CU(ctx, inst_tile.alloc(h_inst.size() * sizeof(uint32_t)));
     PCG_CU(ctx, sort_scr.alloc(so_scratch_bytes(max_tiles)));
-    PCG_CU(ctx, run_scr.alloc(scan_scratch_bytes(static_cast<uint64_t>(max_cells) + 1)));
+    PCG_CU(ctx, run_scr.alloc(so_run_scratch_bytes(max_cells)));
     PCG_CU(ctx, cudaMemsetAsync(ktmp.p, 0, ktmp.bytes, ctx->stream));   // run count 0 until the first order
     inst_dirty = coef_dirty = order_dirty = true;
     return PCG_OK;
@@ -1363,40 +1363,49 @@ int Cells::build_order(uint64_t total_vox)
 {
     PCG_TRY(sync_inst());
     invalid_key = static_cast<uint32_t>(total_vox);
+    // with the constants known, the sort's last pass moves them into the order
+    const bool consts = coef_dt >= 0.0;
+    const uint32_t cap = static_cast<uint32_t>(rates.bytes / (4 * sizeof(double)));
+    if (consts) PCG_TRY(cell_constants(cap));
     cudaError_t e = launch_sec_order(ctx->stream, tiles.as<SegTile>(), ntiles, inst_tile.as<uint32_t>(), n_inst_tiled,
                                      n, so_passes, so_bits, soa.as<float>(),
                                      max_cells, inst.as<CellInst>(), has_active ? active.as<uint8_t>() : nullptr,
                                      cell_inst.as<uint32_t>(), invalid_key, keys.as<uint32_t>(), ktmp.as<uint32_t>(),
                                      vtmp.as<uint32_t>(), skeys.as<uint32_t>(), sorder.as<uint32_t>(), sort_scr.p,
-                                     ktmp.as<uint32_t>(), vals.as<uint32_t>(), vtmp.as<uint32_t>(),
-                                     run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), run_scr.p);
+                                     ktmp.as<uint32_t>() + n, vals.as<uint32_t>(), vtmp.as<uint32_t>(),
+                                     run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), run_scr.p,
+                                     consts ? coef_cells.as<double>() : nullptr, coef.as<double>(), cap,
+                                     coef_flags.as<uint32_t>());
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion order");
     ctx->launches += so_launches(ntiles, so_passes, n);
     order_dirty = false;
-    if (coef_dt >= 0.0) PCG_TRY(sorted_constants());   // constants follow the order
+    return PCG_OK;
+}
+
+int Cells::cell_constants(uint32_t cap)
+{
+    if (!coef_dirty) return PCG_OK;
+    cudaError_t e = launch_sec_cell_consts(ctx->stream, soa.as<float>(), max_cells, n, cell_inst.as<uint32_t>(),
+                                           inst.as<CellInst>(), rates.as<double>(), cap, coef_dt, coef_cells.as<double>(),
+                                           coef_flags.as<uint32_t>(), static_cast<uint32_t>(h_inst.size()));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion constants");
+    if (n) ctx->launches++;
+    coef_dirty = false;
     return PCG_OK;
 }
 
 int Cells::order_launches() const
 {
-    return so_launches(ntiles, so_passes, n) + (n ? 1 : 0);
+    return so_launches(ntiles, so_passes, n);
 }
 
 int Cells::sorted_constants()
 {
     const uint32_t cap = static_cast<uint32_t>(rates.bytes / (4 * sizeof(double)));
-    cudaError_t e;
-    if (coef_dirty) {
-        e = launch_sec_cell_consts(ctx->stream, soa.as<float>(), max_cells, n, cell_inst.as<uint32_t>(),
-                                   inst.as<CellInst>(), rates.as<double>(), cap, coef_dt, coef_cells.as<double>(),
-                                   coef_flags.as<uint32_t>(), static_cast<uint32_t>(h_inst.size()));
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion constants");
-        if (n) ctx->launches++;
-        coef_dirty = false;
-    }
-    e = launch_sec_permute(ctx->stream, skeys.as<uint32_t>(), sorder.as<uint32_t>(), n, cell_inst.as<uint32_t>(),
-                           inst.as<CellInst>(), invalid_key, coef_flags.as<uint32_t>(), coef_cells.as<double>(), cap,
-                           coef.as<double>());
+    PCG_TRY(cell_constants(cap));
+    cudaError_t e = launch_sec_permute(ctx->stream, skeys.as<uint32_t>(), sorder.as<uint32_t>(), n,
+                                       cell_inst.as<uint32_t>(), inst.as<CellInst>(), invalid_key,
+                                       coef_flags.as<uint32_t>(), coef_cells.as<double>(), cap, coef.as<double>());
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion permute");
     if (n) ctx->launches++;
     return PCG_OK;

@@ -284,8 +284,10 @@ public:
     uint32_t invalid_key = 0;
     uint32_t ntiles = 0, max_tiles = 0, n_inst_tiled = 0;
     int so_passes = 1, so_bits = 0;
-    // kernel launches of one build_order (with the constants' permutation)
+    // kernel launches of one build_order (constants already in cell order)
     int order_launches() const;
+    // the constants in cell order, when stale (cap: rate capacity)
+    int cell_constants(uint32_t cap);
 
     int create(pcg_ctx* c, uint32_t max_cells, uint32_t rate_capacity, uint32_t n_instances);
     int sync_inst();

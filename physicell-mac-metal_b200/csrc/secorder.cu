@@ -153,7 +153,9 @@ __global__ void __launch_bounds__(kThreads) k_so_scatter(const SegTile* __restri
                                                          const uint32_t* __restrict__ vin,
                                                          uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                          int shift, uint32_t R, const uint32_t* __restrict__ offs,
-                                                         const CellInst* __restrict__ insts, uint32_t invalid_key)
+                                                         const CellInst* __restrict__ insts, uint32_t invalid_key,
+                                                         const double* __restrict__ cc, double* __restrict__ cs,
+                                                         uint32_t cap, const uint32_t* __restrict__ flags)
 {
     __shared__ uint32_t wcnt[kWarps][kMaxBins];
     __shared__ uint32_t cnt[kMaxBins];
@@ -236,58 +238,138 @@ __global__ void __launch_bounds__(kThreads) k_so_scatter(const SegTile* __restri
         }
     }
     __syncthreads();
-    uint32_t vox_base = 0;
-    if (LAST) vox_base = insts[tl.inst].vox_base;
+    const CellInst& in = insts[tl.inst];
+    const uint32_t vox_base = LAST ? in.vox_base : 0u;
+    // the last pass also moves the secretion constants of every secreting
+    // cell (cc, in cell order) to its place in the order (cs): rate slot
+    // rate_off + (place - cell_off) * S; c0 / c1 only where the instance
+    // has them (flags)
+    const bool consts = LAST && cc != nullptr;
+    const uint32_t S = in.S, f = consts ? flags[tl.inst] : 0u;
     for (uint32_t t = threadIdx.x; t < tl.count; t += kThreads) {
         const uint32_t k = sk[t];
         const uint32_t d = so_digit(k, shift, R);
         const uint32_t dst = gbase[d] + (t - tbase[d]);
+        const uint32_t g = sv[t];
         kout[dst] = LAST ? (k == kInvalid ? invalid_key : vox_base + k) : k;
-        vout[dst] = sv[t];
+        vout[dst] = g;
+        if (consts && k != kInvalid) {
+            const uint64_t src = in.rate_off + static_cast<uint64_t>(g - in.cell_off) * S;
+            const uint64_t to = in.rate_off + static_cast<uint64_t>(dst - in.cell_off) * S;
+            if (S == 2 && f == 0) {   // the common uptake-only case: c2 of both substrates
+                const double a = cc[2ull * cap + src], b = cc[2ull * cap + src + 1];
+                cs[2ull * cap + to] = a;
+                cs[2ull * cap + to + 1] = b;
+            } else {
+                for (uint32_t q = 0; q < S; ++q) {
+                    if (f & 1u) cs[to + q] = cc[src + q];
+                    if (f & 2u) cs[cap + to + q] = cc[cap + src + q];
+                    cs[2ull * cap + to + q] = cc[2ull * cap + src + q];
+                }
+            }
+        }
     }
 }
 
 // Runs of the order: a run starts where the key changes (each instance's
-// non-secreting cells, key invalid_key, form one run).  heads has n + 1
-// entries (heads[n] = 0).
-__global__ void k_so_heads(const uint32_t* __restrict__ skeys, uint32_t n, uint32_t* __restrict__ heads)
+// non-secreting cells, key invalid_key, form one run).  Positions go in
+// tiles of 2048, position base + k * 256 + t to thread t (k = 0..7), so
+// every warp access is contiguous: k_so_run_count counts each tile's run
+// heads, their exclusive scan gives each tile its first run index, and
+// k_so_run_write numbers the tile's heads (ballots, then the 64 warp-row
+// counts in order) and writes the runs.  Run r starts at run_start[r] and
+// ends at run_start[r + 1] (run_start[n_runs] = n, *n_runs = the count).
+// A run of secreting cells gets its instance, the density element of its
+// voxel (substrate 0, padded rows) and the rate slot of its first cell; a
+// run of non-secreting cells gets kNoRunInst.
+__device__ __forceinline__ bool so_head(const uint32_t* __restrict__ skeys, uint32_t n, uint32_t p, uint32_t* key)
 {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p > n) return;
-    heads[p] = p < n && (p == 0 || skeys[p - 1] != skeys[p]) ? 1u : 0u;
+    if (p >= n) return false;
+    *key = skeys[p];
+    return p == 0 || skeys[p - 1] != *key;
 }
 
-// rid = exclusive scan of heads: run r starts at run_start[r] and ends at
-// run_start[r + 1] (run_start[n_runs] = n).  A run of secreting cells gets
-// its instance, the density element of its voxel (substrate 0, padded
-// rows) and the rate slot of its first cell; a run of non-secreting cells
-// gets kNoRunInst.
-__global__ void k_so_runs(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sorder, uint32_t n,
-                          uint32_t invalid_key, const uint32_t* __restrict__ rid,
-                          const uint32_t* __restrict__ cell_inst, const CellInst* __restrict__ insts,
-                          uint32_t* __restrict__ run_start, uint32_t* __restrict__ run_inst,
-                          uint64_t* __restrict__ run_dens, uint32_t* __restrict__ run_slot)
+__global__ void __launch_bounds__(kThreads) k_so_run_count(const uint32_t* __restrict__ skeys, uint32_t n,
+                                                           uint32_t* __restrict__ tile_cnt)
 {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p > n) return;
-    if (p == n) {
-        run_start[rid[n]] = n;
-        return;
+    __shared__ uint32_t ws[kWarps];
+    uint32_t c = 0, key;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) c += so_head(skeys, n, blockIdx.x * kTile + k * kThreads + threadIdx.x, &key);
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) t += ws[w];
+        tile_cnt[blockIdx.x] = t;
     }
-    const uint32_t key = skeys[p];
-    if (p > 0 && skeys[p - 1] == key) return;
-    const uint32_t r = rid[p];
-    run_start[r] = p;
-    if (key >= invalid_key) {
-        run_inst[r] = kNoRunInst;
-        return;
+}
+
+__global__ void __launch_bounds__(kThreads) k_so_run_write(const uint32_t* __restrict__ skeys,
+                                                           const uint32_t* __restrict__ sorder, uint32_t n,
+                                                           uint32_t invalid_key, const uint32_t* __restrict__ tile_off,
+                                                           const uint32_t* __restrict__ tile_cnt, uint32_t ntiles,
+                                                           const uint32_t* __restrict__ cell_inst,
+                                                           const CellInst* __restrict__ insts,
+                                                           uint32_t* __restrict__ run_start, uint32_t* __restrict__ run_inst,
+                                                           uint64_t* __restrict__ run_dens, uint32_t* __restrict__ run_slot,
+                                                           uint32_t* __restrict__ n_runs)
+{
+    __shared__ uint32_t wc[kItems * kWarps];   // heads per (row k, warp), then their exclusive scan
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint32_t key[kItems], hb = 0, rank[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const bool h = so_head(skeys, n, blockIdx.x * kTile + k * kThreads + threadIdx.x, &key[k]);
+        const uint32_t b = __ballot_sync(0xffffffffu, h);
+        hb |= (h ? 1u : 0u) << k;
+        rank[k] = __popc(b & lt_mask);
+        if (lane == 0) wc[k * kWarps + warp] = __popc(b);
     }
-    const uint32_t ii = cell_inst[sorder[p]];
-    const CellInst& in = insts[ii];
-    const uint32_t v = key - in.vox_base;
-    run_inst[r] = ii;
-    run_dens[r] = in.dens_off + static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
-    run_slot[r] = in.rate_off + (p - in.cell_off) * in.S;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = tile_off[blockIdx.x];
+        for (int i = 0; i < kItems * kWarps; ++i) {
+            const uint32_t c = wc[i];
+            wc[i] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    uint32_t ii8[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const bool sec = ((hb >> k) & 1u) && key[k] < invalid_key;
+        ii8[k] = sec ? sorder[blockIdx.x * kTile + k * kThreads + threadIdx.x] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const bool sec = ((hb >> k) & 1u) && key[k] < invalid_key;
+        ii8[k] = sec ? cell_inst[ii8[k]] : kNoRunInst;
+    }
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        if (!((hb >> k) & 1u)) continue;
+        const uint32_t p = blockIdx.x * kTile + k * kThreads + threadIdx.x;
+        const uint32_t r = wc[k * kWarps + warp] + rank[k];
+        const uint32_t ii = ii8[k];
+        run_start[r] = p;
+        run_inst[r] = ii;
+        if (ii != kNoRunInst) {
+            const CellInst& in = insts[ii];
+            const uint32_t v = key[k] - in.vox_base;
+            run_dens[r] = in.dens_off + static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
+            run_slot[r] = in.rate_off + (p - in.cell_off) * in.S;
+        }
+    }
+    if (blockIdx.x == ntiles - 1 && threadIdx.x == 0) {
+        const uint32_t total = tile_off[blockIdx.x] + tile_cnt[blockIdx.x];
+        run_start[total] = n;
+        *n_runs = total;
+    }
 }
 
 // ------------------------------------------------------------------ host
@@ -328,10 +410,18 @@ size_t so_scratch_bytes(uint32_t max_tiles)
     return static_cast<size_t>(max_tiles) * kMaxBins * sizeof(uint32_t);
 }
 
+static uint32_t run_tiles(uint32_t n) { return (n + kTile - 1) / kTile; }
+
+size_t so_run_scratch_bytes(uint32_t max_cells)
+{
+    const uint64_t rt = run_tiles(max_cells) + 1;
+    return 2 * ((rt * sizeof(uint32_t) + 255) / 256) * 256 + scan_scratch_bytes(rt);
+}
+
 int so_launches(uint32_t ntiles, int passes, uint32_t n)
 {
     if (n == 0 || ntiles == 0) return 0;
-    return passes * 3 + 2 + scan_launches(static_cast<uint64_t>(n) + 1);
+    return passes * 3 + 2 + scan_launches(run_tiles(n));
 }
 
 cudaError_t launch_sec_order(cudaStream_t st, const SegTile* tiles, uint32_t ntiles, const uint32_t* inst_tile,
@@ -339,8 +429,9 @@ cudaError_t launch_sec_order(cudaStream_t st, const SegTile* tiles, uint32_t nti
                              int digit_bits, const float* soa, uint32_t stride, const CellInst* insts,
                              const uint8_t* active, const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* keys,
                              uint32_t* ktmp, uint32_t* vtmp, uint32_t* skeys, uint32_t* sorder, void* scratch,
-                             uint32_t* heads_rid, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
-                             uint32_t* run_slot, void* run_scratch)
+                             uint32_t* n_runs, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
+                             uint32_t* run_slot, void* run_scratch, const double* cc, double* cs, uint32_t cap,
+                             const uint32_t* flags)
 {
     if (n == 0 || ntiles == 0) return cudaSuccess;
     if (digit_bits > kMaxDigitBits || passes < 1) return cudaErrorInvalidValue;
@@ -364,8 +455,9 @@ cudaError_t launch_sec_order(cudaStream_t st, const SegTile* tiles, uint32_t nti
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         k_so_offsets<<<n_inst_tiled, kOffThreads, 0, st>>>(tiles, inst_tile, insts, R, hist);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-#define PCG_SO_SCATTER(F, L) \
-    k_so_scatter<F, L><<<ntiles, kThreads, 0, st>>>(tiles, ks, vs, kd, vd, shift, R, hist, insts, invalid_key)
+#define PCG_SO_SCATTER(F, L)                                                                                    \
+    k_so_scatter<F, L><<<ntiles, kThreads, 0, st>>>(tiles, ks, vs, kd, vd, shift, R, hist, insts, invalid_key, cc, cs, \
+                                                    cap, flags)
         if (first && last) PCG_SO_SCATTER(true, true);
         else if (first) PCG_SO_SCATTER(true, false);
         else if (last) PCG_SO_SCATTER(false, true);
@@ -375,12 +467,15 @@ cudaError_t launch_sec_order(cudaStream_t st, const SegTile* tiles, uint32_t nti
         ks = kd;
         vs = vd;
     }
-    k_so_heads<<<(n + 1 + 255) / 256, 256, 0, st>>>(skeys, n, heads_rid);
+    const uint32_t rt = run_tiles(n);
+    uint32_t* tile_cnt = static_cast<uint32_t*>(run_scratch);
+    uint32_t* tile_off = tile_cnt + ((static_cast<uint64_t>(rt + 1) * sizeof(uint32_t) + 255) / 256) * 256 / sizeof(uint32_t);
+    char* rscr = reinterpret_cast<char*>(tile_off) + ((static_cast<uint64_t>(rt + 1) * sizeof(uint32_t) + 255) / 256) * 256;
+    k_so_run_count<<<rt, kThreads, 0, st>>>(skeys, n, tile_cnt);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = scan_exclusive(st, heads_rid, heads_rid, static_cast<uint64_t>(n) + 1, run_scratch)) != cudaSuccess)
-        return e;
-    k_so_runs<<<(n + 1 + 255) / 256, 256, 0, st>>>(skeys, sorder, n, invalid_key, heads_rid, cell_inst, insts,
-                                                    run_start, run_inst, run_dens, run_slot);
+    if ((e = scan_exclusive(st, tile_cnt, tile_off, rt, rscr)) != cudaSuccess) return e;
+    k_so_run_write<<<rt, kThreads, 0, st>>>(skeys, sorder, n, invalid_key, tile_off, tile_cnt, rt, cell_inst, insts,
+                                             run_start, run_inst, run_dens, run_slot, n_runs);
     return cudaGetLastError();
 }
 
