@@ -195,10 +195,32 @@ def gen_removal():
                         sec=rates[0], upt=rates[1], sat=rates[2], ne=rates[3])
 
 
+def gen_scenario():
+    """The reference's parity scenario parity/scenarios/diffusion_only_2d
+    (.json / .xml): a 20 x 20 grid over [-200, 200]^2 um, dx 20, one
+    substrate (D 1e5, decay 0.1, Dirichlet 38), uniform 38 initially, no
+    cells, dt 0.01 min, 2 min (200 steps), saved every minute.  The fields
+    after 100 and 200 steps come from the reference's own sweeps and
+    applyDirichletBC (Q1 moves the field although it starts at the target)."""
+    nx = ny = 20
+    subs_p = [(1e5, 0.1, True, 38.0)]
+    g = po.make_grid(nx, ny, 1, 1, dx=20.0, dt=0.01, x_min=-200.0, y_min=-200.0)
+    subs = po.make_subs(subs_p)
+    d = np.full(nx * ny, 38.0, np.float32)
+    saved = []
+    for step in range(1, 201):
+        po.ref_sweeps(d, g, subs)
+        po.ref_dirichlet(d, g, subs)
+        if step % 100 == 0:
+            saved.append(d.copy())
+    np.savez_compressed(os.path.join(OUT, "scenario_diffusion_only_2d.npz"), nx=nx, ny=ny,
+                        subs=np.array(subs_p, np.float64), steps=np.array([100, 200]), density=np.stack(saved))
+
+
 if __name__ == "__main__":
     if not po.ref_available():
         sys.exit("oracle/_ref/libpcg_ref.so not built (make -C oracle REF=<reference checkout>)")
-    which = sys.argv[1:] or ["diffusion", "secretion", "mechanics", "motility", "matlab", "removal"]
+    which = sys.argv[1:] or ["diffusion", "secretion", "mechanics", "motility", "matlab", "removal", "scenario"]
     for w in which:
         globals()["gen_" + w]()
     print("golden vectors written to", OUT)

@@ -320,3 +320,41 @@ def test_server_respects_budget(ctx, pcg):
     with pytest.raises(pcg.PcgError):
         tiny.submit(insts[0], 10)          # larger than the whole budget
     tiny.close()
+
+
+def test_inactive_cells_in_a_batch(ctx, pcg, po):
+    """Secretion order with non-secreting cells in every instance (instances
+    of one and of two 2048-cell sort tiles): the inactive cells sort after
+    each instance's active ones as one run that secretion skips.  Batch and
+    alone give the same bits; one instance matches the oracle."""
+    insts = small_mix(pcg, seed=9)
+    rng = np.random.default_rng(19)
+    for inst in insts:
+        act = (rng.random(inst.n_cells) < 0.7).astype(np.uint8)
+        act[:5] = 0   # inactive cells at the start of the instance's range too
+        inst.active = act
+    assert any(inst.n_cells > 2048 for inst in insts)
+    steps = 23
+    together = run_batch(pcg, ctx, insts, steps)
+    for i, inst in enumerate(insts):
+        alone = run_batch(pcg, ctx, [inst], steps)[0]
+        assert np.array_equal(together[i][0].view(np.uint32), alone[0].view(np.uint32)), f"density {i}"
+        assert np.array_equal(together[i][1].view(np.uint32), alone[1].view(np.uint32)), f"cells {i}"
+    i = max(range(len(insts)), key=lambda k: insts[k].n_cells)
+    inst = insts[i]
+    g = inst.grid
+    S, n = g.n_substrates, inst.n_cells
+    og = po.make_grid(g.nx, g.ny, g.nz, S, dx=g.dx, dt=g.dt, x_min=g.x_min, y_min=g.y_min, z_min=g.z_min)
+    osubs = po.make_subs([(s.diffusion_coefficient, s.decay_rate, bool(s.dirichlet_enabled), s.target_value)
+                          for s in inst.substrates[:S]])
+    m = inst.mech
+    om = po.Mech(m.dt, m.cell_cell_repulsion, m.cell_cell_adhesion, m.max_interaction_distance,
+                 m.mechanics_voxel_size, m.mech_grid_nx, m.mech_grid_ny, m.mech_grid_nz)
+    dens = np.repeat(inst.initial_values, g.nx * g.ny * g.nz).astype(np.float32)
+    soa = inst.soa.copy()
+    pm = po.master_positions(soa, n)
+    po.run(og, osubs, om, 0.1, dens, soa, n, n, *inst.rates, inst.active, steps, refresh=bool(inst.flags & 1),
+           pos64=pm)
+    b = np.asarray(dens, np.float64)
+    err = np.abs(together[i][0] - b) / np.maximum(np.abs(b), 1e-6 * np.abs(b).max())
+    assert err.max() <= 1e-5, (i, err.max())

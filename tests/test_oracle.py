@@ -48,6 +48,33 @@ def test_oracle_fp64_close_to_reference_shaders(po, path):
         assert err.max() <= 1e-5, f"step {k}: {err.max():.3e}"
 
 
+def test_oracle_reproduces_reference_scenario_diffusion_only_2d(po):
+    """The reference's own parity scenario (parity/scenarios/diffusion_only_2d:
+    20 x 20 over [-200, 200]^2 um, D 1e5, decay 0.1, Dirichlet 38, uniform 38,
+    2 min of 0.01 min steps): the FP32 mode bit for bit after 100 and 200
+    steps.  The FP64 oracle is within 1e-4 there: the reference's FP32
+    roundings over 200 steps of a field that Q1 drives from 38 to ~4000 add
+    up to 2.2e-5 (100 steps) and 4.1e-5 (200 steps) of relative error."""
+    z = np.load(os.path.join(GOLDEN, "scenario_diffusion_only_2d.npz"))
+    subs_p = [(float(a), float(b), bool(c), float(d)) for a, b, c, d in z["subs"]]
+    g = po.make_grid(20, 20, 1, 1, dx=20.0, dt=0.01, x_min=-200.0, y_min=-200.0)
+    subs = po.make_subs(subs_p)
+    d32 = np.full(400, 38.0, np.float32)
+    d64 = d32.copy()
+    saved = list(z["steps"])
+    for step in range(1, max(saved) + 1):
+        po.sweeps(d32, g, subs, po.OR_FP32_REF)
+        po.dirichlet(d32, g, subs)
+        po.sweeps(d64, g, subs, po.OR_FP64)
+        po.dirichlet(d64, g, subs)
+        if step in saved:
+            ref = z["density"][saved.index(step)]
+            assert np.array_equal(d32.view(np.uint32), ref.view(np.uint32)), f"step {step}"
+            r = ref.astype(np.float64)
+            err = np.abs(d64 - r) / np.maximum(np.abs(r), 1e-6 * np.abs(r).max())
+            assert err.max() <= 1e-4, f"step {step}: {err.max():.3e}"
+
+
 def test_secretion_bit_exact_to_reference(po):
     z = np.load(os.path.join(GOLDEN, "secretion.npz"))
     g = po.make_grid(int(z["nx"]), int(z["ny"]), 1, int(z["S"]), dx=20.0, dt=0.01)
