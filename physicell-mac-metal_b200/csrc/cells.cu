@@ -362,8 +362,11 @@ __device__ __forceinline__ void pair_force(float ddx, float ddy, float ddz, floa
 // adds its terms in candidate order either way, so both forms give the same
 // bits; the queued form runs the force terms for the neighbours only,
 // where the direct form runs them whenever any lane of the warp has one.
+// Registers are capped at 48 (five blocks of 256 threads per SM; part of
+// the row table spills to L1): the walk is bound by load latency, and the
+// extra resident warps hide more of it than the spills cost.
 template <int QCAP, bool DIAG>
-__global__ void __launch_bounds__(256) k_mech_forces(const float4* __restrict__ spos, const float4* __restrict__ sprm,
+__global__ void __launch_bounds__(256, 5) k_mech_forces(const float4* __restrict__ spos, const float4* __restrict__ sprm,
                                                      const uint32_t* __restrict__ forder,
                                                      const uint32_t* __restrict__ start, uint32_t n,
                                                      const uint32_t* __restrict__ cell_inst,
