@@ -36,7 +36,7 @@ uint64_t instance_bytes(const pcg_instance_desc& d)
     b += n * (8 + 4);                                      // per-run density element and rate slot
     b += n * (16 + 16 + 8);                                // sorted SoA, diagnostics
     b += (V + 1) * 4 * 2;                                  // counts, start
-    b += (n / 2048 + 1) * 256 * 4 * 2 + 4096;              // sort / scan scratch
+    b += (n / 2048 + 2) * (257 * 4 + sizeof(SegTile) + 8) + 4096;   // sort tiles, digit rows, run scan
     return b;
 }
 
