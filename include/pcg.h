@@ -225,8 +225,8 @@ pcg_status pcg_cells_download_positions64(pcg_cells* cells, double* xyz, uint32_
 
 /* ------------------------------------------------------------------------
  * Mechanics — replaces CellMechanics (src/cell_mechanics.h:15-87).
- * Binning is a stable LSD radix sort of (mech voxel, cell index); the
- * cell-start table replaces the 64-slot hash: voxelCellCount(v) =
+ * Binning is a counting sort over the mechanics voxels, stable in cell
+ * index within a voxel; the cell-start table replaces the 64-slot hash: voxelCellCount(v) =
  * start[v+1] - start[v], voxelCells(v) = sorted + start[v].
  * ---------------------------------------------------------------------- */
 /* CellMechanics::initialize (cell_mechanics.mm:23-82): the mechanics

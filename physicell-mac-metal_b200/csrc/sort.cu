@@ -1,8 +1,9 @@
 // sort.cu — stable LSD radix sort of (key, value) pairs and a warp-shuffle
-// exclusive scan (sm_100a).  The sort orders cells by diffusion voxel for
-// secretion (and backs pcg_sort_pairs_static); the scan turns the per-voxel
-// counts of the mechanics binning into the cell-start table, and serves the
-// sort's digit histograms and the secretion run list.
+// exclusive scan (sm_100a).  The sort backs pcg_sort_pairs_static (the
+// secretion order has its own instance-segmented sort, secorder.cu); the
+// scan turns the per-voxel counts of the mechanics binning into the
+// cell-start table, and serves the sort's digit histograms and the
+// secretion run list's tile counts.
 //
 // One radix pass over D-bit digits:
 //   k_radix_hist     per-tile digit histogram -> hist[digit * tiles + tile]
