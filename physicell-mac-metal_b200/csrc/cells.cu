@@ -317,24 +317,27 @@ __device__ __forceinline__ float slab_gap(float c, float lo, float vs, int idx, 
 // Rj the radii, mp = (sqrt rep_i, sqrt adh_i, relmax_i, 1 / relmax_i), op
 // the strengths of j.  Reciprocal / rsqrt forms and per-cell square roots
 // of the strengths (a few ulp per term against the reference's sqrt and
-// divides); dist / (relmax_i R) is taken as (dist / R) / relmax_i.
+// divides); dist / (relmax_i R) is taken as (dist / R) / relmax_i.  Every
+// product, sum and fused multiply-add is written out with its rounding, so
+// the terms have the same bits in every kernel that inlines this, whatever
+// the compiler would contract around it.
 __device__ __forceinline__ void pair_force(float ddx, float ddy, float ddz, float dsq, float Ri, float Rj,
                                            const float4& mp, const float4& op, float& fx, float& fy, float& fz,
                                            float& P)
 {
     constexpr float kInvPressureScale = 1.0f / 0.027288820670331f;
     const float inv = rsqrtf(dsq);
-    const float dist = dsq * inv;
-    const float u = __fdividef(dist, Ri + Rj);                         // dist / R
-    const float ov = fmaxf(1.0f - u, 0.0f);                            // repulsion overlap
-    const float t = fmaxf(1.0f - u * mp.w, 0.0f);                      // adhesion reach
-    const float ov2 = ov * ov;
-    const float F = ov2 * (mp.x * op.x) - t * t * (mp.y * op.y);
-    P += ov2 * kInvPressureScale;
-    const float Fi = F * inv;
-    fx += Fi * ddx;
-    fy += Fi * ddy;
-    fz += Fi * ddz;
+    const float dist = __fmul_rn(dsq, inv);
+    const float u = __fdividef(dist, __fadd_rn(Ri, Rj));               // dist / R
+    const float ov = fmaxf(__fsub_rn(1.0f, u), 0.0f);                   // repulsion overlap
+    const float t = fmaxf(__fmaf_rn(-u, mp.w, 1.0f), 0.0f);             // adhesion reach
+    const float ov2 = __fmul_rn(ov, ov);
+    const float F = __fmaf_rn(ov2, __fmul_rn(mp.x, op.x), -__fmul_rn(__fmul_rn(t, t), __fmul_rn(mp.y, op.y)));
+    P = __fmaf_rn(ov2, kInvPressureScale, P);
+    const float Fi = __fmul_rn(F, inv);
+    fx = __fmaf_rn(Fi, ddx, fx);
+    fy = __fmaf_rn(Fi, ddy, fy);
+    fz = __fmaf_rn(Fi, ddz, fz);
 }
 
 // One thread per cell, cells in the force order p (by mechanics voxel,
