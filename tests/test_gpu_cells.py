@@ -203,7 +203,12 @@ def secretion_case(pcg, po, nx, ny, nz, S, n, seed):
     return g, og, pcg.make_substrates(subs_p), po.make_subs(subs_p), soa, vox, rates, active, d0
 
 
-@pytest.mark.parametrize("shape", [(10, 10, 1, 2, 400), (30, 20, 10, 3, 5000), (50, 50, 1, 1, 500)])
+# grids of 1 voxel (no digit bits: one pass), 16 voxels (one 4-bit pass), up
+# to 22-bit voxel indices (three 8-bit passes of the secretion order), and
+# stores of one or several 2048-cell tiles
+@pytest.mark.parametrize("shape", [(10, 10, 1, 2, 400), (30, 20, 10, 3, 5000), (50, 50, 1, 1, 500),
+                                   (1, 1, 1, 1, 300), (4, 4, 1, 2, 5000), (256, 256, 40, 1, 20000),
+                                   (128, 128, 128, 2, 7000)])
 def test_secretion_bit_exact(ctx, pcg, po, shape):
     nx, ny, nz, S, n = shape
     g, og, subs, osubs, soa, vox, rates, active, d0 = secretion_case(pcg, po, nx, ny, nz, S, n, sum(shape))
