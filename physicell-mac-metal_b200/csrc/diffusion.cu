@@ -155,6 +155,19 @@ __device__ __forceinline__ void tensor_load2(void* smem_dst, const void* tmap, i
         "l"(tmap), "r"(c0), "r"(c1), "r"(smem_u32(bar))
         : "memory");
 }
+// L2 prefetch of a tensor box (no shared memory, no barrier): the box a
+// later CTA will load then comes from L2.
+__device__ __forceinline__ void tensor_prefetch2(const void* tmap, int c0, int c1)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(tmap), "r"(c0), "r"(c1)
+                 : "memory");
+}
+__device__ __forceinline__ void tensor_prefetch3(const void* tmap, int c0, int c1, int c2)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(tmap), "r"(c0), "r"(c1),
+                 "r"(c2)
+                 : "memory");
+}
 __device__ __forceinline__ void tensor_store2(const void* tmap, int c0, int c1, const void* smem_src)
 {
     asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(tmap), "r"(c0),
@@ -684,12 +697,14 @@ __device__ __forceinline__ void plane_col(float* c, int P, const LineRule& r, co
 // with one tensor store.  The steps on each line are those of the x and y
 // tile kernels, so the result is the same bits, but the plane crosses HBM
 // once for both sweeps.  Several CTAs per SM overlap one plane's copies
-// with another's solves.
+// with another's solves, and each CTA prefetches into L2 (a tensor-box
+// prefetch, no shared memory) the plane of the CTA 'ahead' jobs later, so
+// that CTA's load is served from L2.
 __global__ void __launch_bounds__(kPlaneThreads) k_sweep_planes(const PlaneJob* __restrict__ jobs,
                                                                 const float* __restrict__ tab,
                                                                 const void* __restrict__ tmaps, int apply_faces,
                                                                 const uint8_t* __restrict__ mask,
-                                                                unsigned* __restrict__ status)
+                                                                unsigned* __restrict__ status, uint32_t ahead)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
@@ -717,6 +732,17 @@ __global__ void __launch_bounds__(kPlaneThreads) k_sweep_planes(const PlaneJob* 
             bulk_load(tx, tab + jb.tab_x, tbx, bar);
         }
         bulk_load(ty, tab + jb.tab_y, tby, bar);
+        // the plane of a CTA that starts a little later ('ahead' jobs on,
+        // about a quarter of a residency): into L2 now, so its load is an
+        // L2 hit rather than a wait on HBM
+        if (ahead != 0 && blockIdx.x + ahead < gridDim.x) {
+            const PlaneJob nj = jobs[blockIdx.x + ahead];
+            if (!mask || (mask[nj.inst & kPlaneInstMask] & STEP_DIFFUSE)) {
+                const void* nmap = static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(nj.map) * 128;
+                if (nj.inst & kPlaneZ) tensor_prefetch3(nmap, 0, static_cast<int>(nj.row0), 0);
+                else tensor_prefetch2(nmap, 0, static_cast<int>(nj.row0));
+            }
+        }
     }
     bool got;
     if (status[1] & PCG_DEV_TEST_GIVE_UP) {   // test switch: this wait's bound ran out
@@ -1044,8 +1070,17 @@ cudaError_t launch_sweep_planes(cudaStream_t st, const PlaneJob* jobs, uint32_t 
                                 unsigned* status)
 {
     if (njobs == 0) return cudaSuccess;
+    // prefetch distance: a quarter of the CTAs of this launch resident at
+    // once (measured: a half, one or two residencies ahead gain less or lose)
+    static const int sms = [] {
+        int dev = 0, n = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            n = 1;
+        return n;
+    }();
+    const uint32_t ahead = static_cast<uint32_t>(sweep_planes_ctas(floats) * sms / 4);
     k_sweep_planes<<<njobs, kPlaneThreads, sweep_planes_smem(floats), st>>>(jobs, tab, tmaps, apply_faces, mask,
-                                                                            status);
+                                                                            status, ahead);
     return cudaGetLastError();
 }
 
