@@ -13,9 +13,10 @@ rebuilt), over all instances, one CUDA graph launch per sub-step.
 Reports (one JSON line on rank 0):
   value            aggregate voxel-steps/s of the batched path, inputs resident
   e2e              the same through the C ABI with host buffers: every step
-                   uploads all 28 cell fields from pinned memory and reads
-                   back the density arena and the 12 cell fields the steps
-                   write (the host keeps the fields only it writes)
+                   uploads the 16 cell fields the host owns (radius,
+                   volumes, strengths, phenotype: every field the steps do
+                   not write) from pinned memory and reads back the density
+                   arena and the 12 cell fields the steps write
   roofline         the Thomas sweeps: 8 B per voxel-substrate per sweep
                    launch / average launch time (CUDA events), vs measured HBM
   cpu_baseline     the multi-threaded FP32 CPU port on a bounded sample
@@ -449,13 +450,15 @@ def main():
     batch.download_all_cells(soa_h.array)
     ctx.sync()
 
-    # the host keeps the fields only it writes (radius, volumes, phenotype);
-    # each period it sends all 28 fields up and reads back the density and
-    # the 12 fields the steps write
+    # the host owns the fields the steps do not write (radius, volumes,
+    # strengths, phenotype) and sends them up every period; the device owns
+    # the kinematic state; the density and the 12 fields the steps write come
+    # back every period
     written = pcg.STEP_WRITTEN_FIELDS
+    host_owned = pcg.HOST_OWNED_FIELDS
 
     def e2e_period():
-        batch.upload_all_cells(soa_h.array)
+        batch.upload_cell_fields(soa_h.array, host_owned)
         batch.step(SUB_STEPS)
         batch.download_cell_fields(soa_out.array, written)
         batch.download_all_density(dens_out.array)
@@ -467,7 +470,7 @@ def main():
     wall = time.perf_counter() - t0
     e2e_secs = dist_max(dist, local, max(e2e_secs, 0.0))
     e2e_value = total_vox * SUB_STEPS * args.steps / e2e_secs
-    h2d = n_soa * 4
+    h2d = bin(host_owned).count("1") * cells * 4
     d2h = bin(written).count("1") * cells * 4 + arena * 4
 
     # roofline: phase events on the same kernels (profile mode launches directly)

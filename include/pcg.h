@@ -439,6 +439,13 @@ pcg_status pcg_batch_download_all_density(pcg_batch* batch, float* host, uint64_
      (1u << PCG_F_PREV_VZ) | (1u << PCG_F_PRESSURE) | (1u << PCG_F_VOXEL_IDX) |                   \
      (1u << PCG_F_MECH_VOXEL))
 pcg_status pcg_batch_download_cell_fields(pcg_batch* batch, float* soa, uint64_t n_floats, uint32_t field_mask);
+/* pcg_batch_upload_all_cells for the fields whose bit is set in field_mask,
+ * from the same places of the host SoA; the device's other fields are left
+ * as they are.  A host that owns the phenotype fields and leaves the
+ * kinematic state to the device uploads PCG_HOST_OWNED_FIELDS (every field
+ * the steps do not write). */
+#define PCG_HOST_OWNED_FIELDS (((1u << PCG_NUM_FIELDS) - 1u) & ~PCG_STEP_WRITTEN_FIELDS)
+pcg_status pcg_batch_upload_cell_fields(pcg_batch* batch, const float* soa, uint64_t n_floats, uint32_t field_mask);
 pcg_status pcg_batch_density_layout(pcg_batch* batch, uint32_t instance, uint64_t* offset, uint64_t* row_pitch,
                                     uint64_t* substrate_pitch, uint64_t* arena_floats);
 /* Totals: voxels (sum nx*ny*nz), voxel-substrates, cells. */

@@ -36,6 +36,8 @@ NUM_FIELDS = 28
 PCG_OK = 0
 # fields the sub-steps and mechanics steps write (PCG_STEP_WRITTEN_FIELDS)
 STEP_WRITTEN_FIELDS = sum(1 << f for f in (0, 1, 2, 3, 4, 5, 6, 7, 8, 22, 26, 27))
+# every other field: what a host that owns the phenotype sends (PCG_HOST_OWNED_FIELDS)
+HOST_OWNED_FIELDS = ((1 << 28) - 1) & ~STEP_WRITTEN_FIELDS
 INST_REFRESH_VOXELS = 1
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_CANCELLED = 0, 1, 2, 3
 N_PHASES = 7
@@ -177,6 +179,7 @@ _SIGS = [
     ("pcg_batch_download_all_cells", C.c_int, [_P, _F32P, C.c_uint64]),
     ("pcg_batch_download_all_density", C.c_int, [_P, _F32P, C.c_uint64]),
     ("pcg_batch_download_cell_fields", C.c_int, [_P, _F32P, C.c_uint64, C.c_uint32]),
+    ("pcg_batch_upload_cell_fields", C.c_int, [_P, _F32P, C.c_uint64, C.c_uint32]),
     ("pcg_batch_density_layout", C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                            C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("pcg_join", C.c_int, [_P]),
@@ -766,6 +769,12 @@ class Batch:
         default: the fields the steps write, STEP_WRITTEN_FIELDS)."""
         m = STEP_WRITTEN_FIELDS if mask is None else int(mask)
         self.ctx.check(lib().pcg_batch_download_cell_fields(self.h, _f32(soa), soa.size, m))
+
+    def upload_cell_fields(self, soa, mask=None):
+        """upload_all_cells for the fields in 'mask' (default: the fields the
+        host owns, HOST_OWNED_FIELDS); the device keeps its other fields."""
+        m = HOST_OWNED_FIELDS if mask is None else int(mask)
+        self.ctx.check(lib().pcg_batch_upload_cell_fields(self.h, _f32(soa), soa.size, m))
 
     def download_all_density(self, dens):
         self.ctx.check(lib().pcg_batch_download_all_density(self.h, _f32(dens), dens.size))

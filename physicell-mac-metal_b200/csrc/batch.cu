@@ -675,6 +675,60 @@ pcg_status pcg_batch_download_cell_fields(pcg_batch* b, float* soa, uint64_t n_f
     return PCG_OK;
 }
 
+pcg_status pcg_batch_upload_cell_fields(pcg_batch* b, const float* soa, uint64_t n_floats, uint32_t field_mask)
+{
+    if (!b || !soa) return PCG_ERR_INVALID;
+    Batch& B = b->b;
+    Cells& c = B.c_;
+    pcg_ctx* ctx = B.ctx;
+    if (n_floats != static_cast<uint64_t>(NUM_FIELDS) * c.n) return fail(ctx, PCG_ERR_INVALID, "size mismatch");
+    if (field_mask >> NUM_FIELDS) return fail(ctx, PCG_ERR_INVALID, "field mask names a field past the 28");
+    if (c.n == 0 || field_mask == 0) return PCG_OK;
+    // runs of consecutive fields: each run's place in the host SoA -> staging
+    // (packed) on the copy stream, staging -> the SoA on the context stream
+    std::vector<std::pair<uint32_t, uint32_t>> runs;
+    for (uint32_t f = 0; f < static_cast<uint32_t>(NUM_FIELDS);) {
+        if (!(field_mask >> f & 1u)) {
+            ++f;
+            continue;
+        }
+        uint32_t e = f;
+        while (e < static_cast<uint32_t>(NUM_FIELDS) && (field_mask >> e & 1u)) ++e;
+        runs.emplace_back(f, e);
+        f = e;
+    }
+    const size_t row = static_cast<size_t>(c.n) * sizeof(float);
+    const size_t nsel = static_cast<size_t>(__builtin_popcount(field_mask));
+    PCG_TRY(ensure_copy_streams(ctx));
+    PCG_TRY(ensure_stage(ctx, B.stage_in, row * nsel));
+    PCG_TRY(ensure_event(ctx, &B.ev_in_done));
+    PCG_TRY(ensure_event(ctx, &B.ev_in_used));
+    PCG_CU(ctx, cudaStreamWaitEvent(ctx->h2d, B.ev_in_used, 0));
+    size_t at = 0;
+    for (const auto& r : runs) {
+        PCG_CU(ctx, cudaMemcpyAsync(static_cast<char*>(B.stage_in.p) + at * row,
+                                    soa + static_cast<size_t>(r.first) * c.n, (r.second - r.first) * row,
+                                    cudaMemcpyHostToDevice, ctx->h2d));
+        at += r.second - r.first;
+    }
+    PCG_CU(ctx, cudaEventRecord(B.ev_in_done, ctx->h2d));
+    PCG_CU(ctx, cudaStreamWaitEvent(ctx->stream, B.ev_in_done, 0));
+    at = 0;
+    for (const auto& r : runs) {
+        PCG_CU(ctx, cudaMemcpy2DAsync(c.soa.as<float>() + static_cast<size_t>(r.first) * c.max_cells,
+                                      static_cast<size_t>(c.max_cells) * sizeof(float),
+                                      static_cast<const char*>(B.stage_in.p) + at * row, row, row,
+                                      r.second - r.first, cudaMemcpyDeviceToDevice, ctx->stream));
+        at += r.second - r.first;
+    }
+    PCG_CU(ctx, cudaEventRecord(B.ev_in_used, ctx->stream));
+    // volumes feed the secretion constants, voxel indices the secretion order
+    if (field_mask >> F_TOTAL_VOL & 1u) c.coef_dirty = true;
+    if (field_mask >> F_VOXEL_IDX & 1u) c.order_dirty = true;
+    if (c.coef_dirty || c.order_dirty) PCG_TRY(c.prepare_secretion(B.dt_diff, B.d.total_vox));
+    return PCG_OK;
+}
+
 pcg_status pcg_batch_download_all_density(pcg_batch* b, float* host, uint64_t n_floats)
 {
     if (!b || !host) return PCG_ERR_INVALID;

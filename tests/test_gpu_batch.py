@@ -174,6 +174,50 @@ def test_masked_cell_download(ctx, pcg):
     b.close()
 
 
+def test_masked_cell_upload(ctx, pcg):
+    """pcg_batch_upload_cell_fields: the fields in the mask take the host's
+    values, every other device field keeps its own; after the host-owned
+    fields change (radius, volume and strengths here), stepping gives the
+    same bits as a whole upload of the same state."""
+    insts = small_mix(pcg, seed=15)
+    n_tot = sum(i.n_cells for i in insts)
+    runs = []
+    for whole in (False, True):
+        b = pcg.Batch(ctx, insts)
+        b.step(11)
+        host = pcg.PinnedArray((28 * n_tot,))
+        back = pcg.PinnedArray((28 * n_tot,))
+        b.download_all_cells(host.array)
+        ctx.sync()
+        before = host.array.copy().reshape(28, n_tot)
+        h = host.array.reshape(28, n_tot)
+        for f in (9, 11, 13, 14):                 # radius, total volume, repulsion, adhesion
+            h[f] *= np.float32(1.1)
+        h[0] += np.float32(3.0)                   # a field the device owns: must not reach it
+        if whole:
+            h[0] = before[0]
+            b.upload_all_cells(host.array)
+        else:
+            b.upload_cell_fields(host.array, pcg.HOST_OWNED_FIELDS)
+        b.download_all_cells(back.array)
+        ctx.sync()
+        q = back.array.reshape(28, n_tot)
+        for k in range(28):
+            want = h[k] if (pcg.HOST_OWNED_FIELDS >> k & 1) else before[k]
+            assert np.array_equal(q[k].view(np.uint32), want.view(np.uint32)), k
+        b.step(12)
+        ctx.sync()
+        runs.append([(b.density(i), b.cells(i)) for i in range(len(insts))])
+        with pytest.raises(pcg.PcgError):
+            b.upload_cell_fields(host.array, 1 << 28)
+        host.free()
+        back.free()
+        b.close()
+    for (da, ca), (db, cb) in zip(*runs):
+        assert np.array_equal(da.view(np.uint32), db.view(np.uint32))
+        assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32))
+
+
 def test_sweep_units_count_the_passes(ctx, pcg):
     """pcg_batch_sweep_units: with planes a 3-D instance's sub-step moves
     each voxel-substrate twice (x + y plane pass, z plane pass) and a 2-D
