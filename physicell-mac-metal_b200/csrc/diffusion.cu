@@ -1071,7 +1071,9 @@ cudaError_t launch_sweep_planes(cudaStream_t st, const PlaneJob* jobs, uint32_t 
 {
     if (njobs == 0) return cudaSuccess;
     // prefetch distance: a quarter of the CTAs of this launch resident at
-    // once (measured: a half, one or two residencies ahead gain less or lose)
+    // once (measured: a half, one or two residencies ahead gain less or lose).
+    // The SM count is read once, on the first device used; it only sets this
+    // distance, never which data is read.
     static const int sms = [] {
         int dev = 0, n = 0;
         if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
