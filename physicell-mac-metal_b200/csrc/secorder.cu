@@ -91,31 +91,49 @@ __global__ void __launch_bounds__(kThreads) k_so_hist(const SegTile* __restrict_
 // Exclusive scan of one instance's counts in (digit, tile) order, in place:
 // hist row t (R + 1 counts of tile t) becomes the first place of each of
 // the tile's digit runs.  One block per instance with cells (inst_tile[b]
-// = its first tile); thread j covers digits j, j + 256, ...
+// = its first tile); thread j covers digits j, j + 256, ...  The rows of an
+// instance's tiles are contiguous, so they come into shared memory (up to
+// kOffSmem bytes of rows at a time) with coalesced loads, all in flight
+// together, and go back the same way; the walks over tiles then read
+// shared memory.
 constexpr int kOffThreads = 256;
+constexpr uint32_t kOffSmem = 46 * 1024;
 __global__ void __launch_bounds__(kOffThreads, 1) k_so_offsets(const SegTile* __restrict__ tiles,
                                                             const uint32_t* __restrict__ inst_tile,
                                                             const CellInst* __restrict__ insts, uint32_t R,
                                                             uint32_t* __restrict__ hist)
 {
     __shared__ uint32_t wsum[kOffThreads / 32];
+    __shared__ uint32_t rows[kOffSmem / 4];
     const SegTile t0 = tiles[inst_tile[blockIdx.x]];
     const uint32_t nb = R + 1;
+    const uint32_t chunk = (kOffSmem / 4) / nb;   // tiles per chunk (>= 44: nb <= 257)
+    const bool one = t0.nt <= chunk;               // every row stays in shared memory
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr uint32_t kPer = (kMaxBins + kOffThreads - 1) / kOffThreads;   // digits per thread
     uint32_t tot[kPer];
-    uint32_t* base = hist + static_cast<size_t>(nb) * t0.tb;
 #pragma unroll
-    for (uint32_t k = 0; k < kPer; ++k) {
-        const uint32_t d = threadIdx.x + k * kOffThreads;
-        uint32_t s = 0;
-        if (d < nb)
-            for (uint32_t t = 0; t < t0.nt; ++t) s += base[static_cast<size_t>(t) * nb + d];
-        tot[k] = s;
+    for (uint32_t k = 0; k < kPer; ++k) tot[k] = 0;
+    uint32_t* base = hist + static_cast<size_t>(nb) * t0.tb;
+    for (uint32_t c0 = 0; c0 < t0.nt; c0 += chunk) {
+        const uint32_t words = min(chunk, t0.nt - c0) * nb;
+        const uint32_t* src = base + static_cast<size_t>(c0) * nb;
+        for (uint32_t i = threadIdx.x; i < words; i += kOffThreads) rows[i] = src[i];
+        __syncthreads();
+        const uint32_t cn = words / nb;
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) {
+            const uint32_t d = threadIdx.x + k * kOffThreads;
+            if (d < nb)
+                for (uint32_t t = 0; t < cn; ++t) tot[k] += rows[t * nb + d];
+        }
+        __syncthreads();
     }
     // digits in order: digit d = threadIdx.x + k * 256, so the scan runs
-    // over k-major blocks of 256 digits
+    // over k-major blocks of 256 digits; start[k]: the first place of
+    // this thread's digit k
     uint32_t run = insts[t0.inst].cell_off;
+    uint32_t first[kPer];
 #pragma unroll
     for (uint32_t k = 0; k < kPer; ++k) {
         uint32_t incl = tot[k];
@@ -133,17 +151,34 @@ __global__ void __launch_bounds__(kOffThreads, 1) k_so_offsets(const SegTile* __
             all += x;
         }
         __syncthreads();
-        const uint32_t d = threadIdx.x + k * kOffThreads;
-        if (d < nb) {
-            uint32_t at = run + before + incl - tot[k];
-            for (uint32_t t = 0; t < t0.nt; ++t) {
-                uint32_t* h = base + static_cast<size_t>(t) * nb + d;
-                const uint32_t c = *h;
-                *h = at;
-                at += c;
+        first[k] = run + before + incl - tot[k];
+        run += all;
+    }
+    // each tile's row: the running place of every digit, tiles in order
+    for (uint32_t c0 = 0; c0 < t0.nt; c0 += chunk) {
+        const uint32_t words = min(chunk, t0.nt - c0) * nb;
+        uint32_t* dst = base + static_cast<size_t>(c0) * nb;
+        if (!one) {
+            for (uint32_t i = threadIdx.x; i < words; i += kOffThreads) rows[i] = dst[i];
+            __syncthreads();
+        }
+        const uint32_t cn = words / nb;
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) {
+            const uint32_t d = threadIdx.x + k * kOffThreads;
+            if (d < nb) {
+                uint32_t at = first[k];
+                for (uint32_t t = 0; t < cn; ++t) {
+                    const uint32_t c = rows[t * nb + d];
+                    rows[t * nb + d] = at;
+                    at += c;
+                }
+                first[k] = at;
             }
         }
-        run += all;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < words; i += kOffThreads) dst[i] = rows[i];
+        __syncthreads();
     }
 }
 
