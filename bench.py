@@ -8,7 +8,7 @@ mechanics period of the main loop (src/main.mm:341-391): 10 diffusion
 sub-steps (x/y/z Thomas sweeps, Dirichlet reset, secretion) and one
 mechanics step (binning, cell-start table, forces, AB2, then every cell's
 voxel index recomputed from its new position and the secretion order
-rebuilt), over all instances, one CUDA graph launch per sub-step.
+rebuilt), over all instances, one CUDA graph launch per period.
 
 Reports (one JSON line on rank 0):
   value            aggregate voxel-steps/s of the batched path, inputs resident

@@ -4,8 +4,9 @@
 // key space; every phase of a main-loop sub-step is one persistent kernel
 // over a flat work list of all instances (src/main.mm:341-391 ordering:
 // sweeps -> Dirichlet reset (fused) -> secretion -> [mechanics]).  The
-// sub-step with and without mechanics are each captured once into a CUDA
-// graph, so one step is one graph launch.
+// sub-step with and without mechanics, and a whole mechanics period, are
+// each captured once into a CUDA graph, so one sub-step, or one period
+// where a call covers it, is one graph launch.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -188,6 +189,17 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
     if (use_graphs) {
         PCG_TRY(capture(false, &g_diff, &launches_diff));
         PCG_TRY(capture(true, &g_mech, &launches_mech));
+        // sub-steps from a reset accumulator to the firing one, as step() counts them
+        double a = 0.0;
+        int len = 0;
+        for (bool fire = false; !fire && len <= kMaxPeriod; ++len) {
+            a += dt_diff;
+            fire = a >= dt_mech - 0.5 * dt_diff;
+        }
+        if (!masked && len >= 2 && len <= kMaxPeriod) {
+            period_len = len;
+            PCG_TRY(capture(true, &g_period, &launches_period, len - 1));
+        }
     } else {
         launches_diff = count_launches(false);
         launches_mech = count_launches(true);
@@ -204,8 +216,8 @@ Batch::~Batch()
     }
     for (cudaEvent_t e : {ev_in_done, ev_in_used, ev_cells_ready, ev_cells_done, ev_dens_ready, ev_dens_done})
         if (e) cudaEventDestroy(e);
-    if (g_diff) cudaGraphExecDestroy(g_diff);
-    if (g_mech) cudaGraphExecDestroy(g_mech);
+    for (cudaGraphExec_t g : {g_diff, g_mech, g_period})
+        if (g) cudaGraphExecDestroy(g);
     for (int q = 0; q < 8; ++q)
         if (ev[q]) cudaEventDestroy(ev[q]);
 }
@@ -356,12 +368,15 @@ int Batch::run_step(bool mech, bool timed, const uint8_t* mask)
     return PCG_OK;
 }
 
-int Batch::capture(bool mech, cudaGraphExec_t* out, uint64_t* launches)
+int Batch::capture(bool mech, cudaGraphExec_t* out, uint64_t* launches, int n_diff)
 {
     cudaStream_t st = ctx->stream;
     const uint64_t before = ctx->launches;
     PCG_CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    int rc = run_step(mech, false, masked ? mask_d.as<uint8_t>() : nullptr);
+    const uint8_t* mask = masked ? mask_d.as<uint8_t>() : nullptr;
+    int rc = PCG_OK;
+    for (int k = 0; k < n_diff && rc == PCG_OK; ++k) rc = run_step(false, false, mask);   // sub-steps before mech
+    if (rc == PCG_OK) rc = run_step(mech, false, mask);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (rc != PCG_OK) {
@@ -383,6 +398,15 @@ int Batch::step(int n_steps)
     if (n_steps < 0) return fail(ctx, PCG_ERR_INVALID, "n_steps < 0");
     cudaStream_t st = ctx->stream;
     for (int s = 0; s < n_steps; ++s) {
+        if (!profile && g_period && accum == 0.0 && n_steps - s >= period_len) {
+            // a whole period: the accumulator fires on its last sub-step and resets
+            PCG_CU(ctx, cudaGraphLaunch(g_period, st));
+            ctx->launches += launches_period;
+            s += period_len - 1;
+            diff_steps += static_cast<uint64_t>(period_len);
+            mech_steps++;
+            continue;
+        }
         accum += dt_diff;
         const bool mech = accum >= dt_mech - 0.5 * dt_diff;
         if (mech) accum = 0.0;
@@ -443,7 +467,11 @@ int Batch::set_diagnostics(bool on)
         cudaGraphExecDestroy(g_mech);
         g_mech = nullptr;
     }
-    return capture(true, &g_mech, &launches_mech);
+    PCG_TRY(capture(true, &g_mech, &launches_mech));
+    if (!g_period) return PCG_OK;
+    cudaGraphExecDestroy(g_period);
+    g_period = nullptr;
+    return capture(true, &g_period, &launches_period, period_len - 1);
 }
 
 std::string Batch::describe() const

@@ -31,6 +31,14 @@ public:
     std::string tune_cache;
     cudaGraphExec_t g_diff = nullptr, g_mech = nullptr;
     uint64_t launches_diff = 0, launches_mech = 0;
+    // A whole mechanics period (the sub-steps from a reset accumulator to
+    // the one that fires, mechanics included) as one graph: period_len
+    // sub-steps per launch where a call covers them, single sub-step
+    // graphs elsewhere.
+    static constexpr int kMaxPeriod = 64;   // longer periods run as single sub-steps
+    cudaGraphExec_t g_period = nullptr;
+    uint64_t launches_period = 0;
+    int period_len = 0;
     cudaEvent_t ev[8] = {};
     // Staging of the whole-batch transfers (made on first use): host copies
     // run on the context's copy streams, device-to-device copies on its
@@ -68,7 +76,7 @@ public:
     int set_diagnostics(bool on);
 
 private:
-    int capture(bool mech, cudaGraphExec_t* out, uint64_t* launches);
+    int capture(bool mech, cudaGraphExec_t* out, uint64_t* launches, int n_diff = 0);
     // Launch shapes of the cell kernels: pinned by the options, else cached
     // by shape bucket or measured on the batch's own data (the state the
     // timed launches write is saved first and put back).

@@ -61,6 +61,33 @@ def test_graphs_equal_direct_launches(ctx, pcg):
         assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32))
 
 
+def test_period_graph_equals_single_steps(ctx, pcg):
+    """A call covering whole mechanics periods launches each as one graph;
+    the result is the same bits as one sub-step per call, with the same
+    kernel count."""
+    insts = small_mix(pcg, seed=14)
+
+    def run(calls):
+        b = pcg.Batch(ctx, insts)
+        l0 = ctx.launches
+        for k in calls:
+            b.step(k)
+        ctx.sync()
+        res = [(b.density(i), b.cells(i)) for i in range(len(insts))]
+        n = ctx.launches - l0
+        b.close()
+        return res, n
+
+    whole, n_whole = run([23])          # two period graphs, then three sub-steps
+    single, n_single = run([1] * 23)
+    mixed, n_mixed = run([3, 20])       # single sub-steps up to the first firing, then one period graph
+    assert n_whole == n_single == n_mixed
+    for i in range(len(insts)):
+        for other in (single, mixed):
+            assert np.array_equal(whole[i][0].view(np.uint32), other[i][0].view(np.uint32)), f"density {i}"
+            assert np.array_equal(whole[i][1].view(np.uint32), other[i][1].view(np.uint32)), f"cells {i}"
+
+
 @pytest.mark.parametrize("pins", [(18, 18), (50, 35), (36, 52), (34, 66)])
 def test_pinned_launch_shapes_give_identical_results(ctx, pcg, pins):
     """Warps per CTA and pipeline stages change only the schedule: every
