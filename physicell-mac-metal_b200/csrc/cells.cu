@@ -126,23 +126,23 @@ __device__ __forceinline__ float secrete_cell(float rho32, const double* __restr
 // both are held in registers and advanced together.  Constants: three
 // arrays of cap (c0, c1, c2), entry (cell in sorted order, substrate).
 __global__ void __launch_bounds__(256, 6) k_secrete(float* __restrict__ dens, const uint32_t* __restrict__ run_start,
-                          const uint32_t* __restrict__ run_inst, const uint64_t* __restrict__ run_dens,
-                          const uint32_t* __restrict__ run_slot, const uint32_t* __restrict__ n_runs,
+                          const uint64_t* __restrict__ run_word, const uint32_t* __restrict__ n_runs,
                           const CellInst* __restrict__ insts, const double* __restrict__ cs, uint64_t cap,
                           const uint32_t* __restrict__ flags, const uint8_t* __restrict__ mask)
 {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= *n_runs) return;
-    // everything a run needs first comes from per-run arrays: the voxel's
-    // density element and the first cell's rate slot were placed when the
-    // order was built, so the density and the constants are one load away
-    const uint32_t ii = run_inst[r];
-    if (ii == kNoRunInst) return;   // the instance's non-secreting cells
+    // a run's start and word (instance, the voxel's density element) were
+    // placed when the order was built, so the density is one load away and
+    // the first cell's rate slot one (cached) instance record away
+    const uint64_t w = run_word[r];
+    const uint32_t ii = static_cast<uint32_t>(w >> kRunDensBits);
+    if (ii == kRunNone) return;   // the instance's non-secreting cells
     const uint32_t p0 = run_start[r], p1 = run_start[r + 1];
-    float* d = dens + run_dens[r];
-    const uint64_t base = run_slot[r];
+    float* d = dens + (w & kRunDensMask);
     if (mask && !(mask[ii] & STEP_DIFFUSE)) return;
     const CellInst& in = insts[ii];
+    const uint64_t base = in.rate_off + (p0 - in.cell_off) * in.S;   // 32-bit slots, as the rates
     const uint32_t S = in.S;
     const uint32_t f = flags[ii];
     if (S <= 2) {
@@ -585,15 +585,14 @@ cudaError_t launch_sec_permute(cudaStream_t st, const uint32_t* skeys, const uin
     return cudaGetLastError();
 }
 
-cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_start, const uint32_t* run_inst,
-                           const uint64_t* run_dens, const uint32_t* run_slot, const uint32_t* n_runs,
-                           uint32_t max_runs, uint32_t max_s, const CellInst* insts, const double* cs, uint32_t cap,
+cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_start, const uint64_t* run_word,
+                           const uint32_t* n_runs, uint32_t max_runs, uint32_t max_s, const CellInst* insts, const double* cs, uint32_t cap,
                            const uint32_t* flags, const uint8_t* mask, int block)
 {
     if (max_runs == 0 || max_s == 0) return cudaSuccess;
     if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
-    k_secrete<<<blocks_for(max_runs, block), block, 0, st>>>(dens, run_start, run_inst, run_dens, run_slot, n_runs,
-                                                          insts, cs, cap, flags, mask);
+    k_secrete<<<blocks_for(max_runs, block), block, 0, st>>>(dens, run_start, run_word, n_runs, insts, cs, cap, flags,
+                                                          mask);
     return cudaGetLastError();
 }
 

@@ -237,11 +237,11 @@ cudaError_t launch_sec_permute(cudaStream_t st, const uint32_t* skeys, const uin
                                const uint32_t* cell_inst, const CellInst* insts, uint32_t invalid_key,
                                const uint32_t* flags, const double* cc, uint32_t n_rate, double* cs);
 // n_runs: device count (heads_rid[n]); max_runs >= it; max_s = largest S;
-// runs marked kNoRunInst are skipped.
+// runs whose word names kRunNone are skipped.
 // cs: constants c0, c1, c2 as three arrays of cap; flags: per instance, bit 0
 // some c0 not +0, bit 1 some c1 not +0 (written by launch_sec_cell_consts).
-cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_start, const uint32_t* run_inst,
-                           const uint64_t* run_dens, const uint32_t* run_slot, const uint32_t* n_runs,
+cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_start, const uint64_t* run_word,
+                           const uint32_t* n_runs,
                            uint32_t max_runs, uint32_t max_s, const CellInst* insts, const double* cs, uint32_t cap,
                            const uint32_t* flags, const uint8_t* mask, int block = 256);
 
@@ -294,8 +294,17 @@ struct SegTile {
     uint32_t first, count, inst, tb, nt;
     uint32_t _pad[3];
 };
-// run_inst of a run of non-secreting cells
-constexpr uint32_t kNoRunInst = 0xFFFFFFFFu;
+// A run's word: its instance in the top 24 bits, the density element of its
+// voxel (substrate 0) in the low 40 (the rate slot of its first cell
+// follows from its start and the instance: rate_off + (start - cell_off) *
+// S).  kRunNone in the instance bits: the instance's non-secreting cells.
+constexpr int kRunDensBits = 40;
+constexpr uint64_t kRunDensMask = (uint64_t{1} << kRunDensBits) - 1u;
+constexpr uint32_t kRunNone = 0xFFFFFFu;   // also the bound on instances per batch
+__host__ __device__ __forceinline__ uint64_t make_run_word(uint32_t inst, uint64_t dens_elem)
+{
+    return (static_cast<uint64_t>(inst) << kRunDensBits) | dens_elem;
+}
 // Passes and digit bits for grids of at most max_local_voxels voxels.
 void so_plan(uint32_t max_local_voxels, int* passes, int* digit_bits);
 // Most tiles a store of max_cells cells over n_inst instances can need.
@@ -308,8 +317,8 @@ int so_launches(uint32_t ntiles, int passes, uint32_t n);
 size_t so_run_scratch_bytes(uint32_t max_cells);
 // Keys, the sort and the run list in one call.  Outputs: skeys (global
 // voxel key vox_base + index, or invalid_key) and sorder (cell) per sorted
-// position; *n_runs; run_start (n + 1), run_inst, run_dens, run_slot per
-// run.  keys, ktmp and vtmp are n-entry work arrays (run_inst may be vtmp);
+// position; *n_runs; run_start (n + 1) and run_word per run.  keys, ktmp
+// and vtmp are n-entry work arrays;
 // scratch: so_scratch_bytes, run_scratch: so_run_scratch_bytes; inst_tile:
 // the n_inst_tiled entries of so_tiles.  With cc non-null the last pass
 // also permutes the constants (cc in cell order, three arrays of cap) into
@@ -319,9 +328,8 @@ cudaError_t launch_sec_order(cudaStream_t st, const SegTile* tiles, uint32_t nti
                              int digit_bits, const float* soa, uint32_t stride, const CellInst* insts,
                              const uint8_t* active, const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* keys,
                              uint32_t* ktmp, uint32_t* vtmp, uint32_t* skeys, uint32_t* sorder, void* scratch,
-                             uint32_t* n_runs, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
-                             uint32_t* run_slot, void* run_scratch, const double* cc, double* cs, uint32_t cap,
-                             const uint32_t* flags);
+                             uint32_t* n_runs, uint32_t* run_start, uint64_t* run_word, void* run_scratch,
+                             const double* cc, double* cs, uint32_t cap, const uint32_t* flags);
 
 // Radix sort of (key, value) pairs, stable, 'bits' significant key bits.
 // Scratch from radix_sort_scratch_bytes().  Result lands in (k_out, v_out).

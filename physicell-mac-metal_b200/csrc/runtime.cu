@@ -1214,6 +1214,8 @@ void fill_mech_inst(CellInst& ci, const pcg_mechanics_params& m, float x_min, fl
 int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_instances)
 {
     ctx = c;
+    // a secretion run names its instance in 24 bits (make_run_word)
+    if (n_instances >= kRunNone) return fail(ctx, PCG_ERR_INVALID, "more instances than a batch can hold");
     max_cells = std::max<uint32_t>(maxc, 1);
     n = 0;
     n_rate = 0;
@@ -1233,9 +1235,9 @@ int Cells::create(pcg_ctx* c, uint32_t maxc, uint32_t rate_capacity, uint32_t n_
     PCG_CU(ctx, active.alloc(max_cells));
     PCG_CU(ctx, pos64.alloc(3ull * max_cells * sizeof(double)));
     PCG_CU(ctx, cudaMemsetAsync(pos64.p, 0xFF, pos64.bytes, ctx->stream));   // no masters yet
-    for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp, &run_slot})
+    for (DevBuf* b : {&keys, &vals, &skeys, &sorder, &ktmp, &vtmp})
         PCG_CU(ctx, b->alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint32_t)));
-    PCG_CU(ctx, run_dens.alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint64_t)));
+    PCG_CU(ctx, run_word.alloc((static_cast<size_t>(max_cells) + 1) * sizeof(uint64_t)));
     max_tiles = so_max_tiles(max_cells, static_cast<uint32_t>(h_inst.size()));
     PCG_CU(ctx, tiles.alloc(static_cast<size_t>(max_tiles) * sizeof(SegTile)));
     PCG_CU(ctx, inst_tile.alloc(h_inst.size() * sizeof(uint32_t)));
@@ -1372,8 +1374,7 @@ int Cells::build_order(uint64_t total_vox)
                                      max_cells, inst.as<CellInst>(), has_active ? active.as<uint8_t>() : nullptr,
                                      cell_inst.as<uint32_t>(), invalid_key, keys.as<uint32_t>(), ktmp.as<uint32_t>(),
                                      vtmp.as<uint32_t>(), skeys.as<uint32_t>(), sorder.as<uint32_t>(), sort_scr.p,
-                                     ktmp.as<uint32_t>() + n, vals.as<uint32_t>(), vtmp.as<uint32_t>(),
-                                     run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), run_scr.p,
+                                     ktmp.as<uint32_t>() + n, vals.as<uint32_t>(), run_word.as<uint64_t>(), run_scr.p,
                                      consts ? coef_cells.as<double>() : nullptr, coef.as<double>(), cap,
                                      coef_flags.as<uint32_t>());
     if (e != cudaSuccess) return cuda_fail(ctx, e, "secretion order");
@@ -1426,8 +1427,8 @@ int Cells::secrete(Diffusion& d, const uint8_t* mask)
 {
     uint32_t max_s = 0;
     for (const CellInst& ci : h_inst) max_s = std::max(max_s, ci.S);
-    cudaError_t e = launch_secrete(ctx->stream, d.dens.as<float>(), vals.as<uint32_t>(), vtmp.as<uint32_t>(),
-                                   run_dens.as<uint64_t>(), run_slot.as<uint32_t>(), ktmp.as<uint32_t>() + n, n, max_s,
+    cudaError_t e = launch_secrete(ctx->stream, d.dens.as<float>(), vals.as<uint32_t>(), run_word.as<uint64_t>(),
+                                   ktmp.as<uint32_t>() + n, n, max_s,
                                    inst.as<CellInst>(), coef.as<double>(),
                                    static_cast<uint32_t>(rates.bytes / (4 * sizeof(double))),
                                    coef_flags.as<uint32_t>(), mask, sec_block);
@@ -1442,7 +1443,7 @@ uint64_t Cells::device_bytes() const
            keys.bytes + vals.bytes +
            skeys.bytes + sorder.bytes + ktmp.bytes + vtmp.bytes + sort_scr.bytes + tiles.bytes + inst_tile.bytes +
            run_scr.bytes +
-           run_dens.bytes + run_slot.bytes;
+           run_word.bytes;
 }
 
 // ------------------------------------------------------------------ mechanics

@@ -273,14 +273,14 @@ public:
     double coef_dt = -1.0;
     // secretion ordering (launch_sec_order): keys the first pass's keys in
     // cell order, (skeys, sorder) the order, ktmp / vtmp the passes' work
-    // arrays; after the sort ktmp holds the run index of every position
-    // (+ count), vals the run starts and vtmp the run instances; coef the
+    // arrays; after the sort ktmp[n] holds the run count and vals the run
+    // starts; coef the
     // constants in sorted order (c0, c1, c2 arrays), coef_cells the same
     // constants in cell order (coef_dirty: stale) and coef_flags which of
     // c0 / c1 each instance has.  tiles: the instances' 2048-cell tiles
     // (rebuilt with the instance table), so_passes x so_bits the digits.
     DevBuf keys, vals, skeys, sorder, ktmp, vtmp, sort_scr, run_scr, tiles, inst_tile;
-    DevBuf run_dens, run_slot;   // per run: density element of its voxel, rate slot of its first cell
+    DevBuf run_word;   // per run: instance and density element of its voxel (make_run_word)
     uint32_t invalid_key = 0;
     uint32_t ntiles = 0, max_tiles = 0, n_inst_tiled = 0;
     int so_passes = 1, so_bits = 0;

@@ -31,7 +31,7 @@
 //                 last pass writes global keys (vox_base + index, or the
 //                 invalid key).
 // The run list of the order follows: a run is the cells of one voxel, and
-// each instance's non-secreting cells form one run marked kNoRunInst.
+// each instance's non-secreting cells form one run marked kRunNone.
 #include "pcg_kernels.cuh"
 
 #include <algorithm>
@@ -314,9 +314,9 @@ __global__ void __launch_bounds__(kThreads) k_so_scatter(const SegTile* __restri
 // k_so_run_write numbers the tile's heads (ballots, then the 64 warp-row
 // counts in order) and writes the runs.  Run r starts at run_start[r] and
 // ends at run_start[r + 1] (run_start[n_runs] = n, *n_runs = the count).
-// A run of secreting cells gets its instance, the density element of its
-// voxel (substrate 0, padded rows) and the rate slot of its first cell; a
-// run of non-secreting cells gets kNoRunInst.
+// A run of secreting cells gets one word: its instance and the density
+// element of its voxel (substrate 0, padded rows); a run of non-secreting
+// cells gets kRunNone.
 __device__ __forceinline__ bool so_head(const uint32_t* __restrict__ skeys, uint32_t n, uint32_t p, uint32_t* key)
 {
     if (p >= n) return false;
@@ -348,9 +348,8 @@ __global__ void __launch_bounds__(kThreads) k_so_run_write(const uint32_t* __res
                                                            const uint32_t* __restrict__ tile_cnt, uint32_t ntiles,
                                                            const uint32_t* __restrict__ cell_inst,
                                                            const CellInst* __restrict__ insts,
-                                                           uint32_t* __restrict__ run_start, uint32_t* __restrict__ run_inst,
-                                                           uint64_t* __restrict__ run_dens, uint32_t* __restrict__ run_slot,
-                                                           uint32_t* __restrict__ n_runs)
+                                                           uint32_t* __restrict__ run_start,
+                                                           uint64_t* __restrict__ run_word, uint32_t* __restrict__ n_runs)
 {
     __shared__ uint32_t wc[kItems * kWarps];   // heads per (row k, warp), then their exclusive scan
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -383,7 +382,7 @@ __global__ void __launch_bounds__(kThreads) k_so_run_write(const uint32_t* __res
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
         const bool sec = ((hb >> k) & 1u) && key[k] < invalid_key;
-        ii8[k] = sec ? cell_inst[ii8[k]] : kNoRunInst;
+        ii8[k] = sec ? cell_inst[ii8[k]] : kRunNone;
     }
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
@@ -392,13 +391,13 @@ __global__ void __launch_bounds__(kThreads) k_so_run_write(const uint32_t* __res
         const uint32_t r = wc[k * kWarps + warp] + rank[k];
         const uint32_t ii = ii8[k];
         run_start[r] = p;
-        run_inst[r] = ii;
-        if (ii != kNoRunInst) {
+        uint64_t elem = 0;
+        if (ii != kRunNone) {
             const CellInst& in = insts[ii];
             const uint32_t v = key[k] - in.vox_base;
-            run_dens[r] = in.dens_off + static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
-            run_slot[r] = in.rate_off + (p - in.cell_off) * in.S;
+            elem = in.dens_off + static_cast<uint64_t>(v / in.nx) * in.px + v % in.nx;
         }
+        run_word[r] = make_run_word(ii, elem);
     }
     if (blockIdx.x == ntiles - 1 && threadIdx.x == 0) {
         const uint32_t total = tile_off[blockIdx.x] + tile_cnt[blockIdx.x];
@@ -464,9 +463,8 @@ cudaError_t launch_sec_order(cudaStream_t st, const SegTile* tiles, uint32_t nti
                              int digit_bits, const float* soa, uint32_t stride, const CellInst* insts,
                              const uint8_t* active, const uint32_t* cell_inst, uint32_t invalid_key, uint32_t* keys,
                              uint32_t* ktmp, uint32_t* vtmp, uint32_t* skeys, uint32_t* sorder, void* scratch,
-                             uint32_t* n_runs, uint32_t* run_start, uint32_t* run_inst, uint64_t* run_dens,
-                             uint32_t* run_slot, void* run_scratch, const double* cc, double* cs, uint32_t cap,
-                             const uint32_t* flags)
+                             uint32_t* n_runs, uint32_t* run_start, uint64_t* run_word, void* run_scratch,
+                             const double* cc, double* cs, uint32_t cap, const uint32_t* flags)
 {
     if (n == 0 || ntiles == 0) return cudaSuccess;
     if (digit_bits > kMaxDigitBits || passes < 1) return cudaErrorInvalidValue;
@@ -510,7 +508,7 @@ cudaError_t launch_sec_order(cudaStream_t st, const SegTile* tiles, uint32_t nti
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = scan_exclusive(st, tile_cnt, tile_off, rt, rscr)) != cudaSuccess) return e;
     k_so_run_write<<<rt, kThreads, 0, st>>>(skeys, sorder, n, invalid_key, tile_off, tile_cnt, rt, cell_inst, insts,
-                                             run_start, run_inst, run_dens, run_slot, n_runs);
+                                             run_start, run_word, n_runs);
     return cudaGetLastError();
 }
 
