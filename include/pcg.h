@@ -408,7 +408,8 @@ pcg_status pcg_batch_create(pcg_ctx* ctx, const pcg_instance_desc* instances, ui
 pcg_status pcg_batch_destroy(pcg_batch* batch);
 /* Advance every instance by n_diffusion_steps main-loop sub-steps
  * (src/main.mm:341-391 ordering; mechanics when each instance's accumulator
- * reaches dt_mechanics). */
+ * reaches dt_mechanics).  One graph launch per sub-step, or per mechanics
+ * period where the call covers a whole one; the same results either way. */
 pcg_status pcg_batch_step(pcg_batch* batch, int n_diffusion_steps);
 pcg_status pcg_batch_download_density(pcg_batch* batch, uint32_t instance, float* host, size_t n_floats);
 pcg_status pcg_batch_download_cells(pcg_batch* batch, uint32_t instance, float* soa, uint32_t soa_max_cells);

@@ -692,7 +692,8 @@ class Instance:
 
 
 class Batch:
-    """pcg_batch: many simulations advanced in one graph launch per step."""
+    """pcg_batch: many simulations advanced in one graph launch per sub-step
+    (per mechanics period where a call covers one)."""
 
     def __init__(self, ctx, instances, use_graphs=True, autotune=True, tune_cache=None, profile=False,
                  pin_x=0, pin_cols=0, planes=True, pin_forces=0, pin_cell_threads=0):
