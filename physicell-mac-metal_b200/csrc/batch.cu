@@ -168,6 +168,7 @@ int Batch::create(pcg_ctx* c, const pcg_instance_desc* descs, uint32_t n, const 
     c_.inst_dirty = true;
     PCG_TRY(c_.sync_inst());
     PCG_TRY(m_.create(ctx, moff, cell_cap));
+    m_.lazy_sorder = true;   // only pcg_batch_mech_bins reads the stable order
     PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
     if (c_.n) PCG_TRY(c_.prepare_secretion(dt_diff, d.total_vox));
     if (tune) {
@@ -405,6 +406,7 @@ int Batch::step(int n_steps)
             s += period_len - 1;
             diff_steps += static_cast<uint64_t>(period_len);
             mech_steps++;
+            m_.sorder_valid = false;
             continue;
         }
         accum += dt_diff;
@@ -435,7 +437,10 @@ int Batch::step(int n_steps)
         } else {
             PCG_TRY(run_step(mech, false, nullptr));
         }
-        if (mech) mech_steps++;
+        if (mech) {
+            mech_steps++;
+            m_.sorder_valid = false;   // binned again, stable order not made
+        }
         diff_steps++;
     }
     return PCG_OK;
@@ -453,7 +458,10 @@ int Batch::step_masked(const uint8_t* mask_host, bool any_mech)
         PCG_TRY(run_step(any_mech, false, mask_d.as<uint8_t>()));
     }
     diff_steps++;
-    if (any_mech) mech_steps++;
+    if (any_mech) {
+        mech_steps++;
+        m_.sorder_valid = false;
+    }
     return PCG_OK;
 }
 
@@ -834,6 +842,7 @@ pcg_status pcg_batch_mech_bins(pcg_batch* b, uint32_t i, uint32_t* start, uint32
     if ((nbr_count || nbr_hash) && !B.m_.diag) return fail(ctx, PCG_ERR_INVALID, "diagnostics are off");
     const CellInst& ci = B.c_.h_inst[i];
     const size_t V = static_cast<size_t>(ci.mnx) * ci.mny * ci.mnz;
+    if (sorted_cells) PCG_TRY(B.m_.stable_order(B.c_.n));   // from the last binning, if not yet made
     PCG_CU(ctx, cudaStreamSynchronize(ctx->stream));
     std::vector<uint32_t> st(V + 1);
     PCG_CU(ctx, cudaMemcpy(st.data(), B.m_.start.as<uint32_t>() + ci.mvox_base, (V + 1) * sizeof(uint32_t),

@@ -217,9 +217,14 @@ __global__ void k_cells_move(uint32_t* __restrict__ soa, uint32_t stride, const 
 // start + slot, which groups the voxel's cells in arrival order, and
 // k_mech_order ranks every cell in its voxel twice: by index (the stable
 // order of the cell-start table, sorder: syncHashPointers' voxelCells) and
-// by x position, index breaking ties (the force pass's order, forder, with
-// the sorted positions and strengths).  Bins grow with x, so the cells of a
-// run of voxels along x are in x order as a whole in the force order.
+// by x position, index breaking ties (the force pass's order: the sorted
+// positions and strengths, the cell's index riding in the strengths' third
+// component, which the force terms never read).  Bins grow with x, so the
+// cells of a run of voxels along x are in x order as a whole in the force
+// order.  Every store is a scattered partial sector, and their rate bounds
+// the kernel, so the stable order is only written where it is read
+// (SORDER; a batch makes it on request, k_mech_stable_order) and the force
+// order needs no index array of its own.
 __global__ void k_mech_bin(float* __restrict__ soa, uint32_t stride, uint32_t n, const uint32_t* __restrict__ cell_inst,
                            const CellInst* __restrict__ insts, uint32_t* __restrict__ keys,
                            uint32_t* __restrict__ slots, uint32_t* __restrict__ counts,
@@ -263,10 +268,10 @@ __global__ void k_mech_place(const float* __restrict__ soa, uint32_t stride, con
     placed[start[keys[g]] + slots[g]] = make_uint2(x_order_key(x), g);
 }
 
+template <bool SORDER>
 __global__ void k_mech_order(const float* __restrict__ soa, uint32_t stride, const uint32_t* __restrict__ keys,
                              const uint32_t* __restrict__ start, const uint2* __restrict__ placed, uint32_t n,
-                             uint32_t* __restrict__ sorder, uint32_t* __restrict__ forder, float4* __restrict__ spos,
-                             float4* __restrict__ sprm)
+                             uint32_t* __restrict__ sorder, float4* __restrict__ spos, float4* __restrict__ sprm)
 {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
@@ -280,15 +285,28 @@ __global__ void k_mech_order(const float* __restrict__ soa, uint32_t stride, con
         pi += o.y < g ? 1u : 0u;
         px += (o.x < xk || (o.x == xk && o.y < g)) ? 1u : 0u;
     }
-    sorder[pi] = g;
-    forder[px] = g;
+    if (SORDER) sorder[pi] = g;
     spos[px] = make_float4(x, soa[static_cast<size_t>(F_POS_Y) * stride + g], soa[static_cast<size_t>(F_POS_Z) * stride + g],
                            soa[static_cast<size_t>(F_RADIUS) * stride + g]);
     // square roots of the (non-negative) strengths: the pair factors
-    // sqrt(rep_i rep_j), sqrt(adh_i adh_j) become one product each
+    // sqrt(rep_i rep_j), sqrt(adh_i adh_j) become one product each; the
+    // cell's index in place of relmax, which only its reciprocal serves
     const float relmax = soa[static_cast<size_t>(F_REL_MAX_ADH) * stride + g];
     sprm[px] = make_float4(sqrtf(soa[static_cast<size_t>(F_REPULSION) * stride + g]),
-                           sqrtf(soa[static_cast<size_t>(F_ADHESION) * stride + g]), relmax, 1.0f / relmax);
+                           sqrtf(soa[static_cast<size_t>(F_ADHESION) * stride + g]), __uint_as_float(g), 1.0f / relmax);
+}
+
+// The stable order alone, from the same binning (k_mech_order's first rank).
+__global__ void k_mech_stable_order(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ start,
+                                    const uint2* __restrict__ placed, uint32_t n, uint32_t* __restrict__ sorder)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t key = keys[g];
+    const uint32_t s0 = start[key], s1 = start[key + 1];
+    uint32_t pi = s0;
+    for (uint32_t q = s0; q < s1; ++q) pi += placed[q].y < g ? 1u : 0u;
+    sorder[pi] = g;
 }
 
 __device__ __forceinline__ uint32_t nbr_hash(uint32_t j)
@@ -341,7 +359,7 @@ __device__ __forceinline__ void pair_force(float ddx, float ddy, float ddz, floa
 }
 
 // One thread per cell, cells in the force order p (by mechanics voxel,
-// then x; forder[p] = cell).  Candidates are the cells of the 3 x 3 (x 3)
+// then x; the cell's index is the bits of sprm[p].z).  Candidates are the cells of the 3 x 3 (x 3)
 // voxels around the cell's own (mechanics.metal:125-208), visited row by
 // row (dk, then dj), each row of three voxels along x being one run of the
 // force order sorted by x.  A row whose slab lies beyond the interaction
@@ -370,7 +388,6 @@ __device__ __forceinline__ void pair_force(float ddx, float ddy, float ddz, floa
 // extra resident warps hide more of it than the spills cost.
 template <int QCAP, bool DIAG>
 __global__ void __launch_bounds__(256, 5) k_mech_forces(const float4* __restrict__ spos, const float4* __restrict__ sprm,
-                                                     const uint32_t* __restrict__ forder,
                                                      const uint32_t* __restrict__ start, uint32_t n,
                                                      const uint32_t* __restrict__ cell_inst,
                                                      const CellInst* __restrict__ insts, float* __restrict__ soa,
@@ -381,12 +398,12 @@ __global__ void __launch_bounds__(256, 5) k_mech_forces(const float4* __restrict
     extern __shared__ uint32_t queue[];
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    const uint32_t g = forder[p];
+    const float4 mp = sprm[p];
+    const uint32_t g = __float_as_uint(mp.z);
     const uint32_t ii = cell_inst[g];
     if (mask && !(mask[ii] & STEP_MECH)) return;
     const CellInst& in = insts[ii];
     const float4 me = spos[p];
-    const float4 mp = sprm[p];
     const int mnx = static_cast<int>(in.mnx), mny = static_cast<int>(in.mny), mnz = static_cast<int>(in.mnz);
     // the cell's voxel, from its position exactly as k_mech_bin binned it
     const int ci = clampi(bin_of(me.x, in.mx_min, in.vs), 0, mnx - 1);
@@ -471,7 +488,7 @@ __global__ void __launch_bounds__(256, 5) k_mech_forces(const float4* __restrict
                         if (!(dsq >= maxd2 || dsq < 1e-12f)) {
                             if (DIAG) {
                                 ++cnt;
-                                hsh += nbr_hash(forder[q + k] - in.cell_off);
+                                hsh += nbr_hash(__float_as_uint((k == 0 ? p0 : p1).z) - in.cell_off);
                             }
                             pair_force(ddx, ddy, ddz, dsq, me.w, cur.w, mp, k == 0 ? p0 : p1, fx, fy, fz, P);
                         }
@@ -494,7 +511,7 @@ __global__ void __launch_bounds__(256, 5) k_mech_forces(const float4* __restrict
             const bool nb = !(dsq >= maxd2 || dsq < 1e-12f);
             if (DIAG && nb) {
                 ++cnt;
-                hsh += nbr_hash(forder[q] - in.cell_off);
+                hsh += nbr_hash(__float_as_uint(sprm[q].z) - in.cell_off);
             }
             if (nb) myq[nq++ * qstride] = q;
             if (__any_sync(__activemask(), nq == QCAP)) flush();
@@ -618,26 +635,38 @@ cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32
 
 cudaError_t launch_mech_order(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* keys,
                               const uint32_t* slots, const uint32_t* start, uint32_t n, uint2* placed,
-                              uint32_t* sorder, uint32_t* forder, float4* spos, float4* sprm, int block)
+                              uint32_t* sorder, float4* spos, float4* sprm, int block)
 {
     if (n == 0) return cudaSuccess;
     if (block < 32 || block > 1024 || block % 32) return cudaErrorInvalidValue;
     k_mech_place<<<blocks_for(n, block), block, 0, st>>>(soa, stride, keys, slots, start, n, placed);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_mech_order<<<blocks_for(n, block), block, 0, st>>>(soa, stride, keys, start, placed, n, sorder, forder, spos,
-                                                         sprm);
+    if (sorder)
+        k_mech_order<true><<<blocks_for(n, block), block, 0, st>>>(soa, stride, keys, start, placed, n, sorder, spos,
+                                                                   sprm);
+    else
+        k_mech_order<false><<<blocks_for(n, block), block, 0, st>>>(soa, stride, keys, start, placed, n, nullptr, spos,
+                                                                    sprm);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mech_stable_order(cudaStream_t st, const uint32_t* keys, const uint32_t* start,
+                                     const uint2* placed, uint32_t n, uint32_t* sorder)
+{
+    if (n == 0) return cudaSuccess;
+    k_mech_stable_order<<<blocks_for(n, 256), 256, 0, st>>>(keys, start, placed, n, sorder);
     return cudaGetLastError();
 }
 
 template <int QCAP, bool DIAG>
 static cudaError_t forces_variant(cudaStream_t st, unsigned grid, int block, const float4* spos, const float4* sprm,
-                                  const uint32_t* forder, const uint32_t* start, uint32_t n,
+                                  const uint32_t* start, uint32_t n,
                                   const uint32_t* cell_inst, const CellInst* insts, float* soa, uint32_t stride,
                                   uint32_t* diag_cnt, uint32_t* diag_hash, const uint8_t* mask)
 {
     const size_t smem = static_cast<size_t>(QCAP) * block * sizeof(uint32_t);   // at most 64 KiB
-    k_mech_forces<QCAP, DIAG><<<grid, block, smem, st>>>(spos, sprm, forder, start, n, cell_inst, insts, soa, stride,
+    k_mech_forces<QCAP, DIAG><<<grid, block, smem, st>>>(spos, sprm, start, n, cell_inst, insts, soa, stride,
                                                          diag_cnt, diag_hash, mask);
     return cudaGetLastError();
 }
@@ -653,7 +682,7 @@ cudaError_t mech_forces_prepare()
     return cudaSuccess;
 }
 
-cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* forder,
+cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm,
                                const uint32_t* start, uint32_t n, const uint32_t* cell_inst,
                                const CellInst* insts, float* soa, uint32_t stride, uint32_t* diag_cnt,
                                uint32_t* diag_hash, const uint8_t* mask, ForceShape shape)
@@ -663,10 +692,10 @@ cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4
     const unsigned grid = blocks_for(n, shape.block);
     const bool dg = diag_cnt != nullptr;
 #define PCG_FORCES(Q)                                                                                                \
-    return dg ? forces_variant<Q, true>(st, grid, shape.block, spos, sprm, forder, start, n, cell_inst, insts, soa, \
-                                        stride, diag_cnt, diag_hash, mask)                                           \
-              : forces_variant<Q, false>(st, grid, shape.block, spos, sprm, forder, start, n, cell_inst, insts, soa,\
-                                         stride, diag_cnt, diag_hash, mask)
+    return dg ? forces_variant<Q, true>(st, grid, shape.block, spos, sprm, start, n, cell_inst, insts, soa, stride, \
+                                        diag_cnt, diag_hash, mask)                                                   \
+              : forces_variant<Q, false>(st, grid, shape.block, spos, sprm, start, n, cell_inst, insts, soa, stride, \
+                                         diag_cnt, diag_hash, mask)
     switch (shape.queue) {
     case 0: PCG_FORCES(0);
     case 16: PCG_FORCES(16);

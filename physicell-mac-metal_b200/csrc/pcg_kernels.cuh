@@ -249,15 +249,19 @@ cudaError_t launch_secrete(cudaStream_t st, float* dens, const uint32_t* run_sta
 // global mechanics-voxel key, counts it (counts: V + 1 zeroed words) and
 // records its arrival slot; after the exclusive scan of the counts into
 // start, launch_mech_order (two launches; placed: n scratch pairs) writes
-// the stable order (sorder: cells by voxel, ascending index within a voxel)
-// and the force order (forder: by voxel, then x, index breaking ties) with
-// the positions / radii and strengths in that order (spos, sprm).
+// the stable order (sorder: cells by voxel, ascending index within a voxel;
+// skipped when null) and, in the force order (by voxel, then x, index
+// breaking ties), the positions / radii (spos) and the strengths (sprm:
+// sqrt repulsion, sqrt adhesion, the cell's index as bits, 1 / relmax).
+// launch_mech_stable_order writes sorder alone from the same binning.
 cudaError_t launch_mech_bin(cudaStream_t st, float* soa, uint32_t stride, uint32_t n,
                             const uint32_t* cell_inst, const CellInst* insts,
                             uint32_t* keys, uint32_t* slots, uint32_t* counts, const uint8_t* mask, int block = 256);
 cudaError_t launch_mech_order(cudaStream_t st, const float* soa, uint32_t stride, const uint32_t* keys,
                               const uint32_t* slots, const uint32_t* start, uint32_t n, uint2* placed,
-                              uint32_t* sorder, uint32_t* forder, float4* spos, float4* sprm, int block = 256);
+                              uint32_t* sorder, float4* spos, float4* sprm, int block = 256);
+cudaError_t launch_mech_stable_order(cudaStream_t st, const uint32_t* keys, const uint32_t* start,
+                                     const uint2* placed, uint32_t n, uint32_t* sorder);
 // Launch shape of the force pass: threads per block (a multiple of 32, at
 // most 256) and the neighbour queue per thread (0 = force terms in the walk;
 // 16, 32 or 64 slots of shared memory).  Every shape gives the same bits.
@@ -269,7 +273,7 @@ struct ForceShape {
 // Lets the 64-slot queue variants use 64 KiB of shared memory (current
 // device; once per device, outside stream capture).
 cudaError_t mech_forces_prepare();
-cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm, const uint32_t* forder,
+cudaError_t launch_mech_forces(cudaStream_t st, const float4* spos, const float4* sprm,
                                const uint32_t* start, uint32_t n,
                                const uint32_t* cell_inst, const CellInst* insts, float* soa, uint32_t stride,
                                uint32_t* diag_cnt, uint32_t* diag_hash, const uint8_t* mask, ForceShape shape);

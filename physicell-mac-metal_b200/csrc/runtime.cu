@@ -1454,7 +1454,7 @@ int Mechanics::create(pcg_ctx* c, uint32_t tmv, uint32_t maxc)
     total_mvox = tmv;
     cap = std::max<uint32_t>(maxc, 1);
     PCG_CU(ctx, mech_forces_prepare());
-    for (DevBuf* b : {&keys, &slots, &sorder, &forder, &dcnt, &dhash})
+    for (DevBuf* b : {&keys, &slots, &sorder, &dcnt, &dhash})
         PCG_CU(ctx, b->alloc(static_cast<size_t>(cap) * sizeof(uint32_t)));
     PCG_CU(ctx, placed.alloc(static_cast<size_t>(cap) * sizeof(uint2)));
     PCG_CU(ctx, counts.alloc((static_cast<size_t>(tmv) + 1) * sizeof(uint32_t)));
@@ -1494,10 +1494,22 @@ int Mechanics::binsort(Cells& c, const uint8_t* mask)
     e = scan_exclusive(st, counts.as<uint32_t>(), start.as<uint32_t>(), static_cast<uint64_t>(total_mvox) + 1, scan_scr.p);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "start-table scan");
     e = launch_mech_order(st, c.soa.as<float>(), c.max_cells, keys.as<uint32_t>(), slots.as<uint32_t>(),
-                          start.as<uint32_t>(), c.n, placed.as<uint2>(), sorder.as<uint32_t>(),
-                          forder.as<uint32_t>(), spos.as<float4>(), sprm.as<float4>(), bin_block);
+                          start.as<uint32_t>(), c.n, placed.as<uint2>(), lazy_sorder ? nullptr : sorder.as<uint32_t>(),
+                          spos.as<float4>(), sprm.as<float4>(), bin_block);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "bin order launch");
     ctx->launches += launches_forces(c.n) - 2;   // the memset is not a kernel; forces counted below
+    sorder_valid = !lazy_sorder;
+    return PCG_OK;
+}
+
+int Mechanics::stable_order(uint32_t n)
+{
+    if (sorder_valid || n == 0) return PCG_OK;
+    cudaError_t e = launch_mech_stable_order(ctx->stream, keys.as<uint32_t>(), start.as<uint32_t>(), placed.as<uint2>(),
+                                             n, sorder.as<uint32_t>());
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "stable order launch");
+    ctx->launches++;
+    sorder_valid = true;
     return PCG_OK;
 }
 
@@ -1505,9 +1517,8 @@ int Mechanics::force_pass(Cells& c, const uint8_t* mask)
 {
     if (c.n == 0) return PCG_OK;
     cudaStream_t st = ctx->stream;
-    cudaError_t e = launch_mech_forces(st, spos.as<float4>(), sprm.as<float4>(), forder.as<uint32_t>(),
-                           start.as<uint32_t>(), c.n, c.cell_inst.as<uint32_t>(), c.inst.as<CellInst>(), c.soa.as<float>(),
-                           c.max_cells, diag ? dcnt.as<uint32_t>() : nullptr, diag ? dhash.as<uint32_t>() : nullptr,
+    cudaError_t e = launch_mech_forces(st, spos.as<float4>(), sprm.as<float4>(), start.as<uint32_t>(), c.n,
+                           c.cell_inst.as<uint32_t>(), c.inst.as<CellInst>(), c.soa.as<float>(), c.max_cells, diag ? dcnt.as<uint32_t>() : nullptr, diag ? dhash.as<uint32_t>() : nullptr,
                            mask, fshape);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "forces launch");
     ctx->launches++;
@@ -1531,7 +1542,7 @@ int Mechanics::integrate(Cells& c, float dt_override, const uint8_t* mask)
 
 uint64_t Mechanics::device_bytes() const
 {
-    return keys.bytes + slots.bytes + placed.bytes + sorder.bytes + forder.bytes + counts.bytes +
+    return keys.bytes + slots.bytes + placed.bytes + sorder.bytes + counts.bytes +
            start.bytes + scan_scr.bytes + spos.bytes + sprm.bytes + dcnt.bytes + dhash.bytes;
 }
 

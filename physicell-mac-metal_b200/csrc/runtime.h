@@ -324,16 +324,21 @@ public:
     int bin_block = 256;   // threads per block of the binning kernels
     int int_block = 256;   // threads per block of the AB2 kernel
     bool diag = false;
+    // lazy_sorder: binning leaves the stable order out (a batch's steps never
+    // read it); stable_order() makes it from the same binning on request.
+    // sorder_valid: it matches the last binning.
+    bool lazy_sorder = false, sorder_valid = false;
     // binning: keys / slots (voxel key and arrival slot per cell), counts
     // (per voxel, + 1), start (the cell-start table), placed ((x key, cell)
     // in arrival order per voxel), sorder (the stable order: by voxel, then
-    // index), forder (the force order: by voxel, then x) with spos / sprm
-    // (positions and strengths in the force order)
-    DevBuf keys, slots, placed, sorder, forder, counts, start, scan_scr, spos, sprm, dcnt, dhash;
+    // index), spos / sprm (positions and strengths in the force order: by
+    // voxel, then x; the cell's index in sprm's third component)
+    DevBuf keys, slots, placed, sorder, counts, start, scan_scr, spos, sprm, dcnt, dhash;
 
     int create(pcg_ctx* c, uint32_t total_mvox, uint32_t max_cells);
     int forces(Cells& c, const uint8_t* mask);       // binsort + force_pass
     int binsort(Cells& c, const uint8_t* mask);      // bin, counting sort, cell-start table, sorted SoA
+    int stable_order(uint32_t n);                    // sorder from the last binning, when not yet made
     int force_pass(Cells& c, const uint8_t* mask);
     int integrate(Cells& c, float dt_override, const uint8_t* mask);
     int launches_forces(uint32_t n) const;
