@@ -476,7 +476,10 @@ pcg_status pcg_batch_set_diagnostics(pcg_batch* batch, int on);
  * table (V + 1 entries for its V mechanics voxels, counted from its first
  * sorted place), its sorted cells (n_cells, instance-local indices) and,
  * with diagnostics on, each cell's neighbour count and hash (n_cells, by
- * instance-local cell index).  Any pointer may be NULL. */
+ * instance-local cell index).  Any pointer may be NULL.  The batch's steps
+ * do not need the sorted cells, so the first call after a mechanics step
+ * that asks for them makes them (one kernel launch on the context stream)
+ * from that step's binning. */
 pcg_status pcg_batch_mech_bins(pcg_batch* batch, uint32_t instance, uint32_t* start, uint32_t* sorted_cells,
                                uint32_t* nbr_count, uint32_t* nbr_hash);
 /* Describe the chosen launch shapes as a short string. */
