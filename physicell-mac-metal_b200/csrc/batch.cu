@@ -34,7 +34,7 @@ uint64_t instance_bytes(const pcg_instance_desc& d)
     b += n * 3 * 8;                                        // FP64 master positions
     b += n * S * (4 * 8 + 3 * 8 * 2);                      // rates, secretion constants (cell and sorted order)
     b += n * 4 * 6 * 2;                                    // two sort workspaces
-    b += n * (8 + 4);                                      // per-run density element and rate slot
+    b += n * 8;                                            // per-run word (instance, density element)
     b += n * (16 + 16 + 8);                                // sorted SoA, diagnostics
     b += (V + 1) * 4 * 2;                                  // counts, start
     b += (n / 2048 + 2) * (257 * 4 + sizeof(SegTile) + 8) + 4096;   // sort tiles, digit rows, run scan

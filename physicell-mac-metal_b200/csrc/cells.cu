@@ -332,7 +332,7 @@ __device__ __forceinline__ float slab_gap(float c, float lo, float vs, int idx, 
 
 // One pair's force terms (mechanics.metal:167-208) added to the running
 // sums: d = p_i - p_j with dsq = |d|^2 (the test's exact FP32 value), Ri /
-// Rj the radii, mp = (sqrt rep_i, sqrt adh_i, relmax_i, 1 / relmax_i), op
+// Rj the radii, mp = (sqrt rep_i, sqrt adh_i, -, 1 / relmax_i), op
 // the strengths of j.  Reciprocal / rsqrt forms and per-cell square roots
 // of the strengths (a few ulp per term against the reference's sqrt and
 // divides); dist / (relmax_i R) is taken as (dist / R) / relmax_i.  Every
