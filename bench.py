@@ -402,12 +402,12 @@ def main():
     ap.add_argument("--serve-horizon", type=float, default=10.0,
                     help="seconds of request arrivals for the serving leg (0 = skip)")
     args = ap.parse_args()
-    rank, world, local, dist = setup_dist(args.gpus)
     if args.impl == "reference":
-        run_reference_arm(args, rank, world)
-        if dist is not None:
-            dist.destroy_process_group()
+        # the CPU port on rank 0's host cores: no GPU, no process group (the
+        # other ranks of a torchrun launch exit without work)
+        run_reference_arm(args, int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")))
         return
+    rank, world, local, dist = setup_dist(args.gpus)
 
     import torch
     pcg = load_pcg()
